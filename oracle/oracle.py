@@ -1,0 +1,275 @@
+"""ctypes front end of the test oracles (TEST INFRASTRUCTURE ONLY).
+
+Two checkers live here:
+
+* ``Restatement`` -- liboracle.so, the plain-C restatement of the reference algorithm
+  (oracle/rt_oracle.c), which runs anywhere (it is what travels with the tests);
+* ``Reference`` -- oracle/_ref/<variant>/libref.so, the reference's own BVH sources
+  compiled in place by oracle/build_ref.sh, present where the reference tree was.
+
+Only tests/, the smoke check and bench.py's CPU-baseline leg import this module, and only
+to check or time against the product; the product never imports it.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_LIB = os.path.join(HERE, "lib", "liboracle.so")
+REF_DIR = os.path.join(HERE, "_ref")
+
+# Build parameter sets: the reference's compile-time constants of each oracle/_ref variant
+# (oracle/build_ref.sh) as runtime values.
+VARIANTS = {
+    "hybrid":   dict(lbvh_threshold=64, max_leaf=16, morton_bits=21),
+    "lbvh63":   dict(lbvh_threshold=0, max_leaf=16, morton_bits=21),
+    "lbvh30":   dict(lbvh_threshold=0, max_leaf=16, morton_bits=10),
+    "lbvh63l4": dict(lbvh_threshold=0, max_leaf=4, morton_bits=21),
+    "sah4":     dict(lbvh_threshold=2147483647, max_leaf=4, morton_bits=21),
+    "sah16":    dict(lbvh_threshold=2147483647, max_leaf=16, morton_bits=21),
+    "sah4ns":   dict(lbvh_threshold=2147483647, max_leaf=4, morton_bits=21, spatial_eps=3.0e38),
+}
+
+NODE_DTYPE = np.dtype([("bmin", "<f4", 4), ("bmax", "<f4", 4), ("is_leaf", "u1"), ("pad0", "u1", 3),
+                       ("a", "<u4"), ("b", "<u4"), ("pad1", "<u4")])
+assert NODE_DTYPE.itemsize == 48
+
+
+class OrcCfg(C.Structure):
+    _fields_ = [("lbvh_threshold", C.c_uint32), ("max_leaf", C.c_uint32), ("morton_bits", C.c_uint32),
+                ("bins_min", C.c_uint32), ("bins_max", C.c_uint32), ("c_trav", C.c_float),
+                ("c_isect", C.c_float), ("centroid_eps", C.c_float), ("spatial_eps", C.c_float),
+                ("spatial_mult", C.c_float)]
+
+
+class OrcMaterial(C.Structure):
+    _fields_ = [("albedo", C.c_float * 3), ("emission", C.c_float * 3), ("kind", C.c_uint32),
+                ("pad", C.c_uint32)]
+
+
+class OrcRenderCfg(C.Structure):
+    _fields_ = [("width", C.c_uint32), ("height", C.c_uint32), ("spp", C.c_uint32),
+                ("max_bounce", C.c_uint32), ("rr_after", C.c_int32), ("env_kind", C.c_uint32),
+                ("env_color", C.c_float * 3), ("cam_pos", C.c_float * 3), ("cam_fwd", C.c_float * 3),
+                ("cam_right", C.c_float * 3), ("cam_up", C.c_float * 3), ("tan_half_fov_y", C.c_float),
+                ("seed", C.c_uint32), ("sample_offset", C.c_uint32)]
+
+
+def _p(a):
+    return a.ctypes.data_as(C.c_void_p) if a is not None else None
+
+
+def make_cfg(**kw) -> OrcCfg:
+    c = OrcCfg(64, 16, 21, 8, 32, 1.0, 1.2, 1e-6, 1e-6, 1.5)
+    for k, v in kw.items():
+        setattr(c, k, v)
+    return c
+
+
+class Baked:
+    """A baked BVH in the .bvh v1 layout: nodes (48-byte records), triangles, vertices."""
+
+    def __init__(self, nodes, tris, verts, stats=None):
+        self.nodes, self.tris, self.verts, self.stats = nodes, tris, verts, stats
+
+    @staticmethod
+    def read_bvh(path) -> "Baked":
+        """Reads a .bvh v1 file (src/bvh/bvh_IO.cpp:236-275 writes it)."""
+        raw = np.fromfile(path, dtype=np.uint8)
+        hdr = raw[:16].view("<u4")
+        ver, nn, nt, nv = (int(x) for x in hdr)
+        assert ver == 1, ver
+        o = 16
+        nodes = raw[o:o + 48 * nn].view(NODE_DTYPE).copy(); o += 48 * nn
+        tris = raw[o:o + 12 * nt].view("<u4").reshape(nt, 3).copy(); o += 12 * nt
+        verts = raw[o:o + 24 * nv].view("<f4").reshape(nv, 6).copy(); o += 24 * nv
+        assert o == raw.size
+        return Baked(nodes, tris, verts)
+
+
+class Restatement:
+    """liboracle.so: the C restatement (oracle/rt_oracle.c)."""
+
+    def __init__(self, path: str = ORACLE_LIB):
+        if not os.path.exists(path):
+            raise FileNotFoundError(f"{path} missing: run `make -C oracle`")
+        L = C.CDLL(path)
+        self.L = L
+        vp, u32, u64 = C.c_void_p, C.c_uint32, C.c_uint64
+        L.orc_morton.argtypes = [vp, u32, vp, u32, vp, vp, vp, vp]
+        L.orc_build.restype = vp
+        L.orc_build.argtypes = [vp, u32, vp, u32, vp]
+        L.orc_counts.argtypes = [vp, vp]
+        L.orc_stats.argtypes = [vp, vp]
+        L.orc_get.argtypes = [vp, vp, vp, vp]
+        L.orc_free.argtypes = [vp]
+        L.orc_from_arrays.restype = vp
+        L.orc_from_arrays.argtypes = [vp, u32, vp, u32, vp, u32]
+        L.orc_normalize_normals.argtypes = [vp, u32]
+        L.orc_clip_triangle.argtypes = [vp, vp, vp]
+        L.orc_trace.restype = u64
+        L.orc_trace.argtypes = [vp, vp, u64, u32, vp, vp, vp, vp, C.c_int]
+        L.orc_render.argtypes = [vp, vp, vp, vp, u32, u32, vp, vp, C.c_int]
+        L.orc_philox.argtypes = [u32, u32, u32, u32, u32, u32, vp]
+
+    def morton(self, verts, tris, cfg: OrcCfg):
+        verts = np.ascontiguousarray(verts, np.float32); tris = np.ascontiguousarray(tris, np.uint32)
+        n = tris.shape[0]
+        codes = np.zeros(n, np.uint64); perm = np.zeros(n, np.uint32); sb = np.zeros(6, np.float32)
+        ok = self.L.orc_morton(_p(verts), verts.shape[0], _p(tris), n, C.byref(cfg), _p(codes), _p(perm), _p(sb))
+        assert ok
+        return codes, perm, sb
+
+    def build(self, verts, tris, cfg: OrcCfg) -> Baked | None:
+        verts = np.ascontiguousarray(verts, np.float32); tris = np.ascontiguousarray(tris, np.uint32)
+        h = self.L.orc_build(_p(verts), verts.shape[0], _p(tris), tris.shape[0], C.byref(cfg))
+        if not h:
+            return None
+        cnt = np.zeros(3, np.uint32); st = np.zeros(4, np.uint32)
+        self.L.orc_counts(h, _p(cnt)); self.L.orc_stats(h, _p(st))
+        nodes = np.zeros(int(cnt[0]), NODE_DTYPE)
+        ot = np.zeros((int(cnt[1]), 3), np.uint32)
+        ov = np.zeros((int(cnt[2]), 6), np.float32)
+        self.L.orc_get(h, _p(nodes), _p(ot), _p(ov))
+        self.L.orc_free(h)
+        return Baked(nodes, ot, ov, st)
+
+    def normalize_normals(self, verts):
+        v = np.ascontiguousarray(verts, np.float32).copy()
+        self.L.orc_normalize_normals(_p(v), v.shape[0])
+        return v
+
+    def clip_triangle(self, v9, box6):
+        v9 = np.ascontiguousarray(v9, np.float32); box6 = np.ascontiguousarray(box6, np.float32)
+        out = np.zeros(6, np.float32)
+        self.L.orc_clip_triangle(_p(v9), _p(box6), _p(out))
+        return out
+
+    def trace(self, baked: Baked, rays, flags: int = 0, threads: int = 1, counters: bool = False):
+        """rays: (n, 8) float32 = o.xyz, tmin, d.xyz, tmax. Returns hit, t/u/v/n, tri, counters, overflow."""
+        rays = np.ascontiguousarray(rays, np.float32)
+        n = rays.shape[0]
+        h = self.L.orc_from_arrays(_p(baked.nodes), baked.nodes.shape[0], _p(baked.tris), baked.tris.shape[0],
+                                   _p(baked.verts), baked.verts.shape[0])
+        out = np.zeros((n, 6), np.float32); tri = np.zeros(n, np.uint32); hit = np.zeros(n, np.uint8)
+        ctr = np.zeros((n, 3), np.uint32) if counters else None
+        of = self.L.orc_trace(h, _p(rays), n, flags, _p(out), _p(tri), _p(hit), _p(ctr), threads)
+        self.L.orc_free(h)
+        return hit, out, tri, ctr, int(of)
+
+    def render(self, baked: Baked, rcfg: OrcRenderCfg, mats=None, mat_of_tri=None, rows=None, threads: int = 1,
+               want_sq: bool = False):
+        W, H = rcfg.width, rcfg.height
+        rgb = np.zeros((H, W, 3), np.float32)
+        rgb2 = np.zeros((H, W, 3), np.float32) if want_sq else None
+        hnd = self.L.orc_from_arrays(_p(baked.nodes), baked.nodes.shape[0], _p(baked.tris), baked.tris.shape[0],
+                                     _p(baked.verts), baked.verts.shape[0])
+        r0, r1 = rows if rows is not None else (0, H)
+        mats_arr = None
+        if mats is not None:
+            mats_arr = (OrcMaterial * len(mats))()
+            for i, m in enumerate(mats):
+                mats_arr[i].albedo[:] = list(m["albedo"]); mats_arr[i].emission[:] = list(m.get("emission", (0, 0, 0)))
+                mats_arr[i].kind = int(m.get("kind", 0))
+            mot = np.ascontiguousarray(mat_of_tri, np.uint32)
+        else:
+            mot = None
+        self.L.orc_render(hnd, C.byref(rcfg), mats_arr if mats_arr is not None else None, _p(mot), r0, r1,
+                          _p(rgb), _p(rgb2), threads)
+        self.L.orc_free(hnd)
+        return rgb, rgb2
+
+    def philox(self, c, k):
+        out = np.zeros(4, np.uint32)
+        self.L.orc_philox(*[int(x) for x in c], *[int(x) for x in k], _p(out))
+        return out
+
+
+class Reference:
+    """oracle/_ref/<variant>/libref.so: the reference's own bake/load/trace."""
+
+    def __init__(self, variant: str = "hybrid"):
+        path = os.path.join(REF_DIR, variant, "libref.so")
+        if not os.path.exists(path):
+            raise FileNotFoundError(path)
+        L = C.CDLL(path)
+        self.L = L
+        self.variant = variant
+        vp, u32, u64 = C.c_void_p, C.c_uint32, C.c_uint64
+        L.ref_constants.argtypes = [vp]
+        L.ref_bake_arrays.argtypes = [vp, u32, vp, u32, C.c_char_p]
+        L.ref_bake_scene.argtypes = [C.c_char_p]
+        L.ref_scene_geometry.argtypes = [C.c_char_p, vp, vp, vp]
+        L.ref_morton.argtypes = [vp, u32, vp, u32, vp, vp, vp]
+        L.ref_init_geos.argtypes = [vp, u32, vp, u32]
+        L.ref_load.argtypes = [C.c_char_p]
+        L.ref_trace.argtypes = [vp, u64, vp, vp, vp, C.c_int]
+        L.ref_clip_triangle.argtypes = [vp, vp, vp]
+
+    @staticmethod
+    def available(variant: str = "hybrid") -> bool:
+        return os.path.exists(os.path.join(REF_DIR, variant, "libref.so"))
+
+    def constants(self):
+        out = np.zeros(6, np.int32)
+        self.L.ref_constants(_p(out))
+        return out
+
+    def bake(self, verts, tris) -> Baked | None:
+        verts = np.ascontiguousarray(verts, np.float32); tris = np.ascontiguousarray(tris, np.uint32)
+        with tempfile.TemporaryDirectory() as d:
+            scn = os.path.join(d, "g.scn")
+            ok = self.L.ref_bake_arrays(_p(verts), verts.shape[0], _p(tris), tris.shape[0], scn.encode())
+            if not ok:
+                return None
+            return Baked.read_bvh(os.path.join(d, "g.bvh"))
+
+    def scene_geometry(self, scn_path):
+        cnt = np.zeros(2, np.uint32)
+        assert self.L.ref_scene_geometry(scn_path.encode(), None, None, _p(cnt))
+        v = np.zeros((int(cnt[0]), 6), np.float32); t = np.zeros((int(cnt[1]), 3), np.uint32)
+        assert self.L.ref_scene_geometry(scn_path.encode(), _p(v), _p(t), _p(cnt))
+        return v, t
+
+    def morton(self, verts, tris):
+        verts = np.ascontiguousarray(verts, np.float32); tris = np.ascontiguousarray(tris, np.uint32)
+        n = tris.shape[0]
+        codes = np.zeros(n, np.uint64); perm = np.zeros(n, np.uint32); sb = np.zeros(6, np.float32)
+        assert self.L.ref_morton(_p(verts), verts.shape[0], _p(tris), n, _p(codes), _p(perm), _p(sb))
+        return codes, perm, sb
+
+    def init_geos(self, verts, tris):
+        v = np.ascontiguousarray(verts, np.float32).copy(); tris = np.ascontiguousarray(tris, np.uint32)
+        assert self.L.ref_init_geos(_p(v), v.shape[0], _p(tris), tris.shape[0])
+        return v
+
+    def trace(self, baked: Baked, rays, threads: int = 1):
+        rays = np.ascontiguousarray(rays, np.float32)
+        n = rays.shape[0]
+        with tempfile.TemporaryDirectory() as d:
+            path = os.path.join(d, "t.bvh")
+            write_bvh(path, baked)
+            assert self.L.ref_load(path.encode())
+        out = np.zeros((n, 6), np.float32); tri = np.zeros(n, np.uint32); hit = np.zeros(n, np.uint8)
+        self.L.ref_trace(_p(rays), n, _p(out), _p(tri), _p(hit), threads)
+        return hit, out, tri
+
+    def clip_triangle(self, v9, box6):
+        v9 = np.ascontiguousarray(v9, np.float32); box6 = np.ascontiguousarray(box6, np.float32)
+        out = np.zeros(6, np.float32)
+        self.L.ref_clip_triangle(_p(v9), _p(box6), _p(out))
+        return out
+
+
+def write_bvh(path, baked: Baked):
+    """Writes a .bvh v1 file with the layout of src/bvh/bvh_IO.cpp:256-265."""
+    hdr = np.array([1, baked.nodes.shape[0], baked.tris.shape[0], baked.verts.shape[0]], "<u4")
+    with open(path, "wb") as f:
+        f.write(hdr.tobytes())
+        f.write(np.ascontiguousarray(baked.nodes).tobytes())
+        f.write(np.ascontiguousarray(baked.tris, "<u4").tobytes())
+        f.write(np.ascontiguousarray(baked.verts, "<f4").tobytes())

@@ -1,0 +1,181 @@
+"""Seeded synthetic scenes for the benchmark workloads and the parity tests.
+
+All geometry is float32 in the reference's vertex layout (x, y, z, nx, ny, nz) with
+uint32 triangle index triples. The generators are pinned here in code so that the GPU
+build, the oracle and the CPU baseline all see identical inputs.
+
+* ``soup``       -- the BVH microbenchmark soup: N triangles, centroid uniform in [0,1]^3,
+                    each vertex at centroid + L * u with L log-uniform in [1e-4, 1e-2] and u
+                    uniform on the unit sphere (one independent draw per vertex).
+* ``icosphere``  -- icosahedron subdivided ``level`` times (20 * 4**level triangles, shared
+                    vertices), each vertex pushed radially by uniform[-disp, disp] * radius.
+* ``cornell``    -- a Cornell box of 5 axis-aligned quads (2 triangles each) facing inward
+                    plus one quad area light under the ceiling, facing down.
+* ``incoherent_rays`` / ``pinhole_rays`` -- the microbenchmark ray sets.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+BASE_SEED = 20261203
+
+
+def _face_normals(v, t):
+    p0, p1, p2 = v[t[:, 0], :3], v[t[:, 1], :3], v[t[:, 2], :3]
+    n = np.cross(p1 - p0, p2 - p0)
+    ln = np.linalg.norm(n, axis=1, keepdims=True)
+    return n / np.maximum(ln, 1e-30)
+
+
+def soup(n: int, seed: int = BASE_SEED + 1, lo: float = 1e-4, hi: float = 1e-2):
+    """Random triangle soup; returns (verts (3n, 6) f32, tris (n, 3) u32)."""
+    rng = np.random.default_rng(seed)
+    c = rng.random((n, 1, 3), dtype=np.float64)
+    L = np.exp(rng.uniform(np.log(lo), np.log(hi), size=(n, 3, 1)))
+    u = rng.normal(size=(n, 3, 3))
+    u /= np.linalg.norm(u, axis=2, keepdims=True)
+    p = (c + L * u).reshape(-1, 3).astype(np.float32)
+    tris = np.arange(3 * n, dtype=np.uint32).reshape(n, 3)
+    verts = np.zeros((3 * n, 6), np.float32)
+    verts[:, :3] = p
+    fn = _face_normals(verts, tris).astype(np.float32)
+    verts[:, 3:] = np.repeat(fn, 3, axis=0)
+    return verts, tris
+
+
+def _icosahedron():
+    t = (1.0 + 5.0 ** 0.5) / 2.0
+    v = np.array([[-1, t, 0], [1, t, 0], [-1, -t, 0], [1, -t, 0], [0, -1, t], [0, 1, t], [0, -1, -t], [0, 1, -t],
+                  [t, 0, -1], [t, 0, 1], [-t, 0, -1], [-t, 0, 1]], np.float64)
+    v /= np.linalg.norm(v, axis=1, keepdims=True)
+    f = np.array([[0, 11, 5], [0, 5, 1], [0, 1, 7], [0, 7, 10], [0, 10, 11], [1, 5, 9], [5, 11, 4], [11, 10, 2],
+                  [10, 7, 6], [7, 1, 8], [3, 9, 4], [3, 4, 2], [3, 2, 6], [3, 6, 8], [3, 8, 9], [4, 9, 5],
+                  [2, 4, 11], [6, 2, 10], [8, 6, 7], [9, 8, 1]], np.int64)
+    return v, f
+
+
+def icosphere(level: int, center=(0.0, 0.0, 0.0), radius: float = 1.0, disp: float = 0.05,
+              seed: int = BASE_SEED, max_tris: int | None = None):
+    """Displaced icosphere; outward-facing under the reference's winding convention.
+
+    ``max_tris`` keeps the first faces of the subdivided mesh (the truncation rule of the
+    50,000- and 12,500-triangle variants); unreferenced vertices are kept."""
+    v, f = _icosahedron()
+    for _ in range(level):
+        cache = {}
+        verts = list(v)
+
+        def mid(a, b):
+            key = (a, b) if a < b else (b, a)
+            if key not in cache:
+                m = verts[a] + verts[b]
+                m = m / np.linalg.norm(m)
+                cache[key] = len(verts)
+                verts.append(m)
+            return cache[key]
+
+        nf = []
+        for a, b, c in f:
+            ab, bc, ca = mid(a, b), mid(b, c), mid(c, a)
+            nf += [[a, ab, ca], [b, bc, ab], [c, ca, bc], [ab, bc, ca]]
+        v = np.array(verts)
+        f = np.array(nf, np.int64)
+    rng = np.random.default_rng(seed)
+    scale = 1.0 + rng.uniform(-disp, disp, size=(v.shape[0], 1))
+    p = v * scale * radius + np.asarray(center, np.float64)
+    if max_tris is not None:
+        f = f[:max_tris]
+    # The reference culls triangles whose geometric normal faces along the ray
+    # (src/bvh/bvh_traverse.cpp:57 rejects dot(e1, cross(d, e2)) >= 0), so a surface seen
+    # from outside must be wound clockwise as seen from outside: flip the icosahedron's
+    # counter-clockwise faces.
+    f = f[:, [0, 2, 1]]
+    verts = np.zeros((v.shape[0], 6), np.float32)
+    verts[:, :3] = p.astype(np.float32)
+    # smooth normals: area-weighted face normals accumulated per vertex (outward)
+    fp = p[f]
+    fn = np.cross(fp[:, 2] - fp[:, 0], fp[:, 1] - fp[:, 0])
+    acc = np.zeros_like(p)
+    for k in range(3):
+        np.add.at(acc, f[:, k], fn)
+    ln = np.linalg.norm(acc, axis=1, keepdims=True)
+    acc = np.where(ln > 0, acc / np.maximum(ln, 1e-30), v)
+    verts[:, 3:] = acc.astype(np.float32)
+    return verts, f.astype(np.uint32)
+
+
+def quad(p0, p1, p2, p3, normal):
+    """Two triangles (p0, p1, p2) and (p0, p2, p3); wound so that rays travelling against
+    ``normal`` hit them under the reference's culling rule."""
+    P = np.array([p0, p1, p2, p3], np.float64)
+    n = np.asarray(normal, np.float64)
+    e1, e2 = P[1] - P[0], P[2] - P[0]
+    # accepted iff dot(e1, cross(d, e2)) < 0 for d = -n  <=>  dot(cross(e1, e2), n) < 0
+    if np.dot(np.cross(e1, e2), n) > 0:
+        P = P[[0, 3, 2, 1]]
+    verts = np.zeros((4, 6), np.float32)
+    verts[:, :3] = P.astype(np.float32)
+    verts[:, 3:] = (n / np.linalg.norm(n)).astype(np.float32)
+    tris = np.array([[0, 1, 2], [0, 2, 3]], np.uint32)
+    return verts, tris
+
+
+def cornell(size: float = 2.0, light_size: float = 0.5):
+    """Cornell box spanning [-size/2, size/2]^3 with an open front (z = -size/2); returns
+    (verts, tris, object id per triangle) with object ids 0 floor, 1 ceiling, 2 back,
+    3 left, 4 right, 5 light."""
+    h = size / 2.0
+    walls = [
+        ([-h, -h, -h], [h, -h, -h], [h, -h, h], [-h, -h, h], [0, 1, 0]),     # floor
+        ([-h, h, -h], [h, h, -h], [h, h, h], [-h, h, h], [0, -1, 0]),       # ceiling
+        ([-h, -h, h], [h, -h, h], [h, h, h], [-h, h, h], [0, 0, -1]),       # back
+        ([-h, -h, -h], [-h, -h, h], [-h, h, h], [-h, h, -h], [1, 0, 0]),    # left
+        ([h, -h, -h], [h, -h, h], [h, h, h], [h, h, -h], [-1, 0, 0]),       # right
+    ]
+    l = light_size / 2.0
+    y = h - 1e-3 * size
+    walls.append(([-l, y, -l], [l, y, -l], [l, y, l], [-l, y, l], [0, -1, 0]))
+    return concat([quad(*w) for w in walls])
+
+
+def concat(parts):
+    """Concatenate (verts, tris) parts; returns (verts, tris, part id per triangle)."""
+    vs, ts, ids = [], [], []
+    off = 0
+    for i, (v, t) in enumerate(parts):
+        vs.append(v)
+        ts.append(t.astype(np.uint64) + off)
+        ids.append(np.full(t.shape[0], i, np.uint32))
+        off += v.shape[0]
+    return (np.concatenate(vs).astype(np.float32), np.concatenate(ts).astype(np.uint32),
+            np.concatenate(ids))
+
+
+def incoherent_rays(n: int, lo, hi, seed: int = BASE_SEED + 7, tmin: float = 0.0, tmax: float = np.inf):
+    """Origins uniform in the box [lo, hi], directions uniform on S^2; (n, 8) f32."""
+    rng = np.random.default_rng(seed)
+    o = rng.uniform(np.asarray(lo, np.float64), np.asarray(hi, np.float64), size=(n, 3))
+    d = rng.normal(size=(n, 3))
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    r = np.empty((n, 8), np.float32)
+    r[:, 0:3] = o; r[:, 3] = tmin; r[:, 4:7] = d; r[:, 7] = tmax
+    return r
+
+
+def pinhole_rays(width: int, height: int, pos, target, fov_deg: float = 60.0):
+    """One primary ray per pixel centre of a look-at pinhole camera; (W*H, 8) f32."""
+    pos = np.asarray(pos, np.float64); target = np.asarray(target, np.float64)
+    fwd = target - pos; fwd /= np.linalg.norm(fwd)
+    up0 = np.array([0.0, 1.0, 0.0]) if abs(fwd[1]) < 0.99 else np.array([1.0, 0.0, 0.0])
+    right = np.cross(fwd, up0); right /= np.linalg.norm(right)
+    up = np.cross(right, fwd)
+    th = np.tan(np.radians(fov_deg) * 0.5)
+    aspect = width / height
+    xs = ((np.arange(width) + 0.5) / width * 2 - 1) * aspect * th
+    ys = ((np.arange(height) + 0.5) / height * 2 - 1) * th
+    X, Y = np.meshgrid(xs, ys)
+    d = fwd[None, None, :] + X[..., None] * right + Y[..., None] * up
+    d /= np.linalg.norm(d, axis=2, keepdims=True)
+    r = np.empty((width * height, 8), np.float32)
+    r[:, 0:3] = pos; r[:, 3] = 1e-3; r[:, 4:7] = d.reshape(-1, 3); r[:, 7] = np.inf
+    return r
