@@ -1,0 +1,622 @@
+// build.cu -- the GPU bake: the reference's bvh::bakeBVH (src/bvh/bvh_bake.cpp:180-194) as a
+// handful of data-parallel kernels producing the identical tree.
+//
+//  k_vertices   normal renormalisation of initGeos (src/bvh/bvh_IO.cpp:102-118)
+//  k_tri_prep   index check (bvh_IO.cpp:88-99), per-triangle box and centroid
+//               (bvh_morton.cpp:88-90, bvh_bake.cpp:50-54), scene box (bvh_morton.cpp:49-59)
+//  k_morton     quantisation + 3-way bit interleave (bvh_morton.cpp:19-36,61-101), and the
+//               digit histograms of every radix pass
+//  radix sort   stable onesweep LSD sort (radix_sort.cu; bvh_morton.cpp:109-159)
+//  k_karras     Karras (HPG 2012) radix tree over the sorted codes. Its split of a range whose
+//               first and last codes differ is the reference's Morton split (the first index
+//               where the highest differing bit flips, bvh_bfs.cpp:35-48,98-109)
+//  k_boundary   the reference stops splitting at <= BVH_MAX_LEAF_SIZE triangles, hands ranges of
+//               <= BVH_LBVH_THRESHOLD triangles or of identical codes to the binned SAH
+//               (bvh_bfs.cpp:30-33,79-107); this kernel finds those boundary nodes, computes
+//               their exact range boxes (computeRangeAABB, bvh_bfs.cpp:14-28) and refits the
+//               Morton-split nodes above them bottom-up with arrival counters
+//  sah.cu       the binned SAH / spatial-split subtrees (bvh_sah.cpp:24-460)
+//  k_emit*      the DFS pre-order re-layout of reorderNodes / reorderTriangles
+//               (bvh_bake.cpp:75-149): a node's pre-order index is the number of nodes whose
+//               key range starts before its own plus its depth on its left spine, so every
+//               node finds its output slot from two prefix sums without a tree walk.
+#include "rt_internal.h"
+#include "device_math.cuh"
+#include "cta_utils.cuh"
+#include "sah.cuh"
+#include "layout.cuh"
+
+#include <algorithm>
+#include <cstring>
+
+namespace rtb
+{
+using namespace rtd;
+
+namespace
+{
+
+constexpr int BLK = 256;
+constexpr uint32_t NONE = 0xffffffffu;
+// A Karras tree over n distinct (key, index) pairs is at most key bits + 32 deep.
+constexpr uint32_t MAX_DEPTH = 128;
+
+inline uint32_t blocks_for(uint64_t n, int per = BLK) { return (uint32_t)((n + per - 1) / per); }
+
+// Three-argument hypot by scaling with the largest magnitude -- the evaluation the
+// reference's std::hypot(float, float, float) performs (pinned bit-exactly by the tests).
+__device__ __forceinline__ float hypot3f(float x, float y, float z)
+{
+    x = fabsf(x); y = fabsf(y); z = fabsf(z);
+    const float a = x < y ? (y < z ? z : y) : (x < z ? z : x);
+    if (a == 0.0f) { return 0.0f; }
+    const float xa = x / a, ya = y / a, za = z / a;
+    return a * sqrtf(xa * xa + ya * ya + za * za);
+}
+
+// Spreads the low 21 bits of v so that bit i lands on bit 3i (the standard
+// shift-and-mask interleave for 3-D Morton codes).
+__device__ __forceinline__ uint64_t spread3(uint32_t v)
+{
+    uint64_t x = v & 0x1fffffu;
+    x = (x | (x << 32)) & 0x001f00000000ffffull;
+    x = (x | (x << 16)) & 0x001f0000ff0000ffull;
+    x = (x | (x << 8)) & 0x100f00f00f00f00full;
+    x = (x | (x << 4)) & 0x10c30c30c30c30c3ull;
+    x = (x | (x << 2)) & 0x1249249249249249ull;
+    return x;
+}
+
+__global__ void k_init(uint32_t* scene, uint32_t* hist, uint32_t* counters, uint32_t* status)
+{
+    const int t = threadIdx.x;
+    if (t < 3) { scene[t] = 0xffffffffu; scene[3 + t] = 0u; }
+    for (int i = t; i < 8 * 256; i += blockDim.x) { hist[i] = 0u; }
+    if (t < 16) { counters[t] = 0u; }
+    if (t == 0) { *status = 0u; }
+}
+
+__global__ void __launch_bounds__(BLK) k_vertices(const rt_vertex* __restrict__ in, rt_vertex* __restrict__ out, uint32_t V)
+{
+    const uint32_t i = blockIdx.x * BLK + threadIdx.x;
+    if (i >= V) { return; }
+    rt_vertex v = in[i];
+    const float len = hypot3f(v.nx, v.ny, v.nz);
+    if (len > 1e-6f) { v.nx /= len; v.ny /= len; v.nz /= len; }
+    else { v.nx = 0.f; v.ny = 1.f; v.nz = 0.f; }
+    out[i] = v;
+}
+
+__device__ __forceinline__ f3 vpos(const rt_vertex* v, uint32_t i)
+{
+    const rt_vertex& p = v[i];
+    return mk3(p.x, p.y, p.z);
+}
+
+// Per triangle: index check, box (lo.xyz/hi.xyz) with the centroid in lo.w, hi.w, cz.
+// Block-reduces the scene box into `scene` (order-preserving uint encoding).
+__global__ void __launch_bounds__(BLK)
+k_tri_prep(const rt_triangle* __restrict__ tris, uint32_t N, const rt_vertex* __restrict__ verts, uint32_t V,
+           float4* __restrict__ lo, float4* __restrict__ hi, float* __restrict__ cz, uint32_t* __restrict__ scene,
+           uint32_t* __restrict__ status)
+{
+    const uint32_t i = blockIdx.x * BLK + threadIdx.x;
+    uint32_t om[3] = { 0xffffffffu, 0xffffffffu, 0xffffffffu }, oM[3] = { 0u, 0u, 0u };
+    if (i < N)
+    {
+        uint32_t a = tris[i].v[0], b = tris[i].v[1], c = tris[i].v[2];
+        if (a >= V || b >= V || c >= V) { atomicOr(status, ST_INDEX); a = b = c = 0; }
+        const f3 p0 = vpos(verts, a), p1 = vpos(verts, b), p2 = vpos(verts, c);
+        box3 bx = box_empty();
+        box_pt(bx, p0); box_pt(bx, p1); box_pt(bx, p2);
+        const float cx = (p0.x + p1.x + p2.x) / 3.0f;
+        const float cy = (p0.y + p1.y + p2.y) / 3.0f;
+        const float czv = (p0.z + p1.z + p2.z) / 3.0f;
+        lo[i] = make_float4(bx.mn[0], bx.mn[1], bx.mn[2], cx);
+        hi[i] = make_float4(bx.mx[0], bx.mx[1], bx.mx[2], cy);
+        cz[i] = czv;
+        for (int k = 0; k < 3; k++) { om[k] = f2ord(bx.mn[k]); oM[k] = f2ord(bx.mx[k]); }
+    }
+    __shared__ uint32_t s[6];
+    if (threadIdx.x < 3) { s[threadIdx.x] = 0xffffffffu; s[3 + threadIdx.x] = 0u; }
+    __syncthreads();
+    for (int k = 0; k < 3; k++)
+    {
+        uint32_t m = om[k], M = oM[k];
+        for (int o = 16; o > 0; o >>= 1)
+        {
+            m = min(m, __shfl_xor_sync(0xffffffffu, m, o));
+            M = max(M, __shfl_xor_sync(0xffffffffu, M, o));
+        }
+        if ((threadIdx.x & 31) == 0) { atomicMin(&s[k], m); atomicMax(&s[3 + k], M); }
+    }
+    __syncthreads();
+    if (threadIdx.x < 3)
+    {
+        atomicMin(&scene[threadIdx.x], s[threadIdx.x]);
+        atomicMax(&scene[3 + threadIdx.x], s[3 + threadIdx.x]);
+    }
+}
+
+// Morton code per triangle (input order) and the 8-bit digit histograms of all sort passes.
+template <typename K>
+__global__ void __launch_bounds__(BLK)
+k_morton(const float4* __restrict__ lo, const float4* __restrict__ hi, const float* __restrict__ cz, uint32_t N,
+         const uint32_t* __restrict__ scene, uint32_t bits, int passes, K* __restrict__ keys, uint32_t* __restrict__ hist)
+{
+    __shared__ uint32_t h[8 * 256];
+    for (int t = threadIdx.x; t < passes * 256; t += BLK) { h[t] = 0u; }
+    __syncthreads();
+    const uint32_t i = blockIdx.x * BLK + threadIdx.x;
+    if (i < N)
+    {
+        float mn[3], size[3];
+        for (int k = 0; k < 3; k++)
+        {
+            mn[k] = ord2f(scene[k]);
+            size[k] = ord2f(scene[3 + k]) - mn[k];
+            if (size[k] == 0.f) { size[k] = 1.f; }
+        }
+        const uint32_t qmax = (1u << bits) - 1u;
+        const float fmax = (float)qmax;
+        const float c[3] = { lo[i].w, hi[i].w, cz[i] };
+        uint32_t q[3];
+        for (int k = 0; k < 3; k++)
+        {
+            const uint32_t v = x86_f2u((c[k] - mn[k]) * fmax / size[k]);
+            q[k] = v > qmax ? qmax : v;
+        }
+        const uint64_t code = (spread3(q[0]) << 2) | (spread3(q[1]) << 1) | spread3(q[2]);
+        keys[i] = (K)code;
+        for (int p = 0; p < passes; p++) { atomicAdd(&h[p * 256 + (uint32_t)((code >> (8 * p)) & 255u)], 1u); }
+    }
+    __syncthreads();
+    for (int t = threadIdx.x; t < passes * 256; t += BLK)
+    {
+        if (h[t]) { atomicAdd(&hist[t], h[t]); }
+    }
+}
+
+template <typename K> __device__ __forceinline__ int key_clz(K x);
+template <> __device__ __forceinline__ int key_clz<uint64_t>(uint64_t x) { return __clzll((long long)x); }
+template <> __device__ __forceinline__ int key_clz<uint32_t>(uint32_t x) { return __clz((int)x); }
+
+// Common-prefix length of keys i and j, extended by the index bits for equal keys (Karras).
+template <typename K>
+__device__ __forceinline__ int kdelta(const K* __restrict__ keys, int n, int i, int j)
+{
+    if (j < 0 || j >= n) { return -1; }
+    const K a = keys[i], b = keys[j];
+    if (a != b) { return key_clz<K>(a ^ b); }
+    return (int)(sizeof(K) * 8) + __clz(i ^ j);
+}
+
+// Karras radix tree: inner node i covers [first, last] and splits after gamma.
+// Node ids: inner 0..n-2, leaf k -> n-1+k. knode = {first, last, left, right}.
+template <typename K>
+__global__ void __launch_bounds__(BLK)
+k_karras(const K* __restrict__ keys, uint32_t n, uint4* __restrict__ knode, uint32_t* __restrict__ parent)
+{
+    const int i = (int)(blockIdx.x * BLK + threadIdx.x);
+    const int N = (int)n;
+    if (i >= N - 1) { return; }
+    const int d = (kdelta<K>(keys, N, i, i + 1) - kdelta<K>(keys, N, i, i - 1)) >= 0 ? 1 : -1;
+    const int dmin = kdelta<K>(keys, N, i, i - d);
+    int lmax = 2;
+    while (kdelta<K>(keys, N, i, i + lmax * d) > dmin) { lmax <<= 1; }
+    int l = 0;
+    for (int t = lmax >> 1; t >= 1; t >>= 1)
+    {
+        if (kdelta<K>(keys, N, i, i + (l + t) * d) > dmin) { l += t; }
+    }
+    const int j = i + l * d;
+    const int dnode = kdelta<K>(keys, N, i, j);
+    int s = 0;
+    int t = l;
+    do
+    {
+        t = (t + 1) >> 1;
+        if (kdelta<K>(keys, N, i, i + (s + t) * d) > dnode) { s += t; }
+    } while (t > 1);
+    const int gamma = i + s * d + min(d, 0);
+    const int first = min(i, j), last = max(i, j);
+    const uint32_t left = (first == gamma) ? (uint32_t)(N - 1 + gamma) : (uint32_t)gamma;
+    const uint32_t right = (last == gamma + 1) ? (uint32_t)(N - 1 + gamma + 1) : (uint32_t)(gamma + 1);
+    knode[i] = make_uint4((uint32_t)first, (uint32_t)last, left, right);
+    parent[left] = (uint32_t)i;
+    parent[right] = (uint32_t)i;
+}
+
+template <typename K>
+__device__ __forceinline__ void krange(const uint4* __restrict__ knode, uint32_t n, uint32_t x, uint32_t& f, uint32_t& l)
+{
+    if (x < n - 1) { const uint4 k = knode[x]; f = k.x; l = k.y; }
+    else { f = l = x - (n - 1); }
+}
+
+// The reference splits a node by Morton code only if it has more triangles than both the
+// leaf size and the SAH threshold and its codes are not all equal (bvh_bfs.cpp:79-107).
+template <typename K>
+__device__ __forceinline__ bool morton_split_node(const K* __restrict__ keys, uint32_t f, uint32_t l, uint32_t tm)
+{
+    return (l - f + 1u) > tm && keys[f] != keys[l];
+}
+
+__device__ __forceinline__ void store_box(float4* kbox, uint32_t x, const box3& b)
+{
+    __stcg(&kbox[2 * x], make_float4(b.mn[0], b.mn[1], b.mn[2], 0.f));
+    __stcg(&kbox[2 * x + 1], make_float4(b.mx[0], b.mx[1], b.mx[2], 0.f));
+}
+__device__ __forceinline__ box3 load_box(const float4* kbox, uint32_t x)
+{
+    const float4 a = __ldcg(&kbox[2 * x]), c = __ldcg(&kbox[2 * x + 1]);
+    box3 b;
+    b.mn[0] = a.x; b.mn[1] = a.y; b.mn[2] = a.z; b.mx[0] = c.x; b.mx[1] = c.y; b.mx[2] = c.z;
+    return b;
+}
+
+// One thread per Karras node. Kept nodes (Morton-split nodes and the boundary nodes right
+// below them) record their left-spine rank; boundary nodes compute their range box, mark
+// their positions, register SAH roots, and climb to refit the Morton-split ancestors.
+template <typename K>
+__global__ void __launch_bounds__(BLK)
+k_boundary(const K* __restrict__ keys, const uint32_t* __restrict__ perm, uint32_t n, const uint4* __restrict__ knode,
+           const uint32_t* __restrict__ parent, const float4* __restrict__ lo, const float4* __restrict__ hi,
+           uint32_t tm, uint32_t max_leaf, float4* __restrict__ kbox, uint32_t* __restrict__ visit,
+           uint32_t* __restrict__ rank, uint32_t* __restrict__ wnode, uint32_t* __restrict__ wtri,
+           uint8_t* __restrict__ kpos, SahRoot* __restrict__ roots, uint32_t* __restrict__ counters,
+           uint32_t* __restrict__ status)
+{
+    const uint32_t x = blockIdx.x * BLK + threadIdx.x;
+    if (x >= 2 * n - 1) { return; }
+    uint32_t f, l;
+    krange<K>(knode, n, x, f, l);
+    const bool is_m = morton_split_node<K>(keys, f, l, tm);
+    const uint32_t par = parent[x];
+    bool kept = is_m;
+    if (!is_m)
+    {
+        if (par == NONE) { kept = true; }
+        else
+        {
+            uint32_t pf, pl;
+            krange<K>(knode, n, par, pf, pl);
+            kept = morton_split_node<K>(keys, pf, pl, tm);
+        }
+    }
+    if (!kept) { return; }
+
+    // left-spine rank: consecutive steps up while this chain is a left child
+    uint32_t r = 0, cur = x, p = par;
+    while (p != NONE && knode[p].z == cur)
+    {
+        r++; cur = p; p = parent[p];
+        if (r > MAX_DEPTH) { atomicOr(status, ST_CAPACITY); return; }
+    }
+    rank[x] = r;
+    if (is_m) { return; }
+
+    // boundary node: exact range box from the triangle boxes in sorted order
+    const uint32_t size = l - f + 1u;
+    box3 b = box_empty();
+    for (uint32_t k = f; k <= l; k++)
+    {
+        const uint32_t t = perm[k];
+        const float4 a = lo[t], c = hi[t];
+        b.mn[0] = sse_min(b.mn[0], a.x); b.mn[1] = sse_min(b.mn[1], a.y); b.mn[2] = sse_min(b.mn[2], a.z);
+        b.mx[0] = sse_max(b.mx[0], c.x); b.mx[1] = sse_max(b.mx[1], c.y); b.mx[2] = sse_max(b.mx[2], c.z);
+    }
+    store_box(kbox, x, b);
+    if (size <= max_leaf)
+    {
+        wnode[f] = r + 1u;
+        for (uint32_t k = f; k <= l; k++) { wtri[k] = 1u; kpos[k] = 1u; }
+        atomicAdd(&counters[1], 1u);
+    }
+    else
+    {
+        uint32_t depth = 0;
+        for (uint32_t q = par; q != NONE; q = parent[q])
+        {
+            if (++depth > MAX_DEPTH) { atomicOr(status, ST_CAPACITY); return; }
+        }
+        const uint32_t slot = atomicAdd(&counters[0], 1u);
+        SahRoot sr;
+        sr.kid = x; sr.first = f; sr.count = size; sr.depth = depth; sr.rank = r;
+        for (int k = 0; k < 3; k++) { sr.box[k] = b.mn[k]; sr.box[3 + k] = b.mx[k]; }
+        roots[slot] = sr;
+    }
+    // bottom-up refit of the Morton-split ancestors (second arrival computes the union)
+    cur = x;
+    p = par;
+    for (uint32_t guard = 0; p != NONE; guard++)
+    {
+        if (guard > MAX_DEPTH) { atomicOr(status, ST_CAPACITY); return; }
+        __threadfence();
+        if (atomicAdd(&visit[p], 1u) == 0u) { return; }
+        const uint4 kn = knode[p];
+        box3 u = load_box(kbox, kn.z);
+        const box3 v = load_box(kbox, kn.w);
+        box_box(u, v);
+        store_box(kbox, p, u);
+        cur = p;
+        p = parent[p];
+    }
+}
+
+// Output slots of the kept Karras nodes: pre-order index = snode[first] + rank.
+template <typename K>
+__global__ void __launch_bounds__(BLK)
+k_emit(const K* __restrict__ keys, uint32_t n, const uint4* __restrict__ knode, const uint32_t* __restrict__ parent,
+       uint32_t tm, uint32_t max_leaf, const float4* __restrict__ kbox, const uint32_t* __restrict__ rank,
+       const uint32_t* __restrict__ snode, const uint32_t* __restrict__ stri, rt_bvh_node* __restrict__ out,
+       uint32_t max_nodes, uint32_t* __restrict__ status)
+{
+    const uint32_t x = blockIdx.x * BLK + threadIdx.x;
+    if (x >= 2 * n - 1) { return; }
+    uint32_t f, l;
+    krange<K>(knode, n, x, f, l);
+    const bool is_m = morton_split_node<K>(keys, f, l, tm);
+    const uint32_t par = parent[x];
+    if (!is_m)
+    {
+        if (par != NONE)
+        {
+            uint32_t pf, pl;
+            krange<K>(knode, n, par, pf, pl);
+            if (!morton_split_node<K>(keys, pf, pl, tm)) { return; }
+        }
+        if (l - f + 1u > max_leaf) { return; }  // SAH subtree root: emitted by the SAH builder
+    }
+    const uint32_t pre = snode[f] + rank[x];
+    if (pre >= max_nodes) { atomicOr(status, ST_CAPACITY); return; }
+    const box3 b = load_box(kbox, x);
+    if (is_m)
+    {
+        const uint32_t r = knode[x].w;
+        uint32_t rf, rl;
+        krange<K>(knode, n, r, rf, rl);
+        write_node(out, pre, b, 0, pre + 1u, snode[rf]);
+    }
+    else
+    {
+        write_node(out, pre, b, 1, stri[f], l - f + 1u);
+    }
+}
+
+// Triangles of the Morton leaves, in sorted order at their output offsets.
+__global__ void __launch_bounds__(BLK)
+k_emit_tris(const uint32_t* __restrict__ perm, const uint8_t* __restrict__ kpos, const uint32_t* __restrict__ stri,
+            uint32_t n, const rt_triangle* __restrict__ tris, rt_triangle* __restrict__ out, uint32_t* __restrict__ prim,
+            uint32_t max_tris, uint32_t* __restrict__ status)
+{
+    const uint32_t k = blockIdx.x * BLK + threadIdx.x;
+    if (k >= n || !kpos[k]) { return; }
+    const uint32_t t = perm[k], at = stri[k];
+    if (at >= max_tris) { atomicOr(status, ST_CAPACITY); return; }
+    out[at] = tris[t];
+    prim[at] = t;
+}
+
+// ---- device-wide exclusive scan (reduce, scan of partials, apply) ----
+constexpr int SCAN_TILE = 2048;  // 256 threads x 8
+
+__global__ void __launch_bounds__(256) k_scan_reduce(const uint32_t* __restrict__ in, uint32_t n, uint32_t* __restrict__ part)
+{
+    __shared__ uint32_t sh[9];
+    const uint32_t base = blockIdx.x * SCAN_TILE;
+    uint32_t s = 0;
+    for (int j = 0; j < 8; j++)
+    {
+        const uint32_t i = base + j * 256 + threadIdx.x;
+        if (i < n) { s += in[i]; }
+    }
+    const uint32_t t = block_sum<256>(s, sh);
+    if (threadIdx.x == 0) { part[blockIdx.x] = t; }
+}
+
+__global__ void __launch_bounds__(1024) k_scan_partials(uint32_t* __restrict__ part, uint32_t np, uint32_t* __restrict__ total)
+{
+    __shared__ uint32_t sh[33];
+    uint32_t carry = 0;
+    for (uint32_t base = 0; base < np; base += 1024)
+    {
+        const uint32_t i = base + threadIdx.x;
+        const uint32_t v = i < np ? part[i] : 0u;
+        uint32_t tot;
+        const uint32_t e = block_excl_scan<1024>(v, sh, &tot);
+        if (i < np) { part[i] = carry + e; }
+        carry += tot;
+    }
+    if (threadIdx.x == 0 && total) { *total = carry; }
+}
+
+__global__ void __launch_bounds__(256)
+k_scan_apply(const uint32_t* __restrict__ in, uint32_t n, const uint32_t* __restrict__ part, uint32_t* __restrict__ out)
+{
+    __shared__ uint32_t sh[9];
+    const uint32_t base = blockIdx.x * SCAN_TILE + threadIdx.x * 8;
+    uint32_t v[8];
+    uint32_t s = 0;
+    for (int j = 0; j < 8; j++)
+    {
+        const uint32_t i = base + j;
+        v[j] = i < n ? in[i] : 0u;
+        s += v[j];
+    }
+    uint32_t run = part[blockIdx.x] + block_excl_scan<256>(s, sh, nullptr);
+    for (int j = 0; j < 8; j++)
+    {
+        const uint32_t i = base + j;
+        if (i < n) { out[i] = run; }
+        run += v[j];
+    }
+}
+
+template <typename K>
+int build_typed(rt_bvh* B, const rt_vertex* d_verts, uint32_t V, const rt_triangle* d_tris, uint32_t N,
+                const rt_build_cfg& cfg, cudaStream_t st, uint32_t cap)
+{
+    BuildScratch& S = B->s;
+    const int key_bits = 3 * (int)cfg.morton_bits;
+    const int passes = sort_passes(key_bits);
+    const uint32_t nk = 2 * N - 1;  // Karras nodes
+    if (S.tri_lo.ensure((size_t)N * 16) || S.tri_hi.ensure((size_t)N * 16) || S.tri_cz.ensure((size_t)N * 4) ||
+        S.keys.ensure((size_t)N * sizeof(K)) || S.vals.ensure((size_t)N * 4) || S.hist.ensure(8 * 256 * 4) ||
+        S.scene.ensure(64) || S.status.ensure(64) || S.counters.ensure(64) ||
+        S.knode.ensure((size_t)std::max<uint32_t>(N - 1, 1) * 16) || S.parent.ensure((size_t)nk * 4) ||
+        S.kbox.ensure((size_t)nk * 32) || S.visit.ensure((size_t)N * 4) || S.rank.ensure((size_t)nk * 4) ||
+        S.wnode.ensure((size_t)(N + 1) * 4) || S.wtri.ensure((size_t)(N + 1) * 4) ||
+        S.snode.ensure((size_t)(N + 1) * 4) || S.stri.ensure((size_t)(N + 1) * 4) || S.bnd.ensure((size_t)N) ||
+        S.sah_roots.ensure((size_t)N * sizeof(SahRoot)))
+    {
+        return RT_E_CUDA;
+    }
+    uint32_t* status = S.status.as<uint32_t>();
+    uint32_t* counters = S.counters.as<uint32_t>();
+
+    k_init<<<1, 256, 0, st>>>(S.scene.as<uint32_t>(), S.hist.as<uint32_t>(), counters, status);
+    count_launch();
+    RT_CUDA(cudaMemsetAsync(S.parent.p, 0xff, (size_t)nk * 4, st));
+    RT_CUDA(cudaMemsetAsync(S.visit.p, 0, (size_t)N * 4, st));
+    RT_CUDA(cudaMemsetAsync(S.wnode.p, 0, (size_t)(N + 1) * 4, st));
+    RT_CUDA(cudaMemsetAsync(S.wtri.p, 0, (size_t)(N + 1) * 4, st));
+    RT_CUDA(cudaMemsetAsync(S.bnd.p, 0, (size_t)N, st));
+
+    k_vertices<<<blocks_for(V), BLK, 0, st>>>(d_verts, B->verts.as<rt_vertex>(), V);
+    count_launch();
+    k_tri_prep<<<blocks_for(N), BLK, 0, st>>>(d_tris, N, d_verts, V, S.tri_lo.as<float4>(), S.tri_hi.as<float4>(),
+                                               S.tri_cz.as<float>(), S.scene.as<uint32_t>(), status);
+    count_launch();
+    k_morton<K><<<blocks_for(N), BLK, 0, st>>>(S.tri_lo.as<float4>(), S.tri_hi.as<float4>(), S.tri_cz.as<float>(), N,
+                                               S.scene.as<uint32_t>(), cfg.morton_bits, passes, S.keys.as<K>(),
+                                               S.hist.as<uint32_t>());
+    count_launch();
+    if (int e = check_launch("morton")) { return e; }
+
+    K* skeys = nullptr;
+    uint32_t* perm = nullptr;
+    if (int e = radix_sort_pairs<K>(S.keys.as<K>(), S.vals.as<uint32_t>(), true, N, key_bits, S.hist.as<uint32_t>(),
+                                    S.sort, status, st, &skeys, &perm))
+    {
+        return e;
+    }
+    if (N >= 2)
+    {
+        k_karras<K><<<blocks_for(N - 1), BLK, 0, st>>>(skeys, N, S.knode.as<uint4>(), S.parent.as<uint32_t>());
+        count_launch();
+    }
+    const uint32_t tm = std::max(cfg.max_leaf, cfg.lbvh_threshold);
+    k_boundary<K><<<blocks_for(nk), BLK, 0, st>>>(skeys, perm, N, S.knode.as<uint4>(), S.parent.as<uint32_t>(),
+                                                  S.tri_lo.as<float4>(), S.tri_hi.as<float4>(), tm, cfg.max_leaf,
+                                                  S.kbox.as<float4>(), S.visit.as<uint32_t>(), S.rank.as<uint32_t>(),
+                                                  S.wnode.as<uint32_t>(), S.wtri.as<uint32_t>(), S.bnd.as<uint8_t>(),
+                                                  S.sah_roots.as<SahRoot>(), counters, status);
+    count_launch();
+    if (int e = check_launch("boundary")) { return e; }
+
+    uint32_t hc[2];
+    RT_CUDA(cudaMemcpyAsync(hc, counters, 8, cudaMemcpyDeviceToHost, st));
+    RT_CUDA(cudaStreamSynchronize(st));
+    const uint32_t n_roots = hc[0];
+    B->stats[0] = B->stats[1] = 0;
+    B->stats[2] = n_roots;
+
+    SahResult sah;
+    if (n_roots > 0)
+    {
+        SahInput in;
+        in.verts = B->verts.as<rt_vertex>();
+        in.tris = d_tris;
+        in.lo = S.tri_lo.as<float4>();
+        in.hi = S.tri_hi.as<float4>();
+        in.cz = S.tri_cz.as<float>();
+        in.perm = perm;
+        in.n = N;
+        in.cap = cap;
+        in.roots = S.sah_roots.as<SahRoot>();
+        in.n_roots = n_roots;
+        in.wnode = S.wnode.as<uint32_t>();
+        in.wtri = S.wtri.as<uint32_t>();
+        if (int e = sah_build(B, cfg, in, st, &sah)) { return e; }
+        B->stats[0] = sah.spatial_taken;
+        B->stats[1] = sah.spatial_refused;
+    }
+
+    // pre-order node slots and triangle offsets per start key
+    if (int e = exclusive_scan_u32(S.wnode.as<uint32_t>(), S.snode.as<uint32_t>(), N + 1, counters + 4, S.scan, st)) { return e; }
+    if (int e = exclusive_scan_u32(S.wtri.as<uint32_t>(), S.stri.as<uint32_t>(), N + 1, counters + 5, S.scan, st)) { return e; }
+    k_emit<K><<<blocks_for(nk), BLK, 0, st>>>(skeys, N, S.knode.as<uint4>(), S.parent.as<uint32_t>(), tm, cfg.max_leaf,
+                                              S.kbox.as<float4>(), S.rank.as<uint32_t>(), S.snode.as<uint32_t>(),
+                                              S.stri.as<uint32_t>(), B->nodes.as<rt_bvh_node>(), 2 * cap - 1, status);
+    count_launch();
+    k_emit_tris<<<blocks_for(N), BLK, 0, st>>>(perm, S.bnd.as<uint8_t>(), S.stri.as<uint32_t>(), N, d_tris,
+                                                B->tris.as<rt_triangle>(), B->prim.as<uint32_t>(), cap, status);
+    count_launch();
+    if (n_roots > 0)
+    {
+        if (int e = sah_emit(B, n_roots, S.snode.as<uint32_t>(), S.stri.as<uint32_t>(), d_tris, st, sah, 2 * cap - 1, cap,
+                             status))
+        {
+            return e;
+        }
+    }
+    if (int e = check_launch("emit")) { return e; }
+
+    uint32_t res[8];
+    RT_CUDA(cudaMemcpyAsync(res, counters, 32, cudaMemcpyDeviceToHost, st));
+    uint32_t stat = 0;
+    RT_CUDA(cudaMemcpyAsync(&stat, status, 4, cudaMemcpyDeviceToHost, st));
+    RT_CUDA(cudaStreamSynchronize(st));
+    if (stat & ST_INDEX) { return fail(RT_E_INDEX, "triangle has an out-of-bounds vertex index"); }
+    if (stat & ST_TIMEOUT) { return fail(RT_E_TIMEOUT, "a bounded device wait gave up (radix sort look-back)"); }
+    if (stat & ST_CAPACITY) { return fail(RT_E_CAPACITY, "internal capacity exceeded during the build"); }
+    if (res[4] > 2 * cap - 1 || res[5] > cap) { return fail(RT_E_CAPACITY, "build produced more nodes than its bound"); }
+    B->n_nodes = res[4];
+    B->n_tris = res[5];
+    B->stats[4] = res[1] + sah.leaves;
+    B->stats[3] = B->n_nodes - B->stats[4];
+    return RT_OK;
+}
+
+} // namespace
+
+int exclusive_scan_u32(const uint32_t* in, uint32_t* out, uint32_t n, uint32_t* d_total, ScanScratch& s, cudaStream_t st)
+{
+    const uint32_t np = (n + SCAN_TILE - 1) / SCAN_TILE;
+    if (s.partials.ensure((size_t)std::max<uint32_t>(np, 1) * 4)) { return RT_E_CUDA; }
+    k_scan_reduce<<<np, 256, 0, st>>>(in, n, s.partials.as<uint32_t>());
+    k_scan_partials<<<1, 1024, 0, st>>>(s.partials.as<uint32_t>(), np, d_total);
+    k_scan_apply<<<np, 256, 0, st>>>(in, n, s.partials.as<uint32_t>(), out);
+    count_launch(3);
+    return check_launch("scan");
+}
+
+int build_bvh(rt_bvh* B, const rt_vertex* d_verts, uint32_t V, const rt_triangle* d_tris, uint32_t N,
+              const rt_build_cfg& cfg, cudaStream_t st)
+{
+    if (V == 0 || N == 0) { return fail(RT_E_EMPTY, "no vertices or no triangles"); }
+    if (cfg.morton_bits < 1 || cfg.morton_bits > 21) { return fail(RT_E_INVALID, "morton_bits must be in 1..21"); }
+    if (cfg.bins_min < 1 || cfg.bins_max > SAH_MAX_BINS || cfg.bins_min > cfg.bins_max)
+    {
+        return fail(RT_E_INVALID, "bins must satisfy 1 <= bins_min <= bins_max <= 32");
+    }
+    if (cfg.max_leaf < 1) { return fail(RT_E_INVALID, "max_leaf must be >= 1"); }
+    if (N > (1u << 29)) { return fail(RT_E_CAPACITY, "more than 2^29 triangles"); }
+    uint32_t cap = (uint32_t)((float)N * cfg.spatial_mult);  // bvh_morton.cpp:46-47
+    if (cap < N) { cap = N; }
+    const size_t max_nodes = (size_t)cap * 2 - 1;  // bvh_bfs.cpp:58
+    if (B->nodes.ensure(max_nodes * sizeof(rt_bvh_node)) || B->tris.ensure((size_t)cap * sizeof(rt_triangle)) ||
+        B->prim.ensure((size_t)cap * 4) || B->verts.ensure((size_t)V * sizeof(rt_vertex)))
+    {
+        return RT_E_CUDA;
+    }
+    B->n_verts = V;
+    B->has_prim = true;
+    int e = (3 * cfg.morton_bits > 32) ? build_typed<uint64_t>(B, d_verts, V, d_tris, N, cfg, st, cap)
+                                       : build_typed<uint32_t>(B, d_verts, V, d_tris, N, cfg, st, cap);
+    if (e) { return e; }
+    return make_traversal_layout(B, st);
+}
+
+} // namespace rtb

@@ -1,0 +1,241 @@
+// radix_sort.cu -- stable LSD radix sort of (key, uint32 value) pairs, one kernel per 8-bit
+// digit in the "onesweep" style (Adinets & Merrill, 2022): every tile ranks its keys in
+// shared memory, publishes its digit counts, and learns the counts of all earlier tiles by a
+// decoupled look-back, so each pass reads and writes the data exactly once. The digit
+// histograms of all passes come precomputed from the kernel that produced the keys.
+//
+// This replaces the reference's serial 8-pass LSD sort (src/bvh/bvh_morton.cpp:109-159);
+// stability keeps equal Morton codes in ascending triangle order, as there.
+#include "rt_internal.h"
+
+namespace rtb
+{
+namespace
+{
+
+constexpr int      RS_BLOCK   = 256;
+constexpr int      RS_WARPS   = RS_BLOCK / 32;
+constexpr int      RS_IPT     = 16;                 // keys per thread
+constexpr int      RS_TILE    = RS_BLOCK * RS_IPT;  // 4096 keys per tile
+constexpr uint32_t LB_AGG     = 1u << 30;           // tile aggregate published
+constexpr uint32_t LB_PRE     = 2u << 30;           // inclusive prefix published
+constexpr uint32_t LB_VAL     = (1u << 30) - 1u;
+constexpr uint32_t SPIN_LIMIT = 1u << 22;           // bounded wait per look-back step
+
+__device__ __forceinline__ uint32_t ld_volatile(const uint32_t* p) { return *(const volatile uint32_t*)p; }
+__device__ __forceinline__ void     st_volatile(uint32_t* p, uint32_t v) { *(volatile uint32_t*)p = v; }
+
+// Exclusive scan of one value per thread over a 256-thread block; also returns the total.
+__device__ __forceinline__ uint32_t block_excl_scan_256(uint32_t v, uint32_t* warp_sums, uint32_t* total)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint32_t x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1)
+    {
+        uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) { x += y; }
+    }
+    if (lane == 31) { warp_sums[warp] = x; }
+    __syncthreads();
+    if (warp == 0)
+    {
+        uint32_t w = lane < RS_WARPS ? warp_sums[lane] : 0u;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1)
+        {
+            uint32_t y = __shfl_up_sync(0xffffffffu, w, o);
+            if (lane >= o) { w += y; }
+        }
+        if (lane < RS_WARPS) { warp_sums[lane] = w; }
+    }
+    __syncthreads();
+    uint32_t base = warp > 0 ? warp_sums[warp - 1] : 0u;
+    if (total) { *total = warp_sums[RS_WARPS - 1]; }
+    uint32_t r = base + x - v;
+    __syncthreads();
+    return r;
+}
+
+template <typename K>
+__global__ void __launch_bounds__(RS_BLOCK)
+k_onesweep(const K* __restrict__ kin, const uint32_t* __restrict__ vin, int vals_identity, K* __restrict__ kout,
+           uint32_t* __restrict__ vout, uint32_t n, int shift, const uint32_t* __restrict__ hist,
+           uint32_t* __restrict__ tile_counter, uint32_t* __restrict__ lookback, uint32_t* __restrict__ status)
+{
+    extern __shared__ __align__(16) unsigned char smem[];
+    K*        sk     = reinterpret_cast<K*>(smem);
+    uint32_t* sv     = reinterpret_cast<uint32_t*>(sk + RS_TILE);
+    uint32_t* whist  = sv + RS_TILE;            // [warp][digit]
+    uint32_t* tstart = whist + RS_WARPS * 256;  // tile-local digit start
+    uint32_t* gbase  = tstart + 256;            // global position of digit d minus tstart[d]
+    __shared__ uint32_t s_tile;
+    __shared__ uint32_t s_warp_sums[RS_WARPS];
+
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (threadIdx.x == 0) { s_tile = atomicAdd(tile_counter, 1u); }
+    for (int i = threadIdx.x; i < RS_WARPS * 256; i += RS_BLOCK) { whist[i] = 0u; }
+    __syncthreads();
+    const uint32_t tile = s_tile;
+    const uint32_t tile_base = tile * (uint32_t)RS_TILE;
+    const uint32_t tile_n = min((uint32_t)RS_TILE, n - tile_base);
+
+    // load: warp w owns the contiguous run [w*32*IPT, (w+1)*32*IPT) of the tile, item j of
+    // lane l is element w*32*IPT + j*32 + l, so (warp, j, lane) order is input order.
+    K        key[RS_IPT];
+    uint32_t val[RS_IPT];
+    uint32_t dig[RS_IPT];
+    uint32_t off[RS_IPT];
+#pragma unroll
+    for (int j = 0; j < RS_IPT; j++)
+    {
+        const uint32_t li = (uint32_t)warp * (32u * RS_IPT) + (uint32_t)j * 32u + (uint32_t)lane;
+        if (li < tile_n)
+        {
+            key[j] = kin[tile_base + li];
+            val[j] = vals_identity ? tile_base + li : vin[tile_base + li];
+            dig[j] = (uint32_t)(key[j] >> shift) & 255u;
+        }
+        else
+        {
+            key[j] = 0; val[j] = 0; dig[j] = 0xffffffffu;
+        }
+    }
+    // stable rank inside the warp: peers with the same digit, counted in lane order
+    const uint32_t lt = (1u << lane) - 1u;
+    uint32_t* wh = whist + warp * 256;
+#pragma unroll
+    for (int j = 0; j < RS_IPT; j++)
+    {
+        const uint32_t d = dig[j];
+        const uint32_t peers = __match_any_sync(0xffffffffu, d);
+        const uint32_t before = __popc(peers & lt);
+        const bool valid = d != 0xffffffffu;
+        uint32_t cnt = valid ? wh[d] : 0u;
+        __syncwarp();
+        if (valid && before == 0u) { wh[d] = cnt + __popc(peers); }
+        __syncwarp();
+        off[j] = cnt + before;
+    }
+    __syncthreads();
+
+    // per digit: tile count, and exclusive offsets of each warp
+    const uint32_t d = threadIdx.x;  // RS_BLOCK == 256 digits
+    uint32_t run = 0u;
+#pragma unroll
+    for (int w = 0; w < RS_WARPS; w++)
+    {
+        uint32_t c = whist[w * 256 + d];
+        whist[w * 256 + d] = run;
+        run += c;
+    }
+    const uint32_t my = run;
+    // publish this tile's count at once so later tiles can proceed
+    st_volatile(&lookback[tile * 256u + d], (tile == 0 ? LB_PRE : LB_AGG) | (my & LB_VAL));
+
+    // decoupled look-back over earlier tiles
+    uint32_t excl = 0u;
+    if (tile > 0)
+    {
+        int p = (int)tile - 1;
+        uint32_t spins = 0u;
+        while (p >= 0)
+        {
+            const uint32_t s = ld_volatile(&lookback[(uint32_t)p * 256u + d]);
+            if ((s & ~LB_VAL) == 0u)
+            {
+                if (++spins > SPIN_LIMIT) { atomicOr(status, ST_TIMEOUT); break; }
+                continue;
+            }
+            excl += s & LB_VAL;
+            if (s & LB_PRE) { break; }
+            --p;
+        }
+        st_volatile(&lookback[tile * 256u + d], LB_PRE | ((excl + my) & LB_VAL));
+    }
+    const uint32_t hd = hist[d];
+    const uint32_t ts = block_excl_scan_256(my, s_warp_sums, nullptr);
+    const uint32_t hs = block_excl_scan_256(hd, s_warp_sums, nullptr);
+    tstart[d] = ts;
+    gbase[d] = hs + excl - ts;
+    __syncthreads();
+
+    // scatter into shared memory in digit order, then write out with contiguous runs
+#pragma unroll
+    for (int j = 0; j < RS_IPT; j++)
+    {
+        if (dig[j] != 0xffffffffu)
+        {
+            const uint32_t pos = tstart[dig[j]] + whist[warp * 256 + dig[j]] + off[j];
+            sk[pos] = key[j];
+            sv[pos] = val[j];
+        }
+    }
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < tile_n; i += RS_BLOCK)
+    {
+        const K k = sk[i];
+        const uint32_t g = gbase[(uint32_t)(k >> shift) & 255u] + i;
+        if (g >= n) { atomicOr(status, ST_CAPACITY); continue; }
+        kout[g] = k;
+        vout[g] = sv[i];
+    }
+}
+
+template <typename K>
+constexpr size_t onesweep_smem()
+{
+    return (size_t)RS_TILE * sizeof(K) + (size_t)RS_TILE * 4 + (size_t)RS_WARPS * 256 * 4 + 2 * 256 * 4;
+}
+
+} // namespace
+
+template <typename K>
+int radix_sort_pairs(K* keys, uint32_t* vals, bool vals_identity, uint32_t n, int key_bits, const uint32_t* hist,
+                     SortScratch& s, uint32_t* status, cudaStream_t st, K** keys_out, uint32_t** vals_out)
+{
+    *keys_out = keys;
+    *vals_out = vals;
+    if (n == 0) { return RT_OK; }
+    if (n > LB_VAL) { return fail(RT_E_CAPACITY, "radix sort: more than 2^30 keys"); }
+    const int passes = sort_passes(key_bits);
+    const uint32_t tiles = (n + RS_TILE - 1) / RS_TILE;
+    if (s.keys_alt.ensure((size_t)n * sizeof(K)) || s.vals_alt.ensure((size_t)n * 4) ||
+        s.lookback.ensure((size_t)passes * tiles * 256 * 4) || s.tile_counters.ensure(64 * 4))
+    {
+        return RT_E_CUDA;
+    }
+    RT_CUDA(cudaMemsetAsync(s.lookback.p, 0, (size_t)passes * tiles * 256 * 4, st));
+    RT_CUDA(cudaMemsetAsync(s.tile_counters.p, 0, 64 * 4, st));
+    static bool attr_set[2] = { false, false };
+    const size_t smem = onesweep_smem<K>();
+    if (!attr_set[sizeof(K) == 8])
+    {
+        RT_CUDA(cudaFuncSetAttribute(k_onesweep<K>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        attr_set[sizeof(K) == 8] = true;
+    }
+    K* kin = keys;
+    K* kalt = s.keys_alt.as<K>();
+    uint32_t* vin = vals;
+    uint32_t* valt = s.vals_alt.as<uint32_t>();
+    for (int p = 0; p < passes; p++)
+    {
+        k_onesweep<K><<<tiles, RS_BLOCK, smem, st>>>(kin, vin, (vals_identity && p == 0) ? 1 : 0, kalt, valt, n, 8 * p,
+                                                    hist + 256 * p, s.tile_counters.as<uint32_t>() + p,
+                                                    s.lookback.as<uint32_t>() + (size_t)p * tiles * 256, status);
+        count_launch();
+        if (int e = check_launch("onesweep")) { return e; }
+        K* tk = kin; kin = kalt; kalt = tk;
+        uint32_t* tv = vin; vin = valt; valt = tv;
+    }
+    *keys_out = kin;
+    *vals_out = vin;
+    return RT_OK;
+}
+
+template int radix_sort_pairs<uint64_t>(uint64_t*, uint32_t*, bool, uint32_t, int, const uint32_t*, SortScratch&,
+                                        uint32_t*, cudaStream_t, uint64_t**, uint32_t**);
+template int radix_sort_pairs<uint32_t>(uint32_t*, uint32_t*, bool, uint32_t, int, const uint32_t*, SortScratch&,
+                                        uint32_t*, cudaStream_t, uint32_t**, uint32_t**);
+
+} // namespace rtb

@@ -1,0 +1,145 @@
+// rt_internal.h -- internal declarations shared by the librt_b200 translation units.
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../../include/rt_b200.h"
+
+namespace rtb
+{
+
+// ---- errors ---------------------------------------------------------------------------
+void set_error(const std::string& msg);
+int  fail(int code, const std::string& msg);
+// Wraps a CUDA call: on failure records the error text and returns RT_E_CUDA from the caller.
+#define RT_CUDA(call)                                                                        \
+    do {                                                                                     \
+        cudaError_t e_ = (call);                                                             \
+        if (e_ != cudaSuccess)                                                               \
+        {                                                                                    \
+            return ::rtb::fail(RT_E_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+        }                                                                                    \
+    } while (0)
+
+// Counts this library's kernel launches (rt_kernel_launches()).
+void count_launch(uint64_t n = 1);
+// Checks the last launch; returns RT_OK or RT_E_CUDA.
+int  check_launch(const char* what);
+
+// Device status word bits, written by kernels instead of trapping.
+enum : uint32_t
+{
+    ST_INDEX    = 1u << 0,  // triangle vertex index out of range
+    ST_TIMEOUT  = 1u << 1,  // a bounded spin-wait gave up
+    ST_CAPACITY = 1u << 2,  // an internal capacity was exceeded
+    ST_STACK    = 1u << 3,  // traversal stack overflow
+};
+
+// ---- device memory ---------------------------------------------------------------------
+// Grows on demand and is reused between builds (cudaMalloc only when a larger size is needed).
+struct DevBuf
+{
+    void*  p     = nullptr;
+    size_t bytes = 0;
+    int    ensure(size_t n);
+    void   release();
+    template <typename T> T* as() const { return static_cast<T*>(p); }
+};
+
+// Per-device default stream and the current device's properties.
+cudaStream_t default_stream();
+int          device_sm_count();
+
+// ---- radix sort (radix_sort.cu) ---------------------------------------------------------
+// Stable LSD onesweep sort of `n` keys with uint32 values by their low `key_bits` bits.
+// Histograms of all digit passes must already be in `hist` (256 counters per pass, built
+// by the producer of the keys). keys/vals are ping-ponged: the sorted result ends in the
+// buffer returned through *keys_out / *vals_out.
+struct SortScratch
+{
+    DevBuf keys_alt, vals_alt, lookback, tile_counters;
+};
+template <typename K>
+int radix_sort_pairs(K* keys, uint32_t* vals, bool vals_identity, uint32_t n, int key_bits,
+                     const uint32_t* hist, SortScratch& s, uint32_t* status, cudaStream_t st,
+                     K** keys_out, uint32_t** vals_out);
+// Number of 8-bit digit passes for a key width.
+inline int sort_passes(int key_bits) { return (key_bits + 7) / 8; }
+
+// Device-wide exclusive scan of uint32 (scan.cu is in build.cu); returns total through *d_total.
+struct ScanScratch { DevBuf partials; };
+int exclusive_scan_u32(const uint32_t* in, uint32_t* out, uint32_t n, uint32_t* d_total, ScanScratch& s,
+                       cudaStream_t st);
+
+} // namespace rtb
+
+// ---- the BVH handle ----------------------------------------------------------------------
+
+// Traversal node (64 bytes): the boxes of both children next to their references, so one
+// node fetch (four 128-bit loads) tests both children. cnt = 0x80000000 | triangle count for a
+// leaf child (ref = first triangle), 0 for an inner child (ref = node index).
+struct rt_gnode
+{
+    float4 a;  // l.min.x l.min.y l.min.z l.max.x
+    float4 b;  // l.max.y l.max.z r.min.x r.min.y
+    float4 c;  // r.min.z r.max.x r.max.y r.max.z
+    uint4  d;  // l.ref   r.ref   l.cnt   r.cnt
+};
+
+struct BuildScratch
+{
+    rtb::DevBuf tri_lo, tri_hi, tri_cz, keys, vals, hist, scene, status;
+    rtb::SortScratch sort;
+    rtb::ScanScratch scan;
+    rtb::DevBuf knode;         // Karras inner nodes
+    rtb::DevBuf parent;        // parent of every Karras node (2N-1)
+    rtb::DevBuf kbox;          // boxes of kept Karras nodes (2N-1) x 6 floats
+    rtb::DevBuf visit;         // refit arrival counters
+    rtb::DevBuf rank;          // left-chain rank of kept Karras nodes
+    rtb::DevBuf bnd;           // boundary node id per start key (or ~0)
+    rtb::DevBuf wnode, wtri;   // per start key weights (nodes, triangles)
+    rtb::DevBuf snode, stri;   // their exclusive scans
+    rtb::DevBuf counters;      // small device counters
+    rtb::DevBuf sah_roots;     // SAH subtree roots
+    // SAH builder state
+    rtb::DevBuf sah_refs_a, sah_refs_b, sah_tmp, sah_pos, sah_lvl_a, sah_lvl_b, sah_dec, sah_out, sah_leaf_refs,
+        sah_scan_in, sah_scan_out, sah_node_ids, sah_roots_lvl;
+    rtb::DevBuf in_verts, in_tris;  // staging for host geometry
+};
+
+struct rt_bvh
+{
+    int          device = 0;
+    rtb::DevBuf  nodes, tris, verts, prim, gnodes, tripos;
+    uint32_t     n_nodes = 0, n_tris = 0, n_verts = 0;
+    bool         has_prim = false;
+    float        root_box[6];
+    uint32_t     root_ref = 0, root_cnt = 0; // traversal entry (same encoding as rt_gnode.d)
+    uint32_t     stats[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    BuildScratch s;
+    rtb::DevBuf  trace_status, trace_rays, trace_hits;
+    rtb::DevBuf  wf_rays[2], wf_state[2], wf_hits, wf_acc, wf_ctr;  // wavefront path tracer
+};
+
+namespace rtb
+{
+// build.cu
+int build_bvh(rt_bvh* b, const rt_vertex* d_verts, uint32_t n_verts, const rt_triangle* d_tris, uint32_t n_tris,
+              const rt_build_cfg& cfg, cudaStream_t st);
+// traverse.cu: (re)creates the traversal layout from the .bvh-layout arrays on the device
+int make_traversal_layout(rt_bvh* b, cudaStream_t st);
+int trace(const rt_bvh* b, const rt_ray* d_rays, rt_hit* d_hits, uint64_t n, uint32_t flags, cudaStream_t st,
+          uint32_t* d_status);
+// Launches the persistent trace kernel; n_dev (optional) holds the ray count on the device.
+// d_counter must be zero on entry.
+int trace_launch(const rt_bvh* b, const void* d_rays, void* d_hits, uint64_t n, const uint32_t* n_dev, uint32_t flags,
+                 cudaStream_t st, uint32_t* d_status, unsigned long long* d_counter);
+// render.cu
+int render(const rt_bvh* b, const rt_render_cfg& cfg, const rt_material* mats, uint32_t n_mats, const uint32_t* mat_of_tri,
+           int mode, float* rgb, float* rgb2, cudaStream_t st);
+} // namespace rtb

@@ -1,0 +1,865 @@
+// sah.cu -- the reference's binned SAH with spatial splits (trySAHSplit,
+// src/bvh/bvh_sah.cpp:24-460) for every subtree the Morton-split build hands over, processed
+// level by level over all subtrees at once, one thread block per node.
+//
+// The reference processes its node queue breadth-first (src/bvh/bvh_bfs.cpp:72-134) and lets
+// spatial splits draw on one global budget of triangle references in that order
+// (bvh_sah.cpp:390-394). Levels here are the reference's BFS levels; inside a level the nodes
+// are kept in the reference's queue order (subtree roots by key position, then children in
+// parent order), so the budget is granted in the same order. When the whole level fits in
+// the remaining budget the grants need no ordering at all.
+//
+// The reference reorders triangle references with std::partition, whose result is Hoare's
+// scheme: the k-th element from the left that fails the predicate is exchanged with the k-th
+// element from the right that satisfies it, for k = 1, 2, ... while the two cursors have not
+// met. cta_partition computes that permutation with block scans instead of a serial loop, so
+// leaf contents come out in the reference's exact order.
+#include "sah.cuh"
+#include "device_math.cuh"
+#include "cta_utils.cuh"
+#include "layout.cuh"
+
+#include <algorithm>
+#include <vector>
+
+namespace rtb
+{
+using namespace rtd;
+
+namespace
+{
+
+constexpr int SBLK = 256;
+enum : int { K_LEAF = 0, K_OBJECT = 1, K_SPATIAL = 2 };
+
+struct LvlNode
+{
+    uint32_t ref_off, count, out, root, root_first, pad;
+    float    box[6];
+};
+
+struct OutNode
+{
+    float    box[6];
+    uint32_t is_leaf, a, b;  // inner: a, b = child out ids; leaf: a = leaf-store offset, b = count
+    uint32_t root;           // index into the sorted roots
+    uint32_t size, refs;     // subtree node count and triangle references
+    uint32_t pre, toff;      // pre-order index and triangle offset inside the subtree
+    uint32_t pad[2];
+};
+
+// Split decision of one node. For pre_spatial decisions the two spatial partitions
+// (axis sp_axis, plane) are applied first, as the reference does before falling back
+// (bvh_sah.cpp:303-330, 335-394).
+struct Dec
+{
+    int      kind, pre_spatial;
+    int      axis, bin;          // object split (kind == K_OBJECT) / spatial axis (K_SPATIAL)
+    float    cmin, scale;
+    float    plane;
+    int      sp_axis;
+    int      nb;
+    uint32_t n, straddle, right;
+    int      fb_kind, oaxis, obin;
+    float    ocmin, oscale;
+};
+
+struct Ctx
+{
+    const rt_vertex*   verts;
+    const rt_triangle* tris;
+    const float4*      lo;
+    const float4*      hi;
+    const float*       cz;
+    uint32_t           max_leaf, bins_min, bins_max;
+    float              c_trav, c_isect, centroid_eps, spatial_eps;
+};
+
+__device__ __forceinline__ float centroid(const Ctx& C, uint32_t t, int axis)
+{
+    return axis == 0 ? C.lo[t].w : (axis == 1 ? C.hi[t].w : C.cz[t]);
+}
+__device__ __forceinline__ box3 tri_box(const Ctx& C, uint32_t t)
+{
+    const float4 a = C.lo[t], c = C.hi[t];
+    box3 b;
+    b.mn[0] = a.x; b.mn[1] = a.y; b.mn[2] = a.z; b.mx[0] = c.x; b.mx[1] = c.y; b.mx[2] = c.z;
+    return b;
+}
+__device__ __forceinline__ float tri_lo(const Ctx& C, uint32_t t, int axis)
+{
+    const float4 a = C.lo[t];
+    return axis == 0 ? a.x : (axis == 1 ? a.y : a.z);
+}
+__device__ __forceinline__ float tri_hi(const Ctx& C, uint32_t t, int axis)
+{
+    const float4 a = C.hi[t];
+    return axis == 0 ? a.x : (axis == 1 ? a.y : a.z);
+}
+__device__ __forceinline__ void tri_verts(const Ctx& C, uint32_t t, f3& a, f3& b, f3& c)
+{
+    const rt_triangle tr = C.tris[t];
+    const rt_vertex* v = C.verts;
+    a = mk3(v[tr.v[0]].x, v[tr.v[0]].y, v[tr.v[0]].z);
+    b = mk3(v[tr.v[1]].x, v[tr.v[1]].y, v[tr.v[1]].z);
+    c = mk3(v[tr.v[2]].x, v[tr.v[2]].y, v[tr.v[2]].z);
+}
+
+// Object-split bin of a centroid (bvh_sah.cpp:85, :260); in [0, nb) for centroids inside
+// [cmin, cmax], which is the only case the reference meets.
+__device__ __forceinline__ int obj_bin(float c, float cmin, float scale, int nb)
+{
+    const int b = std_mini(x86_f2i((c - cmin) * scale), nb - 1);
+    return b < 0 ? 0 : b;
+}
+
+// Shared box accumulator in the order-preserving uint encoding.
+struct SBox { uint32_t m[3], M[3]; };
+__device__ __forceinline__ void sbox_clear(SBox& s) { for (int k = 0; k < 3; k++) { s.m[k] = 0xffffffffu; s.M[k] = 0u; } }
+__device__ __forceinline__ void sbox_add(SBox& s, const box3& b)
+{
+    for (int k = 0; k < 3; k++) { atomicMin(&s.m[k], f2ord(b.mn[k])); atomicMax(&s.M[k], f2ord(b.mx[k])); }
+}
+__device__ __forceinline__ box3 sbox_get(const SBox& s)
+{
+    box3 b;
+    for (int k = 0; k < 3; k++) { b.mn[k] = ord2f(s.m[k]); b.mx[k] = ord2f(s.M[k]); }
+    return b;
+}
+// Reads the union of the contributions of a whole block; the empty box when none.
+__device__ __forceinline__ box3 sbox_result(const SBox& s)
+{
+    box3 b = box_empty();
+    if (s.m[0] != 0xffffffffu) { b = sbox_get(s); }
+    return b;
+}
+
+// Hoare-scheme partition of in[0, n) by pred into out[0, n) (in == out allowed). Returns the
+// number of elements satisfying pred. flags/pos: n scratch entries each.
+template <class Pred>
+__device__ uint32_t cta_partition(const uint32_t* in, uint32_t* out, uint32_t n, Pred pred, uint8_t* flags,
+                                  uint32_t* pos, uint32_t* sh)
+{
+    const int tid = threadIdx.x;
+    uint32_t c = 0;
+    for (uint32_t i = tid; i < n; i += SBLK)
+    {
+        const uint8_t f = pred(in[i]) ? 1 : 0;
+        flags[i] = f;
+        c += f;
+    }
+    const uint32_t m = block_sum<SBLK>(c, sh);
+    // satisfying elements right of the split point, in ascending order
+    uint32_t run = 0;
+    for (uint32_t base = m; base < n; base += SBLK)
+    {
+        const uint32_t i = base + tid;
+        const uint32_t f = (i < n) ? flags[i] : 0u;
+        uint32_t tot;
+        const uint32_t e = block_excl_scan<SBLK>(f, sh, &tot);
+        if (f) { pos[run + e] = i; }
+        run += tot;
+    }
+    __syncthreads();
+    const uint32_t tr = run;  // equals the failing elements left of the split point
+    // exchange the k-th failing element from the left with the k-th satisfying one from the right
+    uint32_t k0 = 0;
+    for (uint32_t base = 0; base < m; base += SBLK)
+    {
+        const uint32_t i = base + tid;
+        const uint32_t f = (i < m) ? (flags[i] ? 0u : 1u) : 0u;
+        uint32_t tot;
+        const uint32_t e = block_excl_scan<SBLK>(f, sh, &tot);
+        if (i < m)
+        {
+            if (f)
+            {
+                const uint32_t q = pos[tr - 1u - (k0 + e)];
+                const uint32_t a = in[i], b = in[q];
+                out[i] = b;
+                out[q] = a;
+            }
+            else if (in != out) { out[i] = in[i]; }
+        }
+        k0 += tot;
+    }
+    if (in != out)
+    {
+        for (uint32_t i = m + tid; i < n; i += SBLK)
+        {
+            if (!flags[i]) { out[i] = in[i]; }
+        }
+    }
+    __syncthreads();
+    return m;
+}
+
+// One block per node: evaluates every object and spatial candidate in the reference's order
+// and writes the decision with the side counts of its partitions.
+__global__ void __launch_bounds__(SBLK)
+k_sah_eval(const LvlNode* __restrict__ lv, const uint32_t* __restrict__ refs, Ctx C, Dec* __restrict__ dec)
+{
+    __shared__ uint32_t cnt[SAH_MAX_BINS], cin[SAH_MAX_BINS], cout[SAH_MAX_BINS];
+    __shared__ SBox bins[SAH_MAX_BINS];
+    __shared__ uint32_t s_red[SBLK / 32 + 1];
+    __shared__ uint32_t s_cm, s_cM;
+    __shared__ float best_cost, best_cmin, best_scale, best_node_min, best_sscale;
+    __shared__ int best_axis, best_bin, is_spatial;
+    __shared__ int o_axis, o_bin;
+    __shared__ float o_cmin, o_scale;
+
+    const LvlNode nd = lv[blockIdx.x];
+    const uint32_t n = nd.count;
+    const uint32_t* R = refs + nd.ref_off;
+    const int tid = threadIdx.x;
+    Dec d;
+    memset(&d, 0, sizeof(d));
+    d.n = n;
+    if (n <= C.max_leaf)
+    {
+        if (tid == 0) { d.kind = K_LEAF; dec[blockIdx.x] = d; }
+        return;
+    }
+    const int nb = std_clampi((int)n / 4, (int)C.bins_min, (int)C.bins_max);
+    box3 nbox;
+    for (int k = 0; k < 3; k++) { nbox.mn[k] = nd.box[k]; nbox.mx[k] = nd.box[3 + k]; }
+    const float parent_inv_area = 1.0f / box_half_area(nbox);
+    if (tid == 0)
+    {
+        best_cost = C.c_isect * (float)n;  // leaf cost, bvh_sah.cpp:32
+        best_axis = -1; best_bin = -1; best_cmin = 0.f; best_scale = 0.f; is_spatial = 0;
+        best_node_min = 0.f; best_sscale = 0.f;
+    }
+
+    // phase 1: centroid-binned object split (bvh_sah.cpp:52-126)
+    for (int axis = 0; axis < 3; axis++)
+    {
+        if (tid == 0) { s_cm = 0xffffffffu; s_cM = 0u; }
+        __syncthreads();
+        uint32_t m = 0xffffffffu, M = 0u;
+        for (uint32_t i = tid; i < n; i += SBLK)
+        {
+            const uint32_t o = f2ord(centroid(C, R[i], axis));
+            m = min(m, o); M = max(M, o);
+        }
+        atomicMin(&s_cm, m); atomicMax(&s_cM, M);
+        __syncthreads();
+        // std::min / std::max folds starting from +FLT_MAX / -FLT_MAX (bvh_sah.cpp:54-61)
+        const float cmin = std_min(3.402823466e38f, ord2f(s_cm));
+        const float cmax = std_max(-3.402823466e38f, ord2f(s_cM));
+        if (cmax - cmin < C.centroid_eps) { continue; }
+        const float scale = (float)nb / (cmax - cmin);
+        if (tid < nb) { cnt[tid] = 0u; sbox_clear(bins[tid]); }
+        __syncthreads();
+        for (uint32_t i = tid; i < n; i += SBLK)
+        {
+            const uint32_t t = R[i];
+            const int b = obj_bin(centroid(C, t, axis), cmin, scale, nb);
+            atomicAdd(&cnt[b], 1u);
+            sbox_add(bins[b], tri_box(C, t));
+        }
+        __syncthreads();
+        if (tid == 0)
+        {
+            box3 lbox[SAH_MAX_BINS];
+            uint32_t lcnt[SAH_MAX_BINS];
+            box3 la = box_empty();
+            uint32_t lc = 0;
+            for (int b = 0; b < nb - 1; b++)
+            {
+                if (cnt[b]) { box_box(la, sbox_get(bins[b])); }
+                lc += cnt[b];
+                lbox[b] = la; lcnt[b] = lc;
+            }
+            box3 ra = box_empty();
+            uint32_t rc = 0;
+            for (int b = nb - 1; b >= 1; b--)
+            {
+                if (cnt[b]) { box_box(ra, sbox_get(bins[b])); }
+                rc += cnt[b];
+                const uint32_t lc2 = lcnt[b - 1];
+                if (lc2 == 0 || rc == 0) { continue; }
+                const float cost = C.c_trav + C.c_isect *
+                    (box_half_area(lbox[b - 1]) * (float)lc2 + box_half_area(ra) * (float)rc) * parent_inv_area;
+                if (cost < best_cost)
+                {
+                    best_cost = cost; best_axis = axis; best_bin = b; best_cmin = cmin; best_scale = scale;
+                }
+            }
+        }
+        __syncthreads();
+    }
+    if (tid == 0) { o_axis = best_axis; o_bin = best_bin; o_cmin = best_cmin; o_scale = best_scale; }
+    __syncthreads();
+
+    // phase 2: spatial bins over the node box, triangles clipped per bin (bvh_sah.cpp:135-243)
+    for (int axis = 0; axis < 3; axis++)
+    {
+        const float node_min = nbox.mn[axis], node_max = nbox.mx[axis];
+        if (node_max - node_min < C.spatial_eps) { continue; }
+        const float sscale = (float)nb / (node_max - node_min);
+        if (tid < nb) { cin[tid] = 0u; cout[tid] = 0u; sbox_clear(bins[tid]); }
+        __syncthreads();
+        for (uint32_t i = tid; i < n; i += SBLK)
+        {
+            const uint32_t t = R[i];
+            const int bmin = std_clampi(x86_f2i((tri_lo(C, t, axis) - node_min) * sscale), 0, nb - 1);
+            const int bmax = std_clampi(x86_f2i((tri_hi(C, t, axis) - node_min) * sscale), 0, nb - 1);
+            atomicAdd(&cin[bmin], 1u);
+            atomicAdd(&cout[bmax], 1u);
+            if (bmin <= bmax)
+            {
+                f3 v0, v1, v2;
+                tri_verts(C, t, v0, v1, v2);
+                box3 region = nbox;
+                for (int b = bmin; b <= bmax; b++)
+                {
+                    region.mn[axis] = node_min + (float)b / sscale;
+                    region.mx[axis] = node_min + (float)(b + 1) / sscale;
+                    const box3 cl = clip_triangle(v0, v1, v2, region);
+                    if (box_valid(cl)) { sbox_add(bins[b], cl); }
+                }
+            }
+        }
+        __syncthreads();
+        if (tid == 0)
+        {
+            box3 lbox[SAH_MAX_BINS];
+            uint32_t lcnt[SAH_MAX_BINS];
+            box3 la = box_empty();
+            uint32_t lc = 0;
+            for (int b = 0; b < nb - 1; b++)
+            {
+                box_box(la, sbox_result(bins[b]));
+                lc += cin[b];
+                lbox[b] = la; lcnt[b] = lc;
+            }
+            box3 ra = box_empty();
+            uint32_t rc = 0;
+            for (int b = nb - 1; b >= 1; b--)
+            {
+                box_box(ra, sbox_result(bins[b]));
+                rc += cout[b];
+                const uint32_t lc2 = lcnt[b - 1];
+                if (lc2 == 0 || rc == 0) { continue; }
+                const float cost = C.c_trav + C.c_isect *
+                    (box_half_area(lbox[b - 1]) * (float)lc2 + box_half_area(ra) * (float)rc) * parent_inv_area;
+                if (cost < best_cost)
+                {
+                    best_cost = cost; best_axis = axis; best_bin = b; is_spatial = 1;
+                    best_node_min = node_min; best_sscale = sscale;
+                }
+            }
+        }
+        __syncthreads();
+    }
+
+    // decision and partition side counts (bvh_sah.cpp:249-394)
+    d.nb = nb;
+    d.oaxis = o_axis; d.obin = o_bin; d.ocmin = o_cmin; d.oscale = o_scale;
+    if (best_axis == -1)
+    {
+        d.kind = K_LEAF;
+    }
+    else if (!is_spatial)
+    {
+        uint32_t l = 0;
+        for (uint32_t i = tid; i < n; i += SBLK)
+        {
+            l += obj_bin(centroid(C, R[i], best_axis), best_cmin, best_scale, nb) < best_bin ? 1u : 0u;
+        }
+        l = block_sum<SBLK>(l, s_red);
+        d.kind = (l == 0 || l == n) ? K_LEAF : K_OBJECT;
+        d.axis = best_axis; d.bin = best_bin; d.cmin = best_cmin; d.scale = best_scale;
+    }
+    else
+    {
+        const float plane = best_node_min + (float)best_bin / best_sscale;
+        const int axis = best_axis;
+        const int oa = o_axis, ob = o_bin;
+        const float oc = o_cmin, os = o_scale;
+        uint32_t lo_ = 0, st_ = 0, ol = 0;
+        for (uint32_t i = tid; i < n; i += SBLK)
+        {
+            const uint32_t t = R[i];
+            if (tri_hi(C, t, axis) <= plane) { lo_++; }
+            else if (tri_lo(C, t, axis) < plane) { st_++; }
+            if (oa != -1) { ol += obj_bin(centroid(C, t, oa), oc, os, nb) < ob ? 1u : 0u; }
+        }
+        lo_ = block_sum<SBLK>(lo_, s_red);
+        st_ = block_sum<SBLK>(st_, s_red);
+        ol = block_sum<SBLK>(ol, s_red);
+        const uint32_t ri = n - lo_ - st_;
+        const int fb = (oa == -1 || ol == 0 || ol == n) ? K_LEAF : K_OBJECT;
+        d.sp_axis = axis; d.plane = plane; d.straddle = st_; d.right = ri; d.fb_kind = fb;
+        if ((lo_ + st_ == 0) || (st_ + ri == 0))
+        {
+            // the saved object split, applied after the spatial partitions (bvh_sah.cpp:331-333)
+            d.kind = fb; d.pre_spatial = 1;
+            d.axis = oa; d.bin = ob; d.cmin = oc; d.scale = os;
+        }
+        else
+        {
+            d.kind = K_SPATIAL;
+            d.axis = axis;
+        }
+    }
+    if (tid == 0) { dec[blockIdx.x] = d; }
+}
+
+// One block: grants the spatial-split reference budget in queue order, then allocates child
+// slots (2 per split node), next-level references and leaf-store space by prefix sums.
+// io: [0] used references, [1] spatial taken, [2] spatial refused, [3] next-level nodes,
+//     [4] next-level references, [5] leaf-store entries of this level, [6] leaves
+__global__ void __launch_bounds__(1024)
+k_sah_resolve(Dec* __restrict__ dec, uint32_t n_lvl, uint32_t cap, uint32_t* __restrict__ io,
+              uint32_t* __restrict__ child_slot, uint32_t* __restrict__ ref_off, uint32_t* __restrict__ leaf_off)
+{
+    __shared__ uint32_t sh[33];
+    __shared__ unsigned long long s_need;
+    __shared__ int s_all;
+    const int tid = threadIdx.x;
+    if (tid == 0) { s_need = 0ull; }
+    __syncthreads();
+    unsigned long long need = 0ull;
+    uint32_t nsp = 0;
+    for (uint32_t i = tid; i < n_lvl; i += 1024)
+    {
+        const Dec d = dec[i];
+        if (d.kind == K_SPATIAL) { need += (unsigned long long)d.right + d.straddle; nsp++; }
+    }
+    atomicAdd(&s_need, need);
+    nsp = block_sum<1024>(nsp, sh);
+    if (tid == 0)
+    {
+        const unsigned long long used = io[0];
+        s_all = (used + s_need <= (unsigned long long)cap) ? 1 : 0;
+        if (s_all) { io[0] = (uint32_t)(used + s_need); io[1] += nsp; }
+    }
+    __syncthreads();
+    if (!s_all && tid == 0)
+    {
+        uint32_t used = io[0];
+        for (uint32_t i = 0; i < n_lvl; i++)
+        {
+            Dec d = dec[i];
+            if (d.kind != K_SPATIAL) { continue; }
+            const uint32_t nd = d.right + d.straddle;
+            if ((unsigned long long)used + nd > (unsigned long long)cap)
+            {
+                d.kind = d.fb_kind; d.pre_spatial = 1;
+                d.axis = d.oaxis; d.bin = d.obin; d.cmin = d.ocmin; d.scale = d.oscale;
+                dec[i] = d;
+                io[2]++;
+            }
+            else
+            {
+                used += nd;
+                io[1]++;
+            }
+        }
+        io[0] = used;
+    }
+    __syncthreads();
+    uint32_t c0 = 0, c1 = 0, c2 = 0, nleaf = 0;
+    for (uint32_t base = 0; base < n_lvl; base += 1024)
+    {
+        const uint32_t i = base + tid;
+        uint32_t a = 0, b = 0, c = 0;
+        if (i < n_lvl)
+        {
+            const Dec d = dec[i];
+            if (d.kind == K_LEAF) { c = d.n; nleaf++; }
+            else { a = 2; b = d.kind == K_OBJECT ? d.n : d.n + d.straddle; }
+        }
+        uint32_t ta, tb, tc;
+        const uint32_t ea = block_excl_scan<1024>(a, sh, &ta);
+        const uint32_t eb = block_excl_scan<1024>(b, sh, &tb);
+        const uint32_t ec = block_excl_scan<1024>(c, sh, &tc);
+        if (i < n_lvl) { child_slot[i] = c0 + ea; ref_off[i] = c1 + eb; leaf_off[i] = c2 + ec; }
+        c0 += ta; c1 += tb; c2 += tc;
+    }
+    nleaf = block_sum<1024>(nleaf, sh);
+    if (tid == 0) { io[3] = c0; io[4] = c1; io[5] = c2; io[6] += nleaf; }
+}
+
+__device__ __forceinline__ void set_node(LvlNode& L, uint32_t off, uint32_t cnt, uint32_t out, uint32_t root,
+                                         uint32_t root_first, const box3& b)
+{
+    L.ref_off = off; L.count = cnt; L.out = out; L.root = root; L.root_first = root_first; L.pad = 0;
+    for (int k = 0; k < 3; k++) { L.box[k] = b.mn[k]; L.box[3 + k] = b.mx[k]; }
+}
+
+__device__ __forceinline__ void set_out_child(OutNode& o, const box3& b, uint32_t root)
+{
+    for (int k = 0; k < 3; k++) { o.box[k] = b.mn[k]; o.box[3 + k] = b.mx[k]; }
+    o.root = root;
+    o.is_leaf = 0; o.a = 0; o.b = 0; o.size = 0; o.refs = 0; o.pre = 0; o.toff = 0;
+}
+
+// One block per node: applies the decision -- the reference's partitions in its order, the
+// children's reference lists and boxes (computeRangeAABB for object splits, the union of
+// the triangles clipped to each side for spatial splits, bvh_sah.cpp:426-444).
+__global__ void __launch_bounds__(SBLK)
+k_sah_split(const LvlNode* __restrict__ lv, const uint32_t* __restrict__ refs, const Dec* __restrict__ dec,
+            const uint32_t* __restrict__ child_slot, const uint32_t* __restrict__ ref_off,
+            const uint32_t* __restrict__ leaf_off, Ctx C, uint32_t* __restrict__ tmp, uint32_t* __restrict__ pos,
+            uint8_t* __restrict__ flags, LvlNode* __restrict__ lv_next, uint32_t* __restrict__ refs_next,
+            OutNode* __restrict__ out, uint32_t out_base, uint32_t leaf_base, uint32_t* __restrict__ leaf_refs)
+{
+    __shared__ uint32_t sh[SBLK / 32 + 1];
+    __shared__ SBox sb[2];
+    const LvlNode nd = lv[blockIdx.x];
+    const Dec d = dec[blockIdx.x];
+    const uint32_t n = nd.count;
+    const uint32_t* R = refs + nd.ref_off;
+    uint32_t* T = tmp + nd.ref_off;
+    uint32_t* P = pos + nd.ref_off;
+    uint8_t* F = flags + nd.ref_off;
+    const int tid = threadIdx.x;
+    const uint32_t* W = R;
+    uint32_t left_end = 0, straddle_end = 0;
+    if (d.pre_spatial || d.kind == K_SPATIAL)
+    {
+        const int ax = d.sp_axis;
+        const float plane = d.plane;
+        left_end = cta_partition(R, T, n, [&](uint32_t t) { return tri_hi(C, t, ax) <= plane; }, F, P, sh);
+        straddle_end = left_end + cta_partition(T + left_end, T + left_end, n - left_end,
+                                                [&](uint32_t t) { return tri_lo(C, t, ax) < plane; }, F + left_end,
+                                                P + left_end, sh);
+        W = T;
+    }
+    OutNode* o = &out[nd.out];
+    if (d.kind == K_LEAF)
+    {
+        const uint32_t lo = leaf_base + leaf_off[blockIdx.x];
+        for (uint32_t i = tid; i < n; i += SBLK) { leaf_refs[lo + i] = W[i]; }
+        if (tid == 0) { o->is_leaf = 1; o->a = lo; o->b = n; }
+        return;
+    }
+    const uint32_t slot = child_slot[blockIdx.x];
+    const uint32_t roff = ref_off[blockIdx.x];
+    const uint32_t lid = out_base + slot, rid = lid + 1;
+    uint32_t* Q = refs_next + roff;
+    if (tid < 2) { sbox_clear(sb[tid]); }
+    __syncthreads();
+    uint32_t lsz, rsz;
+    if (d.kind == K_OBJECT)
+    {
+        const int ax = d.axis, bin = d.bin, nb = d.nb;
+        const float cmin = d.cmin, scale = d.scale;
+        const uint32_t m = cta_partition(W, Q, n, [&](uint32_t t) { return obj_bin(centroid(C, t, ax), cmin, scale, nb) < bin; },
+                                         F, P, sh);
+        lsz = m; rsz = n - m;
+        for (uint32_t i = tid; i < n; i += SBLK) { sbox_add(sb[i < m ? 0 : 1], tri_box(C, Q[i])); }
+    }
+    else
+    {
+        const uint32_t st = straddle_end - left_end, rc = n - straddle_end;
+        lsz = left_end + st;
+        rsz = rc + st;
+        for (uint32_t i = tid; i < lsz; i += SBLK) { Q[i] = W[i]; }
+        for (uint32_t i = tid; i < rc; i += SBLK) { Q[lsz + i] = W[straddle_end + i]; }
+        for (uint32_t i = tid; i < st; i += SBLK) { Q[lsz + rc + i] = W[left_end + i]; }
+        const int ax = d.axis;
+        box3 nbox;
+        for (int k = 0; k < 3; k++) { nbox.mn[k] = nd.box[k]; nbox.mx[k] = nd.box[3 + k]; }
+        box3 lclip = nbox, rclip = nbox;
+        lclip.mx[ax] = d.plane;
+        rclip.mn[ax] = d.plane;
+        __syncthreads();
+        for (uint32_t i = tid; i < lsz + rsz; i += SBLK)
+        {
+            f3 v0, v1, v2;
+            tri_verts(C, Q[i], v0, v1, v2);
+            const box3 cl = clip_triangle(v0, v1, v2, i < lsz ? lclip : rclip);
+            if (box_valid(cl)) { sbox_add(sb[i < lsz ? 0 : 1], cl); }
+        }
+    }
+    __syncthreads();
+    if (tid == 0)
+    {
+        const box3 lb = sbox_result(sb[0]), rb = sbox_result(sb[1]);
+        LvlNode L, Rn;
+        set_node(L, roff, lsz, lid, nd.root, nd.root_first, lb);
+        set_node(Rn, roff + lsz, rsz, rid, nd.root, nd.root_first, rb);
+        lv_next[slot] = L;
+        lv_next[slot + 1] = Rn;
+        set_out_child(out[lid], lb, nd.root);
+        set_out_child(out[rid], rb, nd.root);
+        o->is_leaf = 0; o->a = lid; o->b = rid;
+    }
+}
+
+// Copies the Morton-sorted triangles of new subtree roots into the level's reference list.
+__global__ void __launch_bounds__(SBLK)
+k_sah_root_refs(const SahRoot* __restrict__ roots, const uint32_t* __restrict__ new_off, const uint32_t* __restrict__ perm,
+                uint32_t* __restrict__ refs)
+{
+    const SahRoot r = roots[blockIdx.x];
+    const uint32_t off = new_off[blockIdx.x];
+    for (uint32_t i = threadIdx.x; i < r.count; i += SBLK) { refs[off + i] = perm[r.first + i]; }
+}
+
+// Merges new roots (sorted by key position) into the continuing nodes (sorted by their
+// root's key position): the reference's queue order at this level.
+__global__ void __launch_bounds__(SBLK)
+k_sah_merge(const LvlNode* __restrict__ cont, uint32_t n_cont, const SahRoot* __restrict__ roots, uint32_t r0, uint32_t m,
+            const uint32_t* __restrict__ new_off, uint32_t out_base, LvlNode* __restrict__ merged, OutNode* __restrict__ out,
+            uint32_t* __restrict__ root_out)
+{
+    const uint32_t i = blockIdx.x * SBLK + threadIdx.x;
+    if (i < n_cont)
+    {
+        const LvlNode c = cont[i];
+        uint32_t lo = 0, hi = m;  // new roots with first < c.root_first
+        while (lo < hi)
+        {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (roots[r0 + mid].first < c.root_first) { lo = mid + 1; } else { hi = mid; }
+        }
+        merged[i + lo] = c;
+    }
+    else if (i < n_cont + m)
+    {
+        const uint32_t j = i - n_cont;
+        const SahRoot r = roots[r0 + j];
+        uint32_t lo = 0, hi = n_cont;  // continuing nodes whose root starts before this one
+        while (lo < hi)
+        {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (cont[mid].root_first < r.first) { lo = mid + 1; } else { hi = mid; }
+        }
+        box3 b;
+        for (int k = 0; k < 3; k++) { b.mn[k] = r.box[k]; b.mx[k] = r.box[3 + k]; }
+        LvlNode L;
+        set_node(L, new_off[j], r.count, out_base + j, r0 + j, r.first, b);
+        merged[j + lo] = L;
+        set_out_child(out[out_base + j], b, r0 + j);
+        root_out[r0 + j] = out_base + j;
+    }
+}
+
+__global__ void __launch_bounds__(SBLK) k_sah_up(OutNode* __restrict__ out, uint32_t b, uint32_t e)
+{
+    const uint32_t i = b + blockIdx.x * SBLK + threadIdx.x;
+    if (i >= e) { return; }
+    OutNode& o = out[i];
+    if (o.is_leaf) { o.size = 1; o.refs = o.b; }
+    else
+    {
+        o.size = 1 + out[o.a].size + out[o.b].size;
+        o.refs = out[o.a].refs + out[o.b].refs;
+    }
+}
+
+__global__ void __launch_bounds__(SBLK) k_sah_down(OutNode* __restrict__ out, uint32_t b, uint32_t e)
+{
+    const uint32_t i = b + blockIdx.x * SBLK + threadIdx.x;
+    if (i >= e) { return; }
+    const OutNode o = out[i];
+    if (o.is_leaf) { return; }
+    OutNode& l = out[o.a];
+    OutNode& r = out[o.b];
+    l.pre = o.pre + 1;
+    l.toff = o.toff;
+    r.pre = o.pre + 1 + l.size;
+    r.toff = o.toff + l.refs;
+}
+
+__global__ void __launch_bounds__(SBLK)
+k_sah_root_weights(const SahRoot* __restrict__ roots, uint32_t n_roots, const uint32_t* __restrict__ root_out,
+                   const OutNode* __restrict__ out, uint32_t* __restrict__ wnode, uint32_t* __restrict__ wtri)
+{
+    const uint32_t r = blockIdx.x * SBLK + threadIdx.x;
+    if (r >= n_roots) { return; }
+    const OutNode& o = out[root_out[r]];
+    wnode[roots[r].first] = roots[r].rank + o.size;
+    wtri[roots[r].first] = o.refs;
+}
+
+__global__ void __launch_bounds__(SBLK)
+k_sah_emit(const OutNode* __restrict__ out, uint32_t n_out, const SahRoot* __restrict__ roots,
+           const uint32_t* __restrict__ snode, const uint32_t* __restrict__ stri, const uint32_t* __restrict__ leaf_refs,
+           const rt_triangle* __restrict__ tris, rt_bvh_node* __restrict__ nodes, rt_triangle* __restrict__ otris,
+           uint32_t* __restrict__ prim, uint32_t max_nodes, uint32_t max_tris, uint32_t* __restrict__ status)
+{
+    const uint32_t i = blockIdx.x * SBLK + threadIdx.x;
+    if (i >= n_out) { return; }
+    const OutNode o = out[i];
+    const SahRoot r = roots[o.root];
+    const uint32_t base = snode[r.first] + r.rank;
+    box3 b;
+    for (int k = 0; k < 3; k++) { b.mn[k] = o.box[k]; b.mx[k] = o.box[3 + k]; }
+    if (base + o.pre >= max_nodes) { atomicOr(status, ST_CAPACITY); return; }
+    if (o.is_leaf)
+    {
+        const uint32_t t0 = stri[r.first] + o.toff;
+        if ((uint64_t)t0 + o.b > max_tris) { atomicOr(status, ST_CAPACITY); return; }
+        write_node(nodes, base + o.pre, b, 1, t0, o.b);
+        for (uint32_t k = 0; k < o.b; k++)
+        {
+            const uint32_t t = leaf_refs[o.a + k];
+            otris[t0 + k] = tris[t];
+            prim[t0 + k] = t;
+        }
+    }
+    else
+    {
+        write_node(nodes, base + o.pre, b, 0, base + out[o.a].pre, base + out[o.b].pre);
+    }
+}
+
+inline uint32_t nblk(uint64_t n) { return (uint32_t)((n + SBLK - 1) / SBLK); }
+
+} // namespace
+
+int sah_build(rt_bvh* B, const rt_build_cfg& cfg, const SahInput& in, cudaStream_t st, SahResult* res)
+{
+    BuildScratch& S = B->s;
+    const uint32_t cap = in.cap;
+    const uint32_t nr = in.n_roots;
+
+    // subtree roots in the reference's queue order: by depth, then key position
+    std::vector<SahRoot> roots(nr);
+    RT_CUDA(cudaMemcpyAsync(roots.data(), in.roots, (size_t)nr * sizeof(SahRoot), cudaMemcpyDeviceToHost, st));
+    RT_CUDA(cudaStreamSynchronize(st));
+    std::sort(roots.begin(), roots.end(), [](const SahRoot& a, const SahRoot& b) {
+        return a.depth != b.depth ? a.depth < b.depth : a.first < b.first;
+    });
+
+    if (S.sah_roots_lvl.ensure((size_t)nr * sizeof(SahRoot)) || S.sah_lvl_a.ensure((size_t)cap * sizeof(LvlNode)) ||
+        S.sah_lvl_b.ensure((size_t)cap * sizeof(LvlNode)) || S.sah_node_ids.ensure((size_t)cap * sizeof(LvlNode)) ||
+        S.sah_refs_a.ensure((size_t)cap * 4) || S.sah_refs_b.ensure((size_t)cap * 4) || S.sah_tmp.ensure((size_t)cap * 4) ||
+        S.sah_pos.ensure((size_t)cap * 4) || S.sah_scan_in.ensure((size_t)cap) || S.sah_dec.ensure((size_t)cap * sizeof(Dec)) ||
+        S.sah_out.ensure((size_t)2 * cap * sizeof(OutNode)) || S.sah_leaf_refs.ensure((size_t)cap * 4) ||
+        S.sah_scan_out.ensure((size_t)3 * cap * 4 + (size_t)2 * nr * 4 + 64))
+    {
+        return RT_E_CUDA;
+    }
+    SahRoot* d_roots = S.sah_roots_lvl.as<SahRoot>();
+    RT_CUDA(cudaMemcpyAsync(d_roots, roots.data(), (size_t)nr * sizeof(SahRoot), cudaMemcpyHostToDevice, st));
+    uint32_t* child_slot = S.sah_scan_out.as<uint32_t>();
+    uint32_t* ref_offs = child_slot + cap;
+    uint32_t* leaf_offs = ref_offs + cap;
+    uint32_t* root_out = leaf_offs + cap;
+    uint32_t* new_off = root_out + nr;
+    uint32_t* io = new_off + nr;
+    uint32_t io_h[8] = { in.n, 0, 0, 0, 0, 0, 0, 0 };
+    RT_CUDA(cudaMemcpyAsync(io, io_h, 32, cudaMemcpyHostToDevice, st));
+    // host copy of new-root offsets per level (uploaded as one array, sliced per level)
+    std::vector<uint32_t> new_off_h(nr);
+
+    Ctx C;
+    C.verts = in.verts; C.tris = in.tris; C.lo = in.lo; C.hi = in.hi; C.cz = in.cz;
+    C.max_leaf = cfg.max_leaf; C.bins_min = cfg.bins_min; C.bins_max = cfg.bins_max;
+    C.c_trav = cfg.c_trav; C.c_isect = cfg.c_isect; C.centroid_eps = cfg.centroid_eps; C.spatial_eps = cfg.spatial_eps;
+
+    LvlNode* lv_cur = S.sah_lvl_a.as<LvlNode>();
+    LvlNode* lv_next = S.sah_lvl_b.as<LvlNode>();
+    LvlNode* lv_tmp = S.sah_node_ids.as<LvlNode>();
+    uint32_t* refs_cur = S.sah_refs_a.as<uint32_t>();
+    uint32_t* refs_next = S.sah_refs_b.as<uint32_t>();
+    OutNode* out = S.sah_out.as<OutNode>();
+
+    std::vector<std::pair<uint32_t, uint32_t>> levels;
+    uint32_t out_total = 0, n_cur = 0, r_cur = 0, leaf_total = 0, ri = 0;
+    uint32_t depth = nr ? roots[0].depth : 0;
+    for (int guard = 0; guard < 100000; guard++)
+    {
+        // subtree roots entering at this depth
+        uint32_t m = 0, add = 0;
+        while (ri + m < nr && roots[ri + m].depth == depth)
+        {
+            new_off_h[ri + m] = r_cur + add;
+            add += roots[ri + m].count;
+            m++;
+        }
+        const uint32_t lvl_begin = out_total - n_cur;
+        if (m > 0)
+        {
+            if ((uint64_t)r_cur + add > cap || (uint64_t)n_cur + m > cap || (uint64_t)out_total + m > 2ull * cap)
+            {
+                return fail(RT_E_CAPACITY, "SAH builder: level capacity exceeded");
+            }
+            RT_CUDA(cudaMemcpyAsync(new_off + ri, new_off_h.data() + ri, (size_t)m * 4, cudaMemcpyHostToDevice, st));
+            k_sah_root_refs<<<m, SBLK, 0, st>>>(d_roots + ri, new_off + ri, in.perm, refs_cur);
+            k_sah_merge<<<nblk(n_cur + m), SBLK, 0, st>>>(lv_cur, n_cur, d_roots, ri, m, new_off + ri, out_total, lv_tmp,
+                                                          out, root_out);
+            count_launch(2);
+            std::swap(lv_cur, lv_tmp);
+            out_total += m;
+            n_cur += m;
+            r_cur += add;
+            ri += m;
+        }
+        if (n_cur == 0)
+        {
+            if (ri >= nr) { break; }
+            depth = roots[ri].depth;
+            continue;
+        }
+        levels.emplace_back(lvl_begin, out_total);
+        k_sah_eval<<<n_cur, SBLK, 0, st>>>(lv_cur, refs_cur, C, S.sah_dec.as<Dec>());
+        k_sah_resolve<<<1, 1024, 0, st>>>(S.sah_dec.as<Dec>(), n_cur, cap, io, child_slot, ref_offs, leaf_offs);
+        count_launch(2);
+        if (int e = check_launch("sah eval")) { return e; }
+        RT_CUDA(cudaMemcpyAsync(io_h, io, 32, cudaMemcpyDeviceToHost, st));
+        RT_CUDA(cudaStreamSynchronize(st));
+        const uint32_t n_next = io_h[3], r_next = io_h[4], leaf_lvl = io_h[5];
+        if (n_next > cap || r_next > cap || (uint64_t)out_total + n_next > 2ull * cap || (uint64_t)leaf_total + leaf_lvl > cap)
+        {
+            return fail(RT_E_CAPACITY, "SAH builder: capacity exceeded");
+        }
+        k_sah_split<<<n_cur, SBLK, 0, st>>>(lv_cur, refs_cur, S.sah_dec.as<Dec>(), child_slot, ref_offs, leaf_offs, C,
+                                            S.sah_tmp.as<uint32_t>(), S.sah_pos.as<uint32_t>(), S.sah_scan_in.as<uint8_t>(),
+                                            lv_next, refs_next, out, out_total, leaf_total, S.sah_leaf_refs.as<uint32_t>());
+        count_launch();
+        if (int e = check_launch("sah split")) { return e; }
+        out_total += n_next;
+        leaf_total += leaf_lvl;
+        std::swap(lv_cur, lv_next);
+        std::swap(refs_cur, refs_next);
+        n_cur = n_next;
+        r_cur = r_next;
+        depth++;
+    }
+    // subtree sizes bottom-up, then pre-order slots and triangle offsets top-down
+    for (size_t l = levels.size(); l-- > 0;)
+    {
+        const auto& L = levels[l];
+        if (L.second > L.first) { k_sah_up<<<nblk(L.second - L.first), SBLK, 0, st>>>(out, L.first, L.second); count_launch(); }
+    }
+    for (const auto& L : levels)
+    {
+        if (L.second > L.first) { k_sah_down<<<nblk(L.second - L.first), SBLK, 0, st>>>(out, L.first, L.second); count_launch(); }
+    }
+    k_sah_root_weights<<<nblk(nr), SBLK, 0, st>>>(d_roots, nr, root_out, out, in.wnode, in.wtri);
+    count_launch();
+    if (int e = check_launch("sah finish")) { return e; }
+    RT_CUDA(cudaMemcpyAsync(io_h, io, 32, cudaMemcpyDeviceToHost, st));
+    RT_CUDA(cudaStreamSynchronize(st));
+    res->spatial_taken = io_h[1];
+    res->spatial_refused = io_h[2];
+    res->leaves = io_h[6];
+    res->nodes = out_total;
+    res->levels = (uint32_t)levels.size();
+    res->sorted_roots = d_roots;
+    return RT_OK;
+}
+
+int sah_emit(rt_bvh* B, uint32_t n_roots, const uint32_t* snode, const uint32_t* stri, const rt_triangle* tris,
+             cudaStream_t st, const SahResult& res, uint32_t max_nodes, uint32_t max_tris, uint32_t* status)
+{
+    (void)n_roots;
+    BuildScratch& S = B->s;
+    if (res.nodes == 0) { return RT_OK; }
+    k_sah_emit<<<nblk(res.nodes), SBLK, 0, st>>>(S.sah_out.as<OutNode>(), res.nodes, res.sorted_roots, snode, stri,
+                                                  S.sah_leaf_refs.as<uint32_t>(), tris, B->nodes.as<rt_bvh_node>(),
+                                                  B->tris.as<rt_triangle>(), B->prim.as<uint32_t>(), max_nodes,
+                                                  max_tris, status);
+    count_launch();
+    return check_launch("sah emit");
+}
+
+} // namespace rtb

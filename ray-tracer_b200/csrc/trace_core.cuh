@@ -1,0 +1,193 @@
+// trace_core.cuh -- the traversal loop shared by the trace kernels and the path tracers:
+// bvh::trace (src/bvh/bvh_traverse.cpp:91-178) over the 64-byte two-child node layout.
+#pragma once
+
+#include "device_math.cuh"
+#include "rt_internal.h"
+
+namespace rtb
+{
+using namespace rtd;
+
+constexpr int STACK = 64;  // the reference's fixed stack (bvh_traverse.cpp:98)
+constexpr uint32_t LEAF_BIT = 0x80000000u;
+constexpr uint32_t MAX_POPS = 1u << 24;  // per ray
+
+// rayAABB, bvh_traverse.cpp:22-41, with 1/dir precomputed (the same IEEE quotient).
+__device__ __forceinline__ float ray_box(f3 o, f3 inv, float tmin, float tmax, float mnx, float mny, float mnz,
+                                         float mxx, float mxy, float mxz)
+{
+    const float t0x = (mnx - o.x) * inv.x, t1x = (mxx - o.x) * inv.x;
+    const float t0y = (mny - o.y) * inv.y, t1y = (mxy - o.y) * inv.y;
+    const float t0z = (mnz - o.z) * inv.z, t1z = (mxz - o.z) * inv.z;
+    const float tn = std_max(std_max(std_min(t0x, t1x), std_min(t0y, t1y)), std_max(std_min(t0z, t1z), tmin));
+    const float tf = std_min(std_min(std_max(t0x, t1x), std_max(t0y, t1y)), std_min(std_max(t0z, t1z), tmax));
+    return (tn <= tf) ? tn : bits2f(0x7f800000u);
+}
+
+// rayTriangle, bvh_traverse.cpp:47-87: Moller-Trumbore with back faces (a >= 0) culled.
+__device__ __forceinline__ bool ray_tri(f3 o, f3 d, float tmin, float tmax, f3 v0, f3 v1, f3 v2, float& t, float& u,
+                                        float& v)
+{
+    const f3 e1 = sub3(v1, v0), e2 = sub3(v2, v0);
+    const f3 h = cross3(d, e2);
+    const float a = dot3(e1, h);
+    if (a >= 0) { return false; }
+    const float f = 1.f / a;
+    const f3 s = sub3(o, v0);
+    const float uu = f * dot3(s, h);
+    if (uu < 0.f || uu > 1.f) { return false; }
+    const f3 q = cross3(s, e1);
+    const float vv = f * dot3(d, q);
+    if (vv < 0.f || uu + vv > 1.f) { return false; }
+    const float tt = f * dot3(e2, q);
+    if (tt < tmin || tt > tmax) { return false; }
+    t = tt; u = uu; v = vv;
+    return true;
+}
+
+// Watertight ray/triangle test (Woop, Benthin, Wald, JCGT 2013), both faces, as an option.
+__device__ __forceinline__ bool ray_tri_watertight(f3 o, f3 d, float tmin, float tmax, f3 v0, f3 v1, f3 v2, float& t,
+                                                   float& u, float& v)
+{
+    const float ax = fabsf(d.x), ay = fabsf(d.y), az = fabsf(d.z);
+    int kz = (ax > ay) ? (ax > az ? 0 : 2) : (ay > az ? 1 : 2);
+    int kx = kz == 2 ? 0 : kz + 1;
+    int ky = kx == 2 ? 0 : kx + 1;
+    if (get3(d, kz) < 0.f) { const int tmp = kx; kx = ky; ky = tmp; }
+    const float dz = get3(d, kz);
+    const float Sx = get3(d, kx) / dz, Sy = get3(d, ky) / dz, Sz = 1.f / dz;
+    const f3 A = sub3(v0, o), Bv = sub3(v1, o), Cv = sub3(v2, o);
+    const float Ax = get3(A, kx) - Sx * get3(A, kz), Ay = get3(A, ky) - Sy * get3(A, kz);
+    const float Bx = get3(Bv, kx) - Sx * get3(Bv, kz), By = get3(Bv, ky) - Sy * get3(Bv, kz);
+    const float Cx = get3(Cv, kx) - Sx * get3(Cv, kz), Cy = get3(Cv, ky) - Sy * get3(Cv, kz);
+    float U = Cx * By - Cy * Bx, V = Ax * Cy - Ay * Cx, W = Bx * Ay - By * Ax;
+    if (U == 0.f || V == 0.f || W == 0.f)
+    {
+        U = (float)((double)Cx * By - (double)Cy * Bx);
+        V = (float)((double)Ax * Cy - (double)Ay * Cx);
+        W = (float)((double)Bx * Ay - (double)By * Ax);
+    }
+    if ((U < 0.f || V < 0.f || W < 0.f) && (U > 0.f || V > 0.f || W > 0.f)) { return false; }
+    const float det = U + V + W;
+    if (det == 0.f) { return false; }
+    const float Az = Sz * get3(A, kz), Bz = Sz * get3(Bv, kz), Cz = Sz * get3(Cv, kz);
+    const float T = U * Az + V * Bz + W * Cz;
+    const float rd = 1.f / det;
+    const float tt = T * rd;
+    if (!(tt >= tmin && tt <= tmax)) { return false; }
+    t = tt; u = V * rd; v = W * rd;
+    return true;
+}
+
+struct TraceRoot
+{
+    float    box[6];
+    uint32_t ref, cnt;
+};
+
+struct TraceCtx
+{
+    const rt_gnode*    gn;
+    const float4*      tp;
+    const rt_triangle* tris;
+    const rt_vertex*   verts;
+    TraceRoot          root;
+};
+
+struct THit
+{
+    float    t, u, v;
+    uint32_t tri;
+    bool     hit, overflow;
+};
+
+// Closest hit (MODE bit 0 clear) or first accepted hit (bit 0 set); bit 1 selects the
+// watertight triangle test. Reproduces the reference's visiting order exactly.
+template <int MODE>
+__device__ __forceinline__ THit trace_ray(const TraceCtx& T, rtd::f3 o, rtd::f3 d, float tmin, float tmax)
+{
+    using namespace rtd;
+    uint32_t sref[STACK], scnt[STACK];
+    float stn[STACK];
+    const f3 inv = mk3(1.f / d.x, 1.f / d.y, 1.f / d.z);
+    THit H;
+    H.t = tmax; H.u = 0.f; H.v = 0.f; H.tri = 0; H.hit = false; H.overflow = false;
+    float best = tmax;
+    int top = 0;
+    const float troot = ray_box(o, inv, tmin, best, T.root.box[0], T.root.box[1], T.root.box[2], T.root.box[3],
+                                T.root.box[4], T.root.box[5]);
+    if (troot < best) { sref[0] = T.root.ref; scnt[0] = T.root.cnt; stn[0] = troot; top = 1; }
+    uint32_t pops = 0;
+    while (top > 0)
+    {
+        // A validated BVH is a DAG with children after parents; the cap only bounds the work
+        // a malformed one could cause.
+        if (++pops > MAX_POPS) { H.overflow = true; break; }
+        --top;
+        if (stn[top] >= best) { continue; }
+        const uint32_t ref = sref[top], cnt = scnt[top];
+        if (cnt & LEAF_BIT)
+        {
+            const uint32_t c = cnt & ~LEAF_BIT;
+            bool done = false;
+            for (uint32_t k = 0; k < c; k++)
+            {
+                const uint32_t ti = ref + k;
+                const float4 p0 = __ldg(&T.tp[3 * ti]), p1 = __ldg(&T.tp[3 * ti + 1]), p2 = __ldg(&T.tp[3 * ti + 2]);
+                const f3 v0 = mk3(p0.x, p0.y, p0.z), v1 = mk3(p0.w, p1.x, p1.y), v2 = mk3(p1.z, p1.w, p2.x);
+                float t, u, v;
+                const bool acc = (MODE & 2) ? ray_tri_watertight(o, d, tmin, tmax, v0, v1, v2, t, u, v)
+                                            : ray_tri(o, d, tmin, tmax, v0, v1, v2, t, u, v);
+                if (acc && t < best)
+                {
+                    best = t; H.u = u; H.v = v; H.tri = ti; H.hit = true;
+                    if (MODE & 1) { done = true; break; }
+                }
+            }
+            if (done) { break; }
+        }
+        else
+        {
+            const rt_gnode* g = T.gn + ref;
+            const float4 a = __ldg(&g->a), b = __ldg(&g->b), c = __ldg(&g->c);
+            const uint4 dd = __ldg(&g->d);
+            const float tl = ray_box(o, inv, tmin, best, a.x, a.y, a.z, a.w, b.x, b.y);
+            const float tr = ray_box(o, inv, tmin, best, b.z, b.w, c.x, c.y, c.z, c.w);
+            // push the farther child first so the nearer one pops first; left first on ties
+            uint32_t fr, fc, nr, nc;
+            float ft, nt;
+            if (tl <= tr) { fr = dd.y; fc = dd.w; ft = tr; nr = dd.x; nc = dd.z; nt = tl; }
+            else { fr = dd.x; fc = dd.z; ft = tl; nr = dd.y; nc = dd.w; nt = tr; }
+            if (ft < best)
+            {
+                if (top >= STACK) { H.overflow = true; break; }
+                sref[top] = fr; scnt[top] = fc; stn[top] = ft; top++;
+            }
+            if (nt < best)
+            {
+                if (top >= STACK) { H.overflow = true; break; }
+                sref[top] = nr; scnt[top] = nc; stn[top] = nt; top++;
+            }
+        }
+    }
+    H.t = best;
+    return H;
+}
+
+// Interpolated shading normal of a hit: normalize(w n0 + u n1 + v n2), bvh_traverse.cpp:135-139.
+__device__ __forceinline__ rtd::f3 hit_normal(const TraceCtx& T, uint32_t tri, float u, float v)
+{
+    using namespace rtd;
+    const rt_triangle tr = T.tris[tri];
+    const rt_vertex& a = T.verts[tr.v[0]];
+    const rt_vertex& b = T.verts[tr.v[1]];
+    const rt_vertex& c = T.verts[tr.v[2]];
+    const float w = 1.f - u - v;
+    const f3 nn = add3(add3(muls(mk3(a.nx, a.ny, a.nz), w), muls(mk3(b.nx, b.ny, b.nz), u)), muls(mk3(c.nx, c.ny, c.nz), v));
+    return norm3(nn);
+}
+
+TraceCtx make_trace_ctx(const rt_bvh* B);
+
+} // namespace rtb

@@ -1,0 +1,199 @@
+// traverse.cu -- closest-hit / any-hit ray traversal: bvh::trace (src/bvh/bvh_traverse.cpp:91-246)
+// for batches of rays on the GPU.
+//
+// Layout: the .bvh node array is re-laid as 64-byte two-child nodes (rt_gnode: both children's
+// boxes and references, four 128-bit loads per visited inner node) and a 48-byte triangle
+// position record per baked triangle (three 128-bit loads per triangle test). Node indices are
+// those of the .bvh array, so the traversal visits exactly the reference's nodes.
+//
+// Equivalence with the reference loop: the reference pops a node and re-tests its box against
+// the current best t (bvh_traverse.cpp:104-110); here the stack keeps the entry distance tNear
+// computed when the node was pushed. The slab interval's far end depends on the best t only
+// through min(tFar, bestT), so "rayAABB(node, bestT) >= bestT" holds exactly when
+// tNear >= bestT (also with the NaN slabs of axis-parallel rays: tNear, and whether tFar is NaN,
+// do not depend on bestT). Children are tested and pushed in the reference's order (far child
+// first, the left child first on ties, :143-174) and triangles are tested in leaf order with the
+// strict "t < bestT" update (:112-142), so the first triangle at the minimal distance wins as
+// in the reference and hits carry identical triangle indices (trace_core.cuh).
+//
+// The kernel is persistent: each warp claims 32 rays at a time from a global counter until
+// the batch is exhausted, so long incoherent rays do not leave SMs idle at the tail.
+#include "trace_core.cuh"
+
+namespace rtb
+{
+
+namespace
+{
+
+constexpr int TBLK = 128;
+
+// Also validates the structure before any traversal may run on it: children of node i have
+// larger indices (DFS pre-order, so no cycles) inside the array, leaf ranges inside the
+// triangle array. A violation sets ST_CAPACITY and the handle is refused.
+__global__ void k_make_gnodes(const rt_bvh_node* __restrict__ nodes, uint32_t n_nodes, uint32_t n_tris,
+                              rt_gnode* __restrict__ gn, uint32_t* __restrict__ status)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n_nodes) { return; }
+    const rt_bvh_node nd = nodes[i];
+    if (nd.is_leaf)
+    {
+        if ((uint64_t)nd.a + nd.b > n_tris) { atomicOr(status, ST_CAPACITY); }
+        return;
+    }
+    if (nd.a <= i || nd.b <= i || nd.a >= n_nodes || nd.b >= n_nodes)
+    {
+        atomicOr(status, ST_CAPACITY);
+        gn[i] = rt_gnode{ make_float4(0.f, 0.f, 0.f, 0.f), make_float4(0.f, 0.f, 0.f, 0.f), make_float4(0.f, 0.f, 0.f, 0.f),
+                          make_uint4(0u, 0u, LEAF_BIT, LEAF_BIT) };
+        return;
+    }
+    const rt_bvh_node l = nodes[nd.a], r = nodes[nd.b];
+    rt_gnode g;
+    g.a = make_float4(l.bmin[0], l.bmin[1], l.bmin[2], l.bmax[0]);
+    g.b = make_float4(l.bmax[1], l.bmax[2], r.bmin[0], r.bmin[1]);
+    g.c = make_float4(r.bmin[2], r.bmax[0], r.bmax[1], r.bmax[2]);
+    g.d = make_uint4(l.is_leaf ? l.a : nd.a, r.is_leaf ? r.a : nd.b, l.is_leaf ? (LEAF_BIT | l.b) : 0u,
+                     r.is_leaf ? (LEAF_BIT | r.b) : 0u);
+    gn[i] = g;
+}
+
+__global__ void k_make_tripos(const rt_triangle* __restrict__ tris, uint32_t n, const rt_vertex* __restrict__ v,
+                              float4* __restrict__ tp)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) { return; }
+    const rt_triangle t = tris[i];
+    const rt_vertex a = v[t.v[0]], b = v[t.v[1]], c = v[t.v[2]];
+    tp[3 * i + 0] = make_float4(a.x, a.y, a.z, b.x);
+    tp[3 * i + 1] = make_float4(b.y, b.z, c.x, c.y);
+    tp[3 * i + 2] = make_float4(c.z, 0.f, 0.f, 0.f);
+}
+
+// rt_ray records in, rt_hit records out (two 128-bit accesses each). n_dev, when set, holds
+// the ray count on the device (the wavefront path tracer's queue length).
+template <int MODE>
+__global__ void __launch_bounds__(TBLK)
+k_trace(TraceCtx T, const float4* __restrict__ rays, float4* __restrict__ hits, uint64_t n, const uint32_t* __restrict__ n_dev,
+        unsigned long long* __restrict__ counter, uint32_t* __restrict__ status)
+{
+    const int lane = threadIdx.x & 31;
+    if (n_dev) { n = *n_dev; }
+    for (;;)
+    {
+        unsigned long long base = 0;
+        if (lane == 0) { base = atomicAdd(counter, 32ull); }
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (base >= n) { return; }
+        const uint64_t ri = base + (uint64_t)lane;
+        if (ri >= n) { continue; }
+        const float4 r0 = rays[2 * ri], r1 = rays[2 * ri + 1];
+        const THit H = trace_ray<MODE>(T, mk3(r0.x, r0.y, r0.z), mk3(r1.x, r1.y, r1.z), r0.w, r1.w);
+        float4 h0 = make_float4(0.f, 0.f, 0.f, 0.f), h1 = make_float4(0.f, 0.f, 0.f, 0.f);
+        uint32_t flags = 0;
+        if (H.hit)
+        {
+            const f3 nrm = hit_normal(T, H.tri, H.u, H.v);
+            h0 = make_float4(H.t, H.u, H.v, __uint_as_float(H.tri));
+            h1 = make_float4(nrm.x, nrm.y, nrm.z, 0.f);
+            flags = RT_HIT_FLAG_HIT;
+        }
+        if (H.overflow) { flags |= RT_HIT_FLAG_OVERFLOW; atomicOr(status, ST_STACK); }
+        h1.w = __uint_as_float(flags);
+        hits[2 * ri] = h0;
+        hits[2 * ri + 1] = h1;
+    }
+}
+
+int g_blocks_per_sm = 0;
+
+} // namespace
+
+TraceCtx make_trace_ctx(const rt_bvh* B)
+{
+    TraceCtx T;
+    T.gn = B->gnodes.as<rt_gnode>();
+    T.tp = B->tripos.as<float4>();
+    T.tris = B->tris.as<rt_triangle>();
+    T.verts = B->verts.as<rt_vertex>();
+    for (int k = 0; k < 6; k++) { T.root.box[k] = B->root_box[k]; }
+    T.root.ref = B->root_ref;
+    T.root.cnt = B->root_cnt;
+    return T;
+}
+
+int make_traversal_layout(rt_bvh* B, cudaStream_t st)
+{
+    if (B->n_nodes == 0) { return fail(RT_E_EMPTY, "empty BVH"); }
+    if (B->gnodes.ensure((size_t)B->n_nodes * sizeof(rt_gnode)) ||
+        B->tripos.ensure((size_t)(B->n_tris ? B->n_tris : 1) * 48) || B->trace_status.ensure(64))
+    {
+        return RT_E_CUDA;
+    }
+    uint32_t* vstatus = B->trace_status.as<uint32_t>() + 12;
+    RT_CUDA(cudaMemsetAsync(vstatus, 0, 4, st));
+    k_make_gnodes<<<(B->n_nodes + 255) / 256, 256, 0, st>>>(B->nodes.as<rt_bvh_node>(), B->n_nodes, B->n_tris,
+                                                            B->gnodes.as<rt_gnode>(), vstatus);
+    count_launch();
+    if (B->n_tris)
+    {
+        k_make_tripos<<<(B->n_tris + 255) / 256, 256, 0, st>>>(B->tris.as<rt_triangle>(), B->n_tris, B->verts.as<rt_vertex>(),
+                                                               B->tripos.as<float4>());
+        count_launch();
+    }
+    if (int e = check_launch("traversal layout")) { return e; }
+    rt_bvh_node root;
+    uint32_t vs = 0;
+    RT_CUDA(cudaMemcpyAsync(&root, B->nodes.p, sizeof(root), cudaMemcpyDeviceToHost, st));
+    RT_CUDA(cudaMemcpyAsync(&vs, vstatus, 4, cudaMemcpyDeviceToHost, st));
+    RT_CUDA(cudaStreamSynchronize(st));
+    if (vs) { return fail(RT_E_FORMAT, "BVH structure check failed (child or triangle index out of range)"); }
+    for (int k = 0; k < 3; k++) { B->root_box[k] = root.bmin[k]; B->root_box[3 + k] = root.bmax[k]; }
+    if (root.is_leaf) { B->root_ref = root.a; B->root_cnt = LEAF_BIT | root.b; }
+    else { B->root_ref = 0; B->root_cnt = 0; }
+    return RT_OK;
+}
+
+int trace_launch(const rt_bvh* B, const void* d_rays, void* d_hits, uint64_t n, const uint32_t* n_dev, uint32_t flags,
+                 cudaStream_t st, uint32_t* d_status, unsigned long long* d_counter)
+{
+    if (!g_blocks_per_sm)
+    {
+        RT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&g_blocks_per_sm, k_trace<0>, TBLK, 0));
+        if (g_blocks_per_sm < 1) { g_blocks_per_sm = 1; }
+    }
+    uint64_t grid = (uint64_t)device_sm_count() * (uint64_t)g_blocks_per_sm;
+    if (!n_dev)
+    {
+        const uint64_t want = (n + TBLK - 1) / TBLK;
+        if (grid > want) { grid = want; }
+    }
+    if (grid == 0) { return RT_OK; }
+    const TraceCtx T = make_trace_ctx(B);
+    const float4* r = static_cast<const float4*>(d_rays);
+    float4* h = static_cast<float4*>(d_hits);
+    switch (flags & 3u)
+    {
+    case 0: k_trace<0><<<(uint32_t)grid, TBLK, 0, st>>>(T, r, h, n, n_dev, d_counter, d_status); break;
+    case 1: k_trace<1><<<(uint32_t)grid, TBLK, 0, st>>>(T, r, h, n, n_dev, d_counter, d_status); break;
+    case 2: k_trace<2><<<(uint32_t)grid, TBLK, 0, st>>>(T, r, h, n, n_dev, d_counter, d_status); break;
+    default: k_trace<3><<<(uint32_t)grid, TBLK, 0, st>>>(T, r, h, n, n_dev, d_counter, d_status); break;
+    }
+    count_launch();
+    return check_launch("trace");
+}
+
+int trace(const rt_bvh* B, const rt_ray* d_rays, rt_hit* d_hits, uint64_t n, uint32_t flags, cudaStream_t st,
+          uint32_t* d_status)
+{
+    if (n == 0) { return RT_OK; }
+    if (((uintptr_t)d_rays & 15) || ((uintptr_t)d_hits & 15)) { return fail(RT_E_INVALID, "rays/hits must be 16-byte aligned"); }
+    rt_bvh* Bm = const_cast<rt_bvh*>(B);
+    if (Bm->trace_status.ensure(64)) { return RT_E_CUDA; }
+    unsigned long long* counter = Bm->trace_status.as<unsigned long long>();
+    RT_CUDA(cudaMemsetAsync(counter, 0, 8, st));
+    return trace_launch(B, d_rays, d_hits, n, nullptr, flags, st, d_status, counter);
+}
+
+} // namespace rtb

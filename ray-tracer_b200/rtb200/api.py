@@ -1,0 +1,362 @@
+"""Python host API over librt_b200.so (ctypes; the C ABI of include/rt_b200.h).
+
+It mirrors the reference's bake / load / trace interface (src/bvh/bvh.hpp:45-52,
+src/bvh/bvh_traverse.hpp:8-30) for numpy arrays (host memory) and torch CUDA tensors (device
+memory). Every compute call runs the library's CUDA kernels; there is no CPU fallback: if
+the library or a CUDA device is missing the calls raise.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import re
+
+import numpy as np
+
+PKG_DIR = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+LIB_PATH = os.path.join(PKG_DIR, "lib", "librt_b200.so")
+HEADER = os.path.join(os.path.dirname(PKG_DIR), "include", "rt_b200.h")
+
+RT_HOST, RT_DEVICE = 0, 1
+TRACE_CLOSEST, TRACE_ANY_HIT, TRACE_WATERTIGHT = 0, 1, 2
+RENDER_PLAIN, RENDER_WAVEFRONT = 0, 1
+HIT_FLAG_HIT, HIT_FLAG_OVERFLOW = 1, 2
+STATUS = {0: "RT_OK", 1: "RT_E_INVALID", 2: "RT_E_IO", 3: "RT_E_FORMAT", 4: "RT_E_CAPACITY", 5: "RT_E_STACK",
+          6: "RT_E_CUDA", 7: "RT_E_TIMEOUT", 8: "RT_E_EMPTY", 9: "RT_E_INDEX", 10: "RT_E_NOT_LOADED"}
+
+NODE_DTYPE = np.dtype([("bmin", "<f4", 4), ("bmax", "<f4", 4), ("is_leaf", "u1"), ("pad0", "u1", 3),
+                       ("a", "<u4"), ("b", "<u4"), ("pad1", "<u4")])
+HIT_DTYPE = np.dtype([("t", "<f4"), ("u", "<f4"), ("v", "<f4"), ("tri", "<u4"), ("n", "<f4", 3), ("flags", "<u4")])
+assert NODE_DTYPE.itemsize == 48 and HIT_DTYPE.itemsize == 32
+
+
+class RtError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{STATUS.get(code, code)}: {msg}")
+        self.code = code
+
+
+class BuildCfg(C.Structure):
+    _fields_ = [("lbvh_threshold", C.c_uint32), ("max_leaf", C.c_uint32), ("morton_bits", C.c_uint32),
+                ("bins_min", C.c_uint32), ("bins_max", C.c_uint32), ("c_trav", C.c_float), ("c_isect", C.c_float),
+                ("centroid_eps", C.c_float), ("spatial_eps", C.c_float), ("spatial_mult", C.c_float)]
+
+
+class Material(C.Structure):
+    _fields_ = [("albedo", C.c_float * 3), ("emission", C.c_float * 3), ("kind", C.c_uint32), ("pad", C.c_uint32)]
+
+
+class RenderCfg(C.Structure):
+    _fields_ = [("width", C.c_uint32), ("height", C.c_uint32), ("spp", C.c_uint32), ("max_bounce", C.c_uint32),
+                ("rr_after", C.c_int32), ("env_kind", C.c_uint32), ("env_color", C.c_float * 3),
+                ("cam_pos", C.c_float * 3), ("cam_fwd", C.c_float * 3), ("cam_right", C.c_float * 3),
+                ("cam_up", C.c_float * 3), ("tan_half_fov_y", C.c_float), ("seed", C.c_uint32),
+                ("sample_offset", C.c_uint32)]
+
+
+# Build presets: the reference's defaults and the parameter sets of the benchmark builds.
+PRESETS = {
+    "hybrid":   dict(lbvh_threshold=64, max_leaf=16, morton_bits=21),        # the reference as shipped
+    "lbvh63":   dict(lbvh_threshold=0, max_leaf=16, morton_bits=21),         # pure Morton split, 63-bit codes
+    "lbvh30":   dict(lbvh_threshold=0, max_leaf=16, morton_bits=10),         # pure Morton split, 30-bit codes
+    "lbvh63l4": dict(lbvh_threshold=0, max_leaf=4, morton_bits=21),
+    "sah4":     dict(lbvh_threshold=0xFFFFFFFF, max_leaf=4, morton_bits=21), # binned SAH + spatial splits, leaf 4
+    "sah16":    dict(lbvh_threshold=0xFFFFFFFF, max_leaf=16, morton_bits=21),
+    "sah4ns":   dict(lbvh_threshold=0xFFFFFFFF, max_leaf=4, morton_bits=21, spatial_eps=3.0e38),  # no spatial splits
+}
+
+_lib = None
+
+
+def lib():
+    """Loads librt_b200.so (raises if it was not built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise FileNotFoundError(f"{LIB_PATH} is missing: build it with `make -C ray-tracer_b200`")
+        L = C.CDLL(LIB_PATH)
+        vp, u32, u64, i32 = C.c_void_p, C.c_uint32, C.c_uint64, C.c_int
+        L.rt_build_cfg_default.argtypes = [vp]
+        L.rt_build.argtypes = [vp, u32, vp, u32, i32, vp, vp, vp]
+        L.rt_rebuild.argtypes = [vp, vp, u32, vp, u32, i32, vp, vp]
+        L.rt_load_bvh.argtypes = [C.c_char_p, vp]
+        L.rt_write_bvh.argtypes = [vp, C.c_char_p]
+        L.rt_bvh_from_arrays.argtypes = [vp, u32, vp, u32, vp, u32, vp]
+        L.rt_bvh_counts.argtypes = [vp, vp]
+        L.rt_bvh_download.argtypes = [vp, vp, vp, vp]
+        L.rt_bvh_prim_ids.argtypes = [vp, vp, i32]
+        L.rt_bvh_stats.argtypes = [vp, vp]
+        L.rt_bvh_free.argtypes = [vp]
+        L.rt_trace.argtypes = [vp, vp, vp, u64, u32, vp]
+        L.rt_trace_host.argtypes = [vp, vp, vp, u64, u32]
+        L.rt_render.argtypes = [vp, vp, vp, u32, vp, i32, vp, vp, vp]
+        L.rt_camera_lookat.argtypes = [vp, vp, C.c_float, vp]
+        L.rt_camera_quat.argtypes = [vp, vp, C.c_float, vp]
+        L.rt_mesh_create.restype = vp
+        L.rt_mesh_free.argtypes = [vp]
+        L.rt_mesh_add_sphere.argtypes = [vp, C.c_float, C.c_float, C.c_float, C.c_float, i32, i32]
+        L.rt_mesh_add_box.argtypes = [vp] + [C.c_float] * 10
+        L.rt_mesh_read_scene.argtypes = [vp, C.c_char_p]
+        L.rt_mesh_counts.argtypes = [vp, vp]
+        L.rt_mesh_vertices.restype = vp
+        L.rt_mesh_vertices.argtypes = [vp]
+        L.rt_mesh_triangles.restype = vp
+        L.rt_mesh_triangles.argtypes = [vp]
+        L.rt_bake_scene.argtypes = [C.c_char_p, C.c_char_p, vp]
+        L.rt_last_error.restype = C.c_char_p
+        L.rt_version.restype = C.c_char_p
+        L.rt_kernel_launches.restype = u64
+        L.rt_device_sync.argtypes = [vp]
+        _lib = L
+    return _lib
+
+
+def header_symbols(path: str = HEADER) -> list[str]:
+    """Names of the functions include/rt_b200.h declares."""
+    txt = open(path).read()
+    txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+    return sorted(set(re.findall(r"\b(rt_[a-z0-9_]+)\s*\(", txt)))
+
+
+def _check(code: int):
+    if code != 0:
+        raise RtError(code, lib().rt_last_error().decode(errors="replace"))
+
+
+def last_error() -> str:
+    return lib().rt_last_error().decode(errors="replace")
+
+
+def kernel_launches() -> int:
+    return int(lib().rt_kernel_launches())
+
+
+def make_cfg(preset: str = "hybrid", **kw) -> BuildCfg:
+    c = BuildCfg()
+    lib().rt_build_cfg_default(C.byref(c))
+    for k, v in {**PRESETS[preset], **kw}.items():
+        setattr(c, k, v)
+    return c
+
+
+def _is_torch(x) -> bool:
+    return type(x).__module__.startswith("torch")
+
+
+def _ptr(x):
+    if x is None:
+        return None
+    if _is_torch(x):
+        return C.c_void_p(x.data_ptr())
+    return x.ctypes.data_as(C.c_void_p)
+
+
+def _stream_ptr(stream):
+    if stream is None:
+        return None
+    return C.c_void_p(int(stream.cuda_stream) if hasattr(stream, "cuda_stream") else int(stream))
+
+
+class Bvh:
+    """A device-resident BVH (an rt_bvh handle)."""
+
+    def __init__(self, handle):
+        self.h = C.c_void_p(handle) if not isinstance(handle, C.c_void_p) else handle
+
+    # -- construction ------------------------------------------------------------------
+    @staticmethod
+    def build(verts, tris, cfg: BuildCfg | str | None = None, stream=None) -> "Bvh":
+        """verts: (V, 6) float32 (x y z nx ny nz), tris: (N, 3) uint32; numpy (host) or torch
+        CUDA tensors (device)."""
+        if isinstance(cfg, str):
+            cfg = make_cfg(cfg)
+        verts, tris, where = _geometry(verts, tris)
+        out = C.c_void_p()
+        _check(lib().rt_build(_ptr(verts), int(verts.shape[0]), _ptr(tris), int(tris.shape[0]), where,
+                              C.byref(cfg) if cfg is not None else None, _stream_ptr(stream), C.byref(out)))
+        return Bvh(out)
+
+    def rebuild(self, verts, tris, cfg: BuildCfg | str | None = None, stream=None):
+        if isinstance(cfg, str):
+            cfg = make_cfg(cfg)
+        verts, tris, where = _geometry(verts, tris)
+        _check(lib().rt_rebuild(self.h, _ptr(verts), int(verts.shape[0]), _ptr(tris), int(tris.shape[0]), where,
+                                C.byref(cfg) if cfg is not None else None, _stream_ptr(stream)))
+
+    @staticmethod
+    def load(path: str) -> "Bvh":
+        out = C.c_void_p()
+        _check(lib().rt_load_bvh(path.encode(), C.byref(out)))
+        return Bvh(out)
+
+    @staticmethod
+    def from_arrays(nodes, tris, verts) -> "Bvh":
+        nodes = np.ascontiguousarray(nodes, NODE_DTYPE)
+        tris = np.ascontiguousarray(tris, np.uint32)
+        verts = np.ascontiguousarray(verts, np.float32)
+        out = C.c_void_p()
+        _check(lib().rt_bvh_from_arrays(_ptr(nodes), nodes.shape[0], _ptr(tris), tris.shape[0], _ptr(verts),
+                                        verts.shape[0], C.byref(out)))
+        return Bvh(out)
+
+    def free(self):
+        if self.h:
+            lib().rt_bvh_free(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+    # -- inspection --------------------------------------------------------------------
+    def counts(self):
+        c = np.zeros(3, np.uint32)
+        _check(lib().rt_bvh_counts(self.h, _ptr(c)))
+        return int(c[0]), int(c[1]), int(c[2])
+
+    def download(self):
+        """(nodes, tris, verts) in the .bvh v1 layout."""
+        nn, nt, nv = self.counts()
+        nodes = np.zeros(nn, NODE_DTYPE)
+        tris = np.zeros((nt, 3), np.uint32)
+        verts = np.zeros((nv, 6), np.float32)
+        _check(lib().rt_bvh_download(self.h, _ptr(nodes), _ptr(tris), _ptr(verts)))
+        return nodes, tris, verts
+
+    def prim_ids(self):
+        _, nt, _ = self.counts()
+        out = np.zeros(nt, np.uint32)
+        _check(lib().rt_bvh_prim_ids(self.h, _ptr(out), RT_HOST))
+        return out
+
+    def stats(self):
+        s = np.zeros(8, np.uint32)
+        _check(lib().rt_bvh_stats(self.h, _ptr(s)))
+        return dict(spatial_taken=int(s[0]), spatial_refused=int(s[1]), sah_roots=int(s[2]), inner=int(s[3]),
+                    leaves=int(s[4]))
+
+    def write(self, path: str):
+        _check(lib().rt_write_bvh(self.h, path.encode()))
+
+    # -- tracing -----------------------------------------------------------------------
+    def trace(self, rays, flags: int = TRACE_CLOSEST, stream=None):
+        """rays: (n, 8) float32 (o.xyz, tmin, d.xyz, tmax). numpy in -> structured HIT_DTYPE
+        numpy out (host copies inside); torch CUDA in -> (n, 8) float32 tensor of rt_hit
+        records out (device)."""
+        if _is_torch(rays):
+            import torch
+            assert rays.is_cuda and rays.dtype == torch.float32 and rays.shape[-1] == 8
+            rays = rays.contiguous()
+            hits = torch.empty_like(rays)
+            code = lib().rt_trace(self.h, _ptr(rays), _ptr(hits), int(rays.shape[0]), flags, _stream_ptr(stream))
+            if code not in (0, 5):
+                _check(code)
+            return hits
+        rays = np.ascontiguousarray(rays, np.float32)
+        hits = np.zeros(rays.shape[0], HIT_DTYPE)
+        code = lib().rt_trace_host(self.h, _ptr(rays), _ptr(hits), int(rays.shape[0]), flags)
+        if code not in (0, 5):
+            _check(code)
+        return hits
+
+    def render(self, rcfg: RenderCfg, mats=None, mat_of_tri=None, mode: int = RENDER_PLAIN, want_sq: bool = False,
+               stream=None):
+        """Returns (rgb, rgb2) torch CUDA tensors (H, W, 3); mats: list of dicts or None;
+        mat_of_tri: material index per baked triangle (numpy / torch)."""
+        import torch
+        dev = torch.device("cuda")
+        rgb = torch.empty((rcfg.height, rcfg.width, 3), dtype=torch.float32, device=dev)
+        rgb2 = torch.empty_like(rgb) if want_sq else None
+        dm = dmot = None
+        if mats is not None:
+            arr = np.zeros((len(mats), 8), np.float32)
+            for i, m in enumerate(mats):
+                arr[i, 0:3] = m["albedo"]
+                arr[i, 3:6] = m.get("emission", (0.0, 0.0, 0.0))
+                arr[i, 6:8].view(np.uint32)[0] = int(m.get("kind", 0))
+            dm = torch.from_numpy(arr).to(dev)
+            dmot = mat_of_tri if _is_torch(mat_of_tri) else torch.from_numpy(
+                np.ascontiguousarray(mat_of_tri, np.uint32).view(np.int32)).to(dev)
+        _check(lib().rt_render(self.h, C.byref(rcfg), _ptr(dm), len(mats) if mats is not None else 0, _ptr(dmot), mode,
+                               _ptr(rgb), _ptr(rgb2),
+                               _stream_ptr(stream)))
+        return rgb, rgb2
+
+
+def _geometry(verts, tris):
+    if _is_torch(verts):
+        import torch
+        assert verts.is_cuda and tris.is_cuda
+        verts = verts.contiguous().to(torch.float32)
+        tris = tris.contiguous()
+        assert tris.element_size() == 4
+        return verts, tris, RT_DEVICE
+    return np.ascontiguousarray(verts, np.float32), np.ascontiguousarray(tris, np.uint32), RT_HOST
+
+
+def render_cfg(width, height, spp, max_bounce=8, rr_after=2, env_kind=0, env_color=(0.0, 0.0, 0.0), seed=1,
+               sample_offset=0, lookat=None, quat=None) -> RenderCfg:
+    """Render settings; lookat=(pos, target, fov_deg) or quat=(pos, (w, x, y, z), focal)
+    (src/main.cpp:43-66). Defaults are the reference's: 8 bounces, roulette after bounce 2,
+    sky background."""
+    c = RenderCfg()
+    c.width, c.height, c.spp, c.max_bounce, c.rr_after, c.env_kind = width, height, spp, max_bounce, rr_after, env_kind
+    c.env_color[:] = list(env_color)
+    c.seed, c.sample_offset = seed, sample_offset
+    if quat is not None:
+        pos, q, focal = quat
+        lib().rt_camera_quat(_ptr(np.asarray(pos, np.float32)), _ptr(np.asarray(q, np.float32)), float(focal), C.byref(c))
+    else:
+        pos, target, fov = lookat if lookat is not None else ((0.0, 1.0, -5.0), (0.0, 0.0, 0.0), 60.0)
+        lib().rt_camera_lookat(_ptr(np.asarray(pos, np.float32)), _ptr(np.asarray(target, np.float32)), float(fov),
+                               C.byref(c))
+    return c
+
+
+class Mesh:
+    """Host geometry built with the reference's generators (rt_mesh_*)."""
+
+    def __init__(self):
+        self.h = C.c_void_p(lib().rt_mesh_create())
+
+    def __del__(self):
+        try:
+            if self.h:
+                lib().rt_mesh_free(self.h)
+        except Exception:
+            pass
+
+    def add_sphere(self, center, radius, rings=16, sectors=32):
+        _check(lib().rt_mesh_add_sphere(self.h, *[float(x) for x in center], float(radius), int(rings), int(sectors)))
+        return self
+
+    def add_box(self, center, half, q_xyzw=(0.0, 0.0, 0.0, 1.0)):
+        _check(lib().rt_mesh_add_box(self.h, *[float(x) for x in center], *[float(x) for x in half],
+                                     *[float(x) for x in q_xyzw]))
+        return self
+
+    def read_scene(self, path: str):
+        _check(lib().rt_mesh_read_scene(self.h, path.encode()))
+        return self
+
+    def arrays(self):
+        c = np.zeros(2, np.uint32)
+        _check(lib().rt_mesh_counts(self.h, _ptr(c)))
+        nv, nt = int(c[0]), int(c[1])
+        v = np.zeros((nv, 6), np.float32)
+        t = np.zeros((nt, 3), np.uint32)
+        if nv:
+            C.memmove(v.ctypes.data, lib().rt_mesh_vertices(self.h), nv * 24)
+        if nt:
+            C.memmove(t.ctypes.data, lib().rt_mesh_triangles(self.h), nt * 12)
+        return v, t
+
+
+def bake_scene(scn_path: str, out_bvh: str | None = None, cfg: BuildCfg | str | None = None):
+    """bvh::bakeBVH: .scn -> GPU build -> .bvh."""
+    if isinstance(cfg, str):
+        cfg = make_cfg(cfg)
+    _check(lib().rt_bake_scene(scn_path.encode(), out_bvh.encode() if out_bvh else None,
+                               C.byref(cfg) if cfg is not None else None))

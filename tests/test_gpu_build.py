@@ -1,0 +1,93 @@
+"""GPU bake parity: librt_b200's build against the C restatement oracle (itself pinned bit for
+bit against the reference in test_oracle.py), for every build preset on seeded scenes.
+
+Bar: identical tree -- node kinds, child / triangle indices and triangle order equal, boxes
+value-equal (+0 and -0 compare equal: the reference's own choice between them depends on the
+order it extends boxes in), vertices bit-equal (normals renormalised as initGeos does)."""
+import os
+import tempfile
+
+import numpy as np
+import pytest
+
+import rtb200
+from oracle import make_cfg as orc_make_cfg
+from scenes_for_tests import scene_set
+
+pytestmark = pytest.mark.gpu
+
+PRESETS = ["hybrid", "lbvh63", "lbvh30", "lbvh63l4", "sah4", "sah16", "sah4ns"]
+
+
+def read_scn(text):
+    with tempfile.TemporaryDirectory() as d:
+        p = os.path.join(d, "s.scn")
+        open(p, "w").write(text)
+        return rtb200.Mesh().read_scene(p).arrays()
+
+
+SCENES = scene_set(read_scn)
+
+
+def orc_cfg(preset):
+    kw = dict(rtb200.PRESETS[preset])
+    if kw["lbvh_threshold"] == 0xFFFFFFFF:
+        kw["lbvh_threshold"] = 0xFFFFFFFF
+    return orc_make_cfg(**kw)
+
+
+def assert_same_tree(gpu, ref, tag):
+    gn, gt, gv = gpu
+    assert gn.shape == ref.nodes.shape, f"{tag}: node count {gn.shape[0]} vs {ref.nodes.shape[0]}"
+    for f in ("is_leaf", "a", "b"):
+        bad = np.nonzero(gn[f] != ref.nodes[f])[0]
+        assert bad.size == 0, f"{tag}: field {f} differs at nodes {bad[:8]}"
+    for f in ("bmin", "bmax"):
+        bad = np.nonzero(np.any(gn[f] != ref.nodes[f], axis=1))[0]
+        assert bad.size == 0, f"{tag}: {f} differs at nodes {bad[:8]}: {gn[f][bad[:2]]} vs {ref.nodes[f][bad[:2]]}"
+    assert np.array_equal(gt, ref.tris), f"{tag}: triangle order differs"
+    assert np.array_equal(gv.view(np.uint32), ref.verts.view(np.uint32)), f"{tag}: vertices differ"
+
+
+@pytest.mark.parametrize("preset", PRESETS)
+@pytest.mark.parametrize("scene", sorted(SCENES))
+def test_build_matches_oracle(orc, scene, preset):
+    v, t = SCENES[scene]
+    ref = orc.build(v, t, orc_cfg(preset))
+    b = rtb200.Bvh.build(v, t, preset)
+    assert_same_tree(b.download(), ref, f"{scene}/{preset}")
+    # original triangle ids of the baked order
+    pid = b.prim_ids()
+    assert np.array_equal(t[pid], ref.tris)
+    st = b.stats()
+    assert st["spatial_taken"] == int(ref.stats[0]) and st["spatial_refused"] == int(ref.stats[1])
+
+
+def test_build_from_device_tensors(orc):
+    import torch
+    v, t = SCENES["soup20k"]
+    ref = orc.build(v, t, orc_cfg("hybrid"))
+    dv = torch.from_numpy(v).cuda()
+    dt = torch.from_numpy(t.view(np.int32)).cuda()
+    b = rtb200.Bvh.build(dv, dt, "hybrid")
+    assert_same_tree(b.download(), ref, "device-in")
+
+
+def test_rebuild_reuses_handle(orc):
+    b = rtb200.Bvh.build(*SCENES["soup2k"], "lbvh63")
+    for name in ("soup20k", "ico4", "soup2k"):
+        v, t = SCENES[name]
+        b.rebuild(v, t, "lbvh63")
+        assert_same_tree(b.download(), orc.build(v, t, orc_cfg("lbvh63")), f"rebuild {name}")
+
+
+def test_errors_are_reported():
+    v, t = SCENES["soup2k"]
+    bad = t.copy()
+    bad[5, 1] = v.shape[0] + 7
+    with pytest.raises(rtb200.RtError) as e:
+        rtb200.Bvh.build(v, bad)
+    assert e.value.code == 9  # RT_E_INDEX, the reference's initGeos index check
+    with pytest.raises(rtb200.RtError) as e:
+        rtb200.Bvh.build(v[:0], t[:0])
+    assert e.value.code == 8  # RT_E_EMPTY
