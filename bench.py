@@ -1,0 +1,379 @@
+#!/usr/bin/env python3
+"""BVH build + traversal microbenchmark on B200 GPUs.
+
+Workload (one "step"): a full bake of the seeded 1,048,576-triangle soup (centroids uniform in
+[0,1]^3, vertices at centroid + L*u with L log-uniform in [1e-4, 1e-2]) with the reference's
+LBVH semantics (pure Morton split, 63-bit codes, leaf 16), producing the .bvh-layout tree and
+the traversal layout, from inputs already resident in HBM. Metric: BVH build throughput in
+Mtri/s over all ranks (weak scaling: every rank bakes its own soup; no data-path collective).
+
+Also reported: the same build end to end through the C ABI with host buffers (e2e), the other
+build presets, closest-hit / any-hit traversal of 16,777,216 incoherent rays and of 1920x1080
+pinhole rays (Mray/s), the roofline of the dominant kernel (the radix-sort pass), and the
+reference's own CPU bake timed on this host.
+
+usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+       torchrun --nproc-per-node N bench.py --gpus N ...   (one process per GPU)
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(HERE, "ray-tracer_b200"))
+
+N_TRIS = 1 << 20
+N_RAYS = 1 << 24
+METRIC = "BVH Mtri/s"
+WORKLOAD = "BVH build microbenchmark: 1,048,576-triangle soup, LBVH 63-bit Morton codes, leaf 16"
+SORT_BYTES_PER_KEY = (20 + 7 * 24) / 8.0  # per onesweep pass: 8 B key + 4 B value in/out (first pass: no value read)
+
+
+def parse_args():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=20)
+    p.add_argument("--warmup", type=int, default=5)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--n-tris", type=int, default=N_TRIS)
+    p.add_argument("--preset", default="lbvh63")
+    p.add_argument("--no-extra", action="store_true", help="skip the secondary measurements")
+    return p.parse_args()
+
+
+def env_rank():
+    return int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("LOCAL_RANK", "0"))
+
+
+# ---------------------------------------------------------------------------------------------
+# clocks during the timed region
+class ClockSampler:
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.idx = gpu_index
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def start(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.idx), f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                                       "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+        time.sleep(0.3)
+
+    def stop(self):
+        if self.p is None:
+            return None
+        time.sleep(0.25)
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except Exception:
+            self.p.kill()
+        self.f.flush()
+        self.f.seek(0)
+        rows = [r.split(",") for r in self.f.read().strip().splitlines() if r.strip()]
+        os.unlink(self.f.name)
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            r = [x.strip() for x in r]
+            try:
+                sm.append(float(r[1]))
+                smax = float(r[2])
+            except (ValueError, IndexError):
+                continue
+            for k, name in enumerate(names):
+                if len(r) > 5 + k and r[5 + k].lower() == "active":
+                    reasons.add(name)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": smax, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peak_hbm():
+    try:
+        with open(os.path.join(HERE, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def profiled_traffic():
+    """DRAM bytes per onesweep launch per key from the committed ncu summary, if present."""
+    path = os.path.join(HERE, "profiles", "onesweep_soup1m_traffic.txt")
+    try:
+        for line in open(path):
+            if line.startswith("dram_bytes_per_key_per_launch"):
+                return float(line.split("=")[1])
+    except Exception:
+        pass
+    return None
+
+
+# ---------------------------------------------------------------------------------------------
+class quiet_stdout:
+    """Sends file descriptor 1 to /dev/null (the reference prints progress lines from C)."""
+
+    def __enter__(self):
+        sys.stdout.flush()
+        self.saved = os.dup(1)
+        nul = os.open(os.devnull, os.O_WRONLY)
+        os.dup2(nul, 1)
+        os.close(nul)
+
+    def __exit__(self, *exc):
+        sys.stdout.flush()
+        os.dup2(self.saved, 1)
+        os.close(self.saved)
+
+
+def cpu_reference_bake(n_tris: int, seed: int, reps: int):
+    """The reference's own bvh::bakeBVH (oracle/_ref/lbvh63, single-threaded as shipped) on a
+    soup sample; falls back to the C restatement when the reference build is absent."""
+    sys.path.insert(0, os.path.join(HERE, "oracle"))
+    import oracle as orc
+    from rtb200 import scenes
+    v, t = scenes.soup(n_tris, seed=seed)
+    if orc.Reference.available("lbvh63"):
+        ref, kind = orc.Reference("lbvh63"), "reference"
+        fn = lambda: ref.bake(v, t)  # noqa: E731
+    else:
+        R, kind = orc.Restatement(), "port"
+        cfg = orc.make_cfg(**orc.VARIANTS["lbvh63"])
+        fn = lambda: R.build(v, t, cfg)  # noqa: E731
+    fn()
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        fn()
+    dt = (time.perf_counter() - t0) / reps
+    return n_tris / dt / 1e6, kind, dt
+
+
+def _ref_worker(args):
+    n, seed, reps = args
+    with quiet_stdout():
+        return cpu_reference_bake(n, seed, reps)
+
+
+def run_reference(a):
+    rank, world, _ = env_rank()
+    if rank != 0:
+        return 0
+    import multiprocessing as mp
+    cores = os.cpu_count() or 1
+    sample = 1 << 17
+    per = max(1, (a.steps + cores - 1) // cores)
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(cores) as pool:
+        pool.map(_ref_worker, [(1 << 12, 5, 1)] * cores)  # warm-up (loads the library in every worker)
+        t0 = time.perf_counter()
+        res = pool.map(_ref_worker, [(sample, 20261204 + i, per) for i in range(cores)])
+        wall = time.perf_counter() - t0
+    kind = res[0][1]
+    total = sample * per * cores
+    value = total / wall / 1e6
+    out = {"metric": METRIC, "value": round(value, 4), "unit": "Mtri/s", "impl": "reference", "n_gpus": a.gpus,
+           "steps": a.steps, "warmup": a.warmup, "ms_per_step": round(wall / (per) * 1e3, 3), "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded soup)",
+           "config": {"workload": WORKLOAD, "n_tris_sample": sample, "preset": "lbvh63 (reference constants patched: "
+                      "BVH_LBVH_THRESHOLD=0)", "processes": cores},
+           "cpu_baseline": {"value": round(value, 4), "unit": "Mtri/s", "cores": cores, "kind": kind,
+                            "sample": f"{cores} independent bakes of a {sample}-triangle soup per round, "
+                                      f"{per} round(s); the reference bake is single-threaded, one per process"},
+           "e2e": {"value": round(value, 4), "unit": "Mtri/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------------------------------------
+def run_ours(a):
+    import numpy as np
+    import torch
+    import rtb200
+    from rtb200 import scenes
+
+    rank, world, local = env_rank()
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.current_stream()
+    n = a.n_tris
+    verts, tris = scenes.soup(n, seed=scenes.BASE_SEED + 1 + rank)
+    dv = torch.from_numpy(verts).to(dev)
+    dt = torch.from_numpy(tris.view(np.int32)).to(dev)
+    cfg = rtb200.make_cfg(a.preset)
+    bvh = rtb200.Bvh.build(dv, dt, cfg, stream=stream)
+    bvh.profile(True)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)  # 256 MiB > 126 MB L2
+    for _ in range(max(a.warmup, 3)):
+        bvh.rebuild(dv, dt, cfg, stream=stream)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clk = ClockSampler(local)
+    clk.start()
+    l0 = rtb200.kernel_launches()
+    evs = []
+    stages = []
+    for _ in range(a.steps):
+        flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        bvh.rebuild(dv, dt, cfg, stream=stream)
+        e1.record(stream)
+        evs.append((e0, e1))
+        stages.append(bvh.stage_ms())
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    launches = rtb200.kernel_launches() - l0
+    clocks = clk.stop()
+    total_ms = sum(e0.elapsed_time(e1) for e0, e1 in evs)
+    if dist:
+        t = torch.tensor([total_ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    ms_step = total_ms / a.steps
+    value = world * n / (ms_step * 1e-3) / 1e6
+    st = {k: statistics.mean(s[k] for s in stages) for k in stages[0]}
+    nn, nt, _ = bvh.counts()
+
+    # roofline of the dominant kernel: the onesweep radix-sort pass (8 launches per step)
+    passes = (3 * cfg.morton_bits + 7) // 8
+    sort_launch_ms = st["sort"] / passes
+    alg_bytes = SORT_BYTES_PER_KEY * n
+    achieved = alg_bytes / (sort_launch_ms * 1e-3) / 1e9
+    peak, peak_kind = measured_peak_hbm()
+    traffic_per_key = profiled_traffic()
+
+    # end to end through the C ABI with host buffers: H2D of the geometry, the bake, D2H of the
+    # baked .bvh arrays, every step (pinned host memory; host-synchronous calls)
+    hv = torch.from_numpy(verts).pin_memory()
+    ht = torch.from_numpy(tris.view(np.int32)).pin_memory()
+    hn = torch.empty(nn * 48, dtype=torch.uint8).pin_memory()
+    htr = torch.empty(nt * 12, dtype=torch.uint8).pin_memory()
+    hvo = torch.empty(verts.nbytes, dtype=torch.uint8).pin_memory()
+    L = rtb200.lib()
+    import ctypes as C
+
+    def e2e_step():
+        bvh.rebuild(hv.numpy(), ht.numpy().view(np.uint32), cfg)
+        rtb200.api._check(L.rt_bvh_download(bvh.h, C.c_void_p(hn.data_ptr()), C.c_void_p(htr.data_ptr()),
+                                            C.c_void_p(hvo.data_ptr())))
+    for _ in range(2):
+        e2e_step()
+    torch.cuda.synchronize()
+    k_e2e = max(3, a.steps // 2)
+    t0 = time.perf_counter()
+    for _ in range(k_e2e):
+        e2e_step()
+    torch.cuda.synchronize()
+    e2e_s = (time.perf_counter() - t0) / k_e2e
+    if dist:
+        t = torch.tensor([e2e_s], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e_value = world * n / e2e_s / 1e6
+    h2d = verts.nbytes + tris.nbytes
+    d2h = nn * 48 + nt * 12 + verts.nbytes
+
+    extra = {}
+    if not a.no_extra:
+        extra = secondary(a, bvh, dv, dt, verts, stream, dev, flush)
+    out = None
+    if rank == 0:
+        with quiet_stdout():
+            cpu_v, cpu_kind, cpu_dt = cpu_reference_bake(1 << 17, 20261204, 2)
+        out = {"metric": METRIC, "value": round(value, 3), "unit": "Mtri/s", "n_gpus": world, "steps": a.steps,
+               "warmup": a.warmup, "ms_per_step": round(ms_step, 4), "higher_is_better": True, "scaling": "weak",
+               "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded soup, per-rank seed)",
+               "config": {"workload": WORKLOAD, "n_tris": n, "preset": a.preset, "nodes": nn, "baked_tris": nt,
+                          "l2": "flushed between steps (256 MiB write)", "parallelism": f"replicas x{world}"},
+               "e2e": {"value": round(e2e_value, 3), "unit": "Mtri/s", "h2d_bytes_per_step": int(h2d),
+                       "d2h_bytes_per_step": int(d2h)},
+               "gpu_launches": int(launches),
+               "stage_ms": {k: round(v, 4) for k, v in st.items()},
+               "roofline": {"bound": "hbm", "kernel": "k_onesweep (radix sort pass)", "achieved": round(achieved, 1),
+                            "peak": peak, "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4),
+                            "traffic": (round(traffic_per_key * n) if traffic_per_key else None),
+                            "algorithmic_bytes_per_launch": int(alg_bytes), "launch_ms": round(sort_launch_ms, 5)},
+               "cpu_baseline": {"value": round(cpu_v, 4), "unit": "Mtri/s", "cores": 1, "kind": cpu_kind,
+                                "sample": "bvh::bakeBVH of a 131,072-triangle soup of the same generator, LBVH "
+                                          "constants, 2 timed repetitions, 1 thread (the bake is single-threaded)"},
+               "clocks": clocks, "extra": extra}
+        print(json.dumps(out), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def secondary(a, bvh, dv, dt, verts, stream, dev, flush):
+    """Other presets' build rates and traversal rates (single measurements after warm-up)."""
+    import numpy as np
+    import torch
+    import rtb200
+    from rtb200 import scenes
+    n = dv.shape[0]
+    res = {}
+
+    def timed(fn, reps):
+        fn()
+        torch.cuda.synchronize()
+        ms = []
+        for _ in range(reps):
+            flush.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            fn()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ms.append(e0.elapsed_time(e1))
+        return statistics.median(ms)
+
+    for preset in ("lbvh30", "hybrid", "sah4"):
+        b = rtb200.Bvh.build(dv, dt, preset, stream=stream)
+        ms = timed(lambda: b.rebuild(dv, dt, preset, stream=stream), 3 if preset != "sah4" else 1)
+        res[f"build_{preset}_mtri_s"] = round(n / (ms * 1e-3) / 1e6, 3)
+        b.free()
+    lo, hi = verts[:, :3].min(0), verts[:, :3].max(0)
+    rays = torch.from_numpy(scenes.incoherent_rays(N_RAYS, lo, hi, seed=scenes.BASE_SEED + 9)).to(dev)
+    prim = torch.from_numpy(scenes.pinhole_rays(1920, 1080, (0.5, 0.5, -1.5), (0.5, 0.5, 0.5), 60.0)).to(dev)
+    for preset in ("lbvh63", "hybrid", "sah4"):
+        b = rtb200.Bvh.build(dv, dt, preset, stream=stream)
+        for name, r in (("incoherent16M", rays), ("primary1080p", prim)):
+            for fl, fname in ((rtb200.TRACE_CLOSEST, "closest"), (rtb200.TRACE_ANY_HIT, "anyhit")):
+                ms = timed(lambda: b.trace(r, fl, stream=stream), 3)
+                res[f"trace_{preset}_{name}_{fname}_mray_s"] = round(r.shape[0] / (ms * 1e-3) / 1e6, 1)
+        b.free()
+    return res
+
+
+def main():
+    a = parse_args()
+    if a.impl == "reference":
+        return run_reference(a)
+    return run_ours(a)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -114,6 +114,12 @@ int rt_bvh_prim_ids(const rt_bvh* bvh, uint32_t* out, int where);
 /* stats8: spatial splits taken, spatial splits refused for capacity, SAH roots,
  * inner nodes, leaves, tree depth, build kernels launched, reserved */
 int rt_bvh_stats(const rt_bvh* bvh, uint32_t* stats8);
+/* Stage timing of later (re)builds on this handle: CUDA events recorded on the build's
+ * stream between stages. ms8 = prep (normals, triangle boxes, Morton codes), radix sort,
+ * topology (Karras tree, boundary, refit), binned SAH, emit (pre-order layout), traversal
+ * layout, total, reserved. No counterpart in the reference (it has no instrumentation). */
+int rt_bvh_profile(rt_bvh* bvh, int enable);
+int rt_bvh_stage_ms(const rt_bvh* bvh, float* ms8);
 void rt_bvh_free(rt_bvh* bvh);
 
 /* ---- tracing: bvh::trace (src/bvh/bvh_traverse.cpp:237-246), batched ---- */

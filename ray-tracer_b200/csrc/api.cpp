@@ -117,6 +117,12 @@ static void free_bvh(rt_bvh* b)
                        &b->s.sah_scan_in, &b->s.sah_scan_out, &b->s.sah_node_ids, &b->s.sah_roots_lvl,
                        &b->s.in_verts, &b->s.in_tris };
     for (DevBuf* x : bufs) { x->release(); }
+    for (int k = 0; k < 2; k++) { b->wf_rays[k].release(); b->wf_state[k].release(); }
+    b->wf_hits.release(); b->wf_acc.release(); b->wf_ctr.release();
+    for (cudaEvent_t& e : b->ev)
+    {
+        if (e) { cudaEventDestroy(e); e = nullptr; }
+    }
     delete b;
 }
 
@@ -315,6 +321,27 @@ int rt_bvh_stats(const rt_bvh* b, uint32_t* s8)
 }
 
 void rt_bvh_free(rt_bvh* b) { free_bvh(b); }
+
+int rt_bvh_profile(rt_bvh* b, int enable)
+{
+    if (!b) { return fail(RT_E_INVALID, "null handle"); }
+    if (enable)
+    {
+        for (cudaEvent_t& e : b->ev)
+        {
+            if (!e) { RT_CUDA(cudaEventCreate(&e)); }
+        }
+    }
+    b->prof = enable != 0;
+    return RT_OK;
+}
+
+int rt_bvh_stage_ms(const rt_bvh* b, float* ms8)
+{
+    if (!b || !ms8) { return fail(RT_E_INVALID, "null argument"); }
+    std::memcpy(ms8, b->stage_ms, sizeof(b->stage_ms));
+    return RT_OK;
+}
 
 int rt_write_bvh(const rt_bvh* b, const char* path)
 {

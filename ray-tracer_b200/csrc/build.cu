@@ -475,6 +475,7 @@ int build_typed(rt_bvh* B, const rt_vertex* d_verts, uint32_t V, const rt_triang
     uint32_t* status = S.status.as<uint32_t>();
     uint32_t* counters = S.counters.as<uint32_t>();
 
+    prof_mark(B, 0, st);
     k_init<<<1, 256, 0, st>>>(S.scene.as<uint32_t>(), S.hist.as<uint32_t>(), counters, status);
     count_launch();
     RT_CUDA(cudaMemsetAsync(S.parent.p, 0xff, (size_t)nk * 4, st));
@@ -494,6 +495,7 @@ int build_typed(rt_bvh* B, const rt_vertex* d_verts, uint32_t V, const rt_triang
     count_launch();
     if (int e = check_launch("morton")) { return e; }
 
+    prof_mark(B, 1, st);
     K* skeys = nullptr;
     uint32_t* perm = nullptr;
     if (int e = radix_sort_pairs<K>(S.keys.as<K>(), S.vals.as<uint32_t>(), true, N, key_bits, S.hist.as<uint32_t>(),
@@ -501,6 +503,7 @@ int build_typed(rt_bvh* B, const rt_vertex* d_verts, uint32_t V, const rt_triang
     {
         return e;
     }
+    prof_mark(B, 2, st);
     if (N >= 2)
     {
         k_karras<K><<<blocks_for(N - 1), BLK, 0, st>>>(skeys, N, S.knode.as<uint4>(), S.parent.as<uint32_t>());
@@ -514,17 +517,11 @@ int build_typed(rt_bvh* B, const rt_vertex* d_verts, uint32_t V, const rt_triang
                                                   S.sah_roots.as<SahRoot>(), counters, status);
     count_launch();
     if (int e = check_launch("boundary")) { return e; }
-
-    uint32_t hc[2];
-    RT_CUDA(cudaMemcpyAsync(hc, counters, 8, cudaMemcpyDeviceToHost, st));
-    RT_CUDA(cudaStreamSynchronize(st));
-    const uint32_t n_roots = hc[0];
-    B->stats[0] = B->stats[1] = 0;
-    B->stats[2] = n_roots;
+    prof_mark(B, 3, st);
 
     SahResult sah;
-    if (n_roots > 0)
-    {
+    uint32_t n_roots = 0;
+    auto run_sah = [&]() -> int {
         SahInput in;
         in.verts = B->verts.as<rt_vertex>();
         in.tris = d_tris;
@@ -538,36 +535,63 @@ int build_typed(rt_bvh* B, const rt_vertex* d_verts, uint32_t V, const rt_triang
         in.n_roots = n_roots;
         in.wnode = S.wnode.as<uint32_t>();
         in.wtri = S.wtri.as<uint32_t>();
-        if (int e = sah_build(B, cfg, in, st, &sah)) { return e; }
-        B->stats[0] = sah.spatial_taken;
-        B->stats[1] = sah.spatial_refused;
-    }
-
-    // pre-order node slots and triangle offsets per start key
-    if (int e = exclusive_scan_u32(S.wnode.as<uint32_t>(), S.snode.as<uint32_t>(), N + 1, counters + 4, S.scan, st)) { return e; }
-    if (int e = exclusive_scan_u32(S.wtri.as<uint32_t>(), S.stri.as<uint32_t>(), N + 1, counters + 5, S.scan, st)) { return e; }
-    k_emit<K><<<blocks_for(nk), BLK, 0, st>>>(skeys, N, S.knode.as<uint4>(), S.parent.as<uint32_t>(), tm, cfg.max_leaf,
-                                              S.kbox.as<float4>(), S.rank.as<uint32_t>(), S.snode.as<uint32_t>(),
-                                              S.stri.as<uint32_t>(), B->nodes.as<rt_bvh_node>(), 2 * cap - 1, status);
-    count_launch();
-    k_emit_tris<<<blocks_for(N), BLK, 0, st>>>(perm, S.bnd.as<uint8_t>(), S.stri.as<uint32_t>(), N, d_tris,
-                                                B->tris.as<rt_triangle>(), B->prim.as<uint32_t>(), cap, status);
-    count_launch();
-    if (n_roots > 0)
-    {
-        if (int e = sah_emit(B, n_roots, S.snode.as<uint32_t>(), S.stri.as<uint32_t>(), d_tris, st, sah, 2 * cap - 1, cap,
-                             status))
+        return sah_build(B, cfg, in, st, &sah);
+    };
+    // pre-order node slots and triangle offsets per start key, then the nodes and triangles
+    auto emit_all = [&]() -> int {
+        if (int e = exclusive_scan_u32(S.wnode.as<uint32_t>(), S.snode.as<uint32_t>(), N + 1, counters + 4, S.scan, st)) { return e; }
+        if (int e = exclusive_scan_u32(S.wtri.as<uint32_t>(), S.stri.as<uint32_t>(), N + 1, counters + 5, S.scan, st)) { return e; }
+        k_emit<K><<<blocks_for(nk), BLK, 0, st>>>(skeys, N, S.knode.as<uint4>(), S.parent.as<uint32_t>(), tm, cfg.max_leaf,
+                                                  S.kbox.as<float4>(), S.rank.as<uint32_t>(), S.snode.as<uint32_t>(),
+                                                  S.stri.as<uint32_t>(), B->nodes.as<rt_bvh_node>(), 2 * cap - 1, status);
+        count_launch();
+        k_emit_tris<<<blocks_for(N), BLK, 0, st>>>(perm, S.bnd.as<uint8_t>(), S.stri.as<uint32_t>(), N, d_tris,
+                                                    B->tris.as<rt_triangle>(), B->prim.as<uint32_t>(), cap, status);
+        count_launch();
+        if (n_roots > 0)
         {
-            return e;
+            if (int e = sah_emit(B, n_roots, S.snode.as<uint32_t>(), S.stri.as<uint32_t>(), d_tris, st, sah, 2 * cap - 1,
+                                 cap, status))
+            {
+                return e;
+            }
         }
-    }
-    if (int e = check_launch("emit")) { return e; }
+        return check_launch("emit");
+    };
 
+    // When the SAH threshold does not exceed the leaf size (the LBVH presets), subtrees for the
+    // binned SAH only come from runs of identical Morton codes; the layout is emitted at once
+    // and redone in the rare case such runs exist, which saves a host round trip.
+    const bool expect_sah = cfg.lbvh_threshold > cfg.max_leaf;
     uint32_t res[8];
-    RT_CUDA(cudaMemcpyAsync(res, counters, 32, cudaMemcpyDeviceToHost, st));
     uint32_t stat = 0;
-    RT_CUDA(cudaMemcpyAsync(&stat, status, 4, cudaMemcpyDeviceToHost, st));
-    RT_CUDA(cudaStreamSynchronize(st));
+    for (int attempt = 0; attempt < 2; attempt++)
+    {
+        if (expect_sah || attempt == 1)
+        {
+            if (attempt == 0)
+            {
+                RT_CUDA(cudaMemcpyAsync(res, counters, 8, cudaMemcpyDeviceToHost, st));
+                RT_CUDA(cudaStreamSynchronize(st));
+                n_roots = res[0];
+            }
+            if (n_roots > 0)
+            {
+                if (int e = run_sah()) { return e; }
+            }
+        }
+        prof_mark(B, 4, st);
+        if (int e = emit_all()) { return e; }
+        prof_mark(B, 5, st);
+        RT_CUDA(cudaMemcpyAsync(res, counters, 32, cudaMemcpyDeviceToHost, st));
+        RT_CUDA(cudaMemcpyAsync(&stat, status, 4, cudaMemcpyDeviceToHost, st));
+        RT_CUDA(cudaStreamSynchronize(st));
+        if (expect_sah || res[0] == 0) { break; }
+        n_roots = res[0];  // identical-code runs found: build their SAH subtrees and emit again
+    }
+    B->stats[0] = sah.spatial_taken;
+    B->stats[1] = sah.spatial_refused;
+    B->stats[2] = n_roots;
     if (stat & ST_INDEX) { return fail(RT_E_INDEX, "triangle has an out-of-bounds vertex index"); }
     if (stat & ST_TIMEOUT) { return fail(RT_E_TIMEOUT, "a bounded device wait gave up (radix sort look-back)"); }
     if (stat & ST_CAPACITY) { return fail(RT_E_CAPACITY, "internal capacity exceeded during the build"); }
@@ -616,7 +640,16 @@ int build_bvh(rt_bvh* B, const rt_vertex* d_verts, uint32_t V, const rt_triangle
     int e = (3 * cfg.morton_bits > 32) ? build_typed<uint64_t>(B, d_verts, V, d_tris, N, cfg, st, cap)
                                        : build_typed<uint32_t>(B, d_verts, V, d_tris, N, cfg, st, cap);
     if (e) { return e; }
-    return make_traversal_layout(B, st);
+    e = make_traversal_layout(B, st);
+    if (e) { return e; }
+    if (B->prof)
+    {
+        prof_mark(B, 6, st);
+        RT_CUDA(cudaEventSynchronize(B->ev[6]));
+        for (int i = 0; i < 6; i++) { cudaEventElapsedTime(&B->stage_ms[i], B->ev[i], B->ev[i + 1]); }
+        cudaEventElapsedTime(&B->stage_ms[6], B->ev[0], B->ev[6]);
+    }
+    return RT_OK;
 }
 
 } // namespace rtb

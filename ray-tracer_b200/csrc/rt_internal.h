@@ -124,7 +124,20 @@ struct rt_bvh
     BuildScratch s;
     rtb::DevBuf  trace_status, trace_rays, trace_hits;
     rtb::DevBuf  wf_rays[2], wf_state[2], wf_hits, wf_acc, wf_ctr;  // wavefront path tracer
+    // stage timing (rt_bvh_profile): events at the stage boundaries of a build
+    bool         prof = false;
+    cudaEvent_t  ev[8] = { nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr };
+    float        stage_ms[8] = { 0, 0, 0, 0, 0, 0, 0, 0 };
 };
+
+namespace rtb
+{
+// Records the boundary event of stage `i` (0 = build start) when profiling is on.
+inline void prof_mark(rt_bvh* b, int i, cudaStream_t st)
+{
+    if (b->prof) { cudaEventRecord(b->ev[i], st); }
+}
+} // namespace rtb
 
 namespace rtb
 {

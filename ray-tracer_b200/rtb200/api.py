@@ -87,6 +87,8 @@ def lib():
         L.rt_bvh_prim_ids.argtypes = [vp, vp, i32]
         L.rt_bvh_stats.argtypes = [vp, vp]
         L.rt_bvh_free.argtypes = [vp]
+        L.rt_bvh_profile.argtypes = [vp, i32]
+        L.rt_bvh_stage_ms.argtypes = [vp, vp]
         L.rt_trace.argtypes = [vp, vp, vp, u64, u32, vp]
         L.rt_trace_host.argtypes = [vp, vp, vp, u64, u32]
         L.rt_render.argtypes = [vp, vp, vp, u32, vp, i32, vp, vp, vp]
@@ -236,6 +238,16 @@ class Bvh:
         _check(lib().rt_bvh_stats(self.h, _ptr(s)))
         return dict(spatial_taken=int(s[0]), spatial_refused=int(s[1]), sah_roots=int(s[2]), inner=int(s[3]),
                     leaves=int(s[4]))
+
+    def profile(self, enable: bool = True):
+        """Stage timing (CUDA events on the build stream) for later rebuilds of this handle."""
+        _check(lib().rt_bvh_profile(self.h, 1 if enable else 0))
+
+    def stage_ms(self):
+        ms = np.zeros(8, np.float32)
+        _check(lib().rt_bvh_stage_ms(self.h, _ptr(ms)))
+        names = ["prep", "sort", "topology", "sah", "emit", "layout", "total"]
+        return {k: float(ms[i]) for i, k in enumerate(names)}
 
     def write(self, path: str):
         _check(lib().rt_write_bvh(self.h, path.encode()))
