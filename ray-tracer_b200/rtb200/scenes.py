@@ -101,7 +101,7 @@ def icosphere(level: int, center=(0.0, 0.0, 0.0), radius: float = 1.0, disp: flo
     ln = np.linalg.norm(acc, axis=1, keepdims=True)
     acc = np.where(ln > 0, acc / np.maximum(ln, 1e-30), v)
     verts[:, 3:] = acc.astype(np.float32)
-    return verts, f.astype(np.uint32)
+    return verts, np.ascontiguousarray(f, dtype=np.uint32)
 
 
 def quad(p0, p1, p2, p3, normal):
