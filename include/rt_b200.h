@@ -169,6 +169,26 @@ enum rt_render_mode { RT_RENDER_PLAIN = 0, RT_RENDER_WAVEFRONT = 1 };
 int rt_render(const rt_bvh* bvh, const rt_render_cfg* cfg, const rt_material* mats, uint32_t n_mats,
               const uint32_t* mat_of_tri, int mode, float* rgb, float* rgb2, void* stream);
 
+/* ---- allocation-free Morton order ----
+ * No counterpart in the reference. For callers that may not allocate device memory while
+ * they run: a renderer re-baking deforming geometry inside its frame loop, where a cudaMalloc
+ * would synchronise the device and stall the frame, or a host application that owns a fixed
+ * device-memory budget and forbids plugins from growing it. It computes the triangle order
+ * the reference's sortTrisByMorton produces (src/bvh/bvh_morton.cpp:109-159; equal to the
+ * baked triangle order of the LBVH presets on meshes without runs of identical codes) and
+ * calls no cudaMalloc / cudaFree or allocating library routine: its scratch is a fixed
+ * device array of about 3.8 MB inside this library, which every GPU that loads the library
+ * holds until the process exits.
+ *   verts, tris, perm_out: device pointers; perm_out receives n_tris original triangle
+ *   indices in Morton order. At most RT_NOALLOC_MAX_TRIS triangles (larger meshes get
+ *   RT_E_CAPACITY; use rt_build). The first call on a device looks up the scratch array's
+ *   device address (cudaGetSymbolAddress); make that first call before any stream capture.
+ *   Every call shares the one scratch array, so calls whose work overlaps on the GPU
+ *   (different streams or threads at once) race and must be serialised by the caller. */
+#define RT_NOALLOC_MAX_TRIS 65536u
+int rt_morton_order_noalloc(const rt_vertex* verts, uint32_t n_verts, const rt_triangle* tris, uint32_t n_tris,
+                            uint32_t morton_bits, uint32_t* perm_out, void* stream);
+
 /* ---- scene ingestion (src/bvh/bvh_IO.cpp:125-234, src/bvh/bvh_geo.cpp) on the host ---- */
 typedef struct rt_mesh rt_mesh;
 rt_mesh* rt_mesh_create(void);

@@ -28,6 +28,7 @@
 
 #include <algorithm>
 #include <cstring>
+#include <mutex>
 
 namespace rtb
 {
@@ -653,3 +654,108 @@ int build_bvh(rt_bvh* B, const rt_vertex* d_verts, uint32_t V, const rt_triangle
 }
 
 } // namespace rtb
+
+// ---------------------------------------------------------------------------------------------
+// Allocation-free Morton order (rt_morton_order_noalloc). Its scratch is one file-scope device
+// array, shared by every call on a device and kept from call to call; each call clears what
+// must start at zero. Host code reaches the array only through the device address that
+// cudaGetSymbolAddress returns (the symbol itself is a host-side stand-in).
+namespace
+{
+
+constexpr uint32_t NA_MAX_TRIS = RT_NOALLOC_MAX_TRIS;
+constexpr uint32_t NA_TILES = (NA_MAX_TRIS + 4095) / 4096;  // onesweep tiles of 4096 keys
+constexpr size_t NA_OFF_LO = 0;
+constexpr size_t NA_OFF_HI = NA_OFF_LO + 16ull * NA_MAX_TRIS;
+constexpr size_t NA_OFF_CZ = NA_OFF_HI + 16ull * NA_MAX_TRIS;
+constexpr size_t NA_OFF_KEYS = NA_OFF_CZ + 4ull * NA_MAX_TRIS;
+constexpr size_t NA_OFF_KALT = NA_OFF_KEYS + 8ull * NA_MAX_TRIS;
+constexpr size_t NA_OFF_VALT = NA_OFF_KALT + 8ull * NA_MAX_TRIS;
+constexpr size_t NA_OFF_HIST = NA_OFF_VALT + 4ull * NA_MAX_TRIS;
+constexpr size_t NA_OFF_LB = NA_OFF_HIST + 8ull * 256 * 4;
+constexpr size_t NA_OFF_TILE = NA_OFF_LB + 8ull * NA_TILES * 256 * 4;
+constexpr size_t NA_OFF_SMALL = NA_OFF_TILE + 64 * 4;  // scene box, counters, status
+constexpr size_t NA_BYTES = NA_OFF_SMALL + 256;
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[NA_BYTES];
+
+std::mutex g_na_mu;
+unsigned char* g_na_dev[64];  // device address of g_noalloc_scratch, per device
+
+template <typename K>
+int morton_order_noalloc_typed(unsigned char* base, const rt_vertex* verts, uint32_t V, const rt_triangle* tris,
+                               uint32_t N, uint32_t bits, uint32_t* perm_out, cudaStream_t st)
+{
+    using namespace rtb;
+    float4* lo = reinterpret_cast<float4*>(base + NA_OFF_LO);
+    float4* hi = reinterpret_cast<float4*>(base + NA_OFF_HI);
+    float* cz = reinterpret_cast<float*>(base + NA_OFF_CZ);
+    K* keys = reinterpret_cast<K*>(base + NA_OFF_KEYS);
+    K* kalt = reinterpret_cast<K*>(base + NA_OFF_KALT);
+    uint32_t* valt = reinterpret_cast<uint32_t*>(base + NA_OFF_VALT);
+    uint32_t* hist = reinterpret_cast<uint32_t*>(base + NA_OFF_HIST);
+    uint32_t* lookback = reinterpret_cast<uint32_t*>(base + NA_OFF_LB);
+    uint32_t* tiles = reinterpret_cast<uint32_t*>(base + NA_OFF_TILE);
+    uint32_t* scene = reinterpret_cast<uint32_t*>(base + NA_OFF_SMALL);
+    uint32_t* counters = scene + 16;
+    uint32_t* status = scene + 48;
+    const int key_bits = 3 * (int)bits;
+    k_init<<<1, 256, 0, st>>>(scene, hist, counters, status);
+    k_tri_prep<<<blocks_for(N), BLK, 0, st>>>(tris, N, verts, V, lo, hi, cz, scene, status);
+    k_morton<K><<<blocks_for(N), BLK, 0, st>>>(lo, hi, cz, N, scene, bits, sort_passes(key_bits), keys, hist);
+    count_launch(3);
+    if (int e = check_launch("morton (no-alloc)")) { return e; }
+    K* kout = nullptr;
+    uint32_t* vout = nullptr;
+    if (int e = radix_sort_pairs_raw<K>(keys, perm_out, N, key_bits, hist, kalt, valt, lookback, tiles, status, st, &kout,
+                                        &vout))
+    {
+        return e;
+    }
+    if (vout != perm_out)
+    {
+        RT_CUDA(cudaMemcpyAsync(perm_out, vout, (size_t)N * 4, cudaMemcpyDeviceToDevice, st));
+    }
+    uint32_t stat = 0;
+    RT_CUDA(cudaMemcpyAsync(&stat, status, 4, cudaMemcpyDeviceToHost, st));
+    RT_CUDA(cudaStreamSynchronize(st));
+    if (stat & ST_INDEX) { return fail(RT_E_INDEX, "triangle has an out-of-bounds vertex index"); }
+    if (stat & ST_TIMEOUT) { return fail(RT_E_TIMEOUT, "a bounded device wait gave up (radix sort look-back)"); }
+    if (stat & ST_CAPACITY) { return fail(RT_E_CAPACITY, "internal capacity exceeded in the sort"); }
+    return RT_OK;
+}
+
+} // namespace
+
+extern "C" int rt_morton_order_noalloc(const rt_vertex* verts, uint32_t n_verts, const rt_triangle* tris, uint32_t n_tris,
+                                       uint32_t morton_bits, uint32_t* perm_out, void* stream)
+{
+    using namespace rtb;
+    if (!verts || !tris || !perm_out) { return fail(RT_E_INVALID, "null pointer"); }
+    if (n_verts == 0 || n_tris == 0) { return fail(RT_E_EMPTY, "no vertices or no triangles"); }
+    if (n_tris > NA_MAX_TRIS)
+    {
+        return fail(RT_E_CAPACITY, "rt_morton_order_noalloc takes at most " + std::to_string(NA_MAX_TRIS) +
+                                       " triangles (its fixed scratch); use rt_build for larger meshes");
+    }
+    if (morton_bits < 1 || morton_bits > 21) { return fail(RT_E_INVALID, "morton_bits must be in 1..21"); }
+    int dev = 0;
+    RT_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) { return fail(RT_E_INVALID, "device index out of range"); }
+    unsigned char* base = nullptr;
+    {
+        std::lock_guard<std::mutex> lk(g_na_mu);
+        if (!g_na_dev[dev])
+        {
+            void* p = nullptr;
+            RT_CUDA(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+            g_na_dev[dev] = static_cast<unsigned char*>(p);
+        }
+        base = g_na_dev[dev];
+    }
+    cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : default_stream();
+    return (3 * morton_bits > 32) ? morton_order_noalloc_typed<uint64_t>(base, verts, n_verts, tris, n_tris, morton_bits,
+                                                                         perm_out, st)
+                                  : morton_order_noalloc_typed<uint32_t>(base, verts, n_verts, tris, n_tris, morton_bits,
+                                                                         perm_out, st);
+}

@@ -239,3 +239,48 @@ template int radix_sort_pairs<uint32_t>(uint32_t*, uint32_t*, bool, uint32_t, in
                                         uint32_t*, cudaStream_t, uint32_t**, uint32_t**);
 
 } // namespace rtb
+
+namespace rtb
+{
+
+// The same passes on caller-provided scratch (no allocation): keys_alt / vals_alt hold n
+// entries, lookback passes * tiles * 256 words, tile_counters 64 words. Used by the
+// allocation-free entry point; the sort itself is the one above.
+template <typename K>
+int radix_sort_pairs_raw(K* keys, uint32_t* vals, uint32_t n, int key_bits, const uint32_t* hist, K* keys_alt,
+                         uint32_t* vals_alt, uint32_t* lookback, uint32_t* tile_counters, uint32_t* status,
+                         cudaStream_t st, K** keys_out, uint32_t** vals_out)
+{
+    *keys_out = keys;
+    *vals_out = vals;
+    if (n == 0) { return RT_OK; }
+    const int passes = sort_passes(key_bits);
+    const uint32_t tiles = (n + RS_TILE - 1) / RS_TILE;
+    RT_CUDA(cudaMemsetAsync(lookback, 0, (size_t)passes * tiles * 256 * 4, st));
+    RT_CUDA(cudaMemsetAsync(tile_counters, 0, 64 * 4, st));
+    const size_t smem = onesweep_smem<K>();
+    RT_CUDA(cudaFuncSetAttribute(k_onesweep<K>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    K* kin = keys;
+    K* kalt = keys_alt;
+    uint32_t* vin = vals;
+    uint32_t* valt = vals_alt;
+    for (int p = 0; p < passes; p++)
+    {
+        k_onesweep<K><<<tiles, RS_BLOCK, smem, st>>>(kin, vin, p == 0 ? 1 : 0, kalt, valt, n, 8 * p, hist + 256 * p,
+                                                    tile_counters + p, lookback + (size_t)p * tiles * 256, status);
+        count_launch();
+        if (int e = check_launch("onesweep")) { return e; }
+        K* tk = kin; kin = kalt; kalt = tk;
+        uint32_t* tv = vin; vin = valt; valt = tv;
+    }
+    *keys_out = kin;
+    *vals_out = vin;
+    return RT_OK;
+}
+
+template int radix_sort_pairs_raw<uint64_t>(uint64_t*, uint32_t*, uint32_t, int, const uint32_t*, uint64_t*, uint32_t*,
+                                            uint32_t*, uint32_t*, uint32_t*, cudaStream_t, uint64_t**, uint32_t**);
+template int radix_sort_pairs_raw<uint32_t>(uint32_t*, uint32_t*, uint32_t, int, const uint32_t*, uint32_t*, uint32_t*,
+                                            uint32_t*, uint32_t*, uint32_t*, cudaStream_t, uint32_t**, uint32_t**);
+
+} // namespace rtb

@@ -68,6 +68,11 @@ template <typename K>
 int radix_sort_pairs(K* keys, uint32_t* vals, bool vals_identity, uint32_t n, int key_bits,
                      const uint32_t* hist, SortScratch& s, uint32_t* status, cudaStream_t st,
                      K** keys_out, uint32_t** vals_out);
+// The same sort on caller-provided scratch; allocates nothing.
+template <typename K>
+int radix_sort_pairs_raw(K* keys, uint32_t* vals, uint32_t n, int key_bits, const uint32_t* hist, K* keys_alt,
+                         uint32_t* vals_alt, uint32_t* lookback, uint32_t* tile_counters, uint32_t* status,
+                         cudaStream_t st, K** keys_out, uint32_t** vals_out);
 // Number of 8-bit digit passes for a key width.
 inline int sort_passes(int key_bits) { return (key_bits + 7) / 8; }
 

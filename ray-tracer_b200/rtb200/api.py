@@ -109,6 +109,7 @@ def lib():
         L.rt_version.restype = C.c_char_p
         L.rt_kernel_launches.restype = u64
         L.rt_device_sync.argtypes = [vp]
+        L.rt_morton_order_noalloc.argtypes = [vp, u32, vp, u32, u32, vp, vp]
         _lib = L
     return _lib
 
@@ -364,6 +365,24 @@ class Mesh:
         if nt:
             C.memmove(t.ctypes.data, lib().rt_mesh_triangles(self.h), nt * 12)
         return v, t
+
+
+NOALLOC_MAX_TRIS = 65536
+
+
+def morton_order_noalloc(dverts, dtris, perm_out, morton_bits: int = 21, stream=None):
+    """rt_morton_order_noalloc on torch CUDA tensors: writes the Morton-sorted original triangle
+    indices into perm_out (int32/uint32, n_tris entries) without any device allocation, for
+    callers that may not allocate while they run (see include/rt_b200.h). The tensors must be
+    contiguous: making a copy would allocate, so non-contiguous input is refused."""
+    for name, x in (("verts", dverts), ("tris", dtris), ("perm_out", perm_out)):
+        if not x.is_cuda or not x.is_contiguous():
+            raise ValueError(f"{name} must be a contiguous CUDA tensor")
+    if dtris.element_size() != 4 or perm_out.element_size() != 4 or perm_out.numel() < dtris.shape[0]:
+        raise ValueError("tris and perm_out must hold 32-bit integers, perm_out at least n_tris of them")
+    _check(lib().rt_morton_order_noalloc(_ptr(dverts), int(dverts.shape[0]), _ptr(dtris), int(dtris.shape[0]),
+                                         int(morton_bits), _ptr(perm_out), _stream_ptr(stream)))
+    return perm_out
 
 
 def bake_scene(scn_path: str, out_bvh: str | None = None, cfg: BuildCfg | str | None = None):
