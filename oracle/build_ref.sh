@@ -62,3 +62,17 @@ build_variant sah4ns   -e 's/BVH_LBVH_THRESHOLD   = 64/BVH_LBVH_THRESHOLD   = 21
                        -e 's/BVH_MAX_LEAF_SIZE    = 16/BVH_MAX_LEAF_SIZE    = 4/' \
                        -e 's/BVH_SPATIAL_EPS      = 1e-6f/BVH_SPATIAL_EPS      = 3.0e38f/' &
 wait
+
+# The reference's own unit and integration tests, read in place and compiled unchanged against
+# this repository's drop-in headers (include/bvh, include/math) and librt_b200.so: the proof that
+# code written for the reference's bake/load/trace/AABB interface builds and links against the
+# product. Outputs: oracle/_ref/tests/test_aabb, oracle/_ref/tests/test_traverse.
+LIBDIR="$HERE/../ray-tracer_b200/lib"
+if [ -f "$LIBDIR/librt_b200.so" ] && [ -f "$REF/tests/test_aabb.cpp" ]; then
+    mkdir -p "$OUT/tests"
+    for t in test_aabb test_traverse; do
+        g++ -std=c++2b -O2 -w -I"$HERE/../include/bvh" -I"$HERE/../include" "$REF/tests/$t.cpp" \
+            -L"$LIBDIR" -lrt_b200 -Wl,-rpath,'$ORIGIN/../../../ray-tracer_b200/lib' -o "$OUT/tests/$t"
+        echo "built oracle/_ref/tests/$t against librt_b200.so"
+    done
+fi

@@ -154,10 +154,18 @@ def _ptr(x):
     return x.ctypes.data_as(C.c_void_p)
 
 
-def _stream_ptr(stream):
+def _stream_ptr(stream, torch_tensors: bool = False):
+    """The stream handle for a call. None with torch tensors: torch's current stream, so the
+    work is ordered with the torch operations around it; None otherwise: the library's own
+    stream. torch reports its legacy default stream as 0, which the C ABI reads as "the
+    library's stream", so it is passed as cudaStreamLegacy (1) instead."""
     if stream is None:
-        return None
-    return C.c_void_p(int(stream.cuda_stream) if hasattr(stream, "cuda_stream") else int(stream))
+        if not torch_tensors:
+            return None
+        import torch
+        stream = torch.cuda.current_stream()
+    h = int(stream.cuda_stream) if hasattr(stream, "cuda_stream") else int(stream)
+    return C.c_void_p(h if h != 0 else 1)
 
 
 class Bvh:
@@ -176,7 +184,8 @@ class Bvh:
         verts, tris, where = _geometry(verts, tris)
         out = C.c_void_p()
         _check(lib().rt_build(_ptr(verts), int(verts.shape[0]), _ptr(tris), int(tris.shape[0]), where,
-                              C.byref(cfg) if cfg is not None else None, _stream_ptr(stream), C.byref(out)))
+                              C.byref(cfg) if cfg is not None else None, _stream_ptr(stream, where == RT_DEVICE),
+                              C.byref(out)))
         return Bvh(out)
 
     def rebuild(self, verts, tris, cfg: BuildCfg | str | None = None, stream=None):
@@ -184,7 +193,7 @@ class Bvh:
             cfg = make_cfg(cfg)
         verts, tris, where = _geometry(verts, tris)
         _check(lib().rt_rebuild(self.h, _ptr(verts), int(verts.shape[0]), _ptr(tris), int(tris.shape[0]), where,
-                                C.byref(cfg) if cfg is not None else None, _stream_ptr(stream)))
+                                C.byref(cfg) if cfg is not None else None, _stream_ptr(stream, where == RT_DEVICE)))
 
     @staticmethod
     def load(path: str) -> "Bvh":
@@ -263,7 +272,7 @@ class Bvh:
             assert rays.is_cuda and rays.dtype == torch.float32 and rays.shape[-1] == 8
             rays = rays.contiguous()
             hits = torch.empty_like(rays)
-            code = lib().rt_trace(self.h, _ptr(rays), _ptr(hits), int(rays.shape[0]), flags, _stream_ptr(stream))
+            code = lib().rt_trace(self.h, _ptr(rays), _ptr(hits), int(rays.shape[0]), flags, _stream_ptr(stream, True))
             if code not in (0, 5):
                 _check(code)
             return hits
@@ -293,8 +302,7 @@ class Bvh:
             dmot = mat_of_tri if _is_torch(mat_of_tri) else torch.from_numpy(
                 np.ascontiguousarray(mat_of_tri, np.uint32).view(np.int32)).to(dev)
         _check(lib().rt_render(self.h, C.byref(rcfg), _ptr(dm), len(mats) if mats is not None else 0, _ptr(dmot), mode,
-                               _ptr(rgb), _ptr(rgb2),
-                               _stream_ptr(stream)))
+                               _ptr(rgb), _ptr(rgb2), _stream_ptr(stream, True)))
         return rgb, rgb2
 
 
@@ -381,7 +389,7 @@ def morton_order_noalloc(dverts, dtris, perm_out, morton_bits: int = 21, stream=
     if dtris.element_size() != 4 or perm_out.element_size() != 4 or perm_out.numel() < dtris.shape[0]:
         raise ValueError("tris and perm_out must hold 32-bit integers, perm_out at least n_tris of them")
     _check(lib().rt_morton_order_noalloc(_ptr(dverts), int(dverts.shape[0]), _ptr(dtris), int(dtris.shape[0]),
-                                         int(morton_bits), _ptr(perm_out), _stream_ptr(stream)))
+                                         int(morton_bits), _ptr(perm_out), _stream_ptr(stream, True)))
     return perm_out
 
 
