@@ -117,6 +117,7 @@ static void free_bvh(rt_bvh* b)
                        &b->s.sah_scan_in, &b->s.sah_scan_out, &b->s.sah_node_ids, &b->s.sah_roots_lvl,
                        &b->s.in_verts, &b->s.in_tris };
     for (DevBuf* x : bufs) { x->release(); }
+    b->rootbuf.release();
     for (int k = 0; k < 2; k++) { b->wf_rays[k].release(); b->wf_state[k].release(); }
     b->wf_hits.release(); b->wf_acc.release(); b->wf_ctr.release();
     for (cudaEvent_t& e : b->ev)

@@ -7,14 +7,15 @@
 //  k_morton     quantisation + 3-way bit interleave (bvh_morton.cpp:19-36,61-101), and the
 //               digit histograms of every radix pass
 //  radix sort   stable onesweep LSD sort (radix_sort.cu; bvh_morton.cpp:109-159)
-//  k_karras     Karras (HPG 2012) radix tree over the sorted codes. Its split of a range whose
-//               first and last codes differ is the reference's Morton split (the first index
-//               where the highest differing bit flips, bvh_bfs.cpp:35-48,98-109)
-//  k_boundary   the reference stops splitting at <= BVH_MAX_LEAF_SIZE triangles, hands ranges of
-//               <= BVH_LBVH_THRESHOLD triangles or of identical codes to the binned SAH
-//               (bvh_bfs.cpp:30-33,79-107); this kernel finds those boundary nodes, computes
-//               their exact range boxes (computeRangeAABB, bvh_bfs.cpp:14-28) and refits the
-//               Morton-split nodes above them bottom-up with arrival counters
+//  k_climb      the binary radix tree over the sorted codes (Karras, HPG 2012), built bottom-up
+//               in one pass with every node's exact range box (Apetrei, 2014). Its split of a
+//               range whose first and last codes differ is the reference's Morton split (the
+//               first index where the highest differing bit flips, bvh_bfs.cpp:35-48,98-109),
+//               and a range box is the reference's computeRangeAABB (bvh_bfs.cpp:14-28)
+//  k_boundary   the reference stops splitting at <= BVH_MAX_LEAF_SIZE triangles and hands ranges
+//               of <= BVH_LBVH_THRESHOLD triangles or of identical codes to the binned SAH
+//               (bvh_bfs.cpp:30-33,79-107); this kernel finds those boundary nodes, marks their
+//               positions, registers SAH roots and the left-spine ranks of the kept nodes
 //  sah.cu       the binned SAH / spatial-split subtrees (bvh_sah.cpp:24-460)
 //  k_emit*      the DFS pre-order re-layout of reorderNodes / reorderTriangles
 //               (bvh_bake.cpp:75-149): a node's pre-order index is the number of nodes whose
@@ -29,6 +30,8 @@
 #include <algorithm>
 #include <cstring>
 #include <mutex>
+
+#include <cuda/atomic>
 
 namespace rtb
 {
@@ -145,21 +148,22 @@ __global__ void __launch_bounds__(BLK)
 k_morton(const float4* __restrict__ lo, const float4* __restrict__ hi, const float* __restrict__ cz, uint32_t N,
          const uint32_t* __restrict__ scene, uint32_t bits, int passes, K* __restrict__ keys, uint32_t* __restrict__ hist)
 {
+    // grid-stride: the block histograms are flushed to global memory once per block, so the
+    // launch uses a few blocks per SM rather than one block per 256 triangles
     __shared__ uint32_t h[8 * 256];
     for (int t = threadIdx.x; t < passes * 256; t += BLK) { h[t] = 0u; }
     __syncthreads();
-    const uint32_t i = blockIdx.x * BLK + threadIdx.x;
-    if (i < N)
+    float mn[3], size[3];
+    for (int k = 0; k < 3; k++)
     {
-        float mn[3], size[3];
-        for (int k = 0; k < 3; k++)
-        {
-            mn[k] = ord2f(scene[k]);
-            size[k] = ord2f(scene[3 + k]) - mn[k];
-            if (size[k] == 0.f) { size[k] = 1.f; }
-        }
-        const uint32_t qmax = (1u << bits) - 1u;
-        const float fmax = (float)qmax;
+        mn[k] = ord2f(scene[k]);
+        size[k] = ord2f(scene[3 + k]) - mn[k];
+        if (size[k] == 0.f) { size[k] = 1.f; }
+    }
+    const uint32_t qmax = (1u << bits) - 1u;
+    const float fmax = (float)qmax;
+    for (uint32_t i = blockIdx.x * BLK + threadIdx.x; i < N; i += gridDim.x * BLK)
+    {
         const float c[3] = { lo[i].w, hi[i].w, cz[i] };
         uint32_t q[3];
         for (int k = 0; k < 3; k++)
@@ -178,56 +182,8 @@ k_morton(const float4* __restrict__ lo, const float4* __restrict__ hi, const flo
     }
 }
 
-template <typename K> __device__ __forceinline__ int key_clz(K x);
-template <> __device__ __forceinline__ int key_clz<uint64_t>(uint64_t x) { return __clzll((long long)x); }
-template <> __device__ __forceinline__ int key_clz<uint32_t>(uint32_t x) { return __clz((int)x); }
-
-// Common-prefix length of keys i and j, extended by the index bits for equal keys (Karras).
-template <typename K>
-__device__ __forceinline__ int kdelta(const K* __restrict__ keys, int n, int i, int j)
-{
-    if (j < 0 || j >= n) { return -1; }
-    const K a = keys[i], b = keys[j];
-    if (a != b) { return key_clz<K>(a ^ b); }
-    return (int)(sizeof(K) * 8) + __clz(i ^ j);
-}
-
-// Karras radix tree: inner node i covers [first, last] and splits after gamma.
-// Node ids: inner 0..n-2, leaf k -> n-1+k. knode = {first, last, left, right}.
-template <typename K>
-__global__ void __launch_bounds__(BLK)
-k_karras(const K* __restrict__ keys, uint32_t n, uint4* __restrict__ knode, uint32_t* __restrict__ parent)
-{
-    const int i = (int)(blockIdx.x * BLK + threadIdx.x);
-    const int N = (int)n;
-    if (i >= N - 1) { return; }
-    const int d = (kdelta<K>(keys, N, i, i + 1) - kdelta<K>(keys, N, i, i - 1)) >= 0 ? 1 : -1;
-    const int dmin = kdelta<K>(keys, N, i, i - d);
-    int lmax = 2;
-    while (kdelta<K>(keys, N, i, i + lmax * d) > dmin) { lmax <<= 1; }
-    int l = 0;
-    for (int t = lmax >> 1; t >= 1; t >>= 1)
-    {
-        if (kdelta<K>(keys, N, i, i + (l + t) * d) > dmin) { l += t; }
-    }
-    const int j = i + l * d;
-    const int dnode = kdelta<K>(keys, N, i, j);
-    int s = 0;
-    int t = l;
-    do
-    {
-        t = (t + 1) >> 1;
-        if (kdelta<K>(keys, N, i, i + (s + t) * d) > dnode) { s += t; }
-    } while (t > 1);
-    const int gamma = i + s * d + min(d, 0);
-    const int first = min(i, j), last = max(i, j);
-    const uint32_t left = (first == gamma) ? (uint32_t)(N - 1 + gamma) : (uint32_t)gamma;
-    const uint32_t right = (last == gamma + 1) ? (uint32_t)(N - 1 + gamma + 1) : (uint32_t)(gamma + 1);
-    knode[i] = make_uint4((uint32_t)first, (uint32_t)last, left, right);
-    parent[left] = (uint32_t)i;
-    parent[right] = (uint32_t)i;
-}
-
+// Node ids of the binary radix tree: inner 0..n-2, leaf k -> n-1+k; knode = {first, last,
+// left, right} (built by k_climb below).
 template <typename K>
 __device__ __forceinline__ void krange(const uint4* __restrict__ knode, uint32_t n, uint32_t x, uint32_t& f, uint32_t& l)
 {
@@ -263,8 +219,7 @@ template <typename K>
 __global__ void __launch_bounds__(BLK)
 k_boundary(const K* __restrict__ keys, const uint32_t* __restrict__ perm, uint32_t n, const uint4* __restrict__ knode,
            const uint32_t* __restrict__ parent, const float4* __restrict__ lo, const float4* __restrict__ hi,
-           uint32_t tm, uint32_t max_leaf, float4* __restrict__ kbox, uint32_t* __restrict__ visit,
-           uint32_t* __restrict__ rank, uint32_t* __restrict__ wnode, uint32_t* __restrict__ wtri,
+           uint32_t tm, uint32_t max_leaf, float4* __restrict__ kbox, uint32_t* __restrict__ rank, uint32_t* __restrict__ wnode, uint32_t* __restrict__ wtri,
            uint8_t* __restrict__ kpos, SahRoot* __restrict__ roots, uint32_t* __restrict__ counters,
            uint32_t* __restrict__ status)
 {
@@ -297,17 +252,18 @@ k_boundary(const K* __restrict__ keys, const uint32_t* __restrict__ perm, uint32
     rank[x] = r;
     if (is_m) { return; }
 
-    // boundary node: exact range box from the triangle boxes in sorted order
+    // boundary node: its exact range box (computeRangeAABB) -- from the climb for an inner
+    // node, the triangle's own box for a single-key leaf
     const uint32_t size = l - f + 1u;
-    box3 b = box_empty();
-    for (uint32_t k = f; k <= l; k++)
+    box3 b;
+    if (x < n - 1) { b = load_box(kbox, x); }
+    else
     {
-        const uint32_t t = perm[k];
+        const uint32_t t = perm[f];
         const float4 a = lo[t], c = hi[t];
-        b.mn[0] = sse_min(b.mn[0], a.x); b.mn[1] = sse_min(b.mn[1], a.y); b.mn[2] = sse_min(b.mn[2], a.z);
-        b.mx[0] = sse_max(b.mx[0], c.x); b.mx[1] = sse_max(b.mx[1], c.y); b.mx[2] = sse_max(b.mx[2], c.z);
+        b.mn[0] = a.x; b.mn[1] = a.y; b.mn[2] = a.z; b.mx[0] = c.x; b.mx[1] = c.y; b.mx[2] = c.z;
+        store_box(kbox, x, b);
     }
-    store_box(kbox, x, b);
     if (size <= max_leaf)
     {
         wnode[f] = r + 1u;
@@ -327,21 +283,67 @@ k_boundary(const K* __restrict__ keys, const uint32_t* __restrict__ perm, uint32
         for (int k = 0; k < 3; k++) { sr.box[k] = b.mn[k]; sr.box[3 + k] = b.mx[k]; }
         roots[slot] = sr;
     }
-    // bottom-up refit of the Morton-split ancestors (second arrival computes the union)
-    cur = x;
-    p = par;
-    for (uint32_t guard = 0; p != NONE; guard++)
+}
+
+// Bottom-up construction of the binary radix tree with boxes, one thread per sorted key
+// (Apetrei, "Fast and Simple Agglomerative LBVH Construction", 2014): a node covering keys
+// [L, R] becomes a child of the split at R (right boundary) or at L-1 (left boundary),
+// whichever separates keys with the longer common prefix; the second child to arrive
+// completes the parent. Keys are extended by their index so equal codes split as in the
+// Karras tree; the tree is that same binary radix tree. Inner node p is the split between
+// keys p and p+1: it covers [L, R] with children [L, p] and [p+1, R]; its record is
+// {L, R, left id, right id} (leaf k has id n-1+k). other[p] (initially ~0) takes the first
+// arrival's outer bound and id in one exchange; its box is then in kbox (an inner node,
+// written before the release) or is its triangle's box (a leaf).
+template <typename K>
+__device__ __forceinline__ bool split_lower(const K* __restrict__ keys, uint32_t a, uint32_t b)
+{
+    const K xa = keys[a] ^ keys[a + 1], xb = keys[b] ^ keys[b + 1];
+    if (xa != xb) { return xa < xb; }
+    return (a ^ (a + 1)) < (b ^ (b + 1));
+}
+
+template <typename K>
+__global__ void __launch_bounds__(BLK)
+k_climb(const K* __restrict__ keys, const uint32_t* __restrict__ perm, uint32_t n, const float4* __restrict__ lo,
+        const float4* __restrict__ hi, uint4* __restrict__ knode, uint32_t* __restrict__ parent,
+        unsigned long long* __restrict__ other, float4* __restrict__ kbox, uint32_t* __restrict__ status)
+{
+    const uint32_t i = blockIdx.x * BLK + threadIdx.x;
+    if (i >= n || n < 2) { return; }
+    uint32_t L = i, R = i, id = n - 1 + i;
+    const uint32_t t = perm[i];
+    float4 mn = lo[t], mx = hi[t];
+    for (uint32_t guard = 0;; guard++)
     {
         if (guard > MAX_DEPTH) { atomicOr(status, ST_CAPACITY); return; }
-        __threadfence();
-        if (atomicAdd(&visit[p], 1u) == 0u) { return; }
-        const uint4 kn = knode[p];
-        box3 u = load_box(kbox, kn.z);
-        const box3 v = load_box(kbox, kn.w);
-        box_box(u, v);
-        store_box(kbox, p, u);
-        cur = p;
-        p = parent[p];
+        const bool go_right = (L == 0) || (R != n - 1 && split_lower<K>(keys, R, L - 1));
+        const uint32_t p = go_right ? R : L - 1;  // go_right: this node is p's left child
+        parent[id] = p;
+        // an inner node's box was just written: release it before the exchange; a leaf's box
+        // lives in arrays written by an earlier kernel and needs no ordering
+        if (id < n - 1) { cuda::atomic_thread_fence(cuda::memory_order_release, cuda::thread_scope_device); }
+        cuda::atomic_ref<unsigned long long, cuda::thread_scope_device> ex(other[p]);
+        const unsigned long long mine = ((unsigned long long)(go_right ? L : R) << 32) | id;
+        const unsigned long long prev = ex.exchange(mine, cuda::memory_order_relaxed);
+        if (prev == ~0ull) { return; }  // first arrival: the sibling completes p
+        const uint32_t sid = (uint32_t)prev;
+        float4 smn, smx;
+        if (sid < n - 1)
+        {
+            cuda::atomic_thread_fence(cuda::memory_order_acquire, cuda::thread_scope_device);
+            smn = __ldcg(&kbox[2 * sid]);
+            smx = __ldcg(&kbox[2 * sid + 1]);
+        }
+        else { const uint32_t st = perm[sid - (n - 1)]; smn = lo[st]; smx = hi[st]; }
+        if (go_right) { R = (uint32_t)(prev >> 32); } else { L = (uint32_t)(prev >> 32); }
+        mn = make_float4(sse_min(mn.x, smn.x), sse_min(mn.y, smn.y), sse_min(mn.z, smn.z), 0.f);
+        mx = make_float4(sse_max(mx.x, smx.x), sse_max(mx.y, smx.y), sse_max(mx.z, smx.z), 0.f);
+        knode[p] = make_uint4(L, R, go_right ? id : sid, go_right ? sid : id);
+        __stcg(&kbox[2 * p], mn);
+        __stcg(&kbox[2 * p + 1], mx);
+        id = p;
+        if (L == 0 && R == n - 1) { return; }  // the root (internal node): no parent
     }
 }
 
@@ -454,6 +456,95 @@ k_scan_apply(const uint32_t* __restrict__ in, uint32_t n, const uint32_t* __rest
     }
 }
 
+// The same scan over two arrays at once (the pre-order slot and triangle-offset weights):
+// three launches for both.
+struct Scan2
+{
+    const uint32_t* in[2];
+    uint32_t*       out[2];
+    uint32_t*       total[2];
+};
+
+__global__ void __launch_bounds__(256) k_scan2_reduce(Scan2 S, uint32_t n, uint32_t* __restrict__ part, uint32_t np)
+{
+    __shared__ uint32_t sh[9];
+    const uint32_t base = blockIdx.x * SCAN_TILE;
+    for (int a = 0; a < 2; a++)
+    {
+        uint32_t s = 0;
+        for (int j = 0; j < 8; j++)
+        {
+            const uint32_t i = base + j * 256 + threadIdx.x;
+            if (i < n) { s += S.in[a][i]; }
+        }
+        const uint32_t t = block_sum<256>(s, sh);
+        if (threadIdx.x == 0) { part[a * np + blockIdx.x] = t; }
+    }
+}
+
+__global__ void __launch_bounds__(1024) k_scan2_partials(Scan2 S, uint32_t* __restrict__ part, uint32_t np)
+{
+    __shared__ uint32_t sh[33];
+    for (int a = 0; a < 2; a++)
+    {
+        uint32_t carry = 0;
+        for (uint32_t base = 0; base < np; base += 1024)
+        {
+            const uint32_t i = base + threadIdx.x;
+            const uint32_t v = i < np ? part[a * np + i] : 0u;
+            uint32_t tot;
+            const uint32_t e = block_excl_scan<1024>(v, sh, &tot);
+            if (i < np) { part[a * np + i] = carry + e; }
+            carry += tot;
+        }
+        if (threadIdx.x == 0) { *S.total[a] = carry; }
+    }
+}
+
+__global__ void __launch_bounds__(256) k_scan2_apply(Scan2 S, uint32_t n, const uint32_t* __restrict__ part, uint32_t np)
+{
+    __shared__ uint32_t sh[9];
+    const uint32_t base = blockIdx.x * SCAN_TILE + threadIdx.x * 8;
+    for (int a = 0; a < 2; a++)
+    {
+        uint32_t v[8];
+        uint32_t s = 0;
+        for (int j = 0; j < 8; j++)
+        {
+            const uint32_t i = base + j;
+            v[j] = i < n ? S.in[a][i] : 0u;
+            s += v[j];
+        }
+        uint32_t run = part[a * np + blockIdx.x] + block_excl_scan<256>(s, sh, nullptr);
+        for (int j = 0; j < 8; j++)
+        {
+            const uint32_t i = base + j;
+            if (i < n) { S.out[a][i] = run; }
+            run += v[j];
+        }
+    }
+}
+
+// All per-build initialisation in one launch: block 0 also does k_init's work.
+__global__ void __launch_bounds__(BLK)
+k_clear(uint32_t n, uint32_t* __restrict__ parent, unsigned long long* __restrict__ visit, uint32_t* __restrict__ wnode,
+        uint32_t* __restrict__ wtri, uint8_t* __restrict__ kpos, uint32_t* __restrict__ scene, uint32_t* __restrict__ hist,
+        uint32_t* __restrict__ counters, uint32_t* __restrict__ status)
+{
+    const uint32_t i = blockIdx.x * BLK + threadIdx.x;
+    if (i < 2 * n - 1) { parent[i] = NONE; }
+    if (i < n) { visit[i] = ~0ull; kpos[i] = 0u; }
+    if (i <= n) { wnode[i] = 0u; wtri[i] = 0u; }
+    if (blockIdx.x == 0)
+    {
+        const int t = threadIdx.x;
+        if (t < 3) { scene[t] = 0xffffffffu; scene[3 + t] = 0u; }
+        for (int k = t; k < 8 * 256; k += BLK) { hist[k] = 0u; }
+        if (t < 16) { counters[t] = 0u; }
+        if (t == 0) { *status = 0u; }
+    }
+}
+
 template <typename K>
 int build_typed(rt_bvh* B, const rt_vertex* d_verts, uint32_t V, const rt_triangle* d_tris, uint32_t N,
                 const rt_build_cfg& cfg, cudaStream_t st, uint32_t cap)
@@ -466,7 +557,7 @@ int build_typed(rt_bvh* B, const rt_vertex* d_verts, uint32_t V, const rt_triang
         S.keys.ensure((size_t)N * sizeof(K)) || S.vals.ensure((size_t)N * 4) || S.hist.ensure(8 * 256 * 4) ||
         S.scene.ensure(64) || S.status.ensure(64) || S.counters.ensure(64) ||
         S.knode.ensure((size_t)std::max<uint32_t>(N - 1, 1) * 16) || S.parent.ensure((size_t)nk * 4) ||
-        S.kbox.ensure((size_t)nk * 32) || S.visit.ensure((size_t)N * 4) || S.rank.ensure((size_t)nk * 4) ||
+        S.kbox.ensure((size_t)nk * 32) || S.visit.ensure((size_t)N * 8) || S.rank.ensure((size_t)nk * 4) ||
         S.wnode.ensure((size_t)(N + 1) * 4) || S.wtri.ensure((size_t)(N + 1) * 4) ||
         S.snode.ensure((size_t)(N + 1) * 4) || S.stri.ensure((size_t)(N + 1) * 4) || S.bnd.ensure((size_t)N) ||
         S.sah_roots.ensure((size_t)N * sizeof(SahRoot)))
@@ -477,20 +568,18 @@ int build_typed(rt_bvh* B, const rt_vertex* d_verts, uint32_t V, const rt_triang
     uint32_t* counters = S.counters.as<uint32_t>();
 
     prof_mark(B, 0, st);
-    k_init<<<1, 256, 0, st>>>(S.scene.as<uint32_t>(), S.hist.as<uint32_t>(), counters, status);
+    k_clear<<<blocks_for(nk + 1), BLK, 0, st>>>(N, S.parent.as<uint32_t>(), S.visit.as<unsigned long long>(),
+                                                S.wnode.as<uint32_t>(),
+                                                S.wtri.as<uint32_t>(), S.bnd.as<uint8_t>(), S.scene.as<uint32_t>(),
+                                                S.hist.as<uint32_t>(), counters, status);
     count_launch();
-    RT_CUDA(cudaMemsetAsync(S.parent.p, 0xff, (size_t)nk * 4, st));
-    RT_CUDA(cudaMemsetAsync(S.visit.p, 0, (size_t)N * 4, st));
-    RT_CUDA(cudaMemsetAsync(S.wnode.p, 0, (size_t)(N + 1) * 4, st));
-    RT_CUDA(cudaMemsetAsync(S.wtri.p, 0, (size_t)(N + 1) * 4, st));
-    RT_CUDA(cudaMemsetAsync(S.bnd.p, 0, (size_t)N, st));
-
     k_vertices<<<blocks_for(V), BLK, 0, st>>>(d_verts, B->verts.as<rt_vertex>(), V);
     count_launch();
     k_tri_prep<<<blocks_for(N), BLK, 0, st>>>(d_tris, N, d_verts, V, S.tri_lo.as<float4>(), S.tri_hi.as<float4>(),
                                                S.tri_cz.as<float>(), S.scene.as<uint32_t>(), status);
     count_launch();
-    k_morton<K><<<blocks_for(N), BLK, 0, st>>>(S.tri_lo.as<float4>(), S.tri_hi.as<float4>(), S.tri_cz.as<float>(), N,
+    const uint32_t morton_blocks = std::min<uint32_t>(blocks_for(N), 4u * (uint32_t)device_sm_count());
+    k_morton<K><<<morton_blocks, BLK, 0, st>>>(S.tri_lo.as<float4>(), S.tri_hi.as<float4>(), S.tri_cz.as<float>(), N,
                                                S.scene.as<uint32_t>(), cfg.morton_bits, passes, S.keys.as<K>(),
                                                S.hist.as<uint32_t>());
     count_launch();
@@ -507,13 +596,15 @@ int build_typed(rt_bvh* B, const rt_vertex* d_verts, uint32_t V, const rt_triang
     prof_mark(B, 2, st);
     if (N >= 2)
     {
-        k_karras<K><<<blocks_for(N - 1), BLK, 0, st>>>(skeys, N, S.knode.as<uint4>(), S.parent.as<uint32_t>());
+        k_climb<K><<<blocks_for(N), BLK, 0, st>>>(skeys, perm, N, S.tri_lo.as<float4>(), S.tri_hi.as<float4>(),
+                                                  S.knode.as<uint4>(), S.parent.as<uint32_t>(),
+                                                  S.visit.as<unsigned long long>(), S.kbox.as<float4>(), status);
         count_launch();
     }
     const uint32_t tm = std::max(cfg.max_leaf, cfg.lbvh_threshold);
     k_boundary<K><<<blocks_for(nk), BLK, 0, st>>>(skeys, perm, N, S.knode.as<uint4>(), S.parent.as<uint32_t>(),
                                                   S.tri_lo.as<float4>(), S.tri_hi.as<float4>(), tm, cfg.max_leaf,
-                                                  S.kbox.as<float4>(), S.visit.as<uint32_t>(), S.rank.as<uint32_t>(),
+                                                  S.kbox.as<float4>(), S.rank.as<uint32_t>(),
                                                   S.wnode.as<uint32_t>(), S.wtri.as<uint32_t>(), S.bnd.as<uint8_t>(),
                                                   S.sah_roots.as<SahRoot>(), counters, status);
     count_launch();
@@ -540,8 +631,17 @@ int build_typed(rt_bvh* B, const rt_vertex* d_verts, uint32_t V, const rt_triang
     };
     // pre-order node slots and triangle offsets per start key, then the nodes and triangles
     auto emit_all = [&]() -> int {
-        if (int e = exclusive_scan_u32(S.wnode.as<uint32_t>(), S.snode.as<uint32_t>(), N + 1, counters + 4, S.scan, st)) { return e; }
-        if (int e = exclusive_scan_u32(S.wtri.as<uint32_t>(), S.stri.as<uint32_t>(), N + 1, counters + 5, S.scan, st)) { return e; }
+        {
+            const uint32_t n1 = N + 1, np = (n1 + SCAN_TILE - 1) / SCAN_TILE;
+            if (S.scan.partials.ensure((size_t)2 * np * 4)) { return RT_E_CUDA; }
+            Scan2 sc;
+            sc.in[0] = S.wnode.as<uint32_t>(); sc.out[0] = S.snode.as<uint32_t>(); sc.total[0] = counters + 4;
+            sc.in[1] = S.wtri.as<uint32_t>(); sc.out[1] = S.stri.as<uint32_t>(); sc.total[1] = counters + 5;
+            k_scan2_reduce<<<np, 256, 0, st>>>(sc, n1, S.scan.partials.as<uint32_t>(), np);
+            k_scan2_partials<<<1, 1024, 0, st>>>(sc, S.scan.partials.as<uint32_t>(), np);
+            k_scan2_apply<<<np, 256, 0, st>>>(sc, n1, S.scan.partials.as<uint32_t>(), np);
+            count_launch(3);
+        }
         k_emit<K><<<blocks_for(nk), BLK, 0, st>>>(skeys, N, S.knode.as<uint4>(), S.parent.as<uint32_t>(), tm, cfg.max_leaf,
                                                   S.kbox.as<float4>(), S.rank.as<uint32_t>(), S.snode.as<uint32_t>(),
                                                   S.stri.as<uint32_t>(), B->nodes.as<rt_bvh_node>(), 2 * cap - 1, status);
@@ -584,6 +684,9 @@ int build_typed(rt_bvh* B, const rt_vertex* d_verts, uint32_t V, const rt_triang
         prof_mark(B, 4, st);
         if (int e = emit_all()) { return e; }
         prof_mark(B, 5, st);
+        // traversal layout from the device-side counts: the build's only host round trip follows
+        if (int e = launch_traversal_layout(B, st, 2 * cap - 1, cap, counters + 4, status)) { return e; }
+        prof_mark(B, 6, st);
         RT_CUDA(cudaMemcpyAsync(res, counters, 32, cudaMemcpyDeviceToHost, st));
         RT_CUDA(cudaMemcpyAsync(&stat, status, 4, cudaMemcpyDeviceToHost, st));
         RT_CUDA(cudaStreamSynchronize(st));
@@ -641,11 +744,8 @@ int build_bvh(rt_bvh* B, const rt_vertex* d_verts, uint32_t V, const rt_triangle
     int e = (3 * cfg.morton_bits > 32) ? build_typed<uint64_t>(B, d_verts, V, d_tris, N, cfg, st, cap)
                                        : build_typed<uint32_t>(B, d_verts, V, d_tris, N, cfg, st, cap);
     if (e) { return e; }
-    e = make_traversal_layout(B, st);
-    if (e) { return e; }
     if (B->prof)
     {
-        prof_mark(B, 6, st);
         RT_CUDA(cudaEventSynchronize(B->ev[6]));
         for (int i = 0; i < 6; i++) { cudaEventElapsedTime(&B->stage_ms[i], B->ev[i], B->ev[i + 1]); }
         cudaEventElapsedTime(&B->stage_ms[6], B->ev[0], B->ev[6]);

@@ -21,6 +21,7 @@ constexpr uint32_t LB_AGG     = 1u << 30;           // tile aggregate published
 constexpr uint32_t LB_PRE     = 2u << 30;           // inclusive prefix published
 constexpr uint32_t LB_VAL     = (1u << 30) - 1u;
 constexpr uint32_t SPIN_LIMIT = 1u << 22;           // bounded wait per look-back step
+constexpr int      LB_WIN     = 32;                 // predecessors read per look-back step
 
 __device__ __forceinline__ uint32_t ld_volatile(const uint32_t* p) { return *(const volatile uint32_t*)p; }
 __device__ __forceinline__ void     st_volatile(uint32_t* p, uint32_t v) { *(volatile uint32_t*)p = v; }
@@ -60,7 +61,7 @@ __device__ __forceinline__ uint32_t block_excl_scan_256(uint32_t v, uint32_t* wa
 template <typename K>
 __global__ void __launch_bounds__(RS_BLOCK)
 k_onesweep(const K* __restrict__ kin, const uint32_t* __restrict__ vin, int vals_identity, K* __restrict__ kout,
-           uint32_t* __restrict__ vout, uint32_t n, int shift, const uint32_t* __restrict__ hist,
+           uint32_t* __restrict__ vout, uint32_t n, uint32_t tiles, int shift, const uint32_t* __restrict__ hist,
            uint32_t* __restrict__ tile_counter, uint32_t* __restrict__ lookback, uint32_t* __restrict__ status)
 {
     extern __shared__ __align__(16) unsigned char smem[];
@@ -130,37 +131,17 @@ k_onesweep(const K* __restrict__ kin, const uint32_t* __restrict__ vin, int vals
         run += c;
     }
     const uint32_t my = run;
-    // publish this tile's count at once so later tiles can proceed
-    st_volatile(&lookback[tile * 256u + d], (tile == 0 ? LB_PRE : LB_AGG) | (my & LB_VAL));
+    // publish this tile's count at once so later tiles can proceed. Status words are
+    // [tile][digit], so a block reads one predecessor's 256 words as one coalesced row.
+    uint32_t* lb = lookback + d;
+    st_volatile(&lb[(size_t)tile * 256u], (tile == 0 ? LB_PRE : LB_AGG) | (my & LB_VAL));
 
-    // decoupled look-back over earlier tiles
-    uint32_t excl = 0u;
-    if (tile > 0)
-    {
-        int p = (int)tile - 1;
-        uint32_t spins = 0u;
-        while (p >= 0)
-        {
-            const uint32_t s = ld_volatile(&lookback[(uint32_t)p * 256u + d]);
-            if ((s & ~LB_VAL) == 0u)
-            {
-                if (++spins > SPIN_LIMIT) { atomicOr(status, ST_TIMEOUT); break; }
-                continue;
-            }
-            excl += s & LB_VAL;
-            if (s & LB_PRE) { break; }
-            --p;
-        }
-        st_volatile(&lookback[tile * 256u + d], LB_PRE | ((excl + my) & LB_VAL));
-    }
-    const uint32_t hd = hist[d];
+    // scatter into shared memory in digit order; it needs only tile-local offsets, so it runs
+    // before the look-back and frees the item registers
     const uint32_t ts = block_excl_scan_256(my, s_warp_sums, nullptr);
-    const uint32_t hs = block_excl_scan_256(hd, s_warp_sums, nullptr);
+    const uint32_t hs = block_excl_scan_256(hist[d], s_warp_sums, nullptr);
     tstart[d] = ts;
-    gbase[d] = hs + excl - ts;
     __syncthreads();
-
-    // scatter into shared memory in digit order, then write out with contiguous runs
 #pragma unroll
     for (int j = 0; j < RS_IPT; j++)
     {
@@ -171,7 +152,50 @@ k_onesweep(const K* __restrict__ kin, const uint32_t* __restrict__ vin, int vals
             sv[pos] = val[j];
         }
     }
+
+    // decoupled look-back over earlier tiles: each step reads the status words of up to
+    // LB_WIN predecessors with independent loads and folds them newest first until an
+    // inclusive prefix is met. A word not yet published is waited on alone (bounded, with a
+    // short sleep), then the walk resumes there.
+    uint32_t excl = 0u;
+    if (tile > 0)
+    {
+        int p = (int)tile - 1;
+        uint32_t spins = 0u;
+        bool done = false;
+        while (!done && p >= 0)
+        {
+            uint32_t w[LB_WIN];
+#pragma unroll
+            for (int k = 0; k < LB_WIN; k++) { w[k] = (p - k >= 0) ? ld_volatile(&lb[(size_t)(p - k) * 256u]) : LB_PRE; }
+            int used = 0;
+#pragma unroll
+            for (int k = 0; k < LB_WIN; k++)
+            {
+                if (done || used != k) { continue; }
+                if ((w[k] & ~LB_VAL) == 0u) { continue; }  // not published yet: resume here
+                excl += w[k] & LB_VAL;
+                used = k + 1;
+                if (w[k] & LB_PRE) { done = true; }
+            }
+            p -= used;
+            if (!done && used == 0)
+            {
+                // wait for tile p alone
+                while ((ld_volatile(&lb[(size_t)p * 256u]) & ~LB_VAL) == 0u)
+                {
+                    if (++spins > SPIN_LIMIT) { break; }
+                    __nanosleep(32);
+                }
+                if (spins > SPIN_LIMIT) { atomicOr(status, ST_TIMEOUT); break; }
+            }
+        }
+        st_volatile(&lb[(size_t)tile * 256u], LB_PRE | ((excl + my) & LB_VAL));
+    }
+    gbase[d] = hs + excl - ts;
     __syncthreads();
+
+    // write out with contiguous runs per digit
     for (uint32_t i = threadIdx.x; i < tile_n; i += RS_BLOCK)
     {
         const K k = sk[i];
@@ -220,7 +244,7 @@ int radix_sort_pairs(K* keys, uint32_t* vals, bool vals_identity, uint32_t n, in
     uint32_t* valt = s.vals_alt.as<uint32_t>();
     for (int p = 0; p < passes; p++)
     {
-        k_onesweep<K><<<tiles, RS_BLOCK, smem, st>>>(kin, vin, (vals_identity && p == 0) ? 1 : 0, kalt, valt, n, 8 * p,
+        k_onesweep<K><<<tiles, RS_BLOCK, smem, st>>>(kin, vin, (vals_identity && p == 0) ? 1 : 0, kalt, valt, n, tiles, 8 * p,
                                                     hist + 256 * p, s.tile_counters.as<uint32_t>() + p,
                                                     s.lookback.as<uint32_t>() + (size_t)p * tiles * 256, status);
         count_launch();
@@ -266,7 +290,7 @@ int radix_sort_pairs_raw(K* keys, uint32_t* vals, uint32_t n, int key_bits, cons
     uint32_t* valt = vals_alt;
     for (int p = 0; p < passes; p++)
     {
-        k_onesweep<K><<<tiles, RS_BLOCK, smem, st>>>(kin, vin, p == 0 ? 1 : 0, kalt, valt, n, 8 * p, hist + 256 * p,
+        k_onesweep<K><<<tiles, RS_BLOCK, smem, st>>>(kin, vin, p == 0 ? 1 : 0, kalt, valt, n, tiles, 8 * p, hist + 256 * p,
                                                     tile_counters + p, lookback + (size_t)p * tiles * 256, status);
         count_launch();
         if (int e = check_launch("onesweep")) { return e; }

@@ -123,8 +123,7 @@ struct rt_bvh
     rtb::DevBuf  nodes, tris, verts, prim, gnodes, tripos;
     uint32_t     n_nodes = 0, n_tris = 0, n_verts = 0;
     bool         has_prim = false;
-    float        root_box[6];
-    uint32_t     root_ref = 0, root_cnt = 0; // traversal entry (same encoding as rt_gnode.d)
+    rtb::DevBuf  rootbuf;                   // traversal entry record (box and reference of node 0)
     uint32_t     stats[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     BuildScratch s;
     rtb::DevBuf  trace_status, trace_rays, trace_hits;
@@ -151,6 +150,10 @@ int build_bvh(rt_bvh* b, const rt_vertex* d_verts, uint32_t n_verts, const rt_tr
               const rt_build_cfg& cfg, cudaStream_t st);
 // traverse.cu: (re)creates the traversal layout from the .bvh-layout arrays on the device
 int make_traversal_layout(rt_bvh* b, cudaStream_t st);
+// The same kernels without a host synchronisation: grids sized for max_nodes / max_tris,
+// d_counts (optional) = {nodes, triangles} on the device; structure violations set *vstatus.
+int launch_traversal_layout(rt_bvh* b, cudaStream_t st, uint32_t max_nodes, uint32_t max_tris, const uint32_t* d_counts,
+                            uint32_t* vstatus);
 int trace(const rt_bvh* b, const rt_ray* d_rays, rt_hit* d_hits, uint64_t n, uint32_t flags, cudaStream_t st,
           uint32_t* d_status);
 // Launches the persistent trace kernel; n_dev (optional) holds the ray count on the device.

@@ -92,7 +92,7 @@ struct TraceCtx
     const float4*      tp;
     const rt_triangle* tris;
     const rt_vertex*   verts;
-    TraceRoot          root;
+    const TraceRoot*   root;  // device record written by the layout kernel
 };
 
 struct THit
@@ -115,9 +115,9 @@ __device__ __forceinline__ THit trace_ray(const TraceCtx& T, rtd::f3 o, rtd::f3 
     H.t = tmax; H.u = 0.f; H.v = 0.f; H.tri = 0; H.hit = false; H.overflow = false;
     float best = tmax;
     int top = 0;
-    const float troot = ray_box(o, inv, tmin, best, T.root.box[0], T.root.box[1], T.root.box[2], T.root.box[3],
-                                T.root.box[4], T.root.box[5]);
-    if (troot < best) { sref[0] = T.root.ref; scnt[0] = T.root.cnt; stn[0] = troot; top = 1; }
+    const TraceRoot R = *T.root;
+    const float troot = ray_box(o, inv, tmin, best, R.box[0], R.box[1], R.box[2], R.box[3], R.box[4], R.box[5]);
+    if (troot < best) { sref[0] = R.ref; scnt[0] = R.cnt; stn[0] = troot; top = 1; }
     uint32_t pops = 0;
     while (top > 0)
     {

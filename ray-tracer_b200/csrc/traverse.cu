@@ -31,12 +31,24 @@ constexpr int TBLK = 128;
 // Also validates the structure before any traversal may run on it: children of node i have
 // larger indices (DFS pre-order, so no cycles) inside the array, leaf ranges inside the
 // triangle array. A violation sets ST_CAPACITY and the handle is refused.
+// d_counts (optional) holds {nodes, triangles} on the device (a build that has not synchronised);
+// thread 0 also writes the traversal entry record of node 0.
 __global__ void k_make_gnodes(const rt_bvh_node* __restrict__ nodes, uint32_t n_nodes, uint32_t n_tris,
-                              rt_gnode* __restrict__ gn, uint32_t* __restrict__ status)
+                              const uint32_t* __restrict__ d_counts, rt_gnode* __restrict__ gn, TraceRoot* __restrict__ root,
+                              uint32_t* __restrict__ status)
 {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (d_counts) { n_nodes = d_counts[0]; n_tris = d_counts[1]; }
     if (i >= n_nodes) { return; }
     const rt_bvh_node nd = nodes[i];
+    if (i == 0)
+    {
+        TraceRoot r;
+        for (int k = 0; k < 3; k++) { r.box[k] = nd.bmin[k]; r.box[3 + k] = nd.bmax[k]; }
+        r.ref = nd.is_leaf ? nd.a : 0u;
+        r.cnt = nd.is_leaf ? (LEAF_BIT | nd.b) : 0u;
+        *root = r;
+    }
     if (nd.is_leaf)
     {
         if ((uint64_t)nd.a + nd.b > n_tris) { atomicOr(status, ST_CAPACITY); }
@@ -59,10 +71,11 @@ __global__ void k_make_gnodes(const rt_bvh_node* __restrict__ nodes, uint32_t n_
     gn[i] = g;
 }
 
-__global__ void k_make_tripos(const rt_triangle* __restrict__ tris, uint32_t n, const rt_vertex* __restrict__ v,
-                              float4* __restrict__ tp)
+__global__ void k_make_tripos(const rt_triangle* __restrict__ tris, uint32_t n, const uint32_t* __restrict__ d_counts,
+                              const rt_vertex* __restrict__ v, float4* __restrict__ tp)
 {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (d_counts) { n = d_counts[1]; }
     if (i >= n) { return; }
     const rt_triangle t = tris[i];
     const rt_vertex a = v[t.v[0]], b = v[t.v[1]], c = v[t.v[2]];
@@ -117,41 +130,41 @@ TraceCtx make_trace_ctx(const rt_bvh* B)
     T.tp = B->tripos.as<float4>();
     T.tris = B->tris.as<rt_triangle>();
     T.verts = B->verts.as<rt_vertex>();
-    for (int k = 0; k < 6; k++) { T.root.box[k] = B->root_box[k]; }
-    T.root.ref = B->root_ref;
-    T.root.cnt = B->root_cnt;
+    T.root = B->rootbuf.as<TraceRoot>();
     return T;
+}
+
+int launch_traversal_layout(rt_bvh* B, cudaStream_t st, uint32_t max_nodes, uint32_t max_tris, const uint32_t* d_counts,
+                            uint32_t* vstatus)
+{
+    if (B->gnodes.ensure((size_t)max_nodes * sizeof(rt_gnode)) || B->tripos.ensure((size_t)(max_tris ? max_tris : 1) * 48) ||
+        B->rootbuf.ensure(sizeof(TraceRoot)))
+    {
+        return RT_E_CUDA;
+    }
+    k_make_gnodes<<<(max_nodes + 255) / 256, 256, 0, st>>>(B->nodes.as<rt_bvh_node>(), max_nodes, max_tris, d_counts,
+                                                           B->gnodes.as<rt_gnode>(), B->rootbuf.as<TraceRoot>(), vstatus);
+    count_launch();
+    if (max_tris)
+    {
+        k_make_tripos<<<(max_tris + 255) / 256, 256, 0, st>>>(B->tris.as<rt_triangle>(), max_tris, d_counts,
+                                                              B->verts.as<rt_vertex>(), B->tripos.as<float4>());
+        count_launch();
+    }
+    return check_launch("traversal layout");
 }
 
 int make_traversal_layout(rt_bvh* B, cudaStream_t st)
 {
     if (B->n_nodes == 0) { return fail(RT_E_EMPTY, "empty BVH"); }
-    if (B->gnodes.ensure((size_t)B->n_nodes * sizeof(rt_gnode)) ||
-        B->tripos.ensure((size_t)(B->n_tris ? B->n_tris : 1) * 48) || B->trace_status.ensure(64))
-    {
-        return RT_E_CUDA;
-    }
+    if (B->trace_status.ensure(64)) { return RT_E_CUDA; }
     uint32_t* vstatus = B->trace_status.as<uint32_t>() + 12;
     RT_CUDA(cudaMemsetAsync(vstatus, 0, 4, st));
-    k_make_gnodes<<<(B->n_nodes + 255) / 256, 256, 0, st>>>(B->nodes.as<rt_bvh_node>(), B->n_nodes, B->n_tris,
-                                                            B->gnodes.as<rt_gnode>(), vstatus);
-    count_launch();
-    if (B->n_tris)
-    {
-        k_make_tripos<<<(B->n_tris + 255) / 256, 256, 0, st>>>(B->tris.as<rt_triangle>(), B->n_tris, B->verts.as<rt_vertex>(),
-                                                               B->tripos.as<float4>());
-        count_launch();
-    }
-    if (int e = check_launch("traversal layout")) { return e; }
-    rt_bvh_node root;
+    if (int e = launch_traversal_layout(B, st, B->n_nodes, B->n_tris, nullptr, vstatus)) { return e; }
     uint32_t vs = 0;
-    RT_CUDA(cudaMemcpyAsync(&root, B->nodes.p, sizeof(root), cudaMemcpyDeviceToHost, st));
     RT_CUDA(cudaMemcpyAsync(&vs, vstatus, 4, cudaMemcpyDeviceToHost, st));
     RT_CUDA(cudaStreamSynchronize(st));
     if (vs) { return fail(RT_E_FORMAT, "BVH structure check failed (child or triangle index out of range)"); }
-    for (int k = 0; k < 3; k++) { B->root_box[k] = root.bmin[k]; B->root_box[3 + k] = root.bmax[k]; }
-    if (root.is_leaf) { B->root_ref = root.a; B->root_cnt = LEAF_BIT | root.b; }
-    else { B->root_ref = 0; B->root_cnt = 0; }
     return RT_OK;
 }
 
