@@ -169,6 +169,32 @@ enum rt_render_mode { RT_RENDER_PLAIN = 0, RT_RENDER_WAVEFRONT = 1 };
 int rt_render(const rt_bvh* bvh, const rt_render_cfg* cfg, const rt_material* mats, uint32_t n_mats,
               const uint32_t* mat_of_tri, int mode, float* rgb, float* rgb2, void* stream);
 
+/* Shading inputs of the path loop, all device pointers and all optional (extension: the
+ * reference shades every surface with albedo 0.8 and has no emitters). */
+typedef struct rt_shading
+{
+    const rt_material* mats;       /* n_mats materials */
+    const uint32_t*    mat_of_tri; /* material per baked triangle (NULL: material 0; >= n_mats: the last) */
+    const float*       tri_albedo; /* RGB albedo per baked triangle (n_tris*3), replacing the material's */
+    uint32_t           n_mats;
+    uint32_t           pad;
+} rt_shading;
+
+/* rt_render with the shading record (a NULL shading is the reference's albedo 0.8). */
+int rt_render_ex(const rt_bvh* bvh, const rt_render_cfg* cfg, const rt_shading* shading, int mode, float* rgb,
+                 float* rgb2, void* stream);
+
+/* Adjoint of rt_render (no counterpart in the reference): with d_rgb = dLoss/d(rgb) (W*H*3,
+ * device), accumulates (+=) dLoss/d(albedo used at each baked triangle) into grad_albedo
+ * (n_tris*3) and dLoss/d(material emission) into grad_emission (n_mats*3); either may be
+ * NULL. Path-replay backpropagation: each sample's path is traced once for its radiance and
+ * once more, from the same counter-based random numbers, to distribute it; nothing per
+ * sample is stored. Russian-roulette probabilities are treated as constants. Geometry is
+ * held fixed. Pixels with d_rgb = 0 cost nothing. Gradient adds are FP32 atomics combined
+ * per warp first, so the low bits of the sums vary from run to run. */
+int rt_adjoint(const rt_bvh* bvh, const rt_render_cfg* cfg, const rt_shading* shading, const float* d_rgb,
+               float* grad_albedo, float* grad_emission, void* stream);
+
 /* ---- allocation-free Morton order ----
  * No counterpart in the reference. For callers that may not allocate device memory while
  * they run: a renderer re-baking deforming geometry inside its frame loop, where a cudaMalloc

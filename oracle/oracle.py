@@ -114,6 +114,8 @@ class Restatement:
         L.orc_trace.restype = u64
         L.orc_trace.argtypes = [vp, vp, u64, u32, vp, vp, vp, vp, C.c_int]
         L.orc_render.argtypes = [vp, vp, vp, vp, u32, u32, vp, vp, C.c_int]
+        L.orc_render_ex.argtypes = [vp, vp, vp, u32, vp, vp, u32, u32, vp, vp, C.c_int]
+        L.orc_adjoint.argtypes = [vp, vp, vp, u32, vp, vp, vp, vp, vp, C.c_int]
         L.orc_philox.argtypes = [u32, u32, u32, u32, u32, u32, vp]
 
     def morton(self, verts, tris, cfg: OrcCfg):
@@ -161,27 +163,49 @@ class Restatement:
         self.L.orc_free(h)
         return hit, out, tri, ctr, int(of)
 
+    @staticmethod
+    def _mats(mats, mat_of_tri):
+        if mats is None:
+            return None, None
+        arr = (OrcMaterial * len(mats))()
+        for i, m in enumerate(mats):
+            arr[i].albedo[:] = list(m["albedo"]); arr[i].emission[:] = list(m.get("emission", (0, 0, 0)))
+            arr[i].kind = int(m.get("kind", 0))
+        mot = np.ascontiguousarray(mat_of_tri, np.uint32) if mat_of_tri is not None else None
+        return arr, mot
+
+    def _handle(self, baked: Baked):
+        return self.L.orc_from_arrays(_p(baked.nodes), baked.nodes.shape[0], _p(baked.tris), baked.tris.shape[0],
+                                      _p(baked.verts), baked.verts.shape[0])
+
     def render(self, baked: Baked, rcfg: OrcRenderCfg, mats=None, mat_of_tri=None, rows=None, threads: int = 1,
-               want_sq: bool = False):
+               want_sq: bool = False, tri_albedo=None):
+        """Image rows [r0, r1) of the path loop; tri_albedo: (n_tris, 3) albedo per baked triangle."""
         W, H = rcfg.width, rcfg.height
         rgb = np.zeros((H, W, 3), np.float32)
         rgb2 = np.zeros((H, W, 3), np.float32) if want_sq else None
-        hnd = self.L.orc_from_arrays(_p(baked.nodes), baked.nodes.shape[0], _p(baked.tris), baked.tris.shape[0],
-                                     _p(baked.verts), baked.verts.shape[0])
+        hnd = self._handle(baked)
         r0, r1 = rows if rows is not None else (0, H)
-        mats_arr = None
-        if mats is not None:
-            mats_arr = (OrcMaterial * len(mats))()
-            for i, m in enumerate(mats):
-                mats_arr[i].albedo[:] = list(m["albedo"]); mats_arr[i].emission[:] = list(m.get("emission", (0, 0, 0)))
-                mats_arr[i].kind = int(m.get("kind", 0))
-            mot = np.ascontiguousarray(mat_of_tri, np.uint32)
-        else:
-            mot = None
-        self.L.orc_render(hnd, C.byref(rcfg), mats_arr if mats_arr is not None else None, _p(mot), r0, r1,
-                          _p(rgb), _p(rgb2), threads)
+        mats_arr, mot = self._mats(mats, mat_of_tri)
+        ta = np.ascontiguousarray(tri_albedo, np.float32) if tri_albedo is not None else None
+        self.L.orc_render_ex(hnd, C.byref(rcfg), mats_arr, len(mats) if mats is not None else 0, _p(mot), _p(ta),
+                             r0, r1, _p(rgb), _p(rgb2), threads)
         self.L.orc_free(hnd)
         return rgb, rgb2
+
+    def adjoint(self, baked: Baked, rcfg: OrcRenderCfg, d_rgb, mats=None, mat_of_tri=None, tri_albedo=None,
+                threads: int = 1):
+        """FP64 gradients (n_tris, 3) and (n_mats, 3) of sum(d_rgb * image)."""
+        hnd = self._handle(baked)
+        mats_arr, mot = self._mats(mats, mat_of_tri)
+        ta = np.ascontiguousarray(tri_albedo, np.float32) if tri_albedo is not None else None
+        d = np.ascontiguousarray(d_rgb, np.float32)
+        g_alb = np.zeros((baked.tris.shape[0], 3), np.float64)
+        g_em = np.zeros((len(mats), 3), np.float64) if mats is not None else None
+        self.L.orc_adjoint(hnd, C.byref(rcfg), mats_arr, len(mats) if mats is not None else 0, _p(mot), _p(ta), _p(d),
+                           _p(g_alb), _p(g_em), threads)
+        self.L.orc_free(hnd)
+        return g_alb, g_em
 
     def philox(self, c, k):
         out = np.zeros(4, np.uint32)

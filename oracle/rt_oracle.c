@@ -951,20 +951,127 @@ static inline float u01(uint32_t x) { return (float)(x >> 8) * (1.0f / 16777216.
 typedef struct
 {
     const orc_bvh* B; const orc_render_cfg* C; const orc_material* mats; const uint32_t* mot;
-    uint32_t row0, row1; float* rgb; float* rgb2;
-} render_job;
+    const float* talb; uint32_t n_mats;
+} render_ctx;
 
-static void* render_worker(void* p)
+/* One path vertex as the adjoint needs it: the triangle, its material, the albedo and
+ * emission used there and the Russian-roulette probability that divided the throughput
+ * after it (1 when roulette did not run). */
+typedef struct { uint32_t tri, mat; v3 albedo, emission; float p; } path_vtx;
+typedef struct { uint32_t n; path_vtx v[64]; int missed; v3 env; } path_rec;
+
+static void surface(const render_ctx* R, uint32_t tri, v3* albedo, v3* emission, uint32_t* kind, uint32_t* mat)
 {
-    render_job* J = (render_job*)p;
-    const orc_render_cfg* C = J->C;
-    const uint32_t W = C->width, H = C->height;
+    *albedo = mk3(0.8f, 0.8f, 0.8f);
+    *emission = mk3(0.f, 0.f, 0.f);
+    *kind = 0; *mat = 0;
+    if (R->mats)
+    {
+        uint32_t m = R->mot ? R->mot[tri] : 0u;
+        if (m >= R->n_mats) { m = R->n_mats - 1u; }
+        const orc_material* M = &R->mats[m];
+        *albedo = mk3(M->albedo[0], M->albedo[1], M->albedo[2]);
+        *emission = mk3(M->emission[0], M->emission[1], M->emission[2]);
+        *kind = M->kind; *mat = m;
+    }
+    if (R->talb) { const float* a = R->talb + 3 * (size_t)tri; *albedo = mk3(a[0], a[1], a[2]); }
+}
+
+/* primaryRay + pathTrace (src/main.cpp:69-83, 145-204) for one sample of one pixel; rec
+ * (optional) receives the vertices of the path. */
+static v3 path_sample(const render_ctx* R, uint32_t x, uint32_t y, uint32_t sidx, path_rec* rec)
+{
+    const orc_render_cfg* C = R->C;
+    const uint32_t W = C->width, H = C->height, pix = y * W + x;
     const float aspect = (float)W / (float)H;
     const v3 pos = mk3(C->cam_pos[0], C->cam_pos[1], C->cam_pos[2]);
     const v3 fwd = mk3(C->cam_fwd[0], C->cam_fwd[1], C->cam_fwd[2]);
     const v3 rgt = mk3(C->cam_right[0], C->cam_right[1], C->cam_right[2]);
     const v3 up  = mk3(C->cam_up[0], C->cam_up[1], C->cam_up[2]);
     const float th = C->tan_half_fov_y;
+    if (rec) { rec->n = 0; rec->missed = 0; }
+    uint32_t r4[4];
+    orc_philox(pix, sidx, 0u, 0u, C->seed, 0x5EEDu, r4);
+    float u = (((float)x + u01(r4[0])) / (float)W * 2.f - 1.f) * aspect;
+    float v = ((float)y + u01(r4[1])) / (float)H * 2.f - 1.f;
+    oray ray;
+    ray.o = pos;
+    ray.d = norm3(add3(add3(fwd, muls(rgt, u * th)), muls(up, v * th)));
+    ray.tmin = 1e-3f;
+    ray.tmax = INFINITY;
+    v3 tp = mk3(1.f, 1.f, 1.f), L = mk3(0.f, 0.f, 0.f);
+    for (uint32_t bounce = 0; bounce <= C->max_bounce; bounce++)
+    {
+        ohit h;
+        traverse(R->B, &ray, 0u, &h, NULL);
+        if (!h.hit)
+        {
+            v3 env;
+            if (C->env_kind == 0)
+            {
+                float t = ray.d.y * 0.5f + 0.5f;
+                env = add3(muls(mk3(1.0f, 1.0f, 1.0f), 1.f - t), muls(mk3(0.5f, 0.7f, 1.0f), t));
+            }
+            else { env = mk3(C->env_color[0], C->env_color[1], C->env_color[2]); }
+            L = add3(L, mul3(tp, env));
+            if (rec) { rec->missed = 1; rec->env = env; }
+            break;
+        }
+        v3 albedo, emission;
+        uint32_t kind, mat;
+        surface(R, h.tri, &albedo, &emission, &kind, &mat);
+        L = add3(L, mul3(tp, emission));
+        path_vtx* pv = NULL;
+        if (rec && rec->n < 64)
+        {
+            pv = &rec->v[rec->n++];
+            pv->tri = h.tri; pv->mat = mat; pv->albedo = albedo; pv->emission = emission; pv->p = 1.f;
+        }
+        orc_philox(pix, sidx, bounce + 1u, 0u, C->seed, 0x5EEDu, r4);
+        v3 wdir;
+        if (kind == 1)
+        {
+            wdir = sub3(ray.d, muls(h.n, 2.f * dot3(ray.d, h.n)));
+        }
+        else
+        {
+            /* sampleCosineHemisphere + toWorld, src/main.cpp:123-141 */
+            float u1 = u01(r4[0]), u2 = u01(r4[1]);
+            float rr = sqrtf(u1);
+            float theta = 2.f * ORC_PI * u2;
+            v3 ld = mk3(rr * cosf(theta), sqrtf(std_max(0.f, 1.f - u1)), rr * sinf(theta));
+            v3 axis = fabsf(h.n.x) < 0.9f ? mk3(1.f, 0.f, 0.f) : mk3(0.f, 1.f, 0.f);
+            v3 t = norm3(cross3(h.n, axis));
+            v3 b = cross3(h.n, t);
+            wdir = add3(add3(muls(t, ld.x), muls(h.n, ld.y)), muls(b, ld.z));
+        }
+        tp = mul3(tp, albedo);
+        if (C->rr_after >= 0 && (int32_t)bounce > C->rr_after)
+        {
+            float pr = std_max(std_max(tp.x, tp.y), tp.z);
+            if (u01(r4[2]) > pr) { break; }
+            tp = divs(tp, pr);
+            if (pv) { pv->p = pr; }
+        }
+        v3 hp = add3(ray.o, muls(ray.d, h.t));
+        ray.o = hp; ray.d = wdir; ray.tmin = 1e-4f; ray.tmax = INFINITY;
+    }
+    return L;
+}
+
+typedef struct
+{
+    const render_ctx* R;
+    uint32_t row0, row1; float* rgb; float* rgb2;
+    /* adjoint */
+    const float* dimg; double* g_alb; double* g_em;
+} render_job;
+
+static void* render_worker(void* p)
+{
+    render_job* J = (render_job*)p;
+    const orc_render_cfg* C = J->R->C;
+    const uint32_t W = C->width;
     for (uint32_t y = J->row0; y < J->row1; y++)
     {
         for (uint32_t x = 0; x < W; x++)
@@ -973,72 +1080,7 @@ static void* render_worker(void* p)
             v3 acc = mk3(0, 0, 0), acc2 = mk3(0, 0, 0);
             for (uint32_t s = 0; s < C->spp; s++)
             {
-                const uint32_t sidx = C->sample_offset + s;
-                uint32_t r4[4];
-                orc_philox(pix, sidx, 0u, 0u, C->seed, 0x5EEDu, r4);
-                /* primaryRay, src/main.cpp:69-83 */
-                float u = (((float)x + u01(r4[0])) / (float)W * 2.f - 1.f) * aspect;
-                float v = ((float)y + u01(r4[1])) / (float)H * 2.f - 1.f;
-                oray ray;
-                ray.o = pos;
-                ray.d = norm3(add3(add3(fwd, muls(rgt, u * th)), muls(up, v * th)));
-                ray.tmin = 1e-3f;
-                ray.tmax = INFINITY;
-                /* pathTrace, src/main.cpp:145-204 */
-                v3 tp = mk3(1.f, 1.f, 1.f), L = mk3(0.f, 0.f, 0.f);
-                for (uint32_t bounce = 0; bounce <= C->max_bounce; bounce++)
-                {
-                    ohit h;
-                    traverse(J->B, &ray, 0u, &h, NULL);
-                    if (!h.hit)
-                    {
-                        v3 env;
-                        if (C->env_kind == 0)
-                        {
-                            float t = ray.d.y * 0.5f + 0.5f;
-                            env = add3(muls(mk3(1.0f, 1.0f, 1.0f), 1.f - t), muls(mk3(0.5f, 0.7f, 1.0f), t));
-                        }
-                        else { env = mk3(C->env_color[0], C->env_color[1], C->env_color[2]); }
-                        L = add3(L, mul3(tp, env));
-                        break;
-                    }
-                    v3 albedo = mk3(0.8f, 0.8f, 0.8f);
-                    uint32_t kind = 0;
-                    if (J->mats)
-                    {
-                        const orc_material* m = &J->mats[J->mot[h.tri]];
-                        albedo = mk3(m->albedo[0], m->albedo[1], m->albedo[2]);
-                        kind = m->kind;
-                        L = add3(L, mul3(tp, mk3(m->emission[0], m->emission[1], m->emission[2])));
-                    }
-                    orc_philox(pix, sidx, bounce + 1u, 0u, C->seed, 0x5EEDu, r4);
-                    v3 wdir;
-                    if (kind == 1)
-                    {
-                        wdir = sub3(ray.d, muls(h.n, 2.f * dot3(ray.d, h.n)));
-                    }
-                    else
-                    {
-                        /* sampleCosineHemisphere + toWorld, src/main.cpp:123-141 */
-                        float u1 = u01(r4[0]), u2 = u01(r4[1]);
-                        float rr = sqrtf(u1);
-                        float theta = 2.f * ORC_PI * u2;
-                        v3 ld = mk3(rr * cosf(theta), sqrtf(std_max(0.f, 1.f - u1)), rr * sinf(theta));
-                        v3 axis = fabsf(h.n.x) < 0.9f ? mk3(1.f, 0.f, 0.f) : mk3(0.f, 1.f, 0.f);
-                        v3 t = norm3(cross3(h.n, axis));
-                        v3 b = cross3(h.n, t);
-                        wdir = add3(add3(muls(t, ld.x), muls(h.n, ld.y)), muls(b, ld.z));
-                    }
-                    tp = mul3(tp, albedo);
-                    if (C->rr_after >= 0 && (int32_t)bounce > C->rr_after)
-                    {
-                        float pr = std_max(std_max(tp.x, tp.y), tp.z);
-                        if (u01(r4[2]) > pr) { break; }
-                        tp = divs(tp, pr);
-                    }
-                    v3 hp = add3(ray.o, muls(ray.d, h.t));
-                    ray.o = hp; ray.d = wdir; ray.tmin = 1e-4f; ray.tmax = INFINITY;
-                }
+                const v3 L = path_sample(J->R, x, y, C->sample_offset + s, NULL);
                 acc = add3(acc, L);
                 acc2 = add3(acc2, mul3(L, L));
             }
@@ -1055,28 +1097,139 @@ static void* render_worker(void* p)
     return NULL;
 }
 
-void orc_render(const orc_bvh* B, const orc_render_cfg* C, const orc_material* mats, const uint32_t* mot,
-                uint32_t row0, uint32_t row1, float* rgb, float* rgb2, int nthreads)
+/* The adjoint from a stored path, in double precision. With w_j = albedo_j / p_j the
+ * sample's radiance is sum_i T_i E_i (+ T_n env on a miss), T_i = prod_{j<i} w_j, and the
+ * roulette probabilities p_j are held constant (they select the path, as in the forward
+ * estimator). So dL/dE(mat of vertex i) += T_i and dL/dalbedo_k += sum_{i>k} E_i prod_{j<i, j!=k} w_j
+ * / p_k: explicit products over the stored path, no replay and no division by the albedo. */
+static void* adjoint_worker(void* p)
+{
+    render_job* J = (render_job*)p;
+    const orc_render_cfg* C = J->R->C;
+    const uint32_t W = C->width;
+    path_rec rec;
+    double T[65][3];
+    for (uint32_t y = J->row0; y < J->row1; y++)
+    {
+        for (uint32_t x = 0; x < W; x++)
+        {
+            const uint32_t pix = y * W + x;
+            const float* dp = J->dimg + 3 * (size_t)pix;
+            const double dl[3] = { (double)dp[0] / C->spp, (double)dp[1] / C->spp, (double)dp[2] / C->spp };
+            if (dl[0] == 0.0 && dl[1] == 0.0 && dl[2] == 0.0) { continue; }
+            for (uint32_t s = 0; s < C->spp; s++)
+            {
+                (void)path_sample(J->R, x, y, C->sample_offset + s, &rec);
+                const uint32_t n = rec.n;
+                /* T[i] = prod_{j<i} w_j */
+                for (int c = 0; c < 3; c++) { T[0][c] = 1.0; }
+                for (uint32_t i = 0; i < n; i++)
+                {
+                    const double a[3] = { rec.v[i].albedo.x, rec.v[i].albedo.y, rec.v[i].albedo.z };
+                    for (int c = 0; c < 3; c++) { T[i + 1][c] = T[i][c] * a[c] / (double)rec.v[i].p; }
+                }
+                if (J->g_em)
+                {
+                    for (uint32_t i = 0; i < n; i++)
+                    {
+                        double* g = J->g_em + 3 * (size_t)rec.v[i].mat;
+                        for (int c = 0; c < 3; c++) { g[c] += dl[c] * T[i][c]; }
+                    }
+                }
+                if (J->g_alb)
+                {
+                    for (uint32_t k = 0; k < n; k++)
+                    {
+                        double sum[3] = { 0.0, 0.0, 0.0 };
+                        /* contributions of vertices i > k and of the environment after the last one */
+                        for (uint32_t i = k + 1; i <= n; i++)
+                        {
+                            double e[3];
+                            if (i < n) { e[0] = rec.v[i].emission.x; e[1] = rec.v[i].emission.y; e[2] = rec.v[i].emission.z; }
+                            else if (rec.missed) { e[0] = rec.env.x; e[1] = rec.env.y; e[2] = rec.env.z; }
+                            else { break; }
+                            for (int c = 0; c < 3; c++)
+                            {
+                                double w = 1.0 / (double)rec.v[k].p;
+                                for (uint32_t j = 0; j < i; j++)
+                                {
+                                    if (j == k) { continue; }
+                                    const double aj = c == 0 ? rec.v[j].albedo.x : c == 1 ? rec.v[j].albedo.y : rec.v[j].albedo.z;
+                                    w *= aj / (double)rec.v[j].p;
+                                }
+                                sum[c] += w * e[c];
+                            }
+                        }
+                        double* g = J->g_alb + 3 * (size_t)rec.v[k].tri;
+                        for (int c = 0; c < 3; c++) { g[c] += dl[c] * sum[c]; }
+                    }
+                }
+            }
+        }
+    }
+    return NULL;
+}
+
+static void run_rows(render_job* proto, uint32_t row0, uint32_t row1, int nthreads, void* (*fn)(void*),
+                     size_t n_alb, size_t n_em)
 {
     if (nthreads < 1) { nthreads = 1; }
     if (nthreads > 256) { nthreads = 256; }
-    if (row1 > C->height) { row1 = C->height; }
     if (row0 >= row1) { return; }
     uint32_t rows = row1 - row0;
     if ((uint32_t)nthreads > rows) { nthreads = (int)rows; }
     render_job jobs[256];
     pthread_t th[256];
-    /* interleave rows over threads for balance */
     uint32_t per = (rows + (uint32_t)nthreads - 1) / (uint32_t)nthreads;
     int used = 0;
     for (int t = 0; t < nthreads; t++)
     {
         uint32_t b = row0 + (uint32_t)t * per, e = b + per > row1 ? row1 : b + per;
         if (b >= e) { break; }
-        render_job J = { B, C, mats, mot, b, e, rgb, rgb2 };
+        render_job J = *proto;
+        J.row0 = b; J.row1 = e;
+        /* gradient threads accumulate privately, summed in thread order below */
+        if (fn == adjoint_worker && used > 0)
+        {
+            J.g_alb = proto->g_alb ? (double*)calloc(n_alb, sizeof(double)) : NULL;
+            J.g_em = proto->g_em ? (double*)calloc(n_em, sizeof(double)) : NULL;
+        }
         jobs[used++] = J;
     }
-    if (used == 1) { render_worker(&jobs[0]); return; }
-    for (int t = 0; t < used; t++) { pthread_create(&th[t], NULL, render_worker, &jobs[t]); }
+    if (used == 1) { fn(&jobs[0]); return; }
+    for (int t = 0; t < used; t++) { pthread_create(&th[t], NULL, fn, &jobs[t]); }
     for (int t = 0; t < used; t++) { pthread_join(th[t], NULL); }
+    if (fn == adjoint_worker)
+    {
+        for (int t = 1; t < used; t++)
+        {
+            if (jobs[t].g_alb) { for (size_t i = 0; i < n_alb; i++) { proto->g_alb[i] += jobs[t].g_alb[i]; } free(jobs[t].g_alb); }
+            if (jobs[t].g_em) { for (size_t i = 0; i < n_em; i++) { proto->g_em[i] += jobs[t].g_em[i]; } free(jobs[t].g_em); }
+        }
+    }
+}
+
+void orc_render_ex(const orc_bvh* B, const orc_render_cfg* C, const orc_material* mats, uint32_t n_mats,
+                   const uint32_t* mot, const float* tri_albedo, uint32_t row0, uint32_t row1, float* rgb, float* rgb2,
+                   int nthreads)
+{
+    if (row1 > C->height) { row1 = C->height; }
+    render_ctx R = { B, C, mats, mot, tri_albedo, n_mats };
+    render_job P = { &R, 0, 0, rgb, rgb2, NULL, NULL, NULL };
+    run_rows(&P, row0, row1, nthreads, render_worker, 0, 0);
+}
+
+void orc_render(const orc_bvh* B, const orc_render_cfg* C, const orc_material* mats, const uint32_t* mot,
+                uint32_t row0, uint32_t row1, float* rgb, float* rgb2, int nthreads)
+{
+    orc_render_ex(B, C, mats, mats ? 0xFFFFFFFFu : 0u, mot, NULL, row0, row1, rgb, rgb2, nthreads);
+}
+
+void orc_adjoint(const orc_bvh* B, const orc_render_cfg* C, const orc_material* mats, uint32_t n_mats,
+                 const uint32_t* mot, const float* tri_albedo, const float* d_rgb, double* grad_albedo,
+                 double* grad_emission, int nthreads)
+{
+    render_ctx R = { B, C, mats, mot, tri_albedo, n_mats };
+    render_job P = { &R, 0, 0, NULL, NULL, d_rgb, grad_albedo, mats ? grad_emission : NULL };
+    run_rows(&P, 0, C->height, nthreads, adjoint_worker, (size_t)B->n_tris * 3, (size_t)n_mats * 3);
 }

@@ -115,6 +115,21 @@ void orc_render(const orc_bvh* b, const orc_render_cfg* cfg, const orc_material*
                 const uint32_t* mat_of_tri, uint32_t row0, uint32_t row1, float* rgb,
                 float* rgb2, int nthreads);
 
+/* orc_render with a material count (indices >= n_mats use the last material) and an
+ * optional RGB albedo per baked triangle (tri_albedo, n_tris*3) replacing the material's. */
+void orc_render_ex(const orc_bvh* b, const orc_render_cfg* cfg, const orc_material* mats, uint32_t n_mats,
+                   const uint32_t* mat_of_tri, const float* tri_albedo, uint32_t row0, uint32_t row1,
+                   float* rgb, float* rgb2, int nthreads);
+
+/* Gradients of sum(d_rgb * image) with respect to the per-triangle albedo (grad_albedo,
+ * n_tris*3, used when tri_albedo is given or materials supply the albedo) and the material
+ * emission (grad_emission, n_mats*3), accumulated in double precision into the arrays.
+ * Each sample's path is traced once with the same arithmetic as orc_render_ex, stored
+ * (at most 64 vertices), and differentiated by explicit products over its vertices. */
+void orc_adjoint(const orc_bvh* b, const orc_render_cfg* cfg, const orc_material* mats, uint32_t n_mats,
+                 const uint32_t* mat_of_tri, const float* tri_albedo, const float* d_rgb, double* grad_albedo,
+                 double* grad_emission, int nthreads);
+
 /* Counter-based RNG shared with the device code: Philox4x32-10 (Salmon et al., SC'11). */
 void orc_philox(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3, uint32_t k0, uint32_t k1,
                 uint32_t* out4);

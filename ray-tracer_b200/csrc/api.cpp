@@ -412,7 +412,41 @@ int rt_render(const rt_bvh* b, const rt_render_cfg* cfg, const rt_material* mats
     {
         return fail(RT_E_INVALID, "mats (n_mats > 0) and mat_of_tri go together");
     }
-    return rtb::render(b, *cfg, mats, n_mats, mat_of_tri, mode, rgb, rgb2, pick(stream));
+    const rt_shading sh{ mats, mat_of_tri, nullptr, n_mats, 0u };
+    return rtb::render(b, *cfg, sh, mode, rgb, rgb2, pick(stream));
+}
+
+namespace
+{
+int check_render_args(const rt_bvh* b, const rt_render_cfg* cfg, const rt_shading* sh, rt_shading* out)
+{
+    if (!b) { return fail(RT_E_NOT_LOADED, "BVH not loaded"); }
+    if (!cfg) { return fail(RT_E_INVALID, "null argument"); }
+    if (cfg->width == 0 || cfg->height == 0 || cfg->spp == 0) { return fail(RT_E_INVALID, "empty image or spp = 0"); }
+    *out = sh ? *sh : rt_shading{ nullptr, nullptr, nullptr, 0u, 0u };
+    if ((out->mats != nullptr) != (out->n_mats > 0)) { return fail(RT_E_INVALID, "mats and n_mats > 0 go together"); }
+    if (out->mat_of_tri && !out->mats) { return fail(RT_E_INVALID, "mat_of_tri without materials"); }
+    return RT_OK;
+}
+} // namespace
+
+int rt_render_ex(const rt_bvh* b, const rt_render_cfg* cfg, const rt_shading* shading, int mode, float* rgb, float* rgb2,
+                 void* stream)
+{
+    rt_shading sh;
+    if (int e = check_render_args(b, cfg, shading, &sh)) { return e; }
+    if (!rgb) { return fail(RT_E_INVALID, "null argument"); }
+    return rtb::render(b, *cfg, sh, mode, rgb, rgb2, pick(stream));
+}
+
+int rt_adjoint(const rt_bvh* b, const rt_render_cfg* cfg, const rt_shading* shading, const float* d_rgb, float* grad_albedo,
+               float* grad_emission, void* stream)
+{
+    rt_shading sh;
+    if (int e = check_render_args(b, cfg, shading, &sh)) { return e; }
+    if (!d_rgb) { return fail(RT_E_INVALID, "null argument"); }
+    if (!grad_albedo && !grad_emission) { return RT_OK; }
+    return rtb::adjoint(b, *cfg, sh, d_rgb, grad_albedo, grad_emission, pick(stream));
 }
 
 // ---- cameras (src/main.cpp:43-66) ----

@@ -14,6 +14,14 @@
 // Random numbers: Philox4x32-10 (Salmon et al., SC'11) keyed by (seed, 0x5EED), counter
 // (pixel, sample, 0, 0) for the pixel jitter and (pixel, sample, bounce + 1, 0) for the
 // bounce's direction and Russian roulette draws.
+//
+// Adjoint (no counterpart in the reference): gradients of sum(dL/dI * I) with respect to the
+// albedo used at each triangle and each material's emission, by path-replay backpropagation
+// (Vicini, Speierer, Jakob: "Path Replay Backpropagation", SIGGRAPH 2021). Per sample, a first
+// pass computes the path's radiance L; a second pass re-traces the same path from the same
+// counter-based random numbers, and at vertex k the radiance still to come,
+// L - sum_{i<=k} T_i E_i, divided by the albedo there is dL/dalbedo_k. The RNG is recomputed,
+// not stored, so memory stays O(pixels). Russian-roulette probabilities are held constant.
 #include "trace_core.cuh"
 
 #include <algorithm>
@@ -33,7 +41,6 @@ struct RP
     float    pos[3], fwd[3], right[3], up[3];
     float    th;
     uint32_t seed, sample_offset;
-    uint32_t n_mats;
 };
 
 __device__ __forceinline__ uint4 philox(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3, uint32_t k0, uint32_t k1)
@@ -50,6 +57,40 @@ __device__ __forceinline__ uint4 philox(uint32_t c0, uint32_t c1, uint32_t c2, u
     return make_uint4(c0, c1, c2, c3);
 }
 __device__ __forceinline__ float u01(uint32_t x) { return (float)(x >> 8) * (1.0f / 16777216.0f); }
+
+// Shading inputs (all optional): materials, the material of each baked triangle, and an RGB
+// albedo per baked triangle that replaces the material's.
+struct Shade
+{
+    const rt_material* mats;
+    const uint32_t*    mot;
+    const float*       talb;
+    uint32_t           n_mats;
+};
+
+struct Surf
+{
+    f3       albedo, emission;
+    uint32_t kind, mat;
+};
+
+__device__ __forceinline__ Surf surface(const Shade& S, uint32_t tri)
+{
+    Surf r;
+    r.albedo = mk3(0.8f, 0.8f, 0.8f);
+    r.emission = mk3(0.f, 0.f, 0.f);
+    r.kind = 0; r.mat = 0;
+    if (S.mats)
+    {
+        const uint32_t m = min(S.mot ? S.mot[tri] : 0u, S.n_mats - 1u);
+        const rt_material M = S.mats[m];
+        r.albedo = mk3(M.albedo[0], M.albedo[1], M.albedo[2]);
+        r.emission = mk3(M.emission[0], M.emission[1], M.emission[2]);
+        r.kind = M.kind; r.mat = m;
+    }
+    if (S.talb) { r.albedo = mk3(S.talb[3 * tri], S.talb[3 * tri + 1], S.talb[3 * tri + 2]); }
+    return r;
+}
 
 constexpr float kPi = 3.14159265358979323846f;
 
@@ -78,23 +119,14 @@ __device__ __forceinline__ f3 environment(const RP& P, f3 d)
     return mk3(P.env[0], P.env[1], P.env[2]);
 }
 
-// One bounce at a hit (src/main.cpp:178-200): emission (extension), the next direction
-// (cosine hemisphere about the shading normal, or the mirror direction), throughput update
-// and Russian roulette. Returns false when the path is terminated by roulette.
-__device__ __forceinline__ bool scatter(const RP& P, const rt_material* mats, const uint32_t* mot, uint32_t tri, f3 n,
-                                        f3 din, uint32_t pix, uint32_t sidx, uint32_t bounce, f3& tp, f3& L, f3& dout)
+// One bounce at a hit (src/main.cpp:178-200) after the emission of the surface was added:
+// the next direction (cosine hemisphere about the shading normal, or the mirror direction),
+// throughput update and Russian roulette. Returns false when roulette ends the path.
+__device__ __forceinline__ bool scatter(const RP& P, const Surf& sf, f3 n, f3 din, uint32_t pix, uint32_t sidx,
+                                        uint32_t bounce, f3& tp, f3& dout)
 {
-    f3 albedo = mk3(0.8f, 0.8f, 0.8f);
-    uint32_t kind = 0;
-    if (mats)
-    {
-        const rt_material m = mats[min(mot[tri], P.n_mats - 1u)];
-        albedo = mk3(m.albedo[0], m.albedo[1], m.albedo[2]);
-        kind = m.kind;
-        L = add3(L, mul3(tp, mk3(m.emission[0], m.emission[1], m.emission[2])));
-    }
     const uint4 r = philox(pix, sidx, bounce + 1u, 0u, P.seed, 0x5EEDu);
-    if (kind == 1)
+    if (sf.kind == 1)
     {
         dout = sub3(din, muls(n, 2.f * dot3(din, n)));
     }
@@ -110,7 +142,7 @@ __device__ __forceinline__ bool scatter(const RP& P, const rt_material* mats, co
         const f3 b = cross3(n, t);
         dout = add3(add3(muls(t, ld.x), muls(n, ld.y)), muls(b, ld.z));
     }
-    tp = mul3(tp, albedo);
+    tp = mul3(tp, sf.albedo);
     if (P.rr_after >= 0 && (int32_t)bounce > P.rr_after)
     {
         const float p = std_max(std_max(tp.x, tp.y), tp.z);
@@ -120,9 +152,36 @@ __device__ __forceinline__ bool scatter(const RP& P, const rt_material* mats, co
     return true;
 }
 
+// The radiance of one sample of one pixel (primaryRay + pathTrace).
+__device__ __forceinline__ f3 path_sample(const TraceCtx& T, const RP& P, const Shade& S, uint32_t x, uint32_t y,
+                                          uint32_t pix, uint32_t sidx)
+{
+    f3 o, d;
+    primary(P, x, y, pix, sidx, o, d);
+    float tmin = 1e-3f;
+    f3 tp = mk3(1.f, 1.f, 1.f), L = mk3(0.f, 0.f, 0.f);
+    for (uint32_t bounce = 0; bounce <= P.max_bounce; bounce++)
+    {
+        const THit H = trace_ray<0>(T, o, d, tmin, bits2f(0x7f800000u));
+        if (!H.hit)
+        {
+            L = add3(L, mul3(tp, environment(P, d)));
+            break;
+        }
+        const Surf sf = surface(S, H.tri);
+        L = add3(L, mul3(tp, sf.emission));
+        const f3 n = hit_normal(T, H.tri, H.u, H.v);
+        f3 nd;
+        if (!scatter(P, sf, n, d, pix, sidx, bounce, tp, nd)) { break; }
+        o = add3(o, muls(d, H.t));
+        d = nd;
+        tmin = 1e-4f;
+    }
+    return L;
+}
+
 __global__ void __launch_bounds__(128)
-k_render_plain(TraceCtx T, RP P, const rt_material* __restrict__ mats, const uint32_t* __restrict__ mot,
-               float* __restrict__ rgb, float* __restrict__ rgb2)
+k_render_plain(TraceCtx T, RP P, Shade S, float* __restrict__ rgb, float* __restrict__ rgb2)
 {
     const uint32_t x = blockIdx.x * 16 + (threadIdx.x & 15);
     const uint32_t y = blockIdx.y * 8 + (threadIdx.x >> 4);
@@ -131,32 +190,108 @@ k_render_plain(TraceCtx T, RP P, const rt_material* __restrict__ mats, const uin
     f3 acc = mk3(0.f, 0.f, 0.f), acc2 = mk3(0.f, 0.f, 0.f);
     for (uint32_t s = 0; s < P.spp; s++)
     {
-        const uint32_t sidx = P.sample_offset + s;
-        f3 o, d;
-        primary(P, x, y, pix, sidx, o, d);
-        float tmin = 1e-3f;
-        f3 tp = mk3(1.f, 1.f, 1.f), L = mk3(0.f, 0.f, 0.f);
-        for (uint32_t bounce = 0; bounce <= P.max_bounce; bounce++)
-        {
-            const THit H = trace_ray<0>(T, o, d, tmin, bits2f(0x7f800000u));
-            if (!H.hit)
-            {
-                L = add3(L, mul3(tp, environment(P, d)));
-                break;
-            }
-            const f3 n = hit_normal(T, H.tri, H.u, H.v);
-            f3 nd;
-            if (!scatter(P, mats, mot, H.tri, n, d, pix, sidx, bounce, tp, L, nd)) { break; }
-            o = add3(o, muls(d, H.t));
-            d = nd;
-            tmin = 1e-4f;
-        }
+        const f3 L = path_sample(T, P, S, x, y, pix, P.sample_offset + s);
         acc = add3(acc, L);
         acc2 = add3(acc2, mul3(L, L));
     }
     const float fs = (float)P.spp;
     rgb[3 * pix] = acc.x / fs; rgb[3 * pix + 1] = acc.y / fs; rgb[3 * pix + 2] = acc.z / fs;
     if (rgb2) { rgb2[3 * pix] = acc2.x / fs; rgb2[3 * pix + 1] = acc2.y / fs; rgb2[3 * pix + 2] = acc2.z / fs; }
+}
+
+// dst[3 key + c] += v.c for every lane with `valid`, lanes of the warp with equal keys summed
+// first so each distinct key costs one set of atomics per warp. All 32 lanes must call it.
+__device__ __forceinline__ void warp_add3(float* __restrict__ dst, uint32_t key, bool valid, f3 v)
+{
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t k = valid ? key : 0xFFFFFFFFu;
+    const uint32_t peers = __match_any_sync(0xFFFFFFFFu, k);
+    bool pending = valid && __popc(peers) > 1;
+    if (valid && !pending)
+    {
+        atomicAdd(&dst[3 * (size_t)key], v.x); atomicAdd(&dst[3 * (size_t)key + 1], v.y); atomicAdd(&dst[3 * (size_t)key + 2], v.z);
+    }
+    uint32_t pend = __ballot_sync(0xFFFFFFFFu, pending);
+    while (pend)
+    {
+        const int ldr = __ffs(pend) - 1;
+        const uint32_t lk = __shfl_sync(0xFFFFFFFFu, k, ldr);
+        const bool in = pending && k == lk;
+        float sx = in ? v.x : 0.f, sy = in ? v.y : 0.f, sz = in ? v.z : 0.f;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1)
+        {
+            sx += __shfl_xor_sync(0xFFFFFFFFu, sx, o);
+            sy += __shfl_xor_sync(0xFFFFFFFFu, sy, o);
+            sz += __shfl_xor_sync(0xFFFFFFFFu, sz, o);
+        }
+        if ((int)lane == ldr)
+        {
+            atomicAdd(&dst[3 * (size_t)key], sx); atomicAdd(&dst[3 * (size_t)key + 1], sy); atomicAdd(&dst[3 * (size_t)key + 2], sz);
+        }
+        if (in) { pending = false; }
+        pend = __ballot_sync(0xFFFFFFFFu, pending);
+    }
+}
+
+// Path-replay adjoint, one thread per pixel (the plain schedule). Lanes run the replay's
+// bounce loop in step so the gradient adds can be combined per warp; pixels whose dL/dI is
+// zero are skipped.
+__global__ void __launch_bounds__(128)
+k_adjoint(TraceCtx T, RP P, Shade S, const float* __restrict__ dimg, float* __restrict__ g_alb, float* __restrict__ g_em)
+{
+    const uint32_t x = blockIdx.x * 16 + (threadIdx.x & 15);
+    const uint32_t y = blockIdx.y * 8 + (threadIdx.x >> 4);
+    const bool in_img = x < P.W && y < P.H;
+    const uint32_t pix = in_img ? y * P.W + x : 0u;
+    const float fs = (float)P.spp;
+    f3 dl = mk3(0.f, 0.f, 0.f);
+    if (in_img) { dl = mk3(dimg[3 * pix] / fs, dimg[3 * pix + 1] / fs, dimg[3 * pix + 2] / fs); }
+    const bool act = in_img && (dl.x != 0.f || dl.y != 0.f || dl.z != 0.f);
+    if (!__any_sync(0xFFFFFFFFu, act)) { return; }
+    for (uint32_t s = 0; s < P.spp; s++)
+    {
+        const uint32_t sidx = P.sample_offset + s;
+        f3 Ltot = mk3(0.f, 0.f, 0.f);
+        if (act) { Ltot = path_sample(T, P, S, x, y, pix, sidx); }
+        // replay
+        f3 o = mk3(0.f, 0.f, 0.f), d = mk3(0.f, 0.f, 1.f);
+        if (act) { primary(P, x, y, pix, sidx, o, d); }
+        float tmin = 1e-3f;
+        f3 tp = mk3(1.f, 1.f, 1.f), Ssum = mk3(0.f, 0.f, 0.f);
+        bool alive = act;
+        for (uint32_t bounce = 0; bounce <= P.max_bounce; bounce++)
+        {
+            if (!__any_sync(0xFFFFFFFFu, alive)) { break; }
+            bool hv = false;
+            uint32_t tri = 0, mat = 0;
+            f3 ga = mk3(0.f, 0.f, 0.f), ge = mk3(0.f, 0.f, 0.f);
+            if (alive)
+            {
+                const THit H = trace_ray<0>(T, o, d, tmin, bits2f(0x7f800000u));
+                if (!H.hit) { alive = false; }
+                else
+                {
+                    const Surf sf = surface(S, H.tri);
+                    hv = true; tri = H.tri; mat = sf.mat;
+                    ge = mul3(dl, tp);
+                    Ssum = add3(Ssum, mul3(tp, sf.emission));
+                    const f3 rest = sub3(Ltot, Ssum);
+                    ga = mk3(sf.albedo.x != 0.f ? dl.x * rest.x / sf.albedo.x : 0.f,
+                             sf.albedo.y != 0.f ? dl.y * rest.y / sf.albedo.y : 0.f,
+                             sf.albedo.z != 0.f ? dl.z * rest.z / sf.albedo.z : 0.f);
+                    const f3 n = hit_normal(T, H.tri, H.u, H.v);
+                    f3 nd;
+                    if (!scatter(P, sf, n, d, pix, sidx, bounce, tp, nd) || bounce >= P.max_bounce) { alive = false; }
+                    o = add3(o, muls(d, H.t));
+                    d = nd;
+                    tmin = 1e-4f;
+                }
+            }
+            if (g_alb) { warp_add3(g_alb, tri, hv, ga); }
+            if (g_em) { warp_add3(g_em, mat, hv && S.mats != nullptr, ge); }
+        }
+    }
 }
 
 // ---- wavefront ----
@@ -190,7 +325,7 @@ __device__ __forceinline__ void retire(float* acc, float* acc2, uint32_t pix, f3
 }
 
 __global__ void __launch_bounds__(256)
-k_wf_shade(TraceCtx T, RP P, const rt_material* __restrict__ mats, const uint32_t* __restrict__ mot, uint32_t bounce,
+k_wf_shade(TraceCtx T, RP P, Shade S, uint32_t bounce,
            const uint32_t* __restrict__ count_in, const float4* __restrict__ rays, const float4* __restrict__ state,
            const float4* __restrict__ hits, float4* __restrict__ rays_out, float4* __restrict__ state_out,
            uint32_t* __restrict__ count_out, float* __restrict__ acc, float* __restrict__ acc2)
@@ -212,8 +347,10 @@ k_wf_shade(TraceCtx T, RP P, const rt_material* __restrict__ mats, const uint32_
             continue;
         }
         const f3 nrm = mk3(h1.x, h1.y, h1.z);
+        const Surf sf = surface(S, __float_as_uint(h0.w));
+        L = add3(L, mul3(tp, sf.emission));
         f3 nd;
-        const bool alive = scatter(P, mats, mot, __float_as_uint(h0.w), nrm, d, pix, sidx, bounce, tp, L, nd);
+        const bool alive = scatter(P, sf, nrm, d, pix, sidx, bounce, tp, nd);
         if (!alive || bounce >= P.max_bounce)
         {
             retire(acc, acc2, pix, L);
@@ -255,16 +392,16 @@ RP make_rp(const rt_render_cfg& c)
 
 } // namespace
 
-int render(const rt_bvh* B, const rt_render_cfg& cfg, const rt_material* mats, uint32_t n_mats, const uint32_t* mot,
-           int mode, float* rgb, float* rgb2, cudaStream_t st)
+int render(const rt_bvh* B, const rt_render_cfg& cfg, const rt_shading& sh, int mode, float* rgb, float* rgb2,
+           cudaStream_t st)
 {
     const TraceCtx T = make_trace_ctx(B);
     RP P = make_rp(cfg);
-    P.n_mats = n_mats;
+    const Shade S{ sh.mats, sh.mat_of_tri, sh.tri_albedo, sh.n_mats };
     if (mode == RT_RENDER_PLAIN)
     {
         const dim3 grid((cfg.width + 15) / 16, (cfg.height + 7) / 8);
-        k_render_plain<<<grid, 128, 0, st>>>(T, P, mats, mot, rgb, rgb2);
+        k_render_plain<<<grid, 128, 0, st>>>(T, P, S, rgb, rgb2);
         count_launch();
         return check_launch("render plain");
     }
@@ -303,7 +440,7 @@ int render(const rt_bvh* B, const rt_render_cfg& cfg, const rt_material* mats, u
         for (uint32_t b = 0; b <= cfg.max_bounce; b++)
         {
             if (int e = trace_launch(B, Bm->wf_rays[cur].p, Bm->wf_hits.p, 0, counts + b, 0u, st, status, tctr + b)) { return e; }
-            k_wf_shade<<<sms * 8, 256, 0, st>>>(T, P, mats, mot, b, counts + b, Bm->wf_rays[cur].as<float4>(),
+            k_wf_shade<<<sms * 8, 256, 0, st>>>(T, P, S, b, counts + b, Bm->wf_rays[cur].as<float4>(),
                                                 Bm->wf_state[cur].as<float4>(), Bm->wf_hits.as<float4>(),
                                                 Bm->wf_rays[cur ^ 1].as<float4>(), Bm->wf_state[cur ^ 1].as<float4>(),
                                                 counts + b + 1, acc, acc2);
@@ -316,6 +453,18 @@ int render(const rt_bvh* B, const rt_render_cfg& cfg, const rt_material* mats, u
     k_wf_finish<<<(nv + 255) / 256, 256, 0, st>>>(acc, acc2, nv, (float)cfg.spp, rgb, rgb2);
     count_launch();
     return check_launch("wavefront finish");
+}
+
+int adjoint(const rt_bvh* B, const rt_render_cfg& cfg, const rt_shading& sh, const float* d_rgb, float* g_alb,
+            float* g_em, cudaStream_t st)
+{
+    const TraceCtx T = make_trace_ctx(B);
+    const RP P = make_rp(cfg);
+    const Shade S{ sh.mats, sh.mat_of_tri, sh.tri_albedo, sh.n_mats };
+    const dim3 grid((cfg.width + 15) / 16, (cfg.height + 7) / 8);
+    k_adjoint<<<grid, 128, 0, st>>>(T, P, S, d_rgb, g_alb, sh.mats ? g_em : nullptr);
+    count_launch();
+    return check_launch("adjoint");
 }
 
 } // namespace rtb

@@ -161,6 +161,8 @@ int trace(const rt_bvh* b, const rt_ray* d_rays, rt_hit* d_hits, uint64_t n, uin
 int trace_launch(const rt_bvh* b, const void* d_rays, void* d_hits, uint64_t n, const uint32_t* n_dev, uint32_t flags,
                  cudaStream_t st, uint32_t* d_status, unsigned long long* d_counter);
 // render.cu
-int render(const rt_bvh* b, const rt_render_cfg& cfg, const rt_material* mats, uint32_t n_mats, const uint32_t* mat_of_tri,
-           int mode, float* rgb, float* rgb2, cudaStream_t st);
+int render(const rt_bvh* b, const rt_render_cfg& cfg, const rt_shading& sh, int mode, float* rgb, float* rgb2,
+           cudaStream_t st);
+int adjoint(const rt_bvh* b, const rt_render_cfg& cfg, const rt_shading& sh, const float* d_rgb, float* g_alb, float* g_em,
+            cudaStream_t st);
 } // namespace rtb

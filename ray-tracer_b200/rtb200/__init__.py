@@ -2,8 +2,8 @@
 loop of minsuk0519/ray-tracer on a B200). See api.py."""
 from .api import (Bvh, BuildCfg, Material, Mesh, RenderCfg, RtError, PRESETS, NODE_DTYPE, HIT_DTYPE, TRACE_ANY_HIT,
                   TRACE_CLOSEST, TRACE_WATERTIGHT, RENDER_PLAIN, RENDER_WAVEFRONT, bake_scene, header_symbols,
-                  kernel_launches, last_error, lib, make_cfg, render_cfg)
+                  kernel_launches, last_error, lib, make_cfg, materials_array, render_cfg)
 
 __all__ = ["Bvh", "BuildCfg", "Material", "Mesh", "RenderCfg", "RtError", "PRESETS", "NODE_DTYPE", "HIT_DTYPE",
            "TRACE_ANY_HIT", "TRACE_CLOSEST", "TRACE_WATERTIGHT", "RENDER_PLAIN", "RENDER_WAVEFRONT", "bake_scene",
-           "header_symbols", "kernel_launches", "last_error", "lib", "make_cfg", "render_cfg"]
+           "header_symbols", "kernel_launches", "last_error", "lib", "make_cfg", "materials_array", "render_cfg"]

@@ -46,6 +46,11 @@ class Material(C.Structure):
     _fields_ = [("albedo", C.c_float * 3), ("emission", C.c_float * 3), ("kind", C.c_uint32), ("pad", C.c_uint32)]
 
 
+class Shading(C.Structure):
+    _fields_ = [("mats", C.c_void_p), ("mat_of_tri", C.c_void_p), ("tri_albedo", C.c_void_p), ("n_mats", C.c_uint32),
+                ("pad", C.c_uint32)]
+
+
 class RenderCfg(C.Structure):
     _fields_ = [("width", C.c_uint32), ("height", C.c_uint32), ("spp", C.c_uint32), ("max_bounce", C.c_uint32),
                 ("rr_after", C.c_int32), ("env_kind", C.c_uint32), ("env_color", C.c_float * 3),
@@ -92,6 +97,8 @@ def lib():
         L.rt_trace.argtypes = [vp, vp, vp, u64, u32, vp]
         L.rt_trace_host.argtypes = [vp, vp, vp, u64, u32]
         L.rt_render.argtypes = [vp, vp, vp, u32, vp, i32, vp, vp, vp]
+        L.rt_render_ex.argtypes = [vp, vp, vp, i32, vp, vp, vp]
+        L.rt_adjoint.argtypes = [vp, vp, vp, vp, vp, vp, vp]
         L.rt_camera_lookat.argtypes = [vp, vp, C.c_float, vp]
         L.rt_camera_quat.argtypes = [vp, vp, C.c_float, vp]
         L.rt_mesh_create.restype = vp
@@ -284,26 +291,74 @@ class Bvh:
         return hits
 
     def render(self, rcfg: RenderCfg, mats=None, mat_of_tri=None, mode: int = RENDER_PLAIN, want_sq: bool = False,
-               stream=None):
+               stream=None, tri_albedo=None):
         """Returns (rgb, rgb2) torch CUDA tensors (H, W, 3); mats: list of dicts or None;
-        mat_of_tri: material index per baked triangle (numpy / torch)."""
+        mat_of_tri: material index per baked triangle (numpy / torch); tri_albedo: (n_tris, 3)
+        float32 albedo per baked triangle (numpy / torch), replacing the materials' albedo."""
         import torch
-        dev = torch.device("cuda")
-        rgb = torch.empty((rcfg.height, rcfg.width, 3), dtype=torch.float32, device=dev)
+        rgb = torch.empty((rcfg.height, rcfg.width, 3), dtype=torch.float32, device="cuda")
         rgb2 = torch.empty_like(rgb) if want_sq else None
-        dm = dmot = None
-        if mats is not None:
-            arr = np.zeros((len(mats), 8), np.float32)
-            for i, m in enumerate(mats):
-                arr[i, 0:3] = m["albedo"]
-                arr[i, 3:6] = m.get("emission", (0.0, 0.0, 0.0))
-                arr[i, 6:8].view(np.uint32)[0] = int(m.get("kind", 0))
-            dm = torch.from_numpy(arr).to(dev)
-            dmot = mat_of_tri if _is_torch(mat_of_tri) else torch.from_numpy(
-                np.ascontiguousarray(mat_of_tri, np.uint32).view(np.int32)).to(dev)
-        _check(lib().rt_render(self.h, C.byref(rcfg), _ptr(dm), len(mats) if mats is not None else 0, _ptr(dmot), mode,
-                               _ptr(rgb), _ptr(rgb2), _stream_ptr(stream, True)))
+        sh, keep = _shading(mats, mat_of_tri, tri_albedo)
+        _check(lib().rt_render_ex(self.h, C.byref(rcfg), C.byref(sh), mode, _ptr(rgb), _ptr(rgb2),
+                                  _stream_ptr(stream, True)))
+        del keep
         return rgb, rgb2
+
+    def adjoint(self, rcfg: RenderCfg, d_rgb, mats=None, mat_of_tri=None, tri_albedo=None, stream=None):
+        """Path-replay adjoint of render(): d_rgb = dLoss/d(rgb) as an (H, W, 3) float32 CUDA
+        tensor. Returns (grad_albedo (n_tris, 3), grad_emission (n_mats, 3) or None) as float32
+        CUDA tensors, indexed like tri_albedo / mats."""
+        import torch
+        _, nt, _ = self.counts()
+        d_rgb = d_rgb.contiguous().to(torch.float32)
+        assert d_rgb.is_cuda and d_rgb.numel() == rcfg.width * rcfg.height * 3
+        g_alb = torch.zeros((nt, 3), dtype=torch.float32, device="cuda")
+        g_em = torch.zeros((len(mats), 3), dtype=torch.float32, device="cuda") if mats is not None else None
+        sh, keep = _shading(mats, mat_of_tri, tri_albedo)
+        _check(lib().rt_adjoint(self.h, C.byref(rcfg), C.byref(sh), _ptr(d_rgb), _ptr(g_alb), _ptr(g_em),
+                                _stream_ptr(stream, True)))
+        del keep
+        return g_alb, g_em
+
+
+def materials_array(mats) -> np.ndarray:
+    """rt_material records (n, 8) float32 from a list of dicts (albedo, emission, kind)."""
+    arr = np.zeros((len(mats), 8), np.float32)
+    for i, m in enumerate(mats):
+        arr[i, 0:3] = m["albedo"]
+        arr[i, 3:6] = m.get("emission", (0.0, 0.0, 0.0))
+        arr[i, 6:8].view(np.uint32)[0] = int(m.get("kind", 0))
+    return arr
+
+
+def _device_u32(x):
+    import torch
+    if x is None:
+        return None
+    if _is_torch(x):
+        return x.contiguous().cuda()
+    return torch.from_numpy(np.ascontiguousarray(x, np.uint32).view(np.int32)).cuda()
+
+
+def _shading(mats, mat_of_tri, tri_albedo):
+    """An rt_shading record over device copies of the inputs (kept alive by the caller)."""
+    import torch
+    sh = Shading()
+    keep = []
+    if mats is not None:
+        dm = mats.contiguous().cuda() if _is_torch(mats) else torch.from_numpy(materials_array(mats)).cuda()
+        keep.append(dm)
+        sh.mats, sh.n_mats = dm.data_ptr(), int(dm.shape[0])
+        if mat_of_tri is not None:
+            dmot = _device_u32(mat_of_tri)
+            keep.append(dmot)
+            sh.mat_of_tri = dmot.data_ptr()
+    if tri_albedo is not None:
+        ta = tri_albedo.detach() if _is_torch(tri_albedo) else torch.from_numpy(np.ascontiguousarray(tri_albedo, np.float32))
+        ta = ta.to(device="cuda", dtype=torch.float32).contiguous()
+        keep.append(ta)
+        sh.tri_albedo = ta.data_ptr()
+    return sh, keep
 
 
 def _geometry(verts, tris):

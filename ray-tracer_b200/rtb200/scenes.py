@@ -54,12 +54,13 @@ def _icosahedron():
     return v, f
 
 
-def icosphere(level: int, center=(0.0, 0.0, 0.0), radius: float = 1.0, disp: float = 0.05,
-              seed: int = BASE_SEED, max_tris: int | None = None):
-    """Displaced icosphere; outward-facing under the reference's winding convention.
+_SUBDIV = {}
 
-    ``max_tris`` keeps the first faces of the subdivided mesh (the truncation rule of the
-    50,000- and 12,500-triangle variants); unreferenced vertices are kept."""
+
+def _subdivided(level: int):
+    """Unit icosphere after ``level`` midpoint subdivisions (cached)."""
+    if level in _SUBDIV:
+        return _SUBDIV[level]
     v, f = _icosahedron()
     for _ in range(level):
         cache = {}
@@ -80,6 +81,17 @@ def icosphere(level: int, center=(0.0, 0.0, 0.0), radius: float = 1.0, disp: flo
             nf += [[a, ab, ca], [b, bc, ab], [c, ca, bc], [ab, bc, ca]]
         v = np.array(verts)
         f = np.array(nf, np.int64)
+    _SUBDIV[level] = (v, f)
+    return v, f
+
+
+def icosphere(level: int, center=(0.0, 0.0, 0.0), radius: float = 1.0, disp: float = 0.05,
+              seed: int = BASE_SEED, max_tris: int | None = None):
+    """Displaced icosphere; outward-facing under the reference's winding convention.
+
+    ``max_tris`` keeps the first faces of the subdivided mesh (the truncation rule of the
+    50,000- and 12,500-triangle variants); unreferenced vertices are kept."""
+    v, f = _subdivided(level)
     rng = np.random.default_rng(seed)
     scale = 1.0 + rng.uniform(-disp, disp, size=(v.shape[0], 1))
     p = v * scale * radius + np.asarray(center, np.float64)
@@ -179,3 +191,113 @@ def pinhole_rays(width: int, height: int, pos, target, fov_deg: float = 60.0):
     r = np.empty((width * height, 8), np.float32)
     r[:, 0:3] = pos; r[:, 3] = 1e-3; r[:, 4:7] = d.reshape(-1, 3); r[:, 7] = np.inf
     return r
+
+
+# ---- benchmark scenes ---------------------------------------------------------------------
+
+class Scene:
+    """Geometry plus shading: obj = object id per input triangle, mats = material dicts,
+    mat_of_obj = material per object, lookat = (pos, target, fov_deg)."""
+
+    def __init__(self, verts, tris, obj, mats, mat_of_obj, lookat, env_kind=1, env_color=(0.0, 0.0, 0.0)):
+        self.verts, self.tris, self.obj = verts, tris, np.asarray(obj, np.uint32)
+        self.mats, self.mat_of_obj = mats, np.asarray(mat_of_obj, np.uint32)
+        self.lookat, self.env_kind, self.env_color = lookat, env_kind, env_color
+
+    @property
+    def mat_of_tri(self):
+        """material per input triangle"""
+        return self.mat_of_obj[self.obj]
+
+    def baked_materials(self, prim_ids):
+        """material per baked triangle, from the build's original-triangle ids"""
+        return self.mat_of_tri[np.asarray(prim_ids, np.int64)]
+
+
+CORNELL_LOOKAT = ((0.0, 0.0, -3.4), (0.0, 0.0, 0.0), 40.0)
+
+
+def _cornell_parts(light_radiance=15.0):
+    """(verts, tris, obj) of the box and the light (objects 0-5) and its 6 materials."""
+    cv, ct, cid = cornell()
+    mats = [dict(albedo=(0.75, 0.75, 0.75)), dict(albedo=(0.75, 0.75, 0.75)), dict(albedo=(0.75, 0.75, 0.75)),
+            dict(albedo=(0.65, 0.1, 0.1)), dict(albedo=(0.1, 0.6, 0.15)),
+            dict(albedo=(0.0, 0.0, 0.0), emission=(light_radiance,) * 3)]
+    return cv, ct, cid, mats
+
+
+def plain_scene(seed: int = BASE_SEED, sphere_tris=None):
+    """The plain path-tracing workload: the Cornell box (5 quads and a quad light of radiance
+    15), an icosphere subdivided 5 times (20,480 triangles, vertices displaced radially by
+    uniform[-0.05, 0.05]) and two spheres of radius 0.3 from the reference's addSphere
+    (16 rings x 32 sectors), all Lambertian with albedo uniform[0.2, 0.8] per object.
+    sphere_tris: (verts, tris) of one reference sphere at the origin (rtb200.Mesh), passed in
+    so this module needs no library."""
+    cv, ct, cid, mats = _cornell_parts()
+    iv, it = icosphere(5, center=(0.15, -0.45, 0.25), radius=0.5, seed=seed)
+    parts = [(cv, ct), (iv, it)]
+    if sphere_tris is not None:
+        for c in ((-0.55, -0.7, -0.35), (0.6, -0.7, -0.5)):
+            v = sphere_tris[0].copy()
+            v[:, :3] += np.asarray(c, np.float32)
+            parts.append((v, sphere_tris[1]))
+    v, t, part = concat(parts)
+    obj = np.where(part == 0, cid[np.minimum(np.arange(t.shape[0]), ct.shape[0] - 1)], 5 + part).astype(np.uint32)
+    rng = np.random.default_rng(seed + 1)
+    n_obj = 6 + len(parts) - 1
+    for _ in range(6, n_obj):
+        a = rng.uniform(0.2, 0.8)
+        mats.append(dict(albedo=(a, a, a)))
+    # one albedo per object: the box's own walls keep their Cornell colours
+    return Scene(v, t, obj, mats, np.arange(n_obj), CORNELL_LOOKAT)
+
+
+def diff_scene(n_ico_tris: int = 50000, seed: int = BASE_SEED + 3):
+    """The differentiable-rendering workload: the Cornell box and a displaced icosphere
+    subdivided as few times as give n_ico_tris faces (6 times for 50,000) truncated to its first
+    n_ico_tris faces. Returns (Scene, init albedo, ground-truth albedo) with RGB albedos per
+    input triangle, uniform[0.2, 0.8]."""
+    cv, ct, cid, mats = _cornell_parts()
+    level = 0
+    while 20 * 4 ** level < n_ico_tris:
+        level += 1
+    iv, it = icosphere(level, center=(0.0, -0.35, 0.2), radius=0.55, seed=seed, max_tris=n_ico_tris)
+    v, t, part = concat([(cv, ct), (iv, it)])
+    obj = np.concatenate([cid, np.full(it.shape[0], 6, np.uint32)])
+    mats = mats + [dict(albedo=(0.5, 0.5, 0.5))]
+    rng = np.random.default_rng(seed + 1)
+    init = rng.uniform(0.2, 0.8, size=(t.shape[0], 3)).astype(np.float32)
+    gt = rng.uniform(0.2, 0.8, size=(t.shape[0], 3)).astype(np.float32)
+    for alb in (init, gt):      # the box keeps its colours; the light is black
+        alb[:ct.shape[0]] = np.array([mats[o]["albedo"] for o in cid], np.float32)
+    return Scene(v, t, obj, mats, np.arange(7), CORNELL_LOOKAT), init, gt
+
+
+def large_scene(n_spheres: int = 400, tris_per_sphere: int = 12500, seed: int = BASE_SEED + 4):
+    """The large-render workload: n_spheres displaced icospheres (subdivided 6 times, first
+    tris_per_sphere faces) placed uniformly in the unit box with scale log-uniform in
+    [0.01, 0.2], 80 % Lambertian (albedo uniform[0.2, 0.8]) / 20 % mirror, a floor and 4 quad
+    area lights above. Camera outside the box."""
+    rng = np.random.default_rng(seed)
+    level = 5 if tris_per_sphere <= 20480 else 6
+    parts, objs, mats = [], [], []
+    for i in range(n_spheres):
+        c = rng.uniform(0.0, 1.0, size=3)
+        r = float(np.exp(rng.uniform(np.log(0.01), np.log(0.2))))
+        v, t = icosphere(level, center=c, radius=r, seed=seed + 100 + i, max_tris=tris_per_sphere)
+        parts.append((v, t))
+        if rng.uniform() < 0.2:
+            mats.append(dict(albedo=(0.9, 0.9, 0.9), kind=1))
+        else:
+            a = rng.uniform(0.2, 0.8, size=3)
+            mats.append(dict(albedo=tuple(float(x) for x in a)))
+    fv, ft = quad((-1.0, -0.05, -1.0), (2.0, -0.05, -1.0), (2.0, -0.05, 2.0), (-1.0, -0.05, 2.0), (0, 1, 0))
+    parts.append((fv, ft)); mats.append(dict(albedo=(0.6, 0.6, 0.6)))
+    for k, (lx, lz) in enumerate(((0.15, 0.15), (0.85, 0.15), (0.15, 0.85), (0.85, 0.85))):
+        lv, lt = quad((lx - 0.1, 1.6, lz - 0.1), (lx + 0.1, 1.6, lz - 0.1), (lx + 0.1, 1.6, lz + 0.1),
+                      (lx - 0.1, 1.6, lz + 0.1), (0, -1, 0))
+        parts.append((lv, lt))
+        mats.append(dict(albedo=(0.0, 0.0, 0.0), emission=(20.0, 18.0 + 2 * k, 16.0)))
+    v, t, part = concat(parts)
+    return Scene(v, t, part, mats, np.arange(len(parts)), ((0.5, 0.9, -1.6), (0.5, 0.35, 0.5), 45.0),
+                 env_kind=1, env_color=(0.02, 0.02, 0.03))
