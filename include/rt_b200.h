@@ -147,7 +147,8 @@ typedef struct rt_render_cfg
     uint32_t width, height, spp;
     uint32_t max_bounce;    /* bounce = 0..max_bounce inclusive (main.cpp:155; reference 8) */
     int32_t  rr_after;      /* Russian roulette when bounce > rr_after (reference 2); < 0 disables */
-    uint32_t env_kind;      /* 0 sky gradient (main.cpp:167-173), 1 constant env_color */
+    uint32_t env_kind;      /* 0 sky gradient (main.cpp:167-173), 1 constant env_color,
+                               2 the shading's equirectangular map (IBL::sample, main.cpp:107-117) */
     float    env_color[3];
     float    cam_pos[3], cam_fwd[3], cam_right[3], cam_up[3];
     float    tan_half_fov_y;
@@ -176,7 +177,9 @@ typedef struct rt_shading
     const rt_material* mats;       /* n_mats materials */
     const uint32_t*    mat_of_tri; /* material per baked triangle (NULL: material 0; >= n_mats: the last) */
     const float*       tri_albedo; /* RGB albedo per baked triangle (n_tris*3), replacing the material's */
+    const float*       env_map;    /* RGB equirectangular environment, env_h rows of env_w (env_kind 2) */
     uint32_t           n_mats;
+    uint32_t           env_w, env_h;
     uint32_t           pad;
 } rt_shading;
 
@@ -194,6 +197,57 @@ int rt_render_ex(const rt_bvh* bvh, const rt_render_cfg* cfg, const rt_shading* 
  * per warp first, so the low bits of the sums vary from run to run. */
 int rt_adjoint(const rt_bvh* bvh, const rt_render_cfg* cfg, const rt_shading* shading, const float* d_rgb,
                float* grad_albedo, float* grad_emission, void* stream);
+
+/* ---- batched scenes (no counterpart in the reference: it bakes one scene per process) ----
+ * Many independent scenes in one handle: one build (the launches of one rt_build over all
+ * triangles, with the scene id above the Morton code bits of the sort key, so the radix tree
+ * first separates the scenes) and one wavefront render over all their pixels. Each scene's
+ * subtree, triangles and vertices are those rt_build gives for that scene alone, renumbered:
+ * node indices + the scene's root node, triangle indices + its first triangle, vertex indices
+ * + its vertex offset (rt_bvh_scenes). Spatial splits share one budget over the batch, so this
+ * identity needs that budget not to bind (always so for the LBVH presets, where the binned SAH
+ * only runs on ranges of identical Morton codes).
+ *   verts: all scenes' vertices concatenated; tris: all scenes' triangles concatenated with
+ *   vertex indices LOCAL to their scene; vert_offsets / tri_offsets: host arrays of
+ *   n_scenes + 1 ascending offsets starting at 0 (every scene needs a triangle). Key bits
+ *   3 * morton_bits + ceil(log2(n_scenes)) must not exceed 64: 30-bit codes (morton_bits 10)
+ *   take up to 1024 scenes. */
+int rt_build_batch(const void* verts, const uint32_t* vert_offsets, const void* tris, const uint32_t* tri_offsets,
+                   uint32_t n_scenes, int where, const rt_build_cfg* cfg, void* stream, rt_bvh** out);
+/* Re-builds a batch into an existing handle, reusing its device buffers. */
+int rt_rebuild_batch(rt_bvh* bvh, const void* verts, const uint32_t* vert_offsets, const void* tris,
+                     const uint32_t* tri_offsets, uint32_t n_scenes, int where, const rt_build_cfg* cfg, void* stream);
+/* n_scenes (0 for a handle from rt_build) and, if info4 is given, 4 values per scene: root
+ * node, node count of its subtree (contiguous from the root), first triangle, triangle count. */
+int rt_bvh_scenes(const rt_bvh* bvh, uint32_t* n_scenes, uint32_t* info4);
+/* Depth of the tree: inner nodes above the deepest leaf (a traversal stack of depth + 1
+ * entries never overflows). */
+int rt_bvh_depth(rt_bvh* bvh, uint32_t* depth);
+
+/* Launch parameters of the wavefront path tracer. */
+typedef struct rt_wavefront_params
+{
+    uint32_t trace_block;  /* threads per block of the persistent trace kernel (32..256) */
+    uint32_t chunk_paths;  /* paths in flight per generate/extend/shade round */
+    uint32_t stack_depth;  /* traversal stack entries: 64, or 32 when the tree is at most 31 deep */
+    uint32_t shade_block;  /* threads per block of the shade kernel */
+} rt_wavefront_params;
+
+/* Renders every scene of a batched handle in one wavefront kernel set, replayed from a CUDA
+ * graph captured on first use of a configuration. cfgs[s]: camera and seed of scene s;
+ * size, spp, bounces, roulette, background and sample offset come from cfgs[0]. shading:
+ * materials over all scenes, mat_of_tri / tri_albedo per baked triangle of the handle.
+ * rgb (rgb2 optional): n_scenes * H * W * 3 floats, scene-major (device). Scene s gets the
+ * samples that rt_render_ex of scene s alone with cfgs[s] takes (same random numbers).
+ * params NULL: the handle's tuned parameters (rt_autotune_wavefront), else defaults. A
+ * handle from rt_build renders as one scene. */
+int rt_render_batch(rt_bvh* bvh, const rt_render_cfg* cfgs, uint32_t n_scenes, const rt_shading* shading,
+                    const rt_wavefront_params* params, float* rgb, float* rgb2, void* stream);
+/* Times each candidate parameter set (trace block 64/128/256, chunk 1-8 Mi paths, stack
+ * 32/64 where the tree allows) on a one-sample render of the batch and keeps the fastest in
+ * the handle (and in *best). */
+int rt_autotune_wavefront(rt_bvh* bvh, const rt_render_cfg* cfgs, uint32_t n_scenes, const rt_shading* shading,
+                          rt_wavefront_params* best, void* stream);
 
 /* ---- allocation-free Morton order ----
  * No counterpart in the reference. For callers that may not allocate device memory while
@@ -232,6 +286,20 @@ const rt_triangle* rt_mesh_triangles(const rt_mesh* m);
 /* bvh::bakeBVH: reads the .scn, builds on the GPU, writes the .bvh (the reference writes
  * "<scene without extension>.bvh"; out_bvh NULL keeps that rule). */
 int rt_bake_scene(const char* scn_path, const char* out_bvh, const rt_build_cfg* cfg);
+
+/* ---- images and scene settings (the reference's main, src/main.cpp:87-118, 207-386) ---- */
+/* Writes rgb (w*h*3 floats, host) as a Radiance RGBE .hdr file (what stbi_write_hdr writes
+ * for the reference); flip_y != 0 writes row h-1 first (the reference's image has y = 0 at the
+ * bottom and flips before writing, main.cpp:368-376). */
+int rt_write_hdr(const char* path, const float* rgb, uint32_t w, uint32_t h, int flip_y);
+/* Reads a Radiance RGBE .hdr file (stbi_loadf for the IBL map, main.cpp:96-104): with rgb
+ * NULL only *w and *h are set; otherwise rgb receives w*h*3 floats (file row order). */
+int rt_read_hdr(const char* path, float* rgb, uint32_t* w, uint32_t* h);
+/* The settings lines of a .scn file (parseSceneConfig, main.cpp:207-285): sets cfg->width,
+ * height and the camera; copies the ibl path (empty if none) into ibl_path (ibl_cap bytes). */
+int rt_scene_config(const char* scn_path, rt_render_cfg* cfg, char* ibl_path, uint32_t ibl_cap);
+/* rt_render_ex into host memory (rgb_host: W*H*3 floats), for callers without device buffers. */
+int rt_render_host(const rt_bvh* bvh, const rt_render_cfg* cfg, const rt_shading* shading, int mode, float* rgb_host);
 
 /* ---- diagnostics ---- */
 const char* rt_last_error(void);     /* thread-local text of the last failure */

@@ -114,7 +114,7 @@ class Restatement:
         L.orc_trace.restype = u64
         L.orc_trace.argtypes = [vp, vp, u64, u32, vp, vp, vp, vp, C.c_int]
         L.orc_render.argtypes = [vp, vp, vp, vp, u32, u32, vp, vp, C.c_int]
-        L.orc_render_ex.argtypes = [vp, vp, vp, u32, vp, vp, u32, u32, vp, vp, C.c_int]
+        L.orc_render_ex.argtypes = [vp, vp, vp, u32, vp, vp, vp, u32, u32, u32, u32, vp, vp, C.c_int]
         L.orc_adjoint.argtypes = [vp, vp, vp, u32, vp, vp, vp, vp, vp, C.c_int]
         L.orc_philox.argtypes = [u32, u32, u32, u32, u32, u32, vp]
 
@@ -179,8 +179,9 @@ class Restatement:
                                       _p(baked.verts), baked.verts.shape[0])
 
     def render(self, baked: Baked, rcfg: OrcRenderCfg, mats=None, mat_of_tri=None, rows=None, threads: int = 1,
-               want_sq: bool = False, tri_albedo=None):
-        """Image rows [r0, r1) of the path loop; tri_albedo: (n_tris, 3) albedo per baked triangle."""
+               want_sq: bool = False, tri_albedo=None, env_map=None):
+        """Image rows [r0, r1) of the path loop; tri_albedo: (n_tris, 3) albedo per baked triangle;
+        env_map: (h, w, 3) equirectangular map for env_kind 2."""
         W, H = rcfg.width, rcfg.height
         rgb = np.zeros((H, W, 3), np.float32)
         rgb2 = np.zeros((H, W, 3), np.float32) if want_sq else None
@@ -188,8 +189,10 @@ class Restatement:
         r0, r1 = rows if rows is not None else (0, H)
         mats_arr, mot = self._mats(mats, mat_of_tri)
         ta = np.ascontiguousarray(tri_albedo, np.float32) if tri_albedo is not None else None
+        em = np.ascontiguousarray(env_map, np.float32) if env_map is not None else None
+        eh, ew = (em.shape[0], em.shape[1]) if em is not None else (0, 0)
         self.L.orc_render_ex(hnd, C.byref(rcfg), mats_arr, len(mats) if mats is not None else 0, _p(mot), _p(ta),
-                             r0, r1, _p(rgb), _p(rgb2), threads)
+                             _p(em), ew, eh, r0, r1, _p(rgb), _p(rgb2), threads)
         self.L.orc_free(hnd)
         return rgb, rgb2
 

@@ -952,7 +952,23 @@ typedef struct
 {
     const orc_bvh* B; const orc_render_cfg* C; const orc_material* mats; const uint32_t* mot;
     const float* talb; uint32_t n_mats;
+    const float* env_map; uint32_t env_w, env_h;
 } render_ctx;
+
+/* IBL::sample (src/main.cpp:107-117): nearest texel of an equirectangular map. */
+static v3 ibl_sample(const render_ctx* R, v3 d)
+{
+    float phi = atan2f(d.z, d.x);
+    float y = d.y < -1.f ? -1.f : (1.f < d.y ? 1.f : d.y);
+    float theta = acosf(y);
+    float u = (phi + ORC_PI) / (2.f * ORC_PI);
+    float v = theta / ORC_PI;
+    int px = (int)(u * (float)R->env_w), py = (int)(v * (float)R->env_h);
+    if (px > (int)R->env_w - 1) { px = (int)R->env_w - 1; }
+    if (py > (int)R->env_h - 1) { py = (int)R->env_h - 1; }
+    const float* p = R->env_map + ((size_t)py * R->env_w + (size_t)px) * 3;
+    return mk3(p[0], p[1], p[2]);
+}
 
 /* One path vertex as the adjoint needs it: the triangle, its material, the albedo and
  * emission used there and the Russian-roulette probability that divided the throughput
@@ -1012,6 +1028,7 @@ static v3 path_sample(const render_ctx* R, uint32_t x, uint32_t y, uint32_t sidx
                 float t = ray.d.y * 0.5f + 0.5f;
                 env = add3(muls(mk3(1.0f, 1.0f, 1.0f), 1.f - t), muls(mk3(0.5f, 0.7f, 1.0f), t));
             }
+            else if (C->env_kind == 2) { env = ibl_sample(R, ray.d); }
             else { env = mk3(C->env_color[0], C->env_color[1], C->env_color[2]); }
             L = add3(L, mul3(tp, env));
             if (rec) { rec->missed = 1; rec->env = env; }
@@ -1210,11 +1227,11 @@ static void run_rows(render_job* proto, uint32_t row0, uint32_t row1, int nthrea
 }
 
 void orc_render_ex(const orc_bvh* B, const orc_render_cfg* C, const orc_material* mats, uint32_t n_mats,
-                   const uint32_t* mot, const float* tri_albedo, uint32_t row0, uint32_t row1, float* rgb, float* rgb2,
-                   int nthreads)
+                   const uint32_t* mot, const float* tri_albedo, const float* env_map, uint32_t env_w, uint32_t env_h,
+                   uint32_t row0, uint32_t row1, float* rgb, float* rgb2, int nthreads)
 {
     if (row1 > C->height) { row1 = C->height; }
-    render_ctx R = { B, C, mats, mot, tri_albedo, n_mats };
+    render_ctx R = { B, C, mats, mot, tri_albedo, n_mats, env_map, env_w, env_h };
     render_job P = { &R, 0, 0, rgb, rgb2, NULL, NULL, NULL };
     run_rows(&P, row0, row1, nthreads, render_worker, 0, 0);
 }
@@ -1222,14 +1239,14 @@ void orc_render_ex(const orc_bvh* B, const orc_render_cfg* C, const orc_material
 void orc_render(const orc_bvh* B, const orc_render_cfg* C, const orc_material* mats, const uint32_t* mot,
                 uint32_t row0, uint32_t row1, float* rgb, float* rgb2, int nthreads)
 {
-    orc_render_ex(B, C, mats, mats ? 0xFFFFFFFFu : 0u, mot, NULL, row0, row1, rgb, rgb2, nthreads);
+    orc_render_ex(B, C, mats, mats ? 0xFFFFFFFFu : 0u, mot, NULL, NULL, 0, 0, row0, row1, rgb, rgb2, nthreads);
 }
 
 void orc_adjoint(const orc_bvh* B, const orc_render_cfg* C, const orc_material* mats, uint32_t n_mats,
                  const uint32_t* mot, const float* tri_albedo, const float* d_rgb, double* grad_albedo,
                  double* grad_emission, int nthreads)
 {
-    render_ctx R = { B, C, mats, mot, tri_albedo, n_mats };
+    render_ctx R = { B, C, mats, mot, tri_albedo, n_mats, NULL, 0, 0 };
     render_job P = { &R, 0, 0, NULL, NULL, d_rgb, grad_albedo, mats ? grad_emission : NULL };
     run_rows(&P, 0, C->height, nthreads, adjoint_worker, (size_t)B->n_tris * 3, (size_t)n_mats * 3);
 }

@@ -100,7 +100,7 @@ typedef struct orc_render_cfg
     uint32_t width, height, spp;
     uint32_t max_bounce;   /* loop runs bounce = 0..max_bounce (src/main.cpp:155) */
     int32_t  rr_after;     /* Russian roulette when bounce > rr_after; < 0 disables */
-    uint32_t env_kind;     /* 0 sky gradient (src/main.cpp:167-173), 1 constant env_color */
+    uint32_t env_kind;     /* 0 sky gradient (src/main.cpp:167-173), 1 constant env_color, 2 map (main.cpp:107-117) */
     float    env_color[3];
     float    cam_pos[3], cam_fwd[3], cam_right[3], cam_up[3];
     float    tan_half_fov_y;
@@ -115,11 +115,12 @@ void orc_render(const orc_bvh* b, const orc_render_cfg* cfg, const orc_material*
                 const uint32_t* mat_of_tri, uint32_t row0, uint32_t row1, float* rgb,
                 float* rgb2, int nthreads);
 
-/* orc_render with a material count (indices >= n_mats use the last material) and an
- * optional RGB albedo per baked triangle (tri_albedo, n_tris*3) replacing the material's. */
+/* orc_render with a material count (indices >= n_mats use the last material), an optional
+ * RGB albedo per baked triangle (tri_albedo, n_tris*3) replacing the material's, and the
+ * equirectangular environment map of env_kind 2 (env_h rows of env_w RGB texels). */
 void orc_render_ex(const orc_bvh* b, const orc_render_cfg* cfg, const orc_material* mats, uint32_t n_mats,
-                   const uint32_t* mat_of_tri, const float* tri_albedo, uint32_t row0, uint32_t row1,
-                   float* rgb, float* rgb2, int nthreads);
+                   const uint32_t* mat_of_tri, const float* tri_albedo, const float* env_map, uint32_t env_w,
+                   uint32_t env_h, uint32_t row0, uint32_t row1, float* rgb, float* rgb2, int nthreads);
 
 /* Gradients of sum(d_rgb * image) with respect to the per-triangle albedo (grad_albedo,
  * n_tris*3, used when tri_albedo is given or materials supply the albedo) and the material

@@ -115,16 +115,39 @@ static void free_bvh(rt_bvh* b)
                        &b->s.sah_roots, &b->s.sah_refs_a, &b->s.sah_refs_b, &b->s.sah_tmp, &b->s.sah_pos,
                        &b->s.sah_lvl_a, &b->s.sah_lvl_b, &b->s.sah_dec, &b->s.sah_out, &b->s.sah_leaf_refs,
                        &b->s.sah_scan_in, &b->s.sah_scan_out, &b->s.sah_node_ids, &b->s.sah_roots_lvl,
-                       &b->s.in_verts, &b->s.in_tris };
+                       &b->s.in_verts, &b->s.in_tris, &b->s.gtris, &b->s.batch_off, &b->s.sah_budget, &b->scene_info, &b->scene_roots,
+                       &b->wf_cams };
     for (DevBuf* x : bufs) { x->release(); }
     b->rootbuf.release();
-    for (int k = 0; k < 2; k++) { b->wf_rays[k].release(); b->wf_state[k].release(); }
+    for (int k = 0; k < 2; k++) { b->wf_rays[k].release(); b->wf_state[k].release(); b->wf_scene[k].release(); }
     b->wf_hits.release(); b->wf_acc.release(); b->wf_ctr.release();
+    if (b->wf_exec) { cudaGraphExecDestroy(b->wf_exec); b->wf_exec = nullptr; }
+    for (cudaEvent_t& e : b->wf_ev)
+    {
+        if (e) { cudaEventDestroy(e); e = nullptr; }
+    }
+    if (b->wf_stream) { cudaStreamDestroy(b->wf_stream); b->wf_stream = nullptr; }
     for (cudaEvent_t& e : b->ev)
     {
         if (e) { cudaEventDestroy(e); e = nullptr; }
     }
     delete b;
+}
+
+static int check_render_args(const rt_bvh* b, const rt_render_cfg* cfg, const rt_shading* sh, rt_shading* out)
+{
+    if (!b) { return fail(RT_E_NOT_LOADED, "BVH not loaded"); }
+    if (!cfg) { return fail(RT_E_INVALID, "null argument"); }
+    if (cfg->width == 0 || cfg->height == 0 || cfg->spp == 0) { return fail(RT_E_INVALID, "empty image or spp = 0"); }
+    *out = sh ? *sh : rt_shading{ nullptr, nullptr, nullptr, nullptr, 0u, 0u, 0u, 0u };
+    if ((out->mats != nullptr) != (out->n_mats > 0)) { return fail(RT_E_INVALID, "mats and n_mats > 0 go together"); }
+    if (out->mat_of_tri && !out->mats) { return fail(RT_E_INVALID, "mat_of_tri without materials"); }
+    if (cfg->env_kind > 2) { return fail(RT_E_INVALID, "env_kind must be 0, 1 or 2"); }
+    if (cfg->env_kind == 2 && (!out->env_map || out->env_w == 0 || out->env_h == 0))
+    {
+        return fail(RT_E_INVALID, "env_kind 2 needs the shading's env_map with its size");
+    }
+    return RT_OK;
 }
 
 extern "C" {
@@ -179,7 +202,107 @@ int rt_rebuild(rt_bvh* b, const void* verts, uint32_t n_verts, const void* tris,
         dt = b->s.in_tris.as<rt_triangle>();
     }
     else if (where != RT_DEVICE) { return fail(RT_E_INVALID, "where must be RT_HOST or RT_DEVICE"); }
+    b->depth = 0;
     return build_bvh(b, dv, n_verts, dt, n_tris, c, st);
+}
+
+int rt_rebuild_batch(rt_bvh* b, const void* verts, const uint32_t* vert_offsets, const void* tris, const uint32_t* tri_offsets,
+                     uint32_t n_scenes, int where, const rt_build_cfg* cfg, void* stream)
+{
+    if (!b) { return fail(RT_E_INVALID, "null handle"); }
+    if (!verts || !tris || !vert_offsets || !tri_offsets) { return fail(RT_E_INVALID, "null pointer"); }
+    if (n_scenes == 0) { return fail(RT_E_EMPTY, "no scenes"); }
+    if (vert_offsets[0] != 0 || tri_offsets[0] != 0) { return fail(RT_E_INVALID, "offsets must start at 0"); }
+    for (uint32_t s = 0; s < n_scenes; s++)
+    {
+        if (tri_offsets[s + 1] <= tri_offsets[s]) { return fail(RT_E_EMPTY, "scene " + std::to_string(s) + " has no triangles"); }
+        if (vert_offsets[s + 1] <= vert_offsets[s]) { return fail(RT_E_EMPTY, "scene " + std::to_string(s) + " has no vertices"); }
+    }
+    const uint32_t V = vert_offsets[n_scenes], N = tri_offsets[n_scenes];
+    if (int e = require_device()) { return e; }
+    rt_build_cfg c;
+    if (cfg) { c = *cfg; } else { rt_build_cfg_default(&c); }
+    cudaStream_t st = pick(stream);
+    auto bail = [&](int e) { return e; };
+    b->depth = 0;
+    const rt_vertex* dv = static_cast<const rt_vertex*>(verts);
+    const rt_triangle* dt = static_cast<const rt_triangle*>(tris);
+    if (b->s.batch_off.ensure((size_t)2 * (n_scenes + 1) * 4)) { return bail(RT_E_CUDA); }
+    uint32_t* d_toff = b->s.batch_off.as<uint32_t>();
+    uint32_t* d_voff = d_toff + (n_scenes + 1);
+    if (cudaMemcpyAsync(d_toff, tri_offsets, (size_t)(n_scenes + 1) * 4, cudaMemcpyHostToDevice, st) != cudaSuccess ||
+        cudaMemcpyAsync(d_voff, vert_offsets, (size_t)(n_scenes + 1) * 4, cudaMemcpyHostToDevice, st) != cudaSuccess)
+    {
+        return bail(fail(RT_E_CUDA, "offset upload"));
+    }
+    if (where == RT_HOST)
+    {
+        if (b->s.in_verts.ensure((size_t)V * sizeof(rt_vertex)) || b->s.in_tris.ensure((size_t)N * sizeof(rt_triangle)))
+        {
+            return bail(RT_E_CUDA);
+        }
+        if (cudaMemcpyAsync(b->s.in_verts.p, verts, (size_t)V * sizeof(rt_vertex), cudaMemcpyHostToDevice, st) != cudaSuccess ||
+            cudaMemcpyAsync(b->s.in_tris.p, tris, (size_t)N * sizeof(rt_triangle), cudaMemcpyHostToDevice, st) != cudaSuccess)
+        {
+            return bail(fail(RT_E_CUDA, "geometry upload"));
+        }
+        dv = b->s.in_verts.as<rt_vertex>();
+        dt = b->s.in_tris.as<rt_triangle>();
+    }
+    else if (where != RT_DEVICE) { return bail(fail(RT_E_INVALID, "where must be RT_HOST or RT_DEVICE")); }
+    return build_bvh_batch(b, dv, V, dt, N, c, st, n_scenes, d_toff, d_voff, tri_offsets);
+}
+
+int rt_build_batch(const void* verts, const uint32_t* vert_offsets, const void* tris, const uint32_t* tri_offsets,
+                   uint32_t n_scenes, int where, const rt_build_cfg* cfg, void* stream, rt_bvh** out)
+{
+    if (!out) { return fail(RT_E_INVALID, "null output handle"); }
+    *out = nullptr;
+    rt_bvh* b = new rt_bvh();
+    cudaGetDevice(&b->device);
+    const int e = rt_rebuild_batch(b, verts, vert_offsets, tris, tri_offsets, n_scenes, where, cfg, stream);
+    if (e) { free_bvh(b); return e; }
+    *out = b;
+    return RT_OK;
+}
+
+int rt_bvh_scenes(const rt_bvh* b, uint32_t* n_scenes, uint32_t* info4)
+{
+    if (!b) { return fail(RT_E_NOT_LOADED, "BVH not loaded"); }
+    if (n_scenes) { *n_scenes = b->n_scenes; }
+    if (info4 && b->n_scenes) { std::memcpy(info4, b->scene_info_host.data(), (size_t)b->n_scenes * 16); }
+    return RT_OK;
+}
+
+int rt_bvh_depth(rt_bvh* b, uint32_t* depth)
+{
+    if (!b) { return fail(RT_E_NOT_LOADED, "BVH not loaded"); }
+    if (!depth) { return fail(RT_E_INVALID, "null argument"); }
+    return tree_depth(b, default_stream(), depth);
+}
+
+int rt_render_batch(rt_bvh* b, const rt_render_cfg* cfgs, uint32_t n_scenes, const rt_shading* shading,
+                    const rt_wavefront_params* params, float* rgb, float* rgb2, void* stream)
+{
+    rt_shading sh;
+    if (int e = check_render_args(b, cfgs, shading, &sh)) { return e; }
+    if (!rgb) { return fail(RT_E_INVALID, "null argument"); }
+    if (n_scenes != std::max<uint32_t>(b->n_scenes, 1u)) { return fail(RT_E_INVALID, "n_scenes differs from the handle's scenes"); }
+    return rtb::render_batch(b, cfgs, n_scenes, sh, params, rgb, rgb2, pick(stream));
+}
+
+int rt_autotune_wavefront(rt_bvh* b, const rt_render_cfg* cfgs, uint32_t n_scenes, const rt_shading* shading,
+                          rt_wavefront_params* best, void* stream)
+{
+    rt_shading sh;
+    if (int e = check_render_args(b, cfgs, shading, &sh)) { return e; }
+    if (n_scenes != std::max<uint32_t>(b->n_scenes, 1u)) { return fail(RT_E_INVALID, "n_scenes differs from the handle's scenes"); }
+    DevBuf scratch;
+    if (scratch.ensure((size_t)n_scenes * cfgs[0].width * cfgs[0].height * 12)) { return RT_E_CUDA; }
+    const int e = rtb::autotune_wavefront(b, cfgs, n_scenes, sh, best, scratch.as<float>(), pick(stream));
+    cudaStreamSynchronize(pick(stream));
+    scratch.release();
+    return e;
 }
 
 int rt_build(const void* verts, uint32_t n_verts, const void* tris, uint32_t n_tris, int where, const rt_build_cfg* cfg,
@@ -412,23 +535,10 @@ int rt_render(const rt_bvh* b, const rt_render_cfg* cfg, const rt_material* mats
     {
         return fail(RT_E_INVALID, "mats (n_mats > 0) and mat_of_tri go together");
     }
-    const rt_shading sh{ mats, mat_of_tri, nullptr, n_mats, 0u };
+    const rt_shading sh{ mats, mat_of_tri, nullptr, nullptr, n_mats, 0u, 0u, 0u };
     return rtb::render(b, *cfg, sh, mode, rgb, rgb2, pick(stream));
 }
 
-namespace
-{
-int check_render_args(const rt_bvh* b, const rt_render_cfg* cfg, const rt_shading* sh, rt_shading* out)
-{
-    if (!b) { return fail(RT_E_NOT_LOADED, "BVH not loaded"); }
-    if (!cfg) { return fail(RT_E_INVALID, "null argument"); }
-    if (cfg->width == 0 || cfg->height == 0 || cfg->spp == 0) { return fail(RT_E_INVALID, "empty image or spp = 0"); }
-    *out = sh ? *sh : rt_shading{ nullptr, nullptr, nullptr, 0u, 0u };
-    if ((out->mats != nullptr) != (out->n_mats > 0)) { return fail(RT_E_INVALID, "mats and n_mats > 0 go together"); }
-    if (out->mat_of_tri && !out->mats) { return fail(RT_E_INVALID, "mat_of_tri without materials"); }
-    return RT_OK;
-}
-} // namespace
 
 int rt_render_ex(const rt_bvh* b, const rt_render_cfg* cfg, const rt_shading* shading, int mode, float* rgb, float* rgb2,
                  void* stream)
@@ -447,6 +557,72 @@ int rt_adjoint(const rt_bvh* b, const rt_render_cfg* cfg, const rt_shading* shad
     if (!d_rgb) { return fail(RT_E_INVALID, "null argument"); }
     if (!grad_albedo && !grad_emission) { return RT_OK; }
     return rtb::adjoint(b, *cfg, sh, d_rgb, grad_albedo, grad_emission, pick(stream));
+}
+
+int rt_render_host(const rt_bvh* b, const rt_render_cfg* cfg, const rt_shading* shading, int mode, float* rgb_host)
+{
+    rt_shading sh;
+    if (int e = check_render_args(b, cfg, shading, &sh)) { return e; }
+    if (!rgb_host) { return fail(RT_E_INVALID, "null argument"); }
+    const size_t bytes = (size_t)cfg->width * cfg->height * 12;
+    DevBuf out;
+    if (out.ensure(bytes)) { return RT_E_CUDA; }
+    cudaStream_t st = default_stream();
+    int e = rtb::render(b, *cfg, sh, mode, out.as<float>(), nullptr, st);
+    if (!e && (cudaMemcpyAsync(rgb_host, out.p, bytes, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+               cudaStreamSynchronize(st) != cudaSuccess))
+    {
+        e = fail(RT_E_CUDA, "render readback");
+    }
+    out.release();
+    return e;
+}
+
+int rt_write_hdr(const char* path, const float* rgb, uint32_t w, uint32_t h, int flip_y)
+{
+    if (!path || !rgb || w == 0 || h == 0) { return fail(RT_E_INVALID, "bad argument"); }
+    std::string err;
+    int e;
+    if (flip_y)
+    {
+        std::vector<float> fl((size_t)w * h * 3);
+        for (uint32_t y = 0; y < h; y++)
+        {
+            std::memcpy(&fl[(size_t)(h - 1 - y) * w * 3], rgb + (size_t)y * w * 3, (size_t)w * 12);
+        }
+        e = hg::write_hdr(path, fl.data(), w, h, err);
+    }
+    else { e = hg::write_hdr(path, rgb, w, h, err); }
+    return e ? fail(e, err) : RT_OK;
+}
+
+int rt_read_hdr(const char* path, float* rgb, uint32_t* w, uint32_t* h)
+{
+    if (!path || !w || !h) { return fail(RT_E_INVALID, "bad argument"); }
+    std::vector<float> img;
+    std::string err;
+    uint32_t ww = 0, hh = 0;
+    if (int e = hg::read_hdr(path, img, ww, hh, err)) { return fail(e, err); }
+    *w = ww; *h = hh;
+    if (rgb) { std::memcpy(rgb, img.data(), img.size() * 4); }
+    return RT_OK;
+}
+
+int rt_scene_config(const char* scn_path, rt_render_cfg* cfg, char* ibl_path, uint32_t ibl_cap)
+{
+    if (!scn_path || !cfg) { return fail(RT_E_INVALID, "bad argument"); }
+    const hg::SceneConfig sc = hg::parse_scene_config(scn_path);
+    if (sc.width <= 0 || sc.height <= 0) { return fail(RT_E_FORMAT, "screen size must be positive"); }
+    cfg->width = (uint32_t)sc.width;
+    cfg->height = (uint32_t)sc.height;
+    hg::store_camera(sc.camera, cfg);
+    if (ibl_path && ibl_cap)
+    {
+        const size_t n = std::min<size_t>(sc.ibl_path.size(), ibl_cap - 1);
+        std::memcpy(ibl_path, sc.ibl_path.data(), n);
+        ibl_path[n] = 0;
+    }
+    return RT_OK;
 }
 
 // ---- cameras (src/main.cpp:43-66) ----

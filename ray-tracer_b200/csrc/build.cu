@@ -71,6 +71,41 @@ __device__ __forceinline__ uint64_t spread3(uint32_t v)
     return x;
 }
 
+// Batched builds (rt_build_batch): scene s owns input triangles [toff[s], toff[s+1]) whose
+// vertex indices are local to vertices [voff[s], voff[s+1]). Every scene gets its own box for
+// its Morton codes, and its id is placed above the code bits of the sort key (shift `sshift`),
+// so the radix tree first separates the scenes and each scene's subtree is the tree of that
+// scene alone. S = 0: a single scene (no offsets; sshift = 63 never sees a set bit).
+struct Batch
+{
+    uint32_t        S;
+    const uint32_t* toff;
+    const uint32_t* voff;
+    uint32_t        sshift;
+    const uint32_t* h_toff;  // host copy of toff
+};
+constexpr uint32_t MAX_BATCH_SCENES = 1024;
+
+// Key bits that hold a scene id below S.
+inline uint32_t scene_bits(uint32_t S)
+{
+    uint32_t b = 0;
+    while ((1u << b) < S) { b++; }
+    return b;
+}
+
+// Scene of input triangle i: the last s with toff[s] <= i (toff in shared memory).
+__device__ __forceinline__ uint32_t scene_of(const uint32_t* toff, uint32_t S, uint32_t i)
+{
+    uint32_t lo = 0, hi = S;  // toff[lo] <= i < toff[hi]
+    while (hi - lo > 1)
+    {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (toff[mid] <= i) { lo = mid; } else { hi = mid; }
+    }
+    return lo;
+}
+
 __global__ void k_init(uint32_t* scene, uint32_t* hist, uint32_t* counters, uint32_t* status)
 {
     const int t = threadIdx.x;
@@ -98,18 +133,37 @@ __device__ __forceinline__ f3 vpos(const rt_vertex* v, uint32_t i)
 }
 
 // Per triangle: index check, box (lo.xyz/hi.xyz) with the centroid in lo.w, hi.w, cz.
-// Block-reduces the scene box into `scene` (order-preserving uint encoding).
+// Block-reduces the scene box into `scene` (order-preserving uint encoding). In a batched
+// build the triangle's scene box is scene[6 s ..] and its vertex indices are rebased to the
+// concatenated vertex array (written to gtris).
+template <bool BATCH>
 __global__ void __launch_bounds__(BLK)
 k_tri_prep(const rt_triangle* __restrict__ tris, uint32_t N, const rt_vertex* __restrict__ verts, uint32_t V,
            float4* __restrict__ lo, float4* __restrict__ hi, float* __restrict__ cz, uint32_t* __restrict__ scene,
-           uint32_t* __restrict__ status)
+           uint32_t* __restrict__ status, Batch bt, rt_triangle* __restrict__ gtris)
 {
     const uint32_t i = blockIdx.x * BLK + threadIdx.x;
+    __shared__ uint32_t soff[BATCH ? MAX_BATCH_SCENES + 1 : 1];
+    if (BATCH)
+    {
+        for (uint32_t k = threadIdx.x; k <= bt.S; k += BLK) { soff[k] = bt.toff[k]; }
+        __syncthreads();
+    }
     uint32_t om[3] = { 0xffffffffu, 0xffffffffu, 0xffffffffu }, oM[3] = { 0u, 0u, 0u };
+    uint32_t sc = 0;
     if (i < N)
     {
         uint32_t a = tris[i].v[0], b = tris[i].v[1], c = tris[i].v[2];
-        if (a >= V || b >= V || c >= V) { atomicOr(status, ST_INDEX); a = b = c = 0; }
+        uint32_t vb = 0, vn = V;
+        if (BATCH)
+        {
+            sc = scene_of(soff, bt.S, i);
+            vb = bt.voff[sc];
+            vn = bt.voff[sc + 1] - vb;
+        }
+        if (a >= vn || b >= vn || c >= vn) { atomicOr(status, ST_INDEX); a = b = c = 0; }
+        a += vb; b += vb; c += vb;
+        if (BATCH) { gtris[i] = rt_triangle{ { a, b, c } }; }
         const f3 p0 = vpos(verts, a), p1 = vpos(verts, b), p2 = vpos(verts, c);
         box3 bx = box_empty();
         box_pt(bx, p0); box_pt(bx, p1); box_pt(bx, p2);
@@ -120,6 +174,27 @@ k_tri_prep(const rt_triangle* __restrict__ tris, uint32_t N, const rt_vertex* __
         hi[i] = make_float4(bx.mx[0], bx.mx[1], bx.mx[2], cy);
         cz[i] = czv;
         for (int k = 0; k < 3; k++) { om[k] = f2ord(bx.mn[k]); oM[k] = f2ord(bx.mx[k]); }
+    }
+    if (BATCH)
+    {
+        // warps inside one scene reduce first; a warp across a scene boundary adds per lane
+        const uint32_t s0 = __shfl_sync(0xffffffffu, sc, 0);
+        const bool uniform = __all_sync(0xffffffffu, i >= N || sc == s0);
+        for (int k = 0; k < 3; k++)
+        {
+            uint32_t m = om[k], M = oM[k];
+            if (uniform)
+            {
+                for (int o = 16; o > 0; o >>= 1)
+                {
+                    m = min(m, __shfl_xor_sync(0xffffffffu, m, o));
+                    M = max(M, __shfl_xor_sync(0xffffffffu, M, o));
+                }
+                if ((threadIdx.x & 31) == 0 && m != 0xffffffffu) { atomicMin(&scene[6 * s0 + k], m); atomicMax(&scene[6 * s0 + 3 + k], M); }
+            }
+            else if (i < N) { atomicMin(&scene[6 * sc + k], m); atomicMax(&scene[6 * sc + 3 + k], M); }
+        }
+        return;
     }
     __shared__ uint32_t s[6];
     if (threadIdx.x < 3) { s[threadIdx.x] = 0xffffffffu; s[3 + threadIdx.x] = 0u; }
@@ -143,27 +218,39 @@ k_tri_prep(const rt_triangle* __restrict__ tris, uint32_t N, const rt_vertex* __
 }
 
 // Morton code per triangle (input order) and the 8-bit digit histograms of all sort passes.
-template <typename K>
+template <typename K, bool BATCH = false>
 __global__ void __launch_bounds__(BLK)
 k_morton(const float4* __restrict__ lo, const float4* __restrict__ hi, const float* __restrict__ cz, uint32_t N,
-         const uint32_t* __restrict__ scene, uint32_t bits, int passes, K* __restrict__ keys, uint32_t* __restrict__ hist)
+         const uint32_t* __restrict__ scene, uint32_t bits, int passes, K* __restrict__ keys, uint32_t* __restrict__ hist,
+         Batch bt = Batch{ 0u, nullptr, nullptr, 63u, nullptr })
 {
     // grid-stride: the block histograms are flushed to global memory once per block, so the
     // launch uses a few blocks per SM rather than one block per 256 triangles
     __shared__ uint32_t h[8 * 256];
+    __shared__ uint32_t soff[BATCH ? MAX_BATCH_SCENES + 1 : 1];
     for (int t = threadIdx.x; t < passes * 256; t += BLK) { h[t] = 0u; }
+    if (BATCH)
+    {
+        for (uint32_t k = threadIdx.x; k <= bt.S; k += BLK) { soff[k] = bt.toff[k]; }
+    }
     __syncthreads();
     float mn[3], size[3];
-    for (int k = 0; k < 3; k++)
-    {
-        mn[k] = ord2f(scene[k]);
-        size[k] = ord2f(scene[3 + k]) - mn[k];
-        if (size[k] == 0.f) { size[k] = 1.f; }
-    }
+    uint32_t cur = 0xffffffffu;  // scene whose box is in mn/size
     const uint32_t qmax = (1u << bits) - 1u;
     const float fmax = (float)qmax;
     for (uint32_t i = blockIdx.x * BLK + threadIdx.x; i < N; i += gridDim.x * BLK)
     {
+        const uint32_t sc = BATCH ? scene_of(soff, bt.S, i) : 0u;
+        if (sc != cur)
+        {
+            cur = sc;
+            for (int k = 0; k < 3; k++)
+            {
+                mn[k] = ord2f(scene[6 * sc + k]);
+                size[k] = ord2f(scene[6 * sc + 3 + k]) - mn[k];
+                if (size[k] == 0.f) { size[k] = 1.f; }
+            }
+        }
         const float c[3] = { lo[i].w, hi[i].w, cz[i] };
         uint32_t q[3];
         for (int k = 0; k < 3; k++)
@@ -171,7 +258,8 @@ k_morton(const float4* __restrict__ lo, const float4* __restrict__ hi, const flo
             const uint32_t v = x86_f2u((c[k] - mn[k]) * fmax / size[k]);
             q[k] = v > qmax ? qmax : v;
         }
-        const uint64_t code = (spread3(q[0]) << 2) | (spread3(q[1]) << 1) | spread3(q[2]);
+        uint64_t code = (spread3(q[0]) << 2) | (spread3(q[1]) << 1) | spread3(q[2]);
+        if (BATCH) { code |= (uint64_t)sc << bt.sshift; }
         keys[i] = (K)code;
         for (int p = 0; p < passes; p++) { atomicAdd(&h[p * 256 + (uint32_t)((code >> (8 * p)) & 255u)], 1u); }
     }
@@ -193,10 +281,14 @@ __device__ __forceinline__ void krange(const uint4* __restrict__ knode, uint32_t
 
 // The reference splits a node by Morton code only if it has more triangles than both the
 // leaf size and the SAH threshold and its codes are not all equal (bvh_bfs.cpp:79-107).
+// A range over two or more scenes of a batched build is always split (at a scene boundary:
+// the scene bits are the highest key bits).
 template <typename K>
-__device__ __forceinline__ bool morton_split_node(const K* __restrict__ keys, uint32_t f, uint32_t l, uint32_t tm)
+__device__ __forceinline__ bool morton_split_node(const K* __restrict__ keys, uint32_t f, uint32_t l, uint32_t tm,
+                                                  uint32_t sshift)
 {
-    return (l - f + 1u) > tm && keys[f] != keys[l];
+    const uint64_t x = (uint64_t)(keys[f] ^ keys[l]);
+    return ((l - f + 1u) > tm && x != 0) || (x >> sshift) != 0;
 }
 
 __device__ __forceinline__ void store_box(float4* kbox, uint32_t x, const box3& b)
@@ -219,7 +311,8 @@ template <typename K>
 __global__ void __launch_bounds__(BLK)
 k_boundary(const K* __restrict__ keys, const uint32_t* __restrict__ perm, uint32_t n, const uint4* __restrict__ knode,
            const uint32_t* __restrict__ parent, const float4* __restrict__ lo, const float4* __restrict__ hi,
-           uint32_t tm, uint32_t max_leaf, float4* __restrict__ kbox, uint32_t* __restrict__ rank, uint32_t* __restrict__ wnode, uint32_t* __restrict__ wtri,
+           uint32_t tm, uint32_t max_leaf, uint32_t sshift, float4* __restrict__ kbox, uint32_t* __restrict__ rank,
+           uint32_t* __restrict__ wnode, uint32_t* __restrict__ wtri,
            uint8_t* __restrict__ kpos, SahRoot* __restrict__ roots, uint32_t* __restrict__ counters,
            uint32_t* __restrict__ status)
 {
@@ -227,7 +320,7 @@ k_boundary(const K* __restrict__ keys, const uint32_t* __restrict__ perm, uint32
     if (x >= 2 * n - 1) { return; }
     uint32_t f, l;
     krange<K>(knode, n, x, f, l);
-    const bool is_m = morton_split_node<K>(keys, f, l, tm);
+    const bool is_m = morton_split_node<K>(keys, f, l, tm, sshift);
     const uint32_t par = parent[x];
     bool kept = is_m;
     if (!is_m)
@@ -237,7 +330,7 @@ k_boundary(const K* __restrict__ keys, const uint32_t* __restrict__ perm, uint32
         {
             uint32_t pf, pl;
             krange<K>(knode, n, par, pf, pl);
-            kept = morton_split_node<K>(keys, pf, pl, tm);
+            kept = morton_split_node<K>(keys, pf, pl, tm, sshift);
         }
     }
     if (!kept) { return; }
@@ -280,6 +373,7 @@ k_boundary(const K* __restrict__ keys, const uint32_t* __restrict__ perm, uint32
         const uint32_t slot = atomicAdd(&counters[0], 1u);
         SahRoot sr;
         sr.kid = x; sr.first = f; sr.count = size; sr.depth = depth; sr.rank = r;
+        sr.scene = (uint32_t)((uint64_t)keys[f] >> sshift);
         for (int k = 0; k < 3; k++) { sr.box[k] = b.mn[k]; sr.box[3 + k] = b.mx[k]; }
         roots[slot] = sr;
     }
@@ -348,30 +442,39 @@ k_climb(const K* __restrict__ keys, const uint32_t* __restrict__ perm, uint32_t 
 }
 
 // Output slots of the kept Karras nodes: pre-order index = snode[first] + rank.
+// In a batched build, the node covering exactly one scene's keys is that scene's root; it
+// records {root node, subtree node count, first triangle, triangle count} in info[4 s ..].
 template <typename K>
 __global__ void __launch_bounds__(BLK)
 k_emit(const K* __restrict__ keys, uint32_t n, const uint4* __restrict__ knode, const uint32_t* __restrict__ parent,
-       uint32_t tm, uint32_t max_leaf, const float4* __restrict__ kbox, const uint32_t* __restrict__ rank,
+       uint32_t tm, uint32_t max_leaf, uint32_t sshift, const float4* __restrict__ kbox, const uint32_t* __restrict__ rank,
        const uint32_t* __restrict__ snode, const uint32_t* __restrict__ stri, rt_bvh_node* __restrict__ out,
-       uint32_t max_nodes, uint32_t* __restrict__ status)
+       uint32_t max_nodes, uint32_t* __restrict__ info, uint32_t* __restrict__ status)
 {
     const uint32_t x = blockIdx.x * BLK + threadIdx.x;
     if (x >= 2 * n - 1) { return; }
     uint32_t f, l;
     krange<K>(knode, n, x, f, l);
-    const bool is_m = morton_split_node<K>(keys, f, l, tm);
+    const bool is_m = morton_split_node<K>(keys, f, l, tm, sshift);
     const uint32_t par = parent[x];
-    if (!is_m)
+    if (!is_m && par != NONE)
     {
-        if (par != NONE)
-        {
-            uint32_t pf, pl;
-            krange<K>(knode, n, par, pf, pl);
-            if (!morton_split_node<K>(keys, pf, pl, tm)) { return; }
-        }
-        if (l - f + 1u > max_leaf) { return; }  // SAH subtree root: emitted by the SAH builder
+        uint32_t pf, pl;
+        krange<K>(knode, n, par, pf, pl);
+        if (!morton_split_node<K>(keys, pf, pl, tm, sshift)) { return; }
     }
     const uint32_t pre = snode[f] + rank[x];
+    if (info)
+    {
+        const uint64_t sf = (uint64_t)keys[f] >> sshift, sl = (uint64_t)keys[l] >> sshift;
+        if (sf == sl && (f == 0 || ((uint64_t)keys[f - 1] >> sshift) != sf) &&
+            (l == n - 1 || ((uint64_t)keys[l + 1] >> sshift) != sl))
+        {
+            uint32_t* o = info + 4 * (size_t)sf;
+            o[0] = pre; o[1] = snode[l + 1] - pre; o[2] = stri[f]; o[3] = stri[l + 1] - stri[f];
+        }
+    }
+    if (!is_m && l - f + 1u > max_leaf) { return; }  // SAH subtree root: emitted by the SAH builder
     if (pre >= max_nodes) { atomicOr(status, ST_CAPACITY); return; }
     const box3 b = load_box(kbox, x);
     if (is_m)
@@ -528,17 +631,17 @@ __global__ void __launch_bounds__(256) k_scan2_apply(Scan2 S, uint32_t n, const 
 // All per-build initialisation in one launch: block 0 also does k_init's work.
 __global__ void __launch_bounds__(BLK)
 k_clear(uint32_t n, uint32_t* __restrict__ parent, unsigned long long* __restrict__ visit, uint32_t* __restrict__ wnode,
-        uint32_t* __restrict__ wtri, uint8_t* __restrict__ kpos, uint32_t* __restrict__ scene, uint32_t* __restrict__ hist,
-        uint32_t* __restrict__ counters, uint32_t* __restrict__ status)
+        uint32_t* __restrict__ wtri, uint8_t* __restrict__ kpos, uint32_t* __restrict__ scene, uint32_t n_scene_boxes,
+        uint32_t* __restrict__ hist, uint32_t* __restrict__ counters, uint32_t* __restrict__ status)
 {
     const uint32_t i = blockIdx.x * BLK + threadIdx.x;
     if (i < 2 * n - 1) { parent[i] = NONE; }
     if (i < n) { visit[i] = ~0ull; kpos[i] = 0u; }
     if (i <= n) { wnode[i] = 0u; wtri[i] = 0u; }
+    if (i < 6 * n_scene_boxes) { scene[i] = (i % 6) < 3 ? 0xffffffffu : 0u; }
     if (blockIdx.x == 0)
     {
         const int t = threadIdx.x;
-        if (t < 3) { scene[t] = 0xffffffffu; scene[3 + t] = 0u; }
         for (int k = t; k < 8 * 256; k += BLK) { hist[k] = 0u; }
         if (t < 16) { counters[t] = 0u; }
         if (t == 0) { *status = 0u; }
@@ -547,15 +650,20 @@ k_clear(uint32_t n, uint32_t* __restrict__ parent, unsigned long long* __restric
 
 template <typename K>
 int build_typed(rt_bvh* B, const rt_vertex* d_verts, uint32_t V, const rt_triangle* d_tris, uint32_t N,
-                const rt_build_cfg& cfg, cudaStream_t st, uint32_t cap)
+                const rt_build_cfg& cfg, cudaStream_t st, uint32_t cap, const Batch& bt)
 {
     BuildScratch& S = B->s;
-    const int key_bits = 3 * (int)cfg.morton_bits;
+    const bool batch = bt.S > 0;
+    const uint32_t n_boxes = batch ? bt.S : 1u;
+    const int key_bits = batch ? (int)bt.sshift + (int)scene_bits(bt.S) : 3 * (int)cfg.morton_bits;
+    const uint32_t sshift = batch ? bt.sshift : 63u;
     const int passes = sort_passes(key_bits);
     const uint32_t nk = 2 * N - 1;  // Karras nodes
     if (S.tri_lo.ensure((size_t)N * 16) || S.tri_hi.ensure((size_t)N * 16) || S.tri_cz.ensure((size_t)N * 4) ||
         S.keys.ensure((size_t)N * sizeof(K)) || S.vals.ensure((size_t)N * 4) || S.hist.ensure(8 * 256 * 4) ||
-        S.scene.ensure(64) || S.status.ensure(64) || S.counters.ensure(64) ||
+        S.scene.ensure((size_t)n_boxes * 24 + 64) || S.status.ensure(64) || S.counters.ensure(64) ||
+        (batch && (S.gtris.ensure((size_t)N * sizeof(rt_triangle)) || B->scene_info.ensure((size_t)bt.S * 16) ||
+                   B->scene_roots.ensure((size_t)bt.S * 32))) ||
         S.knode.ensure((size_t)std::max<uint32_t>(N - 1, 1) * 16) || S.parent.ensure((size_t)nk * 4) ||
         S.kbox.ensure((size_t)nk * 32) || S.visit.ensure((size_t)N * 8) || S.rank.ensure((size_t)nk * 4) ||
         S.wnode.ensure((size_t)(N + 1) * 4) || S.wtri.ensure((size_t)(N + 1) * 4) ||
@@ -568,21 +676,33 @@ int build_typed(rt_bvh* B, const rt_vertex* d_verts, uint32_t V, const rt_triang
     uint32_t* counters = S.counters.as<uint32_t>();
 
     prof_mark(B, 0, st);
-    k_clear<<<blocks_for(nk + 1), BLK, 0, st>>>(N, S.parent.as<uint32_t>(), S.visit.as<unsigned long long>(),
-                                                S.wnode.as<uint32_t>(),
-                                                S.wtri.as<uint32_t>(), S.bnd.as<uint8_t>(), S.scene.as<uint32_t>(),
-                                                S.hist.as<uint32_t>(), counters, status);
+    k_clear<<<blocks_for(std::max<uint32_t>(nk + 1, 6 * n_boxes)), BLK, 0, st>>>(
+        N, S.parent.as<uint32_t>(), S.visit.as<unsigned long long>(), S.wnode.as<uint32_t>(), S.wtri.as<uint32_t>(),
+        S.bnd.as<uint8_t>(), S.scene.as<uint32_t>(), n_boxes, S.hist.as<uint32_t>(), counters, status);
     count_launch();
     k_vertices<<<blocks_for(V), BLK, 0, st>>>(d_verts, B->verts.as<rt_vertex>(), V);
     count_launch();
-    k_tri_prep<<<blocks_for(N), BLK, 0, st>>>(d_tris, N, d_verts, V, S.tri_lo.as<float4>(), S.tri_hi.as<float4>(),
-                                               S.tri_cz.as<float>(), S.scene.as<uint32_t>(), status);
-    count_launch();
     const uint32_t morton_blocks = std::min<uint32_t>(blocks_for(N), 4u * (uint32_t)device_sm_count());
-    k_morton<K><<<morton_blocks, BLK, 0, st>>>(S.tri_lo.as<float4>(), S.tri_hi.as<float4>(), S.tri_cz.as<float>(), N,
-                                               S.scene.as<uint32_t>(), cfg.morton_bits, passes, S.keys.as<K>(),
-                                               S.hist.as<uint32_t>());
-    count_launch();
+    if (batch)
+    {
+        k_tri_prep<true><<<blocks_for(N), BLK, 0, st>>>(d_tris, N, d_verts, V, S.tri_lo.as<float4>(), S.tri_hi.as<float4>(),
+                                                         S.tri_cz.as<float>(), S.scene.as<uint32_t>(), status, bt,
+                                                         S.gtris.as<rt_triangle>());
+        d_tris = S.gtris.as<rt_triangle>();  // vertex indices of the concatenated array from here on
+        k_morton<K, true><<<morton_blocks, BLK, 0, st>>>(S.tri_lo.as<float4>(), S.tri_hi.as<float4>(), S.tri_cz.as<float>(),
+                                                         N, S.scene.as<uint32_t>(), cfg.morton_bits, passes,
+                                                         S.keys.as<K>(), S.hist.as<uint32_t>(), bt);
+    }
+    else
+    {
+        k_tri_prep<false><<<blocks_for(N), BLK, 0, st>>>(d_tris, N, d_verts, V, S.tri_lo.as<float4>(), S.tri_hi.as<float4>(),
+                                                          S.tri_cz.as<float>(), S.scene.as<uint32_t>(), status, bt,
+                                                          nullptr);
+        k_morton<K><<<morton_blocks, BLK, 0, st>>>(S.tri_lo.as<float4>(), S.tri_hi.as<float4>(), S.tri_cz.as<float>(), N,
+                                                   S.scene.as<uint32_t>(), cfg.morton_bits, passes, S.keys.as<K>(),
+                                                   S.hist.as<uint32_t>());
+    }
+    count_launch(2);
     if (int e = check_launch("morton")) { return e; }
 
     prof_mark(B, 1, st);
@@ -603,7 +723,7 @@ int build_typed(rt_bvh* B, const rt_vertex* d_verts, uint32_t V, const rt_triang
     }
     const uint32_t tm = std::max(cfg.max_leaf, cfg.lbvh_threshold);
     k_boundary<K><<<blocks_for(nk), BLK, 0, st>>>(skeys, perm, N, S.knode.as<uint4>(), S.parent.as<uint32_t>(),
-                                                  S.tri_lo.as<float4>(), S.tri_hi.as<float4>(), tm, cfg.max_leaf,
+                                                  S.tri_lo.as<float4>(), S.tri_hi.as<float4>(), tm, cfg.max_leaf, sshift,
                                                   S.kbox.as<float4>(), S.rank.as<uint32_t>(),
                                                   S.wnode.as<uint32_t>(), S.wtri.as<uint32_t>(), S.bnd.as<uint8_t>(),
                                                   S.sah_roots.as<SahRoot>(), counters, status);
@@ -627,6 +747,21 @@ int build_typed(rt_bvh* B, const rt_vertex* d_verts, uint32_t V, const rt_triang
         in.n_roots = n_roots;
         in.wnode = S.wnode.as<uint32_t>();
         in.wtri = S.wtri.as<uint32_t>();
+        if (batch)
+        {
+            for (uint32_t k = 0; k < bt.S; k++)
+            {
+                const uint32_t ns = bt.h_toff[k + 1] - bt.h_toff[k];
+                const uint32_t c = (uint32_t)((float)ns * cfg.spatial_mult);  // bvh_morton.cpp:46-47, per scene
+                in.budget_used.push_back(ns);
+                in.budget_cap.push_back(std::max(c, ns));
+            }
+        }
+        else
+        {
+            in.budget_used.push_back(N);
+            in.budget_cap.push_back(cap);
+        }
         return sah_build(B, cfg, in, st, &sah);
     };
     // pre-order node slots and triangle offsets per start key, then the nodes and triangles
@@ -643,8 +778,9 @@ int build_typed(rt_bvh* B, const rt_vertex* d_verts, uint32_t V, const rt_triang
             count_launch(3);
         }
         k_emit<K><<<blocks_for(nk), BLK, 0, st>>>(skeys, N, S.knode.as<uint4>(), S.parent.as<uint32_t>(), tm, cfg.max_leaf,
-                                                  S.kbox.as<float4>(), S.rank.as<uint32_t>(), S.snode.as<uint32_t>(),
-                                                  S.stri.as<uint32_t>(), B->nodes.as<rt_bvh_node>(), 2 * cap - 1, status);
+                                                  sshift, S.kbox.as<float4>(), S.rank.as<uint32_t>(), S.snode.as<uint32_t>(),
+                                                  S.stri.as<uint32_t>(), B->nodes.as<rt_bvh_node>(), 2 * cap - 1,
+                                                  batch ? B->scene_info.as<uint32_t>() : nullptr, status);
         count_launch();
         k_emit_tris<<<blocks_for(N), BLK, 0, st>>>(perm, S.bnd.as<uint8_t>(), S.stri.as<uint32_t>(), N, d_tris,
                                                     B->tris.as<rt_triangle>(), B->prim.as<uint32_t>(), cap, status);
@@ -664,6 +800,7 @@ int build_typed(rt_bvh* B, const rt_vertex* d_verts, uint32_t V, const rt_triang
     // binned SAH only come from runs of identical Morton codes; the layout is emitted at once
     // and redone in the rare case such runs exist, which saves a host round trip.
     const bool expect_sah = cfg.lbvh_threshold > cfg.max_leaf;
+    if (batch) { RT_CUDA(cudaMemsetAsync(B->scene_info.p, 0xff, (size_t)bt.S * 16, st)); }
     uint32_t res[8];
     uint32_t stat = 0;
     for (int attempt = 0; attempt < 2; attempt++)
@@ -686,6 +823,12 @@ int build_typed(rt_bvh* B, const rt_vertex* d_verts, uint32_t V, const rt_triang
         prof_mark(B, 5, st);
         // traversal layout from the device-side counts: the build's only host round trip follows
         if (int e = launch_traversal_layout(B, st, 2 * cap - 1, cap, counters + 4, status)) { return e; }
+        if (batch)
+        {
+            if (int e = launch_scene_roots(B, bt.S, counters + 4, status, st)) { return e; }
+            B->scene_info_host.resize((size_t)4 * bt.S);
+            RT_CUDA(cudaMemcpyAsync(B->scene_info_host.data(), B->scene_info.p, (size_t)bt.S * 16, cudaMemcpyDeviceToHost, st));
+        }
         prof_mark(B, 6, st);
         RT_CUDA(cudaMemcpyAsync(res, counters, 32, cudaMemcpyDeviceToHost, st));
         RT_CUDA(cudaMemcpyAsync(&stat, status, 4, cudaMemcpyDeviceToHost, st));
@@ -702,6 +845,15 @@ int build_typed(rt_bvh* B, const rt_vertex* d_verts, uint32_t V, const rt_triang
     if (res[4] > 2 * cap - 1 || res[5] > cap) { return fail(RT_E_CAPACITY, "build produced more nodes than its bound"); }
     B->n_nodes = res[4];
     B->n_tris = res[5];
+    B->n_scenes = bt.S;
+    for (uint32_t k = 0; k < bt.S; k++)
+    {
+        const uint32_t* in = &B->scene_info_host[4 * (size_t)k];
+        if (in[0] >= B->n_nodes || (uint64_t)in[0] + in[1] > B->n_nodes || (uint64_t)in[2] + in[3] > B->n_tris)
+        {
+            return fail(RT_E_CAPACITY, "batched build: a scene's root record is out of range");
+        }
+    }
     B->stats[4] = res[1] + sah.leaves;
     B->stats[3] = B->n_nodes - B->stats[4];
     return RT_OK;
@@ -723,6 +875,13 @@ int exclusive_scan_u32(const uint32_t* in, uint32_t* out, uint32_t n, uint32_t* 
 int build_bvh(rt_bvh* B, const rt_vertex* d_verts, uint32_t V, const rt_triangle* d_tris, uint32_t N,
               const rt_build_cfg& cfg, cudaStream_t st)
 {
+    return build_bvh_batch(B, d_verts, V, d_tris, N, cfg, st, 0, nullptr, nullptr, nullptr);
+}
+
+int build_bvh_batch(rt_bvh* B, const rt_vertex* d_verts, uint32_t V, const rt_triangle* d_tris, uint32_t N,
+                    const rt_build_cfg& cfg, cudaStream_t st, uint32_t n_scenes, const uint32_t* d_toff,
+                    const uint32_t* d_voff, const uint32_t* h_toff)
+{
     if (V == 0 || N == 0) { return fail(RT_E_EMPTY, "no vertices or no triangles"); }
     if (cfg.morton_bits < 1 || cfg.morton_bits > 21) { return fail(RT_E_INVALID, "morton_bits must be in 1..21"); }
     if (cfg.bins_min < 1 || cfg.bins_max > SAH_MAX_BINS || cfg.bins_min > cfg.bins_max)
@@ -741,8 +900,17 @@ int build_bvh(rt_bvh* B, const rt_vertex* d_verts, uint32_t V, const rt_triangle
     }
     B->n_verts = V;
     B->has_prim = true;
-    int e = (3 * cfg.morton_bits > 32) ? build_typed<uint64_t>(B, d_verts, V, d_tris, N, cfg, st, cap)
-                                       : build_typed<uint32_t>(B, d_verts, V, d_tris, N, cfg, st, cap);
+    B->n_scenes = 0;
+    Batch bt{ n_scenes, d_toff, d_voff, 3 * cfg.morton_bits, h_toff };
+    if (n_scenes > MAX_BATCH_SCENES) { return fail(RT_E_CAPACITY, "more than 1024 scenes in one batched build"); }
+    const uint32_t key_bits = 3 * cfg.morton_bits + (n_scenes ? scene_bits(n_scenes) : 0u);
+    if (key_bits > 64)
+    {
+        return fail(RT_E_INVALID, "batched build: 3 * morton_bits + ceil(log2(n_scenes)) must not exceed 64 "
+                                  "(use 30-bit codes, morton_bits = 10, for more than 2 scenes)");
+    }
+    int e = (key_bits > 32) ? build_typed<uint64_t>(B, d_verts, V, d_tris, N, cfg, st, cap, bt)
+                            : build_typed<uint32_t>(B, d_verts, V, d_tris, N, cfg, st, cap, bt);
     if (e) { return e; }
     if (B->prof)
     {
@@ -801,7 +969,8 @@ int morton_order_noalloc_typed(unsigned char* base, const rt_vertex* verts, uint
     uint32_t* status = scene + 48;
     const int key_bits = 3 * (int)bits;
     k_init<<<1, 256, 0, st>>>(scene, hist, counters, status);
-    k_tri_prep<<<blocks_for(N), BLK, 0, st>>>(tris, N, verts, V, lo, hi, cz, scene, status);
+    k_tri_prep<false><<<blocks_for(N), BLK, 0, st>>>(tris, N, verts, V, lo, hi, cz, scene, status,
+                                                      Batch{ 0u, nullptr, nullptr, 63u, nullptr }, nullptr);
     k_morton<K><<<blocks_for(N), BLK, 0, st>>>(lo, hi, cz, N, scene, bits, sort_passes(key_bits), keys, hist);
     count_launch(3);
     if (int e = check_launch("morton (no-alloc)")) { return e; }

@@ -1,6 +1,8 @@
 // host_geom.cpp -- see host_geom.h.
 #include "host_geom.h"
 
+#include <algorithm>
+#include <cmath>
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
@@ -467,6 +469,212 @@ int load_ply(const std::string& path, V3 tr, float scale, Q orient, std::vector<
     }
     for (const rt_triangle& tri : nt) { t.push_back(mkt(voff + tri.v[0], voff + tri.v[1], voff + tri.v[2])); }
     return RT_OK;
+}
+
+// ---- Radiance RGBE images (Ward, "Real Pixels", Graphics Gems II, 1991) ----
+// A pixel is three 8-bit mantissas sharing one exponent byte: for v = max(r, g, b) = m 2^e
+// with m in [0.5, 1), the bytes are (r, g, b) * 256 m / v and e + 128. Scanlines of width
+// 8..32767 are written run-length encoded per component ("new" RLE: 2, 2, width, then for each
+// of the four planes runs of (128 + n, value) for n >= 4 repeats and literals (n, bytes...)).
+
+static void to_rgbe(const float* c, unsigned char* o)
+{
+    const float v = std::max(c[0], std::max(c[1], c[2]));
+    if (!(v >= 1e-32f)) { o[0] = o[1] = o[2] = o[3] = 0; return; }
+    int e = 0;
+    const float m = std::frexp(v, &e) * 256.0f / v;
+    o[0] = (unsigned char)std::max(0.0f, c[0] * m);
+    o[1] = (unsigned char)std::max(0.0f, c[1] * m);
+    o[2] = (unsigned char)std::max(0.0f, c[2] * m);
+    o[3] = (unsigned char)(e + 128);
+}
+
+static void from_rgbe(const unsigned char* in, float* c)
+{
+    if (in[3] == 0) { c[0] = c[1] = c[2] = 0.0f; return; }
+    const float f = std::ldexp(1.0f, (int)in[3] - (128 + 8));
+    c[0] = (float)in[0] * f; c[1] = (float)in[1] * f; c[2] = (float)in[2] * f;
+}
+
+static void rle_plane(const unsigned char* d, uint32_t n, std::vector<unsigned char>& out)
+{
+    uint32_t i = 0;
+    while (i < n)
+    {
+        // find the next run of >= 4 equal bytes
+        uint32_t run_at = i, run_len = 0;
+        while (run_at < n)
+        {
+            run_len = 1;
+            while (run_at + run_len < n && run_len < 127 && d[run_at + run_len] == d[run_at]) { run_len++; }
+            if (run_len >= 4) { break; }
+            run_at += run_len;
+        }
+        if (run_at >= n) { run_len = 0; run_at = n; }
+        // literals before it, at most 128 per chunk
+        while (i < run_at)
+        {
+            const uint32_t k = std::min<uint32_t>(128, run_at - i);
+            out.push_back((unsigned char)k);
+            out.insert(out.end(), d + i, d + i + k);
+            i += k;
+        }
+        if (run_len >= 4)
+        {
+            out.push_back((unsigned char)(128 + run_len));
+            out.push_back(d[run_at]);
+            i = run_at + run_len;
+        }
+    }
+}
+
+int write_hdr(const std::string& path, const float* rgb, uint32_t w, uint32_t h, std::string& err)
+{
+    std::ofstream f(path, std::ios::binary);
+    if (!f) { err = "cannot open " + path + " for writing"; return RT_E_IO; }
+    std::ostringstream hdr;
+    hdr << "#?RADIANCE\n# Written by librt_b200\nFORMAT=32-bit_rle_rgbe\nEXPOSURE=1.0\n\n-Y " << h << " +X " << w << "\n";
+    const std::string hs = hdr.str();
+    f.write(hs.data(), (std::streamsize)hs.size());
+    std::vector<unsigned char> px((size_t)w * 4), plane(w), out;
+    for (uint32_t y = 0; y < h; y++)
+    {
+        for (uint32_t x = 0; x < w; x++) { to_rgbe(rgb + 3 * ((size_t)y * w + x), &px[4 * (size_t)x]); }
+        out.clear();
+        if (w < 8 || w > 32767)
+        {
+            out.assign(px.begin(), px.end());
+        }
+        else
+        {
+            out.push_back(2); out.push_back(2); out.push_back((unsigned char)(w >> 8)); out.push_back((unsigned char)(w & 255));
+            for (int c = 0; c < 4; c++)
+            {
+                for (uint32_t x = 0; x < w; x++) { plane[x] = px[4 * (size_t)x + c]; }
+                rle_plane(plane.data(), w, out);
+            }
+        }
+        f.write(reinterpret_cast<const char*>(out.data()), (std::streamsize)out.size());
+    }
+    if (!f) { err = "write failed: " + path; return RT_E_IO; }
+    return RT_OK;
+}
+
+int read_hdr(const std::string& path, std::vector<float>& rgb, uint32_t& w, uint32_t& h, std::string& err)
+{
+    std::ifstream f(path, std::ios::binary);
+    if (!f) { err = "cannot open " + path; return RT_E_IO; }
+    std::string line;
+    if (!std::getline(f, line) || line.rfind("#?", 0) != 0) { err = path + ": not a Radiance file"; return RT_E_FORMAT; }
+    bool fmt_ok = false;
+    while (std::getline(f, line) && !line.empty())
+    {
+        if (line == "FORMAT=32-bit_rle_rgbe") { fmt_ok = true; }
+    }
+    if (!fmt_ok) { err = path + ": not 32-bit_rle_rgbe"; return RT_E_FORMAT; }
+    if (!std::getline(f, line)) { err = path + ": no resolution line"; return RT_E_FORMAT; }
+    long hh = 0, ww = 0;
+    char ya[3] = { 0 }, xa[3] = { 0 };
+    if (std::sscanf(line.c_str(), "%2s %ld %2s %ld", ya, &hh, xa, &ww) != 4 || std::string(ya) != "-Y" ||
+        std::string(xa) != "+X" || hh <= 0 || ww <= 0 || hh > 65536 || ww > 65536)
+    {
+        err = path + ": unsupported resolution line '" + line + "'";
+        return RT_E_FORMAT;
+    }
+    w = (uint32_t)ww; h = (uint32_t)hh;
+    rgb.assign((size_t)w * h * 3, 0.0f);
+    std::vector<unsigned char> px((size_t)w * 4);
+    for (uint32_t y = 0; y < h; y++)
+    {
+        unsigned char head[4];
+        if (!f.read(reinterpret_cast<char*>(head), 4)) { err = path + ": truncated"; return RT_E_FORMAT; }
+        if (w >= 8 && w <= 32767 && head[0] == 2 && head[1] == 2 && ((uint32_t)head[2] << 8 | head[3]) == w)
+        {
+            for (int c = 0; c < 4; c++)
+            {
+                uint32_t x = 0;
+                while (x < w)
+                {
+                    int cnt = f.get();
+                    if (cnt == EOF) { err = path + ": truncated"; return RT_E_FORMAT; }
+                    if (cnt > 128)
+                    {
+                        cnt -= 128;
+                        const int v = f.get();
+                        if (v == EOF || x + (uint32_t)cnt > w) { err = path + ": bad run"; return RT_E_FORMAT; }
+                        for (int k = 0; k < cnt; k++) { px[4 * (size_t)(x++) + c] = (unsigned char)v; }
+                    }
+                    else
+                    {
+                        if (cnt == 0 || x + (uint32_t)cnt > w) { err = path + ": bad literal"; return RT_E_FORMAT; }
+                        for (int k = 0; k < cnt; k++)
+                        {
+                            const int v = f.get();
+                            if (v == EOF) { err = path + ": truncated"; return RT_E_FORMAT; }
+                            px[4 * (size_t)(x++) + c] = (unsigned char)v;
+                        }
+                    }
+                }
+            }
+        }
+        else
+        {
+            std::memcpy(px.data(), head, 4);
+            if (w > 1 && !f.read(reinterpret_cast<char*>(px.data() + 4), (std::streamsize)(4 * ((size_t)w - 1))))
+            {
+                err = path + ": truncated";
+                return RT_E_FORMAT;
+            }
+        }
+        for (uint32_t x = 0; x < w; x++) { from_rgbe(&px[4 * (size_t)x], &rgb[3 * ((size_t)y * w + x)]); }
+    }
+    return RT_OK;
+}
+
+SceneConfig parse_scene_config(const std::string& path)
+{
+    SceneConfig cfg;
+    cfg.camera = camera_lookat(V3(0.f, 1.f, -5.f), V3(0.f, 0.f, 0.f), 60.f);
+    std::ifstream f(path);
+    if (!f.is_open()) { return cfg; }
+    std::string line;
+    while (std::getline(f, line))
+    {
+        std::istringstream iss(line);
+        std::string token;
+        if (!(iss >> token) || token[0] == '#') { continue; }
+        if (token == "screen") { iss >> cfg.width >> cfg.height; }
+        else if (token == "camera")
+        {
+            float px, py, pz;
+            if (!(iss >> px >> py >> pz)) { continue; }
+            std::string next;
+            if (!(iss >> next)) { continue; }
+            if (next == "lookat")
+            {
+                float tx, ty, tz, fov = 60.f;
+                if (iss >> tx >> ty >> tz) { iss >> fov; }
+                cfg.camera = camera_lookat(V3(px, py, pz), V3(tx, ty, tz), fov);
+            }
+            else
+            {
+                float focal = 0.f;
+                try { focal = std::stof(next); } catch (...) { continue; }
+                float qx = 0.f, qy = 0.f, qz = 0.f, qw = 1.f;
+                std::string orient;
+                if ((iss >> orient) && orient == "q") { iss >> qx >> qy >> qz >> qw; }
+                cfg.camera = camera_quat(V3(px, py, pz), quat_normalize(Q(qx, qy, qz, qw)), focal);
+            }
+            cfg.has_camera = true;
+        }
+        else if (token == "ambient")
+        {
+            float r, g, b;
+            if (iss >> r >> g >> b) { cfg.ambient[0] = r; cfg.ambient[1] = g; cfg.ambient[2] = b; }
+        }
+        else if (token == "ibl") { iss >> cfg.ibl_path; }
+    }
+    return cfg;
 }
 
 } // namespace hg

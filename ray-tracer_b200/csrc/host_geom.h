@@ -73,4 +73,21 @@ int load_ply(const std::string& path, V3 translate, float scale, Q orient, std::
              std::vector<rt_triangle>& t, std::string& err);
 std::string replace_extension(const std::string& path, const std::string& ext);
 
+// Radiance RGBE (.hdr) images, RGB float in memory, rows in file order (top row first).
+int write_hdr(const std::string& path, const float* rgb, uint32_t w, uint32_t h, std::string& err);
+int read_hdr(const std::string& path, std::vector<float>& rgb, uint32_t& w, uint32_t& h, std::string& err);
+
+// The non-geometry lines of a .scn file (parseSceneConfig, src/main.cpp:207-285): screen,
+// camera (lookat or focal + quaternion), ambient, ibl. Defaults: 800 x 600, the look-at camera
+// from (0, 1, -5) to the origin with 60 degrees.
+struct SceneConfig
+{
+    int         width = 800, height = 600;
+    Camera      camera;
+    bool        has_camera = false;
+    float       ambient[3] = { 0.1f, 0.1f, 0.1f };
+    std::string ibl_path;
+};
+SceneConfig parse_scene_config(const std::string& path);
+
 } // namespace hg

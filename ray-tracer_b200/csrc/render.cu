@@ -10,6 +10,11 @@
 //                       one bounce per step; extend is the persistent trace kernel over the
 //                       compacted ray queue, shade writes the next queue and retires finished
 //                       paths into the image with atomics.
+// The wavefront also renders the scenes of a batched build together (rt_render_batch): a path
+// carries its scene, extend traces it from that scene's root, and each scene has its own
+// camera and seed, so scene s of a batch gets the samples a render of scene s alone gets. Its
+// launch sequence is replayed from a CUDA graph captured once per configuration, and its
+// block size, queue chunk and stack depth can be chosen by rt_autotune_wavefront.
 //
 // Random numbers: Philox4x32-10 (Salmon et al., SC'11) keyed by (seed, 0x5EED), counter
 // (pixel, sample, 0, 0) for the pixel jitter and (pixel, sample, bounce + 1, 0) for the
@@ -25,9 +30,19 @@
 #include "trace_core.cuh"
 
 #include <algorithm>
+#include <cstring>
+#include <vector>
 
 namespace rtb
 {
+
+// camera basis and RNG key of one scene (src/main.cpp:43-83)
+struct Cam
+{
+    float    pos[3], fwd[3], right[3], up[3];
+    float    th;
+    uint32_t seed;
+};
 
 namespace
 {
@@ -38,9 +53,10 @@ struct RP
     int32_t  rr_after;
     uint32_t env_kind;
     float    env[3];
-    float    pos[3], fwd[3], right[3], up[3];
-    float    th;
-    uint32_t seed, sample_offset;
+    Cam      cam;
+    uint32_t sample_offset;
+    uint32_t env_w, env_h;
+    const float* env_map;
 };
 
 __device__ __forceinline__ uint4 philox(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3, uint32_t k0, uint32_t k1)
@@ -95,20 +111,22 @@ __device__ __forceinline__ Surf surface(const Shade& S, uint32_t tri)
 constexpr float kPi = 3.14159265358979323846f;
 
 // primaryRay, src/main.cpp:69-83
-__device__ __forceinline__ void primary(const RP& P, uint32_t x, uint32_t y, uint32_t pix, uint32_t sidx, f3& o, f3& d)
+__device__ __forceinline__ void primary(const RP& P, const Cam& C, uint32_t x, uint32_t y, uint32_t pix, uint32_t sidx,
+                                        f3& o, f3& d)
 {
-    const uint4 r = philox(pix, sidx, 0u, 0u, P.seed, 0x5EEDu);
+    const uint4 r = philox(pix, sidx, 0u, 0u, C.seed, 0x5EEDu);
     const float aspect = (float)P.W / (float)P.H;
     const float u = (((float)x + u01(r.x)) / (float)P.W * 2.f - 1.f) * aspect;
     const float v = ((float)y + u01(r.y)) / (float)P.H * 2.f - 1.f;
-    const f3 fwd = mk3(P.fwd[0], P.fwd[1], P.fwd[2]);
-    const f3 rgt = mk3(P.right[0], P.right[1], P.right[2]);
-    const f3 up = mk3(P.up[0], P.up[1], P.up[2]);
-    o = mk3(P.pos[0], P.pos[1], P.pos[2]);
-    d = norm3(add3(add3(fwd, muls(rgt, u * P.th)), muls(up, v * P.th)));
+    const f3 fwd = mk3(C.fwd[0], C.fwd[1], C.fwd[2]);
+    const f3 rgt = mk3(C.right[0], C.right[1], C.right[2]);
+    const f3 up = mk3(C.up[0], C.up[1], C.up[2]);
+    o = mk3(C.pos[0], C.pos[1], C.pos[2]);
+    d = norm3(add3(add3(fwd, muls(rgt, u * C.th)), muls(up, v * C.th)));
 }
 
-// background (src/main.cpp:162-173)
+// background (src/main.cpp:162-173); env_kind 2: IBL::sample (main.cpp:107-117), the
+// nearest texel of an equirectangular map
 __device__ __forceinline__ f3 environment(const RP& P, f3 d)
 {
     if (P.env_kind == 0)
@@ -116,16 +134,28 @@ __device__ __forceinline__ f3 environment(const RP& P, f3 d)
         const float t = d.y * 0.5f + 0.5f;
         return add3(muls(mk3(1.0f, 1.0f, 1.0f), 1.f - t), muls(mk3(0.5f, 0.7f, 1.0f), t));
     }
+    if (P.env_kind == 2)
+    {
+        const float phi = atan2f(d.z, d.x);
+        const float y = d.y < -1.f ? -1.f : (1.f < d.y ? 1.f : d.y);  // std::clamp
+        const float theta = acosf(y);
+        const float u = (phi + kPi) / (2.f * kPi);
+        const float v = theta / kPi;
+        const int px = min((int)(u * (float)P.env_w), (int)P.env_w - 1);
+        const int py = min((int)(v * (float)P.env_h), (int)P.env_h - 1);
+        const float* p = P.env_map + ((size_t)py * P.env_w + px) * 3;
+        return mk3(__ldg(p), __ldg(p + 1), __ldg(p + 2));
+    }
     return mk3(P.env[0], P.env[1], P.env[2]);
 }
 
 // One bounce at a hit (src/main.cpp:178-200) after the emission of the surface was added:
 // the next direction (cosine hemisphere about the shading normal, or the mirror direction),
 // throughput update and Russian roulette. Returns false when roulette ends the path.
-__device__ __forceinline__ bool scatter(const RP& P, const Surf& sf, f3 n, f3 din, uint32_t pix, uint32_t sidx,
-                                        uint32_t bounce, f3& tp, f3& dout)
+__device__ __forceinline__ bool scatter(const RP& P, uint32_t seed, const Surf& sf, f3 n, f3 din, uint32_t pix,
+                                        uint32_t sidx, uint32_t bounce, f3& tp, f3& dout)
 {
-    const uint4 r = philox(pix, sidx, bounce + 1u, 0u, P.seed, 0x5EEDu);
+    const uint4 r = philox(pix, sidx, bounce + 1u, 0u, seed, 0x5EEDu);
     if (sf.kind == 1)
     {
         dout = sub3(din, muls(n, 2.f * dot3(din, n)));
@@ -157,7 +187,7 @@ __device__ __forceinline__ f3 path_sample(const TraceCtx& T, const RP& P, const 
                                           uint32_t pix, uint32_t sidx)
 {
     f3 o, d;
-    primary(P, x, y, pix, sidx, o, d);
+    primary(P, P.cam, x, y, pix, sidx, o, d);
     float tmin = 1e-3f;
     f3 tp = mk3(1.f, 1.f, 1.f), L = mk3(0.f, 0.f, 0.f);
     for (uint32_t bounce = 0; bounce <= P.max_bounce; bounce++)
@@ -172,7 +202,7 @@ __device__ __forceinline__ f3 path_sample(const TraceCtx& T, const RP& P, const 
         L = add3(L, mul3(tp, sf.emission));
         const f3 n = hit_normal(T, H.tri, H.u, H.v);
         f3 nd;
-        if (!scatter(P, sf, n, d, pix, sidx, bounce, tp, nd)) { break; }
+        if (!scatter(P, P.cam.seed, sf, n, d, pix, sidx, bounce, tp, nd)) { break; }
         o = add3(o, muls(d, H.t));
         d = nd;
         tmin = 1e-4f;
@@ -256,7 +286,7 @@ k_adjoint(TraceCtx T, RP P, Shade S, const float* __restrict__ dimg, float* __re
         if (act) { Ltot = path_sample(T, P, S, x, y, pix, sidx); }
         // replay
         f3 o = mk3(0.f, 0.f, 0.f), d = mk3(0.f, 0.f, 1.f);
-        if (act) { primary(P, x, y, pix, sidx, o, d); }
+        if (act) { primary(P, P.cam, x, y, pix, sidx, o, d); }
         float tmin = 1e-3f;
         f3 tp = mk3(1.f, 1.f, 1.f), Ssum = mk3(0.f, 0.f, 0.f);
         bool alive = act;
@@ -282,7 +312,10 @@ k_adjoint(TraceCtx T, RP P, Shade S, const float* __restrict__ dimg, float* __re
                              sf.albedo.z != 0.f ? dl.z * rest.z / sf.albedo.z : 0.f);
                     const f3 n = hit_normal(T, H.tri, H.u, H.v);
                     f3 nd;
-                    if (!scatter(P, sf, n, d, pix, sidx, bounce, tp, nd) || bounce >= P.max_bounce) { alive = false; }
+                    if (!scatter(P, P.cam.seed, sf, n, d, pix, sidx, bounce, tp, nd) || bounce >= P.max_bounce)
+                    {
+                        alive = false;
+                    }
                     o = add3(o, muls(d, H.t));
                     d = nd;
                     tmin = 1e-4f;
@@ -295,65 +328,77 @@ k_adjoint(TraceCtx T, RP P, Shade S, const float* __restrict__ dimg, float* __re
 }
 
 // ---- wavefront ----
-// ray queue: rt_ray records (o, tmin, d, tmax); path state: (tp.xyz, pixel), (L.xyz, sample)
+// ray queue: rt_ray records (o, tmin, d, tmax); path state: (tp.xyz, image pixel), (L.xyz,
+// sample); scene queue: the scene of each ray (batched renders). Image pixel = scene * W * H
+// + pixel of the scene. Paths are numbered sample-major: g = (sample * S + scene) * W * H + pixel.
 
 __global__ void __launch_bounds__(256)
-k_wf_generate(RP P, uint32_t s0, uint32_t n_paths, float4* __restrict__ rays, float4* __restrict__ state,
-              uint32_t* __restrict__ count)
+k_wf_generate(RP P, const Cam* __restrict__ cams, uint32_t S, uint64_t g0, uint32_t n_paths, float4* __restrict__ rays,
+              float4* __restrict__ state, uint32_t* __restrict__ rscene, uint32_t* __restrict__ count)
 {
     const uint32_t i = blockIdx.x * 256 + threadIdx.x;
     if (i == 0) { *count = n_paths; }
     if (i >= n_paths) { return; }
-    const uint32_t npix = P.W * P.H;
-    const uint32_t pix = i % npix, s = s0 + i / npix;
+    const uint64_t npix = (uint64_t)P.W * P.H;
+    const uint64_t g = g0 + i;
+    const uint32_t s = (uint32_t)(g / (npix * S));
+    const uint64_t rem = g - (uint64_t)s * npix * S;
+    const uint32_t sc = (uint32_t)(rem / npix);
+    const uint32_t pix = (uint32_t)(rem - (uint64_t)sc * npix);
     const uint32_t x = pix % P.W, y = pix / P.W;
+    const Cam C = cams ? cams[sc] : P.cam;
     f3 o, d;
-    primary(P, x, y, pix, P.sample_offset + s, o, d);
+    primary(P, C, x, y, pix, P.sample_offset + s, o, d);
     rays[2 * i] = make_float4(o.x, o.y, o.z, 1e-3f);
     rays[2 * i + 1] = make_float4(d.x, d.y, d.z, bits2f(0x7f800000u));
-    state[2 * i] = make_float4(1.f, 1.f, 1.f, __uint_as_float(pix));
+    state[2 * i] = make_float4(1.f, 1.f, 1.f, __uint_as_float((uint32_t)(sc * npix + pix)));
     state[2 * i + 1] = make_float4(0.f, 0.f, 0.f, __uint_as_float(P.sample_offset + s));
+    if (rscene) { rscene[i] = sc; }
 }
 
-__device__ __forceinline__ void retire(float* acc, float* acc2, uint32_t pix, f3 L)
+__device__ __forceinline__ void retire(float* acc, float* acc2, uint32_t gpix, f3 L)
 {
-    atomicAdd(&acc[3 * pix], L.x); atomicAdd(&acc[3 * pix + 1], L.y); atomicAdd(&acc[3 * pix + 2], L.z);
+    atomicAdd(&acc[3 * (size_t)gpix], L.x); atomicAdd(&acc[3 * (size_t)gpix + 1], L.y); atomicAdd(&acc[3 * (size_t)gpix + 2], L.z);
     if (acc2)
     {
-        atomicAdd(&acc2[3 * pix], L.x * L.x); atomicAdd(&acc2[3 * pix + 1], L.y * L.y); atomicAdd(&acc2[3 * pix + 2], L.z * L.z);
+        atomicAdd(&acc2[3 * (size_t)gpix], L.x * L.x); atomicAdd(&acc2[3 * (size_t)gpix + 1], L.y * L.y);
+        atomicAdd(&acc2[3 * (size_t)gpix + 2], L.z * L.z);
     }
 }
 
 __global__ void __launch_bounds__(256)
-k_wf_shade(TraceCtx T, RP P, Shade S, uint32_t bounce,
-           const uint32_t* __restrict__ count_in, const float4* __restrict__ rays, const float4* __restrict__ state,
-           const float4* __restrict__ hits, float4* __restrict__ rays_out, float4* __restrict__ state_out,
+k_wf_shade(TraceCtx T, RP P, Shade S, const Cam* __restrict__ cams, uint32_t bounce, const uint32_t* __restrict__ count_in,
+           const float4* __restrict__ rays, const float4* __restrict__ state, const float4* __restrict__ hits,
+           float4* __restrict__ rays_out, float4* __restrict__ state_out, uint32_t* __restrict__ rscene_out,
            uint32_t* __restrict__ count_out, float* __restrict__ acc, float* __restrict__ acc2)
 {
     const uint32_t n = *count_in;
-    for (uint32_t i = blockIdx.x * 256 + threadIdx.x; i < n; i += gridDim.x * 256)
+    const uint32_t npix = P.W * P.H;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
     {
         const float4 r0 = rays[2 * i], r1 = rays[2 * i + 1];
         const float4 s0 = state[2 * i], s1 = state[2 * i + 1];
         const float4 h0 = hits[2 * i], h1 = hits[2 * i + 1];
-        const uint32_t pix = __float_as_uint(s0.w), sidx = __float_as_uint(s1.w);
+        const uint32_t gpix = __float_as_uint(s0.w), sidx = __float_as_uint(s1.w);
         f3 tp = mk3(s0.x, s0.y, s0.z), L = mk3(s1.x, s1.y, s1.z);
         const f3 o = mk3(r0.x, r0.y, r0.z), d = mk3(r1.x, r1.y, r1.z);
         const uint32_t flags = __float_as_uint(h1.w);
         if (!(flags & RT_HIT_FLAG_HIT))
         {
             L = add3(L, mul3(tp, environment(P, d)));
-            retire(acc, acc2, pix, L);
+            retire(acc, acc2, gpix, L);
             continue;
         }
+        const uint32_t sc = gpix / npix, pix = gpix - sc * npix;
+        const uint32_t seed = cams ? cams[sc].seed : P.cam.seed;
         const f3 nrm = mk3(h1.x, h1.y, h1.z);
         const Surf sf = surface(S, __float_as_uint(h0.w));
         L = add3(L, mul3(tp, sf.emission));
         f3 nd;
-        const bool alive = scatter(P, sf, nrm, d, pix, sidx, bounce, tp, nd);
+        const bool alive = scatter(P, seed, sf, nrm, d, pix, sidx, bounce, tp, nd);
         if (!alive || bounce >= P.max_bounce)
         {
-            retire(acc, acc2, pix, L);
+            retire(acc, acc2, gpix, L);
             continue;
         }
         const f3 no = add3(o, muls(d, h0.x));
@@ -362,32 +407,200 @@ k_wf_shade(TraceCtx T, RP P, Shade S, uint32_t bounce,
         rays_out[2 * j + 1] = make_float4(nd.x, nd.y, nd.z, bits2f(0x7f800000u));
         state_out[2 * j] = make_float4(tp.x, tp.y, tp.z, s0.w);
         state_out[2 * j + 1] = make_float4(L.x, L.y, L.z, s1.w);
+        if (rscene_out) { rscene_out[j] = sc; }
     }
 }
 
-__global__ void k_wf_finish(const float* __restrict__ acc, const float* __restrict__ acc2, uint32_t n, float spp,
+__global__ void k_wf_finish(const float* __restrict__ acc, const float* __restrict__ acc2, uint64_t n, float spp,
                             float* __restrict__ rgb, float* __restrict__ rgb2)
 {
-    const uint32_t i = blockIdx.x * 256 + threadIdx.x;
+    const uint64_t i = (uint64_t)blockIdx.x * 256 + threadIdx.x;
     if (i >= n) { return; }
     rgb[i] = acc[i] / spp;
     if (rgb2) { rgb2[i] = acc2[i] / spp; }
 }
 
-RP make_rp(const rt_render_cfg& c)
+Cam make_cam(const rt_render_cfg& c)
+{
+    Cam C;
+    for (int k = 0; k < 3; k++) { C.pos[k] = c.cam_pos[k]; C.fwd[k] = c.cam_fwd[k]; C.right[k] = c.cam_right[k]; C.up[k] = c.cam_up[k]; }
+    C.th = c.tan_half_fov_y;
+    C.seed = c.seed;
+    return C;
+}
+
+RP make_rp(const rt_render_cfg& c, const rt_shading& sh)
 {
     RP P;
+    std::memset(&P, 0, sizeof(P));
+    P.env_map = sh.env_map; P.env_w = sh.env_w; P.env_h = sh.env_h;
     P.W = c.width; P.H = c.height; P.spp = c.spp; P.max_bounce = c.max_bounce; P.rr_after = c.rr_after;
     P.env_kind = c.env_kind;
-    for (int k = 0; k < 3; k++)
-    {
-        P.env[k] = c.env_color[k]; P.pos[k] = c.cam_pos[k]; P.fwd[k] = c.cam_fwd[k];
-        P.right[k] = c.cam_right[k]; P.up[k] = c.cam_up[k];
-    }
-    P.th = c.tan_half_fov_y;
-    P.seed = c.seed;
+    for (int k = 0; k < 3; k++) { P.env[k] = c.env_color[k]; }
+    P.cam = make_cam(c);
     P.sample_offset = c.sample_offset;
     return P;
+}
+
+// One wavefront render: S scenes (1 for a plain handle), per-scene cameras on the device
+// (nullptr: P.cam) and subtree roots (nullptr: the handle's root).
+struct WfJob
+{
+    RP              P;
+    const Cam*      cams;
+    uint32_t        S;
+    Shade           sh;
+    const TraceRoot* roots;
+    float*          rgb;
+    float*          rgb2;
+};
+
+constexpr uint32_t kMaxBounceQueues = 64;
+
+int wf_buffers(rt_bvh* B, const WfJob& J, const rt_wavefront_params& W)
+{
+    const uint64_t chunk = W.chunk_paths;
+    const uint64_t nimg = (uint64_t)J.S * J.P.W * J.P.H * 3;
+    for (int k = 0; k < 2; k++)
+    {
+        if (B->wf_rays[k].ensure(chunk * 32) || B->wf_state[k].ensure(chunk * 32) ||
+            (J.S > 1 && B->wf_scene[k].ensure(chunk * 4)))
+        {
+            return RT_E_CUDA;
+        }
+    }
+    if (B->wf_hits.ensure(chunk * 32) || B->wf_acc.ensure(nimg * 4 * 2) ||
+        B->wf_ctr.ensure((size_t)kMaxBounceQueues * 16 + 64) || B->trace_status.ensure(64))
+    {
+        return RT_E_CUDA;
+    }
+    return RT_OK;
+}
+
+// Issues every launch of the render on st: no host synchronisation and no allocation, so the
+// sequence can be captured into a CUDA graph. Returns the kernel launches issued via *n_kernels.
+int wf_issue(rt_bvh* B, const WfJob& J, const rt_wavefront_params& W, cudaStream_t st, uint32_t* n_kernels)
+{
+    const TraceCtx T = make_trace_ctx(B);
+    const RP& P = J.P;
+    const uint64_t npix = (uint64_t)P.W * P.H;
+    const uint64_t total = npix * J.S * P.spp;
+    const uint64_t nimg = npix * J.S * 3;
+    const uint32_t nb = P.max_bounce + 2;
+    float* acc = B->wf_acc.as<float>();
+    float* acc2 = J.rgb2 ? acc + nimg : nullptr;
+    uint32_t* counts = B->wf_ctr.as<uint32_t>();  // per bounce queue length
+    unsigned long long* tctr = reinterpret_cast<unsigned long long*>(counts + 2 * kMaxBounceQueues);  // per bounce trace counter
+    uint32_t* status = B->trace_status.as<uint32_t>() + 4;
+    const int sms = device_sm_count();
+    const int sblk = W.shade_block ? (int)W.shade_block : 256;
+    uint32_t nk = 0;
+    RT_CUDA(cudaMemsetAsync(acc, 0, nimg * 4 * (J.rgb2 ? 2 : 1), st));
+    TraceLaunch tl;
+    tl.block = (int)W.trace_block;
+    tl.stack = (int)W.stack_depth;
+    tl.roots = J.roots;
+    for (uint64_t g0 = 0; g0 < total; g0 += W.chunk_paths)
+    {
+        const uint32_t n_paths = (uint32_t)std::min<uint64_t>(W.chunk_paths, total - g0);
+        RT_CUDA(cudaMemsetAsync(counts, 0, (size_t)kMaxBounceQueues * 16, st));
+        k_wf_generate<<<(n_paths + 255) / 256, 256, 0, st>>>(P, J.cams, J.S, g0, n_paths, B->wf_rays[0].as<float4>(),
+                                                              B->wf_state[0].as<float4>(),
+                                                              J.S > 1 ? B->wf_scene[0].as<uint32_t>() : nullptr, counts);
+        nk++;
+        int cur = 0;
+        for (uint32_t b = 0; b <= P.max_bounce; b++)
+        {
+            tl.rscene = J.S > 1 ? B->wf_scene[cur].as<uint32_t>() : nullptr;
+            if (int e = trace_launch(B, B->wf_rays[cur].p, B->wf_hits.p, 0, counts + b, 0u, st, status, tctr + b, tl)) { return e; }
+            k_wf_shade<<<sms * 2048 / sblk, sblk, 0, st>>>(T, P, J.sh, J.cams, b, counts + b, B->wf_rays[cur].as<float4>(),
+                                                         B->wf_state[cur].as<float4>(), B->wf_hits.as<float4>(),
+                                                         B->wf_rays[cur ^ 1].as<float4>(), B->wf_state[cur ^ 1].as<float4>(),
+                                                         J.S > 1 ? B->wf_scene[cur ^ 1].as<uint32_t>() : nullptr,
+                                                         counts + b + 1, acc, acc2);
+            nk += 2;
+            cur ^= 1;
+        }
+        if (int e = check_launch("wavefront")) { return e; }
+        (void)nb;
+    }
+    k_wf_finish<<<(uint32_t)((nimg + 255) / 256), 256, 0, st>>>(acc, acc2, nimg, (float)P.spp, J.rgb, J.rgb2);
+    nk++;
+    if (n_kernels) { *n_kernels = nk; }
+    return check_launch("wavefront finish");
+}
+
+rt_wavefront_params default_params()
+{
+    rt_wavefront_params W;
+    W.trace_block = 128;
+    W.chunk_paths = 1u << 22;
+    W.stack_depth = 64;
+    W.shade_block = 256;
+    return W;
+}
+
+int check_params(const rt_wavefront_params& W)
+{
+    if (W.trace_block == 0 || W.trace_block % 32 || W.trace_block > 256) { return fail(RT_E_INVALID, "trace_block must be 32..256, a multiple of 32"); }
+    if (W.shade_block == 0 || W.shade_block % 32 || W.shade_block > 1024) { return fail(RT_E_INVALID, "shade_block must be 32..1024, a multiple of 32"); }
+    if (W.chunk_paths < 1024 || W.chunk_paths > (1u << 26)) { return fail(RT_E_INVALID, "chunk_paths must be in [1024, 2^26]"); }
+    if (W.stack_depth != 32 && W.stack_depth != 64) { return fail(RT_E_INVALID, "stack_depth must be 32 or 64"); }
+    return RT_OK;
+}
+
+// Replays the job from the handle's cached CUDA graph (captured on first use of a
+// configuration) on the handle's own stream, ordered after / before the caller's stream.
+int wf_run_graph(rt_bvh* B, const WfJob& J, const rt_wavefront_params& W, cudaStream_t st)
+{
+    if (int e = wf_buffers(B, J, W)) { return e; }
+    // the graph bakes in kernel arguments and buffer addresses: all of them form its key
+    std::vector<unsigned char> key(sizeof(WfJob) + sizeof(W) + 16 * sizeof(void*));
+    std::memset(key.data(), 0, key.size());
+    std::memcpy(key.data(), &J, sizeof(WfJob));
+    std::memcpy(key.data() + sizeof(WfJob), &W, sizeof(W));
+    const void* ptrs[] = { B->wf_rays[0].p, B->wf_rays[1].p, B->wf_state[0].p, B->wf_state[1].p, B->wf_scene[0].p,
+                           B->wf_scene[1].p, B->wf_hits.p, B->wf_acc.p, B->wf_ctr.p, B->trace_status.p, B->gnodes.p,
+                           B->tripos.p, B->tris.p, B->verts.p, B->rootbuf.p, B->scene_roots.p };
+    std::memcpy(key.data() + sizeof(WfJob) + sizeof(W), ptrs, sizeof(ptrs));
+    if (!B->wf_stream)
+    {
+        RT_CUDA(cudaStreamCreateWithFlags(&B->wf_stream, cudaStreamNonBlocking));
+        RT_CUDA(cudaEventCreateWithFlags(&B->wf_ev[0], cudaEventDisableTiming));
+        RT_CUDA(cudaEventCreateWithFlags(&B->wf_ev[1], cudaEventDisableTiming));
+    }
+    if (!B->wf_exec || key != B->wf_key)
+    {
+        if (B->wf_exec) { cudaGraphExecDestroy(B->wf_exec); B->wf_exec = nullptr; }
+        RT_CUDA(cudaStreamBeginCapture(B->wf_stream, cudaStreamCaptureModeThreadLocal));
+        uint32_t nk = 0;
+        const int e = wf_issue(B, J, W, B->wf_stream, &nk);
+        cudaGraph_t g = nullptr;
+        const cudaError_t ce = cudaStreamEndCapture(B->wf_stream, &g);
+        if (e) { if (g) { cudaGraphDestroy(g); } return e; }
+        if (ce != cudaSuccess) { return fail(RT_E_CUDA, std::string("graph capture: ") + cudaGetErrorString(ce)); }
+        const cudaError_t ie = cudaGraphInstantiate(&B->wf_exec, g, 0);
+        cudaGraphDestroy(g);
+        if (ie != cudaSuccess) { B->wf_exec = nullptr; return fail(RT_E_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ie)); }
+        B->wf_key = key;
+        B->wf_kernels = nk;
+    }
+    RT_CUDA(cudaEventRecord(B->wf_ev[0], st));
+    RT_CUDA(cudaStreamWaitEvent(B->wf_stream, B->wf_ev[0], 0));
+    RT_CUDA(cudaGraphLaunch(B->wf_exec, B->wf_stream));
+    count_launch(B->wf_kernels);
+    RT_CUDA(cudaEventRecord(B->wf_ev[1], B->wf_stream));
+    RT_CUDA(cudaStreamWaitEvent(st, B->wf_ev[1], 0));
+    return RT_OK;
+}
+
+// A valid parameter set for this handle: the tuned one, else the defaults (with the
+// stack the tree needs).
+rt_wavefront_params pick_params(const rt_bvh* B, const rt_wavefront_params* W)
+{
+    if (W) { return *W; }
+    if (B->wf_tuned_valid) { return B->wf_tuned; }
+    return default_params();
 }
 
 } // namespace
@@ -396,7 +609,7 @@ int render(const rt_bvh* B, const rt_render_cfg& cfg, const rt_shading& sh, int 
            cudaStream_t st)
 {
     const TraceCtx T = make_trace_ctx(B);
-    RP P = make_rp(cfg);
+    const RP P = make_rp(cfg, sh);
     const Shade S{ sh.mats, sh.mat_of_tri, sh.tri_albedo, sh.n_mats };
     if (mode == RT_RENDER_PLAIN)
     {
@@ -406,60 +619,104 @@ int render(const rt_bvh* B, const rt_render_cfg& cfg, const rt_shading& sh, int 
         return check_launch("render plain");
     }
     if (mode != RT_RENDER_WAVEFRONT) { return fail(RT_E_INVALID, "unknown render mode"); }
+    if (cfg.max_bounce + 2 > kMaxBounceQueues) { return fail(RT_E_INVALID, "max_bounce must be below 62 for the wavefront"); }
     rt_bvh* Bm = const_cast<rt_bvh*>(B);
-    const uint64_t npix = (uint64_t)cfg.width * cfg.height;
-    const uint64_t max_paths = 1ull << 22;  // paths in flight per chunk
-    uint32_t spc = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(cfg.spp, max_paths / std::max<uint64_t>(npix, 1)));
-    const uint64_t chunk = npix * spc;
-    const uint32_t nb = cfg.max_bounce + 2;
-    for (int k = 0; k < 2; k++)
+    WfJob J;
+    std::memset(&J, 0, sizeof(J));
+    J.P = P; J.cams = nullptr; J.S = 1; J.sh = S; J.roots = nullptr; J.rgb = rgb; J.rgb2 = rgb2;
+    rt_wavefront_params W = pick_params(B, nullptr);
+    if (W.stack_depth < 64) { W.stack_depth = 64; }  // tuned for a batch; a plain handle keeps the full stack
+    return wf_run_graph(Bm, J, W, st);
+}
+
+int render_batch(rt_bvh* B, const rt_render_cfg* cfgs, uint32_t S, const rt_shading& sh, const rt_wavefront_params* params,
+                 float* rgb, float* rgb2, cudaStream_t st)
+{
+    const rt_render_cfg& c0 = cfgs[0];
+    if (c0.max_bounce + 2 > kMaxBounceQueues) { return fail(RT_E_INVALID, "max_bounce must be below 62 for the wavefront"); }
+    const rt_wavefront_params W = pick_params(B, params);
+    if (int e = check_params(W)) { return e; }
+    if (W.stack_depth < 64)
     {
-        if (Bm->wf_rays[k].ensure(chunk * 32) || Bm->wf_state[k].ensure(chunk * 32)) { return RT_E_CUDA; }
+        uint32_t depth = 0;
+        if (int e = tree_depth(B, st, &depth)) { return e; }
+        if (depth + 1 > W.stack_depth) { return fail(RT_E_INVALID, "stack_depth is smaller than the tree needs"); }
     }
-    if (Bm->wf_hits.ensure(chunk * 32) || Bm->wf_acc.ensure(npix * 3 * 4 * 2) || Bm->wf_ctr.ensure((size_t)nb * 16 + 64) ||
-        Bm->trace_status.ensure(64))
+    std::vector<Cam> cams(S);
+    for (uint32_t s = 0; s < S; s++) { cams[s] = make_cam(cfgs[s]); }
+    if (B->wf_cams.ensure((size_t)S * sizeof(Cam))) { return RT_E_CUDA; }
+    RT_CUDA(cudaMemcpyAsync(B->wf_cams.p, cams.data(), (size_t)S * sizeof(Cam), cudaMemcpyHostToDevice, st));
+    WfJob J;
+    std::memset(&J, 0, sizeof(J));
+    J.P = make_rp(c0, sh);
+    J.cams = B->wf_cams.as<Cam>();
+    J.S = S;
+    J.sh = Shade{ sh.mats, sh.mat_of_tri, sh.tri_albedo, sh.n_mats };
+    J.roots = S > 1 ? B->scene_roots.as<TraceRoot>() : nullptr;  // one scene: the whole tree
+    J.rgb = rgb; J.rgb2 = rgb2;
+    if (S == 1) { J.cams = nullptr; J.P.cam = cams[0]; }
+    // (an upload from pageable memory has left the host vector when cudaMemcpyAsync returns)
+    return wf_run_graph(B, J, W, st);
+}
+
+int autotune_wavefront(rt_bvh* B, const rt_render_cfg* cfgs, uint32_t S, const rt_shading& sh, rt_wavefront_params* best,
+                       float* scratch_rgb, cudaStream_t st)
+{
+    uint32_t depth = 0;
+    if (int e = tree_depth(B, st, &depth)) { return e; }
+    std::vector<rt_render_cfg> c1(cfgs, cfgs + S);
+    for (auto& c : c1) { c.spp = 1; c.sample_offset = 0; }
+    const uint32_t blocks[] = { 64, 128, 256 };
+    const uint32_t chunks[] = { 1u << 20, 1u << 21, 1u << 22, 1u << 23 };
+    const uint32_t stacks[] = { 32, 64 };
+    cudaEvent_t a, b;
+    RT_CUDA(cudaEventCreate(&a));
+    RT_CUDA(cudaEventCreate(&b));
+    float best_ms = 1e30f;
+    rt_wavefront_params bw = default_params();
+    int err = RT_OK;
+    for (uint32_t stack : stacks)
     {
-        return RT_E_CUDA;
-    }
-    float* acc = Bm->wf_acc.as<float>();
-    float* acc2 = rgb2 ? acc + npix * 3 : nullptr;
-    RT_CUDA(cudaMemsetAsync(acc, 0, npix * 3 * 4 * 2, st));
-    uint32_t* counts = Bm->wf_ctr.as<uint32_t>();                                   // per bounce queue length
-    unsigned long long* tctr = reinterpret_cast<unsigned long long*>(counts + 2 * nb + 2);  // per bounce trace counter
-    uint32_t* status = Bm->trace_status.as<uint32_t>() + 4;
-    const int sms = device_sm_count();
-    for (uint32_t s0 = 0; s0 < cfg.spp; s0 += spc)
-    {
-        const uint32_t ns = std::min(spc, cfg.spp - s0);
-        const uint32_t n_paths = (uint32_t)(npix * ns);
-        RT_CUDA(cudaMemsetAsync(counts, 0, (size_t)nb * 16 + 64 - 0, st));
-        k_wf_generate<<<(n_paths + 255) / 256, 256, 0, st>>>(P, s0, n_paths, Bm->wf_rays[0].as<float4>(),
-                                                              Bm->wf_state[0].as<float4>(), counts);
-        count_launch();
-        int cur = 0;
-        for (uint32_t b = 0; b <= cfg.max_bounce; b++)
+        if (stack < 64 && depth + 1 > stack) { continue; }
+        for (uint32_t blk : blocks)
         {
-            if (int e = trace_launch(B, Bm->wf_rays[cur].p, Bm->wf_hits.p, 0, counts + b, 0u, st, status, tctr + b)) { return e; }
-            k_wf_shade<<<sms * 8, 256, 0, st>>>(T, P, S, b, counts + b, Bm->wf_rays[cur].as<float4>(),
-                                                Bm->wf_state[cur].as<float4>(), Bm->wf_hits.as<float4>(),
-                                                Bm->wf_rays[cur ^ 1].as<float4>(), Bm->wf_state[cur ^ 1].as<float4>(),
-                                                counts + b + 1, acc, acc2);
-            count_launch();
-            cur ^= 1;
+            for (uint32_t ch : chunks)
+            {
+                rt_wavefront_params W = default_params();
+                W.trace_block = blk; W.chunk_paths = ch; W.stack_depth = stack;
+                float ms = 0.f;
+                for (int rep = 0; rep < 2 && !err; rep++)  // the first run captures the graph
+                {
+                    if (cudaEventRecord(a, st) != cudaSuccess) { err = fail(RT_E_CUDA, "event"); break; }
+                    err = render_batch(B, c1.data(), S, sh, &W, scratch_rgb, nullptr, st);
+                    if (err) { break; }
+                    if (cudaEventRecord(b, st) != cudaSuccess || cudaEventSynchronize(b) != cudaSuccess)
+                    {
+                        err = fail(RT_E_CUDA, "event"); break;
+                    }
+                    cudaEventElapsedTime(&ms, a, b);
+                }
+                if (err) { break; }
+                if (ms < best_ms) { best_ms = ms; bw = W; }
+            }
+            if (err) { break; }
         }
-        if (int e = check_launch("wavefront")) { return e; }
+        if (err) { break; }
     }
-    const uint32_t nv = (uint32_t)(npix * 3);
-    k_wf_finish<<<(nv + 255) / 256, 256, 0, st>>>(acc, acc2, nv, (float)cfg.spp, rgb, rgb2);
-    count_launch();
-    return check_launch("wavefront finish");
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    if (err) { return err; }
+    B->wf_tuned = bw;
+    B->wf_tuned_valid = true;
+    if (best) { *best = bw; }
+    return RT_OK;
 }
 
 int adjoint(const rt_bvh* B, const rt_render_cfg& cfg, const rt_shading& sh, const float* d_rgb, float* g_alb,
             float* g_em, cudaStream_t st)
 {
     const TraceCtx T = make_trace_ctx(B);
-    const RP P = make_rp(cfg);
+    const RP P = make_rp(cfg, sh);
     const Shade S{ sh.mats, sh.mat_of_tri, sh.tri_albedo, sh.n_mats };
     const dim3 grid((cfg.width + 15) / 16, (cfg.height + 7) / 8);
     k_adjoint<<<grid, 128, 0, st>>>(T, P, S, d_rgb, g_alb, sh.mats ? g_em : nullptr);

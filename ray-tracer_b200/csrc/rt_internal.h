@@ -115,6 +115,9 @@ struct BuildScratch
     rtb::DevBuf sah_refs_a, sah_refs_b, sah_tmp, sah_pos, sah_lvl_a, sah_lvl_b, sah_dec, sah_out, sah_leaf_refs,
         sah_scan_in, sah_scan_out, sah_node_ids, sah_roots_lvl;
     rtb::DevBuf in_verts, in_tris;  // staging for host geometry
+    rtb::DevBuf gtris;              // batched build: triangles with concatenated-array vertex indices
+    rtb::DevBuf batch_off;          // batched build: triangle and vertex offsets per scene
+    rtb::DevBuf sah_budget;         // spatial-split budget per scene: used, cap
 };
 
 struct rt_bvh
@@ -124,10 +127,24 @@ struct rt_bvh
     uint32_t     n_nodes = 0, n_tris = 0, n_verts = 0;
     bool         has_prim = false;
     rtb::DevBuf  rootbuf;                   // traversal entry record (box and reference of node 0)
+    // batched builds: per scene {root node, node count, first triangle, triangle count} and the
+    // traversal entry record of each scene's root
+    uint32_t     n_scenes = 0;
+    rtb::DevBuf  scene_info, scene_roots;
+    std::vector<uint32_t> scene_info_host;
+    uint32_t     depth = 0;                 // tree depth (computed on demand; 0 = unknown)
     uint32_t     stats[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     BuildScratch s;
     rtb::DevBuf  trace_status, trace_rays, trace_hits;
     rtb::DevBuf  wf_rays[2], wf_state[2], wf_hits, wf_acc, wf_ctr;  // wavefront path tracer
+    rtb::DevBuf  wf_scene[2], wf_cams;      // scene of each queued ray; per-scene cameras
+    cudaStream_t wf_stream = nullptr;       // the graph replays here, fenced by wf_ev
+    cudaEvent_t  wf_ev[2] = { nullptr, nullptr };
+    cudaGraphExec_t wf_exec = nullptr;      // the captured launch sequence and its key
+    std::vector<unsigned char> wf_key;
+    uint32_t     wf_kernels = 0;
+    rt_wavefront_params wf_tuned = { 0, 0, 0, 0 };
+    bool         wf_tuned_valid = false;
     // stage timing (rt_bvh_profile): events at the stage boundaries of a build
     bool         prof = false;
     cudaEvent_t  ev[8] = { nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr };
@@ -148,6 +165,15 @@ namespace rtb
 // build.cu
 int build_bvh(rt_bvh* b, const rt_vertex* d_verts, uint32_t n_verts, const rt_triangle* d_tris, uint32_t n_tris,
               const rt_build_cfg& cfg, cudaStream_t st);
+// n_scenes scenes in one build; d_toff / d_voff: n_scenes + 1 triangle / vertex offsets on the
+// device, triangle vertex indices local to their scene.
+int build_bvh_batch(rt_bvh* b, const rt_vertex* d_verts, uint32_t n_verts, const rt_triangle* d_tris, uint32_t n_tris,
+                    const rt_build_cfg& cfg, cudaStream_t st, uint32_t n_scenes, const uint32_t* d_toff,
+                    const uint32_t* d_voff, const uint32_t* h_toff);
+// traverse.cu: the traversal entry record of every scene root of a batched build
+int launch_scene_roots(rt_bvh* b, uint32_t n_scenes, const uint32_t* d_counts, uint32_t* status, cudaStream_t st);
+// traverse.cu: depth of the tree (levels of inner nodes above the deepest leaf), cached in b->depth
+int tree_depth(rt_bvh* b, cudaStream_t st, uint32_t* depth);
 // traverse.cu: (re)creates the traversal layout from the .bvh-layout arrays on the device
 int make_traversal_layout(rt_bvh* b, cudaStream_t st);
 // The same kernels without a host synchronisation: grids sized for max_nodes / max_tris,
@@ -156,13 +182,27 @@ int launch_traversal_layout(rt_bvh* b, cudaStream_t st, uint32_t max_nodes, uint
                             uint32_t* vstatus);
 int trace(const rt_bvh* b, const rt_ray* d_rays, rt_hit* d_hits, uint64_t n, uint32_t flags, cudaStream_t st,
           uint32_t* d_status);
+// Launch options of the persistent trace kernel: block size (0: default), stack entries
+// (32 or 64; 32 only for closest hits), and per-ray subtree roots (roots[rscene[i]], device).
+struct TraceRoot;
+struct TraceLaunch
+{
+    int              block = 0;
+    int              stack = 64;
+    const TraceRoot* roots = nullptr;
+    const uint32_t*  rscene = nullptr;
+};
 // Launches the persistent trace kernel; n_dev (optional) holds the ray count on the device.
 // d_counter must be zero on entry.
 int trace_launch(const rt_bvh* b, const void* d_rays, void* d_hits, uint64_t n, const uint32_t* n_dev, uint32_t flags,
-                 cudaStream_t st, uint32_t* d_status, unsigned long long* d_counter);
+                 cudaStream_t st, uint32_t* d_status, unsigned long long* d_counter, const TraceLaunch& opt);
 // render.cu
 int render(const rt_bvh* b, const rt_render_cfg& cfg, const rt_shading& sh, int mode, float* rgb, float* rgb2,
            cudaStream_t st);
 int adjoint(const rt_bvh* b, const rt_render_cfg& cfg, const rt_shading& sh, const float* d_rgb, float* g_alb, float* g_em,
             cudaStream_t st);
+int render_batch(rt_bvh* b, const rt_render_cfg* cfgs, uint32_t n_scenes, const rt_shading& sh,
+                 const rt_wavefront_params* params, float* rgb, float* rgb2, cudaStream_t st);
+int autotune_wavefront(rt_bvh* b, const rt_render_cfg* cfgs, uint32_t n_scenes, const rt_shading& sh,
+                       rt_wavefront_params* best, float* scratch_rgb, cudaStream_t st);
 } // namespace rtb

@@ -409,43 +409,54 @@ k_sah_eval(const LvlNode* __restrict__ lv, const uint32_t* __restrict__ refs, Ct
 
 // One block: grants the spatial-split reference budget in queue order, then allocates child
 // slots (2 per split node), next-level references and leaf-store space by prefix sums.
-// io: [0] used references, [1] spatial taken, [2] spatial refused, [3] next-level nodes,
+// Each scene of a batched build has its own budget (used[s] of cap[s]), as a bake of that
+// scene alone would; the scene of level node i is that of its subtree root.
+// io: [1] spatial taken, [2] spatial refused, [3] next-level nodes,
 //     [4] next-level references, [5] leaf-store entries of this level, [6] leaves
+constexpr uint32_t MAX_BUDGET_SCENES = 1024;
+
 __global__ void __launch_bounds__(1024)
-k_sah_resolve(Dec* __restrict__ dec, uint32_t n_lvl, uint32_t cap, uint32_t* __restrict__ io,
+k_sah_resolve(Dec* __restrict__ dec, const LvlNode* __restrict__ lv, const SahRoot* __restrict__ roots, uint32_t n_lvl,
+              uint32_t n_scenes, uint32_t* __restrict__ used, const uint32_t* __restrict__ cap, uint32_t* __restrict__ io,
               uint32_t* __restrict__ child_slot, uint32_t* __restrict__ ref_off, uint32_t* __restrict__ leaf_off)
 {
     __shared__ uint32_t sh[33];
-    __shared__ unsigned long long s_need;
+    __shared__ unsigned long long s_need[MAX_BUDGET_SCENES];
     __shared__ int s_all;
     const int tid = threadIdx.x;
-    if (tid == 0) { s_need = 0ull; }
+    for (uint32_t k = tid; k < n_scenes; k += 1024) { s_need[k] = 0ull; }
+    if (tid == 0) { s_all = 1; }
     __syncthreads();
-    unsigned long long need = 0ull;
     uint32_t nsp = 0;
     for (uint32_t i = tid; i < n_lvl; i += 1024)
     {
         const Dec d = dec[i];
-        if (d.kind == K_SPATIAL) { need += (unsigned long long)d.right + d.straddle; nsp++; }
+        if (d.kind == K_SPATIAL)
+        {
+            atomicAdd(&s_need[min(roots[lv[i].root].scene, n_scenes - 1u)], (unsigned long long)d.right + d.straddle);
+            nsp++;
+        }
     }
-    atomicAdd(&s_need, need);
-    nsp = block_sum<1024>(nsp, sh);
-    if (tid == 0)
+    nsp = block_sum<1024>(nsp, sh);  // (synchronises the block)
+    for (uint32_t k = tid; k < n_scenes; k += 1024)
     {
-        const unsigned long long used = io[0];
-        s_all = (used + s_need <= (unsigned long long)cap) ? 1 : 0;
-        if (s_all) { io[0] = (uint32_t)(used + s_need); io[1] += nsp; }
+        if ((unsigned long long)used[k] + s_need[k] > (unsigned long long)cap[k]) { s_all = 0; }
     }
     __syncthreads();
-    if (!s_all && tid == 0)
+    if (s_all)
     {
-        uint32_t used = io[0];
+        for (uint32_t k = tid; k < n_scenes; k += 1024) { used[k] = (uint32_t)(used[k] + s_need[k]); }
+        if (tid == 0) { io[1] += nsp; }
+    }
+    else if (tid == 0)
+    {
         for (uint32_t i = 0; i < n_lvl; i++)
         {
             Dec d = dec[i];
             if (d.kind != K_SPATIAL) { continue; }
+            const uint32_t sc = min(roots[lv[i].root].scene, n_scenes - 1u);
             const uint32_t nd = d.right + d.straddle;
-            if ((unsigned long long)used + nd > (unsigned long long)cap)
+            if ((unsigned long long)used[sc] + nd > (unsigned long long)cap[sc])
             {
                 d.kind = d.fb_kind; d.pre_spatial = 1;
                 d.axis = d.oaxis; d.bin = d.obin; d.cmin = d.ocmin; d.scale = d.oscale;
@@ -454,11 +465,10 @@ k_sah_resolve(Dec* __restrict__ dec, uint32_t n_lvl, uint32_t cap, uint32_t* __r
             }
             else
             {
-                used += nd;
+                used[sc] += nd;
                 io[1]++;
             }
         }
-        io[0] = used;
     }
     __syncthreads();
     uint32_t c0 = 0, c1 = 0, c2 = 0, nleaf = 0;
@@ -747,6 +757,16 @@ int sah_build(rt_bvh* B, const rt_build_cfg& cfg, const SahInput& in, cudaStream
     uint32_t* io = new_off + nr;
     uint32_t io_h[8] = { in.n, 0, 0, 0, 0, 0, 0, 0 };
     RT_CUDA(cudaMemcpyAsync(io, io_h, 32, cudaMemcpyHostToDevice, st));
+    const uint32_t n_budget = (uint32_t)in.budget_used.size();
+    if (n_budget == 0 || n_budget > MAX_BUDGET_SCENES || in.budget_cap.size() != n_budget)
+    {
+        return fail(RT_E_INVALID, "SAH builder: bad spatial-split budget");
+    }
+    std::vector<uint32_t> budget(in.budget_used);
+    budget.insert(budget.end(), in.budget_cap.begin(), in.budget_cap.end());
+    if (S.sah_budget.ensure((size_t)budget.size() * 4)) { return RT_E_CUDA; }
+    uint32_t* d_used = S.sah_budget.as<uint32_t>();
+    RT_CUDA(cudaMemcpyAsync(d_used, budget.data(), budget.size() * 4, cudaMemcpyHostToDevice, st));
     // host copy of new-root offsets per level (uploaded as one array, sliced per level)
     std::vector<uint32_t> new_off_h(nr);
 
@@ -801,7 +821,8 @@ int sah_build(rt_bvh* B, const rt_build_cfg& cfg, const SahInput& in, cudaStream
         }
         levels.emplace_back(lvl_begin, out_total);
         k_sah_eval<<<n_cur, SBLK, 0, st>>>(lv_cur, refs_cur, C, S.sah_dec.as<Dec>());
-        k_sah_resolve<<<1, 1024, 0, st>>>(S.sah_dec.as<Dec>(), n_cur, cap, io, child_slot, ref_offs, leaf_offs);
+        k_sah_resolve<<<1, 1024, 0, st>>>(S.sah_dec.as<Dec>(), lv_cur, d_roots, n_cur, n_budget, d_used, d_used + n_budget,
+                                          io, child_slot, ref_offs, leaf_offs);
         count_launch(2);
         if (int e = check_launch("sah eval")) { return e; }
         RT_CUDA(cudaMemcpyAsync(io_h, io, 32, cudaMemcpyDeviceToHost, st));

@@ -3,6 +3,8 @@
 
 #include "rt_internal.h"
 
+#include <vector>
+
 namespace rtb
 {
 
@@ -18,7 +20,7 @@ struct SahRoot
     uint32_t depth;  // depth in the whole tree (BFS level of the reference's queue)
     uint32_t rank;   // left-spine rank in the Morton-split tree
     float    box[6]; // exact range box
-    uint32_t pad;
+    uint32_t scene;  // scene of a batched build (0 otherwise)
 };
 
 struct SahInput
@@ -34,6 +36,9 @@ struct SahInput
     uint32_t           n_roots;
     uint32_t*          wnode;  // per start key weights to fill for the roots
     uint32_t*          wtri;
+    // spatial-split budget per scene (one scene unless batched): references in use at the
+    // start (the scene's triangles) and the cap (bvh_morton.cpp:46-47)
+    std::vector<uint32_t> budget_used, budget_cap;
 };
 
 struct SahResult

@@ -103,19 +103,21 @@ struct THit
 };
 
 // Closest hit (MODE bit 0 clear) or first accepted hit (bit 0 set); bit 1 selects the
-// watertight triangle test. Reproduces the reference's visiting order exactly.
-template <int MODE>
-__device__ __forceinline__ THit trace_ray(const TraceCtx& T, rtd::f3 o, rtd::f3 d, float tmin, float tmax)
+// watertight triangle test. Reproduces the reference's visiting order exactly. STK entries of
+// stack: the loop holds at most one entry per level of the tree plus one, so a stack deeper
+// than the tree never overflows (overflow is reported, never silent). R: the subtree to trace.
+template <int MODE, int STK = STACK>
+__device__ __forceinline__ THit trace_ray(const TraceCtx& T, const TraceRoot& R, rtd::f3 o, rtd::f3 d, float tmin,
+                                          float tmax)
 {
     using namespace rtd;
-    uint32_t sref[STACK], scnt[STACK];
-    float stn[STACK];
+    uint32_t sref[STK], scnt[STK];
+    float stn[STK];
     const f3 inv = mk3(1.f / d.x, 1.f / d.y, 1.f / d.z);
     THit H;
     H.t = tmax; H.u = 0.f; H.v = 0.f; H.tri = 0; H.hit = false; H.overflow = false;
     float best = tmax;
     int top = 0;
-    const TraceRoot R = *T.root;
     const float troot = ray_box(o, inv, tmin, best, R.box[0], R.box[1], R.box[2], R.box[3], R.box[4], R.box[5]);
     if (troot < best) { sref[0] = R.ref; scnt[0] = R.cnt; stn[0] = troot; top = 1; }
     uint32_t pops = 0;
@@ -161,18 +163,26 @@ __device__ __forceinline__ THit trace_ray(const TraceCtx& T, rtd::f3 o, rtd::f3 
             else { fr = dd.x; fc = dd.z; ft = tl; nr = dd.y; nc = dd.w; nt = tr; }
             if (ft < best)
             {
-                if (top >= STACK) { H.overflow = true; break; }
+                if (top >= STK) { H.overflow = true; break; }
                 sref[top] = fr; scnt[top] = fc; stn[top] = ft; top++;
             }
             if (nt < best)
             {
-                if (top >= STACK) { H.overflow = true; break; }
+                if (top >= STK) { H.overflow = true; break; }
                 sref[top] = nr; scnt[top] = nc; stn[top] = nt; top++;
             }
         }
     }
     H.t = best;
     return H;
+}
+
+// The whole tree (the handle's root record).
+template <int MODE, int STK = STACK>
+__device__ __forceinline__ THit trace_ray(const TraceCtx& T, rtd::f3 o, rtd::f3 d, float tmin, float tmax)
+{
+    const TraceRoot R = *T.root;
+    return trace_ray<MODE, STK>(T, R, o, d, tmin, tmax);
 }
 
 // Interpolated shading normal of a hit: normalize(w n0 + u n1 + v n2), bvh_traverse.cpp:135-139.

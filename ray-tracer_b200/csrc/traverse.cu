@@ -20,6 +20,9 @@
 // the batch is exhausted, so long incoherent rays do not leave SMs idle at the tail.
 #include "trace_core.cuh"
 
+#include <mutex>
+#include <vector>
+
 namespace rtb
 {
 
@@ -84,15 +87,61 @@ __global__ void k_make_tripos(const rt_triangle* __restrict__ tris, uint32_t n, 
     tp[3 * i + 2] = make_float4(c.z, 0.f, 0.f, 0.f);
 }
 
+// Entry record of each scene root of a batched build; d_counts[0] = node count. A root
+// outside the node array (a record the build did not write) sets ST_CAPACITY.
+__global__ void k_scene_roots(const rt_bvh_node* __restrict__ nodes, const uint32_t* __restrict__ info, uint32_t S,
+                              const uint32_t* __restrict__ d_counts, TraceRoot* __restrict__ out,
+                              uint32_t* __restrict__ status)
+{
+    const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= S) { return; }
+    if (info[4 * s] >= d_counts[0])
+    {
+        atomicOr(status, ST_CAPACITY);
+        out[s] = TraceRoot{ { 0.f, 0.f, 0.f, 0.f, 0.f, 0.f }, 0u, LEAF_BIT };
+        return;
+    }
+    const rt_bvh_node nd = nodes[info[4 * s]];
+    TraceRoot r;
+    for (int k = 0; k < 3; k++) { r.box[k] = nd.bmin[k]; r.box[3 + k] = nd.bmax[k]; }
+    r.ref = nd.is_leaf ? nd.a : info[4 * s];
+    r.cnt = nd.is_leaf ? (LEAF_BIT | nd.b) : 0u;
+    out[s] = r;
+}
+
+// Tree depth: parent links (children of node i have larger indices), then every leaf counts
+// its ancestors (bounded by the node count).
+__global__ void k_parents(const rt_bvh_node* __restrict__ nodes, uint32_t n, uint32_t* __restrict__ par)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) { return; }
+    if (i == 0) { par[0] = 0xffffffffu; }
+    const rt_bvh_node nd = nodes[i];
+    if (!nd.is_leaf && nd.a < n && nd.b < n) { par[nd.a] = i; par[nd.b] = i; }
+}
+__global__ void k_depth(const rt_bvh_node* __restrict__ nodes, uint32_t n, const uint32_t* __restrict__ par,
+                        uint32_t* __restrict__ depth)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n || !nodes[i].is_leaf) { return; }
+    uint32_t d = 0;
+    for (uint32_t p = par[i]; p != 0xffffffffu && d < n; p = par[p]) { d++; }
+    atomicMax(depth, d);
+}
+
 // rt_ray records in, rt_hit records out (two 128-bit accesses each). n_dev, when set, holds
-// the ray count on the device (the wavefront path tracer's queue length).
-template <int MODE>
-__global__ void __launch_bounds__(TBLK)
+// the ray count on the device (the wavefront path tracer's queue length). ROOTS: ray i
+// traces the subtree roots[rscene[i]] (a scene of a batched build).
+template <int MODE, int STK, bool ROOTS>
+__global__ void __launch_bounds__(256)
 k_trace(TraceCtx T, const float4* __restrict__ rays, float4* __restrict__ hits, uint64_t n, const uint32_t* __restrict__ n_dev,
-        unsigned long long* __restrict__ counter, uint32_t* __restrict__ status)
+        unsigned long long* __restrict__ counter, uint32_t* __restrict__ status, const TraceRoot* __restrict__ roots,
+        const uint32_t* __restrict__ rscene)
 {
     const int lane = threadIdx.x & 31;
     if (n_dev) { n = *n_dev; }
+    TraceRoot R0;
+    if (!ROOTS) { R0 = *T.root; }
     for (;;)
     {
         unsigned long long base = 0;
@@ -102,7 +151,8 @@ k_trace(TraceCtx T, const float4* __restrict__ rays, float4* __restrict__ hits, 
         const uint64_t ri = base + (uint64_t)lane;
         if (ri >= n) { continue; }
         const float4 r0 = rays[2 * ri], r1 = rays[2 * ri + 1];
-        const THit H = trace_ray<MODE>(T, mk3(r0.x, r0.y, r0.z), mk3(r1.x, r1.y, r1.z), r0.w, r1.w);
+        const THit H = trace_ray<MODE, STK>(T, ROOTS ? roots[rscene[ri]] : R0, mk3(r0.x, r0.y, r0.z), mk3(r1.x, r1.y, r1.z),
+                                            r0.w, r1.w);
         float4 h0 = make_float4(0.f, 0.f, 0.f, 0.f), h1 = make_float4(0.f, 0.f, 0.f, 0.f);
         uint32_t flags = 0;
         if (H.hit)
@@ -119,7 +169,44 @@ k_trace(TraceCtx T, const float4* __restrict__ rays, float4* __restrict__ hits, 
     }
 }
 
-int g_blocks_per_sm = 0;
+using TraceFn = void (*)(TraceCtx, const float4*, float4*, uint64_t, const uint32_t*, unsigned long long*, uint32_t*,
+                         const TraceRoot*, const uint32_t*);
+
+TraceFn trace_fn(uint32_t flags, int stack, bool roots)
+{
+    if (stack <= 32)
+    {
+        if (roots) { return k_trace<0, 32, true>; }
+        return (flags & 3u) == 0 ? k_trace<0, 32, false> : nullptr;
+    }
+    if (roots) { return k_trace<0, STACK, true>; }
+    switch (flags & 3u)
+    {
+    case 0: return k_trace<0, STACK, false>;
+    case 1: return k_trace<1, STACK, false>;
+    case 2: return k_trace<2, STACK, false>;
+    default: return k_trace<3, STACK, false>;
+    }
+}
+
+// Resident blocks per SM, per kernel variant and block size.
+std::mutex g_occ_mu;
+struct OccKey { TraceFn fn; int block; int v; };
+std::vector<OccKey> g_occ;
+
+int blocks_per_sm(TraceFn fn, int block)
+{
+    std::lock_guard<std::mutex> lk(g_occ_mu);
+    for (const OccKey& k : g_occ)
+    {
+        if (k.fn == fn && k.block == block) { return k.v; }
+    }
+    int v = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, fn, block, 0) != cudaSuccess) { cudaGetLastError(); v = 1; }
+    if (v < 1) { v = 1; }
+    g_occ.push_back(OccKey{ fn, block, v });
+    return v;
+}
 
 } // namespace
 
@@ -169,32 +256,61 @@ int make_traversal_layout(rt_bvh* B, cudaStream_t st)
 }
 
 int trace_launch(const rt_bvh* B, const void* d_rays, void* d_hits, uint64_t n, const uint32_t* n_dev, uint32_t flags,
-                 cudaStream_t st, uint32_t* d_status, unsigned long long* d_counter)
+                 cudaStream_t st, uint32_t* d_status, unsigned long long* d_counter, const TraceLaunch& opt)
 {
-    if (!g_blocks_per_sm)
-    {
-        RT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&g_blocks_per_sm, k_trace<0>, TBLK, 0));
-        if (g_blocks_per_sm < 1) { g_blocks_per_sm = 1; }
-    }
-    uint64_t grid = (uint64_t)device_sm_count() * (uint64_t)g_blocks_per_sm;
+    const TraceFn fn = trace_fn(flags, opt.stack, opt.roots != nullptr);
+    if (!fn) { return fail(RT_E_INVALID, "no trace kernel for this mode and stack depth"); }
+    const int block = opt.block > 0 ? opt.block : TBLK;
+    if (block % 32 || block > 256) { return fail(RT_E_INVALID, "trace block must be a multiple of 32, at most 256"); }
+    uint64_t grid = (uint64_t)device_sm_count() * (uint64_t)blocks_per_sm(fn, block);
     if (!n_dev)
     {
-        const uint64_t want = (n + TBLK - 1) / TBLK;
+        const uint64_t want = (n + block - 1) / block;
         if (grid > want) { grid = want; }
     }
     if (grid == 0) { return RT_OK; }
     const TraceCtx T = make_trace_ctx(B);
-    const float4* r = static_cast<const float4*>(d_rays);
-    float4* h = static_cast<float4*>(d_hits);
-    switch (flags & 3u)
-    {
-    case 0: k_trace<0><<<(uint32_t)grid, TBLK, 0, st>>>(T, r, h, n, n_dev, d_counter, d_status); break;
-    case 1: k_trace<1><<<(uint32_t)grid, TBLK, 0, st>>>(T, r, h, n, n_dev, d_counter, d_status); break;
-    case 2: k_trace<2><<<(uint32_t)grid, TBLK, 0, st>>>(T, r, h, n, n_dev, d_counter, d_status); break;
-    default: k_trace<3><<<(uint32_t)grid, TBLK, 0, st>>>(T, r, h, n, n_dev, d_counter, d_status); break;
-    }
+    fn<<<(uint32_t)grid, block, 0, st>>>(T, static_cast<const float4*>(d_rays), static_cast<float4*>(d_hits), n, n_dev,
+                                         d_counter, d_status, opt.roots, opt.rscene);
     count_launch();
     return check_launch("trace");
+}
+
+int launch_scene_roots(rt_bvh* B, uint32_t S, const uint32_t* d_counts, uint32_t* status, cudaStream_t st)
+{
+    k_scene_roots<<<(S + 127) / 128, 128, 0, st>>>(B->nodes.as<rt_bvh_node>(), B->scene_info.as<uint32_t>(), S, d_counts,
+                                                   B->scene_roots.as<TraceRoot>(), status);
+    count_launch();
+    return check_launch("scene roots");
+}
+
+int tree_depth(rt_bvh* B, cudaStream_t st, uint32_t* depth)
+{
+    if (B->depth) { *depth = B->depth; return RT_OK; }
+    const uint32_t n = B->n_nodes;
+    DevBuf tmp;
+    if (tmp.ensure((size_t)n * 4 + 16)) { return RT_E_CUDA; }
+    uint32_t* par = tmp.as<uint32_t>();
+    uint32_t* d = par + n;
+    int e = RT_OK;
+    if (cudaMemsetAsync(d, 0, 4, st) != cudaSuccess) { e = fail(RT_E_CUDA, "memset"); }
+    if (!e)
+    {
+        k_parents<<<(n + 255) / 256, 256, 0, st>>>(B->nodes.as<rt_bvh_node>(), n, par);
+        k_depth<<<(n + 255) / 256, 256, 0, st>>>(B->nodes.as<rt_bvh_node>(), n, par, d);
+        count_launch(2);
+        e = check_launch("depth");
+    }
+    uint32_t v = 0;
+    if (!e && (cudaMemcpyAsync(&v, d, 4, cudaMemcpyDeviceToHost, st) != cudaSuccess || cudaStreamSynchronize(st) != cudaSuccess))
+    {
+        e = fail(RT_E_CUDA, "depth readback");
+    }
+    tmp.release();
+    if (e) { return e; }
+    B->depth = v;
+    *depth = v;
+    return RT_OK;
 }
 
 int trace(const rt_bvh* B, const rt_ray* d_rays, rt_hit* d_hits, uint64_t n, uint32_t flags, cudaStream_t st,
@@ -206,7 +322,7 @@ int trace(const rt_bvh* B, const rt_ray* d_rays, rt_hit* d_hits, uint64_t n, uin
     if (Bm->trace_status.ensure(64)) { return RT_E_CUDA; }
     unsigned long long* counter = Bm->trace_status.as<unsigned long long>();
     RT_CUDA(cudaMemsetAsync(counter, 0, 8, st));
-    return trace_launch(B, d_rays, d_hits, n, nullptr, flags, st, d_status, counter);
+    return trace_launch(B, d_rays, d_hits, n, nullptr, flags, st, d_status, counter, TraceLaunch{});
 }
 
 } // namespace rtb

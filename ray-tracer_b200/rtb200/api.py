@@ -47,8 +47,16 @@ class Material(C.Structure):
 
 
 class Shading(C.Structure):
-    _fields_ = [("mats", C.c_void_p), ("mat_of_tri", C.c_void_p), ("tri_albedo", C.c_void_p), ("n_mats", C.c_uint32),
-                ("pad", C.c_uint32)]
+    _fields_ = [("mats", C.c_void_p), ("mat_of_tri", C.c_void_p), ("tri_albedo", C.c_void_p), ("env_map", C.c_void_p),
+                ("n_mats", C.c_uint32), ("env_w", C.c_uint32), ("env_h", C.c_uint32), ("pad", C.c_uint32)]
+
+
+class WavefrontParams(C.Structure):
+    _fields_ = [("trace_block", C.c_uint32), ("chunk_paths", C.c_uint32), ("stack_depth", C.c_uint32),
+                ("shade_block", C.c_uint32)]
+
+    def as_dict(self):
+        return {k: int(getattr(self, k)) for k, _ in self._fields_}
 
 
 class RenderCfg(C.Structure):
@@ -99,6 +107,16 @@ def lib():
         L.rt_render.argtypes = [vp, vp, vp, u32, vp, i32, vp, vp, vp]
         L.rt_render_ex.argtypes = [vp, vp, vp, i32, vp, vp, vp]
         L.rt_adjoint.argtypes = [vp, vp, vp, vp, vp, vp, vp]
+        L.rt_build_batch.argtypes = [vp, vp, vp, vp, u32, i32, vp, vp, vp]
+        L.rt_rebuild_batch.argtypes = [vp, vp, vp, vp, vp, u32, i32, vp, vp]
+        L.rt_write_hdr.argtypes = [C.c_char_p, vp, u32, u32, i32]
+        L.rt_read_hdr.argtypes = [C.c_char_p, vp, vp, vp]
+        L.rt_scene_config.argtypes = [C.c_char_p, vp, C.c_char_p, u32]
+        L.rt_render_host.argtypes = [vp, vp, vp, i32, vp]
+        L.rt_bvh_scenes.argtypes = [vp, vp, vp]
+        L.rt_bvh_depth.argtypes = [vp, vp]
+        L.rt_render_batch.argtypes = [vp, vp, u32, vp, vp, vp, vp, vp]
+        L.rt_autotune_wavefront.argtypes = [vp, vp, u32, vp, vp, vp]
         L.rt_camera_lookat.argtypes = [vp, vp, C.c_float, vp]
         L.rt_camera_quat.argtypes = [vp, vp, C.c_float, vp]
         L.rt_mesh_create.restype = vp
@@ -203,6 +221,57 @@ class Bvh:
                                 C.byref(cfg) if cfg is not None else None, _stream_ptr(stream, where == RT_DEVICE)))
 
     @staticmethod
+    def build_batch(verts, tris, vert_offsets, tri_offsets, cfg: BuildCfg | str | None = None, stream=None) -> "Bvh":
+        """Many scenes in one build (rt_build_batch): verts / tris concatenated over the scenes
+        with vertex indices local to each scene, offsets (n_scenes + 1,) ascending from 0.
+        batch_arrays() makes these from a list of (verts, tris)."""
+        if isinstance(cfg, str):
+            cfg = make_cfg(cfg)
+        verts, tris, where = _geometry(verts, tris)
+        vo = np.ascontiguousarray(vert_offsets, np.uint32)
+        to = np.ascontiguousarray(tri_offsets, np.uint32)
+        out = C.c_void_p()
+        _check(lib().rt_build_batch(_ptr(verts), _ptr(vo), _ptr(tris), _ptr(to), int(to.shape[0] - 1), where,
+                                    C.byref(cfg) if cfg is not None else None, _stream_ptr(stream, where == RT_DEVICE),
+                                    C.byref(out)))
+        return Bvh(out)
+
+    def rebuild_batch(self, verts, tris, vert_offsets, tri_offsets, cfg: BuildCfg | str | None = None, stream=None):
+        if isinstance(cfg, str):
+            cfg = make_cfg(cfg)
+        verts, tris, where = _geometry(verts, tris)
+        vo = np.ascontiguousarray(vert_offsets, np.uint32)
+        to = np.ascontiguousarray(tri_offsets, np.uint32)
+        _check(lib().rt_rebuild_batch(self.h, _ptr(verts), _ptr(vo), _ptr(tris), _ptr(to), int(to.shape[0] - 1), where,
+                                      C.byref(cfg) if cfg is not None else None, _stream_ptr(stream, where == RT_DEVICE)))
+
+    def scenes(self):
+        """(n_scenes, 4) uint32: root node, node count, first triangle, triangle count per scene."""
+        n = C.c_uint32(0)
+        _check(lib().rt_bvh_scenes(self.h, C.byref(n), None))
+        info = np.zeros((n.value, 4), np.uint32)
+        if n.value:
+            _check(lib().rt_bvh_scenes(self.h, C.byref(n), _ptr(info)))
+        return info
+
+    def scene_arrays(self, s: int, vert_offsets, download=None):
+        """Scene s of a batched build in its own numbering: (nodes, tris, verts) as rt_build of
+        that scene alone lays them out."""
+        nodes, tris, verts = download if download is not None else self.download()
+        root, nn, t0, nt = (int(x) for x in self.scenes()[s])
+        v0, v1 = int(vert_offsets[s]), int(vert_offsets[s + 1])
+        sn = nodes[root:root + nn].copy()
+        inner = sn["is_leaf"] == 0
+        sn["a"] = np.where(inner, sn["a"] - root, sn["a"] - t0)
+        sn["b"] = np.where(inner, sn["b"] - root, sn["b"])
+        return sn, tris[t0:t0 + nt] - np.uint32(v0), verts[v0:v1]
+
+    def depth(self) -> int:
+        d = C.c_uint32(0)
+        _check(lib().rt_bvh_depth(self.h, C.byref(d)))
+        return int(d.value)
+
+    @staticmethod
     def load(path: str) -> "Bvh":
         out = C.c_void_p()
         _check(lib().rt_load_bvh(path.encode(), C.byref(out)))
@@ -291,14 +360,15 @@ class Bvh:
         return hits
 
     def render(self, rcfg: RenderCfg, mats=None, mat_of_tri=None, mode: int = RENDER_PLAIN, want_sq: bool = False,
-               stream=None, tri_albedo=None):
+               stream=None, tri_albedo=None, env_map=None):
         """Returns (rgb, rgb2) torch CUDA tensors (H, W, 3); mats: list of dicts or None;
         mat_of_tri: material index per baked triangle (numpy / torch); tri_albedo: (n_tris, 3)
-        float32 albedo per baked triangle (numpy / torch), replacing the materials' albedo."""
+        float32 albedo per baked triangle (numpy / torch), replacing the materials' albedo; env_map:
+        (h, w, 3) float32 equirectangular environment for env_kind 2."""
         import torch
         rgb = torch.empty((rcfg.height, rcfg.width, 3), dtype=torch.float32, device="cuda")
         rgb2 = torch.empty_like(rgb) if want_sq else None
-        sh, keep = _shading(mats, mat_of_tri, tri_albedo)
+        sh, keep = _shading(mats, mat_of_tri, tri_albedo, env_map)
         _check(lib().rt_render_ex(self.h, C.byref(rcfg), C.byref(sh), mode, _ptr(rgb), _ptr(rgb2),
                                   _stream_ptr(stream, True)))
         del keep
@@ -321,6 +391,68 @@ class Bvh:
         return g_alb, g_em
 
 
+    def render_batch(self, rcfgs, mats=None, mat_of_tri=None, params: WavefrontParams | None = None, want_sq=False,
+                     stream=None, tri_albedo=None):
+        """All scenes of a batched handle in one wavefront render: rcfgs = one RenderCfg per scene
+        (camera and seed; the rest from rcfgs[0]). Returns (rgb, rgb2) (n_scenes, H, W, 3)."""
+        import torch
+        n = len(rcfgs)
+        arr = (RenderCfg * n)(*rcfgs)
+        c0 = rcfgs[0]
+        rgb = torch.empty((n, c0.height, c0.width, 3), dtype=torch.float32, device="cuda")
+        rgb2 = torch.empty_like(rgb) if want_sq else None
+        sh, keep = _shading(mats, mat_of_tri, tri_albedo)
+        _check(lib().rt_render_batch(self.h, arr, n, C.byref(sh), C.byref(params) if params is not None else None,
+                                     _ptr(rgb), _ptr(rgb2), _stream_ptr(stream, True)))
+        del keep
+        return rgb, rgb2
+
+    def autotune(self, rcfgs, mats=None, mat_of_tri=None, stream=None) -> WavefrontParams:
+        n = len(rcfgs)
+        arr = (RenderCfg * n)(*rcfgs)
+        best = WavefrontParams()
+        sh, keep = _shading(mats, mat_of_tri, None)
+        _check(lib().rt_autotune_wavefront(self.h, arr, n, C.byref(sh), C.byref(best), _stream_ptr(stream, True)))
+        del keep
+        return best
+
+
+def write_hdr(path: str, rgb, flip_y: bool = False):
+    """Writes an (h, w, 3) float32 image as a Radiance RGBE .hdr file."""
+    a = np.ascontiguousarray(rgb, np.float32)
+    _check(lib().rt_write_hdr(path.encode(), _ptr(a), int(a.shape[1]), int(a.shape[0]), 1 if flip_y else 0))
+
+
+def read_hdr(path: str) -> np.ndarray:
+    """Reads a Radiance RGBE .hdr file into an (h, w, 3) float32 array (file row order)."""
+    w, h = C.c_uint32(0), C.c_uint32(0)
+    _check(lib().rt_read_hdr(path.encode(), None, C.byref(w), C.byref(h)))
+    out = np.zeros((h.value, w.value, 3), np.float32)
+    _check(lib().rt_read_hdr(path.encode(), _ptr(out), C.byref(w), C.byref(h)))
+    return out
+
+
+def scene_config(path: str, rcfg: RenderCfg | None = None):
+    """(RenderCfg with the .scn file's screen size and camera, ibl path or '')."""
+    c = rcfg if rcfg is not None else render_cfg(1, 1, 1)
+    buf = C.create_string_buffer(4096)
+    _check(lib().rt_scene_config(path.encode(), C.byref(c), buf, 4096))
+    return c, buf.value.decode()
+
+
+def batch_arrays(parts):
+    """(verts, tris, vert_offsets, tri_offsets) for rt_build_batch from a list of (verts, tris)
+    with per-scene vertex indices."""
+    vo = np.zeros(len(parts) + 1, np.uint32)
+    to = np.zeros(len(parts) + 1, np.uint32)
+    for i, (v, t) in enumerate(parts):
+        vo[i + 1] = vo[i] + v.shape[0]
+        to[i + 1] = to[i] + t.shape[0]
+    verts = np.concatenate([np.asarray(v, np.float32) for v, _ in parts])
+    tris = np.concatenate([np.asarray(t, np.uint32) for _, t in parts])
+    return verts, tris, vo, to
+
+
 def materials_array(mats) -> np.ndarray:
     """rt_material records (n, 8) float32 from a list of dicts (albedo, emission, kind)."""
     arr = np.zeros((len(mats), 8), np.float32)
@@ -340,11 +472,16 @@ def _device_u32(x):
     return torch.from_numpy(np.ascontiguousarray(x, np.uint32).view(np.int32)).cuda()
 
 
-def _shading(mats, mat_of_tri, tri_albedo):
+def _shading(mats, mat_of_tri, tri_albedo, env_map=None):
     """An rt_shading record over device copies of the inputs (kept alive by the caller)."""
     import torch
     sh = Shading()
     keep = []
+    if env_map is not None:
+        em = env_map if _is_torch(env_map) else torch.from_numpy(np.ascontiguousarray(env_map, np.float32))
+        em = em.to(device="cuda", dtype=torch.float32).contiguous()
+        keep.append(em)
+        sh.env_map, sh.env_h, sh.env_w = em.data_ptr(), int(em.shape[0]), int(em.shape[1])
     if mats is not None:
         dm = mats.contiguous().cuda() if _is_torch(mats) else torch.from_numpy(materials_array(mats)).cuda()
         keep.append(dm)

@@ -301,3 +301,43 @@ def large_scene(n_spheres: int = 400, tris_per_sphere: int = 12500, seed: int = 
     v, t, part = concat(parts)
     return Scene(v, t, part, mats, np.arange(len(parts)), ((0.5, 0.9, -1.6), (0.5, 0.35, 0.5), 45.0),
                  env_kind=1, env_color=(0.02, 0.02, 0.03))
+
+
+def batch_scene(n_tris: int, seed: int):
+    """One scene of the batched workload: a displaced icosphere (the smallest subdivision with
+    n_tris faces, truncated to them) or a triangle soup of n_tris triangles in the unit box
+    (even / odd seed), a floor and one quad area light above, all Lambertian, object albedo
+    uniform[0.2, 0.8]."""
+    rng = np.random.default_rng(seed)
+    if seed % 2 == 0:
+        level = 0
+        while 20 * 4 ** level < n_tris:
+            level += 1
+        ov, ot = icosphere(level, center=(0.5, 0.45, 0.5), radius=0.4, seed=seed, max_tris=n_tris)
+    else:
+        ov, ot = soup(n_tris, seed=seed)
+    fv, ft = quad((-1.0, -0.05, -1.0), (2.0, -0.05, -1.0), (2.0, -0.05, 2.0), (-1.0, -0.05, 2.0), (0, 1, 0))
+    lv, lt = quad((0.3, 1.5, 0.3), (0.7, 1.5, 0.3), (0.7, 1.5, 0.7), (0.3, 1.5, 0.7), (0, -1, 0))
+    v, t, part = concat([(ov, ot), (fv, ft), (lv, lt)])
+    a = rng.uniform(0.2, 0.8, size=3)
+    mats = [dict(albedo=tuple(float(x) for x in a)), dict(albedo=(0.5, 0.5, 0.5)),
+            dict(albedo=(0.0, 0.0, 0.0), emission=(12.0, 12.0, 12.0))]
+    return Scene(v, t, part, mats, np.arange(3), ((0.5, 0.9, -1.4), (0.5, 0.4, 0.5), 45.0))
+
+
+def batch_scenes(n_scenes: int = 64, lo: int = 1000, hi: int = 500000, seed: int = BASE_SEED + 2):
+    """The batched workload: n_scenes scenes with triangle counts log-uniform in [lo, hi]."""
+    rng = np.random.default_rng(seed)
+    counts = np.exp(rng.uniform(np.log(lo), np.log(hi), size=n_scenes)).astype(np.int64)
+    return [batch_scene(int(c), seed + 1 + i) for i, c in enumerate(counts)]
+
+
+def batch_shading(scs):
+    """Materials of a list of scenes concatenated, and the material of every input triangle
+    of the concatenated batch."""
+    mats, mot, off = [], [], 0
+    for sc in scs:
+        mats += sc.mats
+        mot.append(sc.mat_of_tri + off)
+        off += len(sc.mats)
+    return mats, np.concatenate(mot).astype(np.uint32)
