@@ -9,8 +9,15 @@ Mtri/s over all ranks (weak scaling: every rank bakes its own soup; no data-path
 
 Also reported: the same build end to end through the C ABI with host buffers (e2e), the other
 build presets, closest-hit / any-hit traversal of 16,777,216 incoherent rays and of 1920x1080
-pinhole rays (Mray/s), the roofline of the dominant kernel (the radix-sort pass), and the
-reference's own CPU bake timed on this host.
+pinhole rays (Mray/s), the roofline of the dominant kernel (the radix-sort pass), the
+reference's own CPU bake timed on this host, and under "render" the path-loop workloads:
+plain path tracing (256x256, 16 spp, depth 4, Cornell box + 20,480-triangle icosphere + two
+spheres; plain vs wavefront, and the CPU restatement on all host cores), the batched workload
+(64 scenes of 1,000-500,000 triangles built in one launch sequence and rendered at 512x512,
+4 spp, depth 5 by the graph-replayed wavefront vs the plain kernel per scene), the adjoint
+(512x512, 32 spp, depth 4, Cornell box + 50,000-triangle icosphere: adjoint / forward time)
+and the large render (1920x1080, 64 spp, depth 8, roulette after bounce 2, 5,000,000
+triangles, binned SAH with spatial splits).
 
 usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
        torchrun --nproc-per-node N bench.py --gpus N ...   (one process per GPU)
@@ -45,6 +52,7 @@ def parse_args():
     p.add_argument("--n-tris", type=int, default=N_TRIS)
     p.add_argument("--preset", default="lbvh63")
     p.add_argument("--no-extra", action="store_true", help="skip the secondary measurements")
+    p.add_argument("--no-render", action="store_true", help="skip the path-loop workloads")
     return p.parse_args()
 
 
@@ -299,6 +307,9 @@ def run_ours(a):
     extra = {}
     if not a.no_extra:
         extra = secondary(a, bvh, dv, dt, verts, stream, dev, flush)
+    render = {}
+    if not a.no_render and rank == 0:
+        render = render_workloads(stream, dev)
     out = None
     if rank == 0:
         with quiet_stdout():
@@ -319,7 +330,7 @@ def run_ours(a):
                "cpu_baseline": {"value": round(cpu_v, 4), "unit": "Mtri/s", "cores": 1, "kind": cpu_kind,
                                 "sample": "bvh::bakeBVH of a 131,072-triangle soup of the same generator, LBVH "
                                           "constants, 2 timed repetitions, 1 thread (the bake is single-threaded)"},
-               "clocks": clocks, "extra": extra}
+               "clocks": clocks, "extra": extra, "render": render}
         print(json.dumps(out), flush=True)
     if dist:
         dist.barrier()
@@ -366,6 +377,169 @@ def secondary(a, bvh, dv, dt, verts, stream, dev, flush):
                 res[f"trace_{preset}_{name}_{fname}_mray_s"] = round(r.shape[0] / (ms * 1e-3) / 1e6, 1)
         b.free()
     return res
+
+
+def _ev_ms(fn, stream, reps=3):
+    """Median CUDA-event time of fn on `stream` after one warm-up call."""
+    import torch
+    fn()
+    torch.cuda.synchronize()
+    ms = []
+    for _ in range(reps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms.append(e0.elapsed_time(e1))
+    return statistics.median(ms)
+
+
+def render_workloads(stream, dev):
+    """The path-loop workloads (GPU numbers by CUDA events on torch's stream)."""
+    import numpy as np
+    import torch
+    import rtb200
+    from rtb200 import scenes
+    sys.path.insert(0, os.path.join(HERE, "oracle"))
+    import oracle as orc
+    out = {}
+    mpx = lambda n, ms: round(n / (ms * 1e-3) / 1e6, 1)  # noqa: E731
+
+    # plain path tracing
+    sv, st_ = rtb200.Mesh().add_sphere((0.0, 0.0, 0.0), 0.3).arrays()
+    sc = scenes.plain_scene(sphere_tris=(sv, st_))
+    b = rtb200.Bvh.build(sc.verts, sc.tris, "lbvh30")
+    mot = torch.from_numpy(sc.baked_materials(b.prim_ids()).astype(np.int32)).to(dev)
+    mats = torch.from_numpy(rtb200.materials_array(sc.mats)).to(dev)
+    rc = rtb200.render_cfg(256, 256, 16, max_bounce=4, rr_after=-1, env_kind=1, seed=7, lookat=sc.lookat)
+    n = 256 * 256 * 16
+    tp = _ev_ms(lambda: b.render(rc, mats, mot, mode=rtb200.RENDER_PLAIN, stream=stream), stream)
+    tw = _ev_ms(lambda: b.render(rc, mats, mot, mode=rtb200.RENDER_WAVEFRONT, stream=stream), stream)
+    ip, _ = b.render(rc, mats, mot, mode=rtb200.RENDER_PLAIN)
+    iw, _ = b.render(rc, mats, mot, mode=rtb200.RENDER_WAVEFRONT)
+    ip64, iw64 = ip.double(), iw.double()
+    # CPU baseline: the restated path loop (the reference's pathTrace with per-pixel counter RNG,
+    # reference traversal) over 16 rows on all host cores, scaled to the metric
+    nodes, tris, vv = b.download()
+    R = orc.Restatement()
+    ocfg = orc.OrcRenderCfg()
+    for name, _ in orc.OrcRenderCfg._fields_:
+        val = getattr(rc, name)
+        if hasattr(val, "__len__"):
+            getattr(ocfg, name)[:] = list(val)
+        else:
+            setattr(ocfg, name, val)
+    cores = os.cpu_count() or 1
+    rows = 16
+    t0 = time.perf_counter()
+    ref, _ = R.render(orc.Baked(nodes, tris, vv), ocfg, sc.mats, sc.baked_materials(b.prim_ids()), rows=(120, 120 + rows),
+                      threads=cores)
+    cpu_s = time.perf_counter() - t0
+    sl = ip.cpu().numpy()[120:120 + rows].astype(np.float64)
+    out["plain_c1"] = {
+        "workload": "256x256, 16 spp, depth 4, no roulette; Cornell box + 20,480-tri icosphere + 2 spheres (21,462 tris), "
+                    "LBVH 30-bit",
+        "plain_mpx_spp_s": mpx(n, tp), "wavefront_mpx_spp_s": mpx(n, tw), "plain_ms": round(tp, 3), "wavefront_ms": round(tw, 3),
+        "wavefront_vs_plain_max_rel_diff": float(((iw64 - ip64).abs().max() / ip64.abs().max()).item()),
+        "cpu_mpx_spp_s": round(256 * rows * 16 / cpu_s / 1e6, 4), "cpu_cores": cores,
+        "cpu_kind": "port (the oracle's restated path loop over the reference traversal)",
+        "cpu_sample": f"{rows} image rows (of 256) at 16 spp",
+        "cpu_rows_rel_mean_error": float(abs(sl.mean() - ref[120:120 + rows].astype(np.float64).mean()) /
+                                         max(ref[120:120 + rows].mean(), 1e-12))}
+    b.free()
+
+    # batched scenes
+    scs = scenes.batch_scenes(64)
+    v, t, vo, to = rtb200.batch_arrays([(s_.verts, s_.tris) for s_ in scs])
+    dvb = torch.from_numpy(v).to(dev)
+    dtb = torch.from_numpy(t.view(np.int32)).to(dev)
+    cfg30 = rtb200.make_cfg("lbvh30")
+    bb = rtb200.Bvh.build_batch(dvb, dtb, vo, to, cfg30, stream=stream)
+    tbb = _ev_ms(lambda: bb.rebuild_batch(dvb, dtb, vo, to, cfg30, stream=stream), stream)
+    singles = [rtb200.Bvh.build(torch.from_numpy(s_.verts).to(dev), torch.from_numpy(s_.tris.view(np.int32)).to(dev), cfg30)
+               for s_ in scs]
+    sdev = [(torch.from_numpy(s_.verts).to(dev), torch.from_numpy(s_.tris.view(np.int32)).to(dev)) for s_ in scs]
+
+    def rebuild_all():
+        for bs, (x, y) in zip(singles, sdev):
+            bs.rebuild(x, y, cfg30, stream=stream)
+    tbs = _ev_ms(rebuild_all, stream)
+    bmats, bmot_in = scenes.batch_shading(scs)
+    bmot = torch.from_numpy(bmot_in[bb.prim_ids()].astype(np.int32)).to(dev)
+    bmats_d = torch.from_numpy(rtb200.materials_array(bmats)).to(dev)
+    rcs = [rtb200.render_cfg(512, 512, 4, max_bounce=5, rr_after=-1, env_kind=1, seed=31 + i, lookat=s_.lookat)
+           for i, s_ in enumerate(scs)]
+    t0 = time.perf_counter()
+    tuned = bb.autotune(rcs, bmats_d, bmot, stream=stream)
+    tune_s = time.perf_counter() - t0
+    tbr = _ev_ms(lambda: bb.render_batch(rcs, bmats_d, bmot, stream=stream), stream)
+    smats = [torch.from_numpy(rtb200.materials_array(s_.mats)).to(dev) for s_ in scs]
+    smot = [torch.from_numpy(s_.baked_materials(bs.prim_ids()).astype(np.int32)).to(dev) for s_, bs in zip(scs, singles)]
+
+    def plain_all():
+        for i, bs in enumerate(singles):
+            bs.render(rcs[i], smats[i], smot[i], mode=rtb200.RENDER_PLAIN, stream=stream)
+    tpa = _ev_ms(plain_all, stream, 2)
+    nb = 64 * 512 * 512 * 4
+    img, _ = bb.render_batch(rcs, bmats_d, bmot)
+    diffs = []
+    for i in (0, 21, 42, 63):
+        r_, _ = singles[i].render(rcs[i], smats[i], smot[i], mode=rtb200.RENDER_PLAIN)
+        diffs.append(float(((img[i].double() - r_.double()).abs().max() / max(float(r_.abs().max()), 1e-12))))
+    out["batched_c3"] = {
+        "workload": f"64 scenes, {int(to[-1])} triangles (log-uniform 1,000-500,000 per scene), 512x512, 4 spp, depth 5",
+        "build_batched_ms": round(tbb, 3), "build_batched_mtri_s": round(int(to[-1]) / tbb / 1e3, 1),
+        "build_64_separate_ms": round(tbs, 3),
+        "render_batched_wavefront_mpx_spp_s": mpx(nb, tbr), "render_plain_per_scene_mpx_spp_s": mpx(nb, tpa),
+        "render_batched_ms": round(tbr, 2), "render_plain_per_scene_ms": round(tpa, 2),
+        "autotuned": tuned.as_dict(), "autotune_s": round(tune_s, 2),
+        "batched_vs_plain_max_rel_diff": max(diffs)}
+    for bs in singles:
+        bs.free()
+    bb.free()
+    del dvb, dtb
+
+    # differentiable rendering: adjoint / forward
+    dsc, init, _gt = scenes.diff_scene()
+    bd = rtb200.Bvh.build(dsc.verts, dsc.tris, "lbvh30")
+    prim = bd.prim_ids()
+    dmot = torch.from_numpy(dsc.baked_materials(prim).astype(np.int32)).to(dev)
+    dmats = torch.from_numpy(rtb200.materials_array(dsc.mats)).to(dev)
+    talb = torch.from_numpy(init[prim]).to(dev)
+    rcd = rtb200.render_cfg(512, 512, 32, max_bounce=4, rr_after=-1, env_kind=1, seed=9, lookat=dsc.lookat)
+    fwd = _ev_ms(lambda: bd.render(rcd, dmats, dmot, tri_albedo=talb, stream=stream), stream)
+    img, _ = bd.render(rcd, dmats, dmot, tri_albedo=talb)
+    dimg = (2.0 * (img - 0.5 * img.mean())).contiguous()
+    adj = _ev_ms(lambda: bd.adjoint(rcd, dimg, dmats, dmot, tri_albedo=talb, stream=stream), stream)
+    out["adjoint_c4"] = {
+        "workload": "512x512, 32 spp, depth 4; Cornell box + 50,000-triangle icosphere; gradients of per-triangle RGB "
+                    "albedo and material emission",
+        "forward_ms": round(fwd, 2), "adjoint_ms": round(adj, 2), "adjoint_over_forward": round(adj / fwd, 3),
+        "forward_mpx_spp_s": mpx(512 * 512 * 32, fwd)}
+    bd.free()
+
+    # large render
+    lsc = scenes.large_scene()
+    dvl = torch.from_numpy(lsc.verts).to(dev)
+    dtl = torch.from_numpy(lsc.tris.view(np.int32)).to(dev)
+    bl = rtb200.Bvh.build(dvl, dtl, "sah4", stream=stream)
+    tsah = _ev_ms(lambda: bl.rebuild(dvl, dtl, "sah4", stream=stream), stream, 1)
+    lmot = torch.from_numpy(lsc.baked_materials(bl.prim_ids()).astype(np.int32)).to(dev)
+    lmats = torch.from_numpy(rtb200.materials_array(lsc.mats)).to(dev)
+    rcl = rtb200.render_cfg(1920, 1080, 64, max_bounce=8, rr_after=2, env_kind=1, env_color=lsc.env_color, seed=5,
+                            lookat=lsc.lookat)
+    tlp = _ev_ms(lambda: bl.render(rcl, lmats, lmot, mode=rtb200.RENDER_PLAIN, stream=stream), stream, 1)
+    tlw = _ev_ms(lambda: bl.render(rcl, lmats, lmot, mode=rtb200.RENDER_WAVEFRONT, stream=stream), stream, 1)
+    nl = 1920 * 1080 * 64
+    out["large_c5"] = {
+        "workload": "1920x1080, 64 spp, depth 8, roulette after bounce 2; 400 icospheres x 12,500 triangles + floor + "
+                    "4 quad lights (5,000,010 triangles), 80/20 Lambertian/mirror; binned SAH + spatial splits, leaf 4",
+        "sah_build_ms": round(tsah, 1), "sah_build_mtri_s": round(lsc.tris.shape[0] / tsah / 1e3, 3),
+        "plain_mpx_spp_s": mpx(nl, tlp), "wavefront_mpx_spp_s": mpx(nl, tlw),
+        "plain_ms": round(tlp, 1), "wavefront_ms": round(tlw, 1)}
+    bl.free()
+    return out
 
 
 def main():

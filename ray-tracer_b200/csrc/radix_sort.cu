@@ -15,8 +15,10 @@ namespace
 
 constexpr int      RS_BLOCK   = 256;
 constexpr int      RS_WARPS   = RS_BLOCK / 32;
-constexpr int      RS_IPT     = 16;                 // keys per thread
-constexpr int      RS_TILE    = RS_BLOCK * RS_IPT;  // 4096 keys per tile
+// Two tile shapes: up to 2^21 keys, tiles of 16 keys per thread (4096) with 2 resident blocks
+// per SM; above, 8 keys per thread (2048) with 5 resident blocks per SM (48 registers), whose
+// extra occupancy hides the memory latency of the long passes.
+constexpr uint32_t RS_SMALL_MAX = 1u << 21;
 constexpr uint32_t LB_AGG     = 1u << 30;           // tile aggregate published
 constexpr uint32_t LB_PRE     = 2u << 30;           // inclusive prefix published
 constexpr uint32_t LB_VAL     = (1u << 30) - 1u;
@@ -58,12 +60,13 @@ __device__ __forceinline__ uint32_t block_excl_scan_256(uint32_t v, uint32_t* wa
     return r;
 }
 
-template <typename K>
-__global__ void __launch_bounds__(RS_BLOCK)
+template <typename K, int RS_IPT, int MINB>
+__global__ void __launch_bounds__(RS_BLOCK, MINB)
 k_onesweep(const K* __restrict__ kin, const uint32_t* __restrict__ vin, int vals_identity, K* __restrict__ kout,
            uint32_t* __restrict__ vout, uint32_t n, uint32_t tiles, int shift, const uint32_t* __restrict__ hist,
            uint32_t* __restrict__ tile_counter, uint32_t* __restrict__ lookback, uint32_t* __restrict__ status)
 {
+    constexpr int RS_TILE = RS_BLOCK * RS_IPT;
     extern __shared__ __align__(16) unsigned char smem[];
     K*        sk     = reinterpret_cast<K*>(smem);
     uint32_t* sv     = reinterpret_cast<uint32_t*>(sk + RS_TILE);
@@ -206,13 +209,56 @@ k_onesweep(const K* __restrict__ kin, const uint32_t* __restrict__ vin, int vals
     }
 }
 
-template <typename K>
+template <typename K, int IPT>
 constexpr size_t onesweep_smem()
 {
-    return (size_t)RS_TILE * sizeof(K) + (size_t)RS_TILE * 4 + (size_t)RS_WARPS * 256 * 4 + 2 * 256 * 4;
+    return (size_t)RS_BLOCK * IPT * sizeof(K) + (size_t)RS_BLOCK * IPT * 4 + (size_t)RS_WARPS * 256 * 4 + 2 * 256 * 4;
+}
+
+// All passes of one tile shape on the given scratch.
+template <typename K, int IPT, int MINB>
+int onesweep_passes(K* keys, uint32_t* vals, bool vals_identity, uint32_t n, int passes, const uint32_t* hist, K* keys_alt,
+                    uint32_t* vals_alt, uint32_t* lookback, uint32_t* tile_counters, uint32_t* status, cudaStream_t st,
+                    K** keys_out, uint32_t** vals_out)
+{
+    constexpr uint32_t tile = RS_BLOCK * IPT;
+    const uint32_t tiles = (n + tile - 1) / tile;
+    RT_CUDA(cudaMemsetAsync(lookback, 0, (size_t)passes * tiles * 256 * 4, st));
+    RT_CUDA(cudaMemsetAsync(tile_counters, 0, 64 * 4, st));
+    constexpr size_t smem = onesweep_smem<K, IPT>();
+    static bool attr_set = false;  // per instantiation
+    if (!attr_set)
+    {
+        RT_CUDA(cudaFuncSetAttribute(k_onesweep<K, IPT, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        attr_set = true;
+    }
+    K* kin = keys;
+    K* kalt = keys_alt;
+    uint32_t* vin = vals;
+    uint32_t* valt = vals_alt;
+    for (int p = 0; p < passes; p++)
+    {
+        k_onesweep<K, IPT, MINB><<<tiles, RS_BLOCK, smem, st>>>(kin, vin, (vals_identity && p == 0) ? 1 : 0, kalt, valt, n,
+                                                                tiles, 8 * p, hist + 256 * p, tile_counters + p,
+                                                                lookback + (size_t)p * tiles * 256, status);
+        count_launch();
+        if (int e = check_launch("onesweep")) { return e; }
+        K* tk = kin; kin = kalt; kalt = tk;
+        uint32_t* tv = vin; vin = valt; valt = tv;
+    }
+    *keys_out = kin;
+    *vals_out = vin;
+    return RT_OK;
 }
 
 } // namespace
+
+// Look-back words the sort of n keys needs (passes x tiles x 256).
+size_t sort_lookback_words(uint32_t n, int passes)
+{
+    const uint32_t tile = n <= RS_SMALL_MAX ? RS_BLOCK * 16 : RS_BLOCK * 8;
+    return (size_t)passes * ((n + tile - 1) / tile) * 256;
+}
 
 template <typename K>
 int radix_sort_pairs(K* keys, uint32_t* vals, bool vals_identity, uint32_t n, int key_bits, const uint32_t* hist,
@@ -223,38 +269,20 @@ int radix_sort_pairs(K* keys, uint32_t* vals, bool vals_identity, uint32_t n, in
     if (n == 0) { return RT_OK; }
     if (n > LB_VAL) { return fail(RT_E_CAPACITY, "radix sort: more than 2^30 keys"); }
     const int passes = sort_passes(key_bits);
-    const uint32_t tiles = (n + RS_TILE - 1) / RS_TILE;
-    if (s.keys_alt.ensure((size_t)n * sizeof(K)) || s.vals_alt.ensure((size_t)n * 4) ||
-        s.lookback.ensure((size_t)passes * tiles * 256 * 4) || s.tile_counters.ensure(64 * 4))
+    const size_t lbw = sort_lookback_words(n, passes);
+    if (s.keys_alt.ensure((size_t)n * sizeof(K)) || s.vals_alt.ensure((size_t)n * 4) || s.lookback.ensure(lbw * 4) ||
+        s.tile_counters.ensure(64 * 4))
     {
         return RT_E_CUDA;
     }
-    RT_CUDA(cudaMemsetAsync(s.lookback.p, 0, (size_t)passes * tiles * 256 * 4, st));
-    RT_CUDA(cudaMemsetAsync(s.tile_counters.p, 0, 64 * 4, st));
-    static bool attr_set[2] = { false, false };
-    const size_t smem = onesweep_smem<K>();
-    if (!attr_set[sizeof(K) == 8])
+    if (n <= RS_SMALL_MAX)
     {
-        RT_CUDA(cudaFuncSetAttribute(k_onesweep<K>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        attr_set[sizeof(K) == 8] = true;
+        return onesweep_passes<K, 16, 2>(keys, vals, vals_identity, n, passes, hist, s.keys_alt.as<K>(), s.vals_alt.as<uint32_t>(),
+                                         s.lookback.as<uint32_t>(), s.tile_counters.as<uint32_t>(), status, st, keys_out,
+                                         vals_out);
     }
-    K* kin = keys;
-    K* kalt = s.keys_alt.as<K>();
-    uint32_t* vin = vals;
-    uint32_t* valt = s.vals_alt.as<uint32_t>();
-    for (int p = 0; p < passes; p++)
-    {
-        k_onesweep<K><<<tiles, RS_BLOCK, smem, st>>>(kin, vin, (vals_identity && p == 0) ? 1 : 0, kalt, valt, n, tiles, 8 * p,
-                                                    hist + 256 * p, s.tile_counters.as<uint32_t>() + p,
-                                                    s.lookback.as<uint32_t>() + (size_t)p * tiles * 256, status);
-        count_launch();
-        if (int e = check_launch("onesweep")) { return e; }
-        K* tk = kin; kin = kalt; kalt = tk;
-        uint32_t* tv = vin; vin = valt; valt = tv;
-    }
-    *keys_out = kin;
-    *vals_out = vin;
-    return RT_OK;
+    return onesweep_passes<K, 8, 5>(keys, vals, vals_identity, n, passes, hist, s.keys_alt.as<K>(), s.vals_alt.as<uint32_t>(),
+                                    s.lookback.as<uint32_t>(), s.tile_counters.as<uint32_t>(), status, st, keys_out, vals_out);
 }
 
 template int radix_sort_pairs<uint64_t>(uint64_t*, uint32_t*, bool, uint32_t, int, const uint32_t*, SortScratch&,
@@ -279,27 +307,9 @@ int radix_sort_pairs_raw(K* keys, uint32_t* vals, uint32_t n, int key_bits, cons
     *vals_out = vals;
     if (n == 0) { return RT_OK; }
     const int passes = sort_passes(key_bits);
-    const uint32_t tiles = (n + RS_TILE - 1) / RS_TILE;
-    RT_CUDA(cudaMemsetAsync(lookback, 0, (size_t)passes * tiles * 256 * 4, st));
-    RT_CUDA(cudaMemsetAsync(tile_counters, 0, 64 * 4, st));
-    const size_t smem = onesweep_smem<K>();
-    RT_CUDA(cudaFuncSetAttribute(k_onesweep<K>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    K* kin = keys;
-    K* kalt = keys_alt;
-    uint32_t* vin = vals;
-    uint32_t* valt = vals_alt;
-    for (int p = 0; p < passes; p++)
-    {
-        k_onesweep<K><<<tiles, RS_BLOCK, smem, st>>>(kin, vin, p == 0 ? 1 : 0, kalt, valt, n, tiles, 8 * p, hist + 256 * p,
-                                                    tile_counters + p, lookback + (size_t)p * tiles * 256, status);
-        count_launch();
-        if (int e = check_launch("onesweep")) { return e; }
-        K* tk = kin; kin = kalt; kalt = tk;
-        uint32_t* tv = vin; vin = valt; valt = tv;
-    }
-    *keys_out = kin;
-    *vals_out = vin;
-    return RT_OK;
+    if (n > RS_SMALL_MAX) { return fail(RT_E_CAPACITY, "radix sort on fixed scratch: at most 2^21 keys"); }
+    return onesweep_passes<K, 16, 2>(keys, vals, true, n, passes, hist, keys_alt, vals_alt, lookback, tile_counters, status, st,
+                                     keys_out, vals_out);
 }
 
 template int radix_sort_pairs_raw<uint64_t>(uint64_t*, uint32_t*, uint32_t, int, const uint32_t*, uint64_t*, uint32_t*,

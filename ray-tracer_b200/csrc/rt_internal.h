@@ -75,6 +75,8 @@ int radix_sort_pairs_raw(K* keys, uint32_t* vals, uint32_t n, int key_bits, cons
                          cudaStream_t st, K** keys_out, uint32_t** vals_out);
 // Number of 8-bit digit passes for a key width.
 inline int sort_passes(int key_bits) { return (key_bits + 7) / 8; }
+// Look-back words (passes x tiles x 256) a sort of n keys uses.
+size_t sort_lookback_words(uint32_t n, int passes);
 
 // Device-wide exclusive scan of uint32 (scan.cu is in build.cu); returns total through *d_total.
 struct ScanScratch { DevBuf partials; };
