@@ -211,6 +211,7 @@ def run_ours(a):
     import torch
     import rtb200
     from rtb200 import scenes
+    from rtb200.dist import max_over_ranks
 
     rank, world, local = env_rank()
     torch.cuda.set_device(local)
@@ -255,11 +256,7 @@ def run_ours(a):
     torch.cuda.synchronize()
     launches = rtb200.kernel_launches() - l0
     clocks = clk.stop()
-    total_ms = sum(e0.elapsed_time(e1) for e0, e1 in evs)
-    if dist:
-        t = torch.tensor([total_ms], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
+    total_ms = max_over_ranks(sum(e0.elapsed_time(e1) for e0, e1 in evs), dist, dev)
     ms_step = total_ms / a.steps
     value = world * n / (ms_step * 1e-3) / 1e6
     st = {k: statistics.mean(s[k] for s in stages) for k in stages[0]}
@@ -295,11 +292,7 @@ def run_ours(a):
     for _ in range(k_e2e):
         e2e_step()
     torch.cuda.synchronize()
-    e2e_s = (time.perf_counter() - t0) / k_e2e
-    if dist:
-        t = torch.tensor([e2e_s], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
+    e2e_s = max_over_ranks((time.perf_counter() - t0) / k_e2e, dist, dev)
     e2e_value = world * n / e2e_s / 1e6
     h2d = verts.nbytes + tris.nbytes
     d2h = nn * 48 + nt * 12 + verts.nbytes

@@ -379,16 +379,8 @@ k_boundary(const K* __restrict__ keys, const uint32_t* __restrict__ perm, uint32
     }
 }
 
-// Bottom-up construction of the binary radix tree with boxes, one thread per sorted key
-// (Apetrei, "Fast and Simple Agglomerative LBVH Construction", 2014): a node covering keys
-// [L, R] becomes a child of the split at R (right boundary) or at L-1 (left boundary),
-// whichever separates keys with the longer common prefix; the second child to arrive
-// completes the parent. Keys are extended by their index so equal codes split as in the
-// Karras tree; the tree is that same binary radix tree. Inner node p is the split between
-// keys p and p+1: it covers [L, R] with children [L, p] and [p+1, R]; its record is
-// {L, R, left id, right id} (leaf k has id n-1+k). other[p] (initially ~0) takes the first
-// arrival's outer bound and id in one exchange; its box is then in kbox (an inner node,
-// written before the release) or is its triangle's box (a leaf).
+// Whether the split after key a separates keys with a shorter common prefix than the split
+// after key b (keys extended by their index so that equal codes still differ).
 template <typename K>
 __device__ __forceinline__ bool split_lower(const K* __restrict__ keys, uint32_t a, uint32_t b)
 {
@@ -397,47 +389,145 @@ __device__ __forceinline__ bool split_lower(const K* __restrict__ keys, uint32_t
     return (a ^ (a + 1)) < (b ^ (b + 1));
 }
 
+// The climb runs in two phases so that most nodes need no device-scope fence:
+//  k_climb_local   one block per tile of CL_T sorted keys. A node whose parent split lies in
+//                  the tile (keys p and p + 1 both in it) meets its sibling through a slot in
+//                  shared memory, with boxes of the tile's inner nodes in shared memory, so only
+//                  block-scope ordering is needed. A node whose parent split is outside the
+//                  tile stops and becomes a frontier node; a slot where only one child arrived
+//                  is copied to the global slot array at the end of the block.
+//  k_climb_global  one thread per frontier node continues with global slots and device-scope
+//                  release / acquire fences (about depth x tiles nodes instead of all n - 1).
+// Both phases take the same parent for every node, so the tree is the one-pass tree.
+constexpr int CL_T = 1024;
+constexpr unsigned long long CL_DONE = ~0ull - 1ull;
+
+template <typename K>
+__global__ void __launch_bounds__(CL_T)
+k_climb_local(const K* __restrict__ keys, const uint32_t* __restrict__ perm, uint32_t n, const float4* __restrict__ lo,
+              const float4* __restrict__ hi, uint4* __restrict__ knode, uint32_t* __restrict__ parent,
+              unsigned long long* __restrict__ other, float4* __restrict__ kbox, uint32_t* __restrict__ frontier,
+              uint32_t* __restrict__ n_frontier, uint32_t* __restrict__ status)
+{
+    __shared__ unsigned long long s_other[CL_T];  // slot of split p at p - t0
+    __shared__ float4 s_box[2 * CL_T];            // box of inner node p at 2 (p - t0)
+    const uint32_t t0 = blockIdx.x * (uint32_t)CL_T;
+    const uint32_t t1 = min(t0 + (uint32_t)CL_T, n);
+    for (int i = threadIdx.x; i < CL_T; i += CL_T) { s_other[i] = ~0ull; }
+    __syncthreads();
+    const uint32_t k = t0 + threadIdx.x;
+    if (k < n && n >= 2)
+    {
+        uint32_t L = k, R = k, id = n - 1 + k;
+        const uint32_t t = perm[k];
+        float4 mn = lo[t], mx = hi[t];
+        for (uint32_t guard = 0;; guard++)
+        {
+            if (guard > MAX_DEPTH) { atomicOr(status, ST_CAPACITY); break; }
+            const bool go_right = (L == 0) || (R != n - 1 && split_lower<K>(keys, R, L - 1));
+            const uint32_t p = go_right ? R : L - 1;
+            parent[id] = p;
+            if (p < t0 || p + 1 >= t1)
+            {
+                frontier[atomicAdd(n_frontier, 1u)] = id;  // parent split outside the tile
+                break;
+            }
+            if (id < n - 1) { __threadfence_block(); }  // this node's box (s_box) before the exchange
+            const unsigned long long mine = ((unsigned long long)(go_right ? L : R) << 32) | id;
+            const unsigned long long prev = atomicExch(&s_other[p - t0], mine);
+            if (prev == ~0ull) { break; }  // first arrival
+            __threadfence_block();
+            const uint32_t sid = (uint32_t)prev;
+            float4 smn, smx;
+            if (sid < n - 1) { smn = s_box[2 * (sid - t0)]; smx = s_box[2 * (sid - t0) + 1]; }  // completed in this block
+            else { const uint32_t st = perm[sid - (n - 1)]; smn = lo[st]; smx = hi[st]; }
+            if (go_right) { R = (uint32_t)(prev >> 32); } else { L = (uint32_t)(prev >> 32); }
+            mn = make_float4(sse_min(mn.x, smn.x), sse_min(mn.y, smn.y), sse_min(mn.z, smn.z), 0.f);
+            mx = make_float4(sse_max(mx.x, smx.x), sse_max(mx.y, smx.y), sse_max(mx.z, smx.z), 0.f);
+            knode[p] = make_uint4(L, R, go_right ? id : sid, go_right ? sid : id);
+            __stcg(&kbox[2 * p], mn);
+            __stcg(&kbox[2 * p + 1], mx);
+            s_box[2 * (p - t0)] = mn;
+            s_box[2 * (p - t0) + 1] = mx;
+            s_other[p - t0] = CL_DONE;
+            id = p;
+            if (L == 0 && R == n - 1) { break; }  // the root
+        }
+    }
+    __syncthreads();
+    // slots with one arrival continue in the global phase
+    for (uint32_t i = threadIdx.x; t0 + i + 1 < t1; i += CL_T)
+    {
+        const unsigned long long v = s_other[i];
+        if (v != ~0ull && v != CL_DONE) { other[t0 + i] = v; }
+    }
+}
+
+// Bottom-up construction of the binary radix tree with boxes (Apetrei, "Fast and Simple
+// Agglomerative LBVH Construction", 2014), from the frontier nodes of k_climb_local: a node
+// covering keys [L, R] becomes a child of the split at R (right boundary) or at L-1 (left
+// boundary), whichever separates keys with the longer common prefix; the second child to
+// arrive completes the parent. Keys are extended by their index so equal codes split as in
+// the Karras tree; the tree is that same binary radix tree. Inner node p is the split between
+// keys p and p+1: it covers [L, R] with children [L, p] and [p+1, R]; its record is
+// {L, R, left id, right id} (leaf k has id n-1+k). other[p] (initially ~0) takes the first
+// arrival's outer bound and id in one exchange; its box is then in kbox (an inner node,
+// written before the release) or is its triangle's box (a leaf).
 template <typename K>
 __global__ void __launch_bounds__(BLK)
-k_climb(const K* __restrict__ keys, const uint32_t* __restrict__ perm, uint32_t n, const float4* __restrict__ lo,
-        const float4* __restrict__ hi, uint4* __restrict__ knode, uint32_t* __restrict__ parent,
-        unsigned long long* __restrict__ other, float4* __restrict__ kbox, uint32_t* __restrict__ status)
+k_climb_global(const K* __restrict__ keys, const uint32_t* __restrict__ perm, uint32_t n, const float4* __restrict__ lo,
+               const float4* __restrict__ hi, uint4* __restrict__ knode, uint32_t* __restrict__ parent,
+               unsigned long long* __restrict__ other, float4* __restrict__ kbox, const uint32_t* __restrict__ frontier,
+               const uint32_t* __restrict__ n_frontier, uint32_t* __restrict__ status)
 {
-    const uint32_t i = blockIdx.x * BLK + threadIdx.x;
-    if (i >= n || n < 2) { return; }
-    uint32_t L = i, R = i, id = n - 1 + i;
-    const uint32_t t = perm[i];
-    float4 mn = lo[t], mx = hi[t];
-    for (uint32_t guard = 0;; guard++)
+    const uint32_t nf = *n_frontier;
+    for (uint32_t f = blockIdx.x * BLK + threadIdx.x; f < nf; f += gridDim.x * BLK)
     {
-        if (guard > MAX_DEPTH) { atomicOr(status, ST_CAPACITY); return; }
-        const bool go_right = (L == 0) || (R != n - 1 && split_lower<K>(keys, R, L - 1));
-        const uint32_t p = go_right ? R : L - 1;  // go_right: this node is p's left child
-        parent[id] = p;
-        // an inner node's box was just written: release it before the exchange; a leaf's box
-        // lives in arrays written by an earlier kernel and needs no ordering
-        if (id < n - 1) { cuda::atomic_thread_fence(cuda::memory_order_release, cuda::thread_scope_device); }
-        cuda::atomic_ref<unsigned long long, cuda::thread_scope_device> ex(other[p]);
-        const unsigned long long mine = ((unsigned long long)(go_right ? L : R) << 32) | id;
-        const unsigned long long prev = ex.exchange(mine, cuda::memory_order_relaxed);
-        if (prev == ~0ull) { return; }  // first arrival: the sibling completes p
-        const uint32_t sid = (uint32_t)prev;
-        float4 smn, smx;
-        if (sid < n - 1)
+        uint32_t id = frontier[f], L, R;
+        float4 mn, mx;
+        if (id < n - 1)
         {
-            cuda::atomic_thread_fence(cuda::memory_order_acquire, cuda::thread_scope_device);
-            smn = __ldcg(&kbox[2 * sid]);
-            smx = __ldcg(&kbox[2 * sid + 1]);
+            const uint4 kn = __ldcg(&knode[id]);  // completed by the local phase
+            L = kn.x; R = kn.y;
+            mn = __ldcg(&kbox[2 * id]); mx = __ldcg(&kbox[2 * id + 1]);
         }
-        else { const uint32_t st = perm[sid - (n - 1)]; smn = lo[st]; smx = hi[st]; }
-        if (go_right) { R = (uint32_t)(prev >> 32); } else { L = (uint32_t)(prev >> 32); }
-        mn = make_float4(sse_min(mn.x, smn.x), sse_min(mn.y, smn.y), sse_min(mn.z, smn.z), 0.f);
-        mx = make_float4(sse_max(mx.x, smx.x), sse_max(mx.y, smx.y), sse_max(mx.z, smx.z), 0.f);
-        knode[p] = make_uint4(L, R, go_right ? id : sid, go_right ? sid : id);
-        __stcg(&kbox[2 * p], mn);
-        __stcg(&kbox[2 * p + 1], mx);
-        id = p;
-        if (L == 0 && R == n - 1) { return; }  // the root (internal node): no parent
+        else
+        {
+            L = R = id - (n - 1);
+            const uint32_t t = perm[L];
+            mn = lo[t]; mx = hi[t];
+        }
+        for (uint32_t guard = 0;; guard++)
+        {
+            if (guard > MAX_DEPTH) { atomicOr(status, ST_CAPACITY); break; }
+            const bool go_right = (L == 0) || (R != n - 1 && split_lower<K>(keys, R, L - 1));
+            const uint32_t p = go_right ? R : L - 1;  // go_right: this node is p's left child
+            parent[id] = p;
+            // an inner node's box was just written: release it before the exchange; a leaf's box
+            // lives in arrays written by an earlier kernel and needs no ordering
+            if (id < n - 1) { cuda::atomic_thread_fence(cuda::memory_order_release, cuda::thread_scope_device); }
+            cuda::atomic_ref<unsigned long long, cuda::thread_scope_device> ex(other[p]);
+            const unsigned long long mine = ((unsigned long long)(go_right ? L : R) << 32) | id;
+            const unsigned long long prev = ex.exchange(mine, cuda::memory_order_relaxed);
+            if (prev == ~0ull) { break; }  // first arrival: the sibling completes p
+            const uint32_t sid = (uint32_t)prev;
+            float4 smn, smx;
+            if (sid < n - 1)
+            {
+                cuda::atomic_thread_fence(cuda::memory_order_acquire, cuda::thread_scope_device);
+                smn = __ldcg(&kbox[2 * sid]);
+                smx = __ldcg(&kbox[2 * sid + 1]);
+            }
+            else { const uint32_t st = perm[sid - (n - 1)]; smn = lo[st]; smx = hi[st]; }
+            if (go_right) { R = (uint32_t)(prev >> 32); } else { L = (uint32_t)(prev >> 32); }
+            mn = make_float4(sse_min(mn.x, smn.x), sse_min(mn.y, smn.y), sse_min(mn.z, smn.z), 0.f);
+            mx = make_float4(sse_max(mx.x, smx.x), sse_max(mx.y, smx.y), sse_max(mx.z, smx.z), 0.f);
+            knode[p] = make_uint4(L, R, go_right ? id : sid, go_right ? sid : id);
+            __stcg(&kbox[2 * p], mn);
+            __stcg(&kbox[2 * p + 1], mx);
+            id = p;
+            if (L == 0 && R == n - 1) { break; }  // the root (internal node): no parent
+        }
     }
 }
 
@@ -716,10 +806,16 @@ int build_typed(rt_bvh* B, const rt_vertex* d_verts, uint32_t V, const rt_triang
     prof_mark(B, 2, st);
     if (N >= 2)
     {
-        k_climb<K><<<blocks_for(N), BLK, 0, st>>>(skeys, perm, N, S.tri_lo.as<float4>(), S.tri_hi.as<float4>(),
-                                                  S.knode.as<uint4>(), S.parent.as<uint32_t>(),
-                                                  S.visit.as<unsigned long long>(), S.kbox.as<float4>(), status);
-        count_launch();
+        // the frontier list lives in the rank array, which k_boundary fills only afterwards
+        uint32_t* frontier = S.rank.as<uint32_t>();
+        k_climb_local<K><<<blocks_for(N, CL_T), CL_T, 0, st>>>(skeys, perm, N, S.tri_lo.as<float4>(), S.tri_hi.as<float4>(),
+                                                               S.knode.as<uint4>(), S.parent.as<uint32_t>(),
+                                                               S.visit.as<unsigned long long>(), S.kbox.as<float4>(),
+                                                               frontier, counters + 8, status);
+        k_climb_global<K><<<std::min<uint32_t>(blocks_for(N), 4u * (uint32_t)device_sm_count()), BLK, 0, st>>>(
+            skeys, perm, N, S.tri_lo.as<float4>(), S.tri_hi.as<float4>(), S.knode.as<uint4>(), S.parent.as<uint32_t>(),
+            S.visit.as<unsigned long long>(), S.kbox.as<float4>(), frontier, counters + 8, status);
+        count_launch(2);
     }
     const uint32_t tm = std::max(cfg.max_leaf, cfg.lbvh_threshold);
     k_boundary<K><<<blocks_for(nk), BLK, 0, st>>>(skeys, perm, N, S.knode.as<uint4>(), S.parent.as<uint32_t>(),

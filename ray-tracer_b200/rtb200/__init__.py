@@ -9,3 +9,5 @@ __all__ = ["Bvh", "BuildCfg", "WavefrontParams", "batch_arrays", "Material", "Me
            "TRACE_ANY_HIT", "TRACE_CLOSEST", "TRACE_WATERTIGHT", "RENDER_PLAIN", "RENDER_WAVEFRONT", "bake_scene",
            "header_symbols", "kernel_launches", "last_error", "lib", "make_cfg", "materials_array", "read_hdr", "render_cfg",
            "scene_config", "write_hdr"]
+
+from . import dist  # noqa: E402  (multi-process plumbing)

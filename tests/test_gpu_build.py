@@ -12,6 +12,7 @@ import pytest
 
 import rtb200
 from oracle import make_cfg as orc_make_cfg
+from rtb200 import scenes
 from scenes_for_tests import scene_set
 
 pytestmark = pytest.mark.gpu
@@ -91,3 +92,23 @@ def test_errors_are_reported():
     with pytest.raises(rtb200.RtError) as e:
         rtb200.Bvh.build(v[:0], t[:0])
     assert e.value.code == 8  # RT_E_EMPTY
+
+
+@pytest.mark.parametrize("preset", ["lbvh63", "lbvh30", "hybrid"])
+def test_large_odd_soup_matches_oracle(orc, preset):
+    """262,147 triangles: 257 tiles of the local tree phase (the last one partial), frontier
+    nodes on every tile edge, and the large-input tile shape of the radix sort."""
+    v, t = scenes.soup(262147, seed=77)
+    ref = orc.build(v, t, orc_cfg(preset))
+    b = rtb200.Bvh.build(v, t, preset)
+    assert_same_tree(b.download(), ref, f"soup262147/{preset}")
+
+
+def test_sort_tile_shapes_agree(orc):
+    """2^21 + 5 triangles run the 8-keys-per-thread sort; its Morton order is the oracle's."""
+    v, t = scenes.soup((1 << 21) + 5, seed=78)
+    codes, perm, _ = orc.morton(v, t, orc_cfg("lbvh63"))
+    b = rtb200.Bvh.build(v, t, "lbvh63l4")
+    pid = b.prim_ids()
+    # leaves of the LBVH presets hold sorted runs: the baked order is the stable Morton order
+    assert np.array_equal(pid, perm)
