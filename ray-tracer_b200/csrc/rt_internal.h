@@ -120,6 +120,7 @@ struct BuildScratch
     rtb::DevBuf gtris;              // batched build: triangles with concatenated-array vertex indices
     rtb::DevBuf batch_off;          // batched build: triangle and vertex offsets per scene
     rtb::DevBuf sah_budget;         // spatial-split budget per scene: used, cap
+    rtb::DevBuf sah_wide;           // SAH nodes evaluated by many blocks: bins, list, block offsets
 };
 
 struct rt_bvh

@@ -136,27 +136,27 @@ __device__ __forceinline__ box3 sbox_result(const SBox& s)
 
 // Hoare-scheme partition of in[0, n) by pred into out[0, n) (in == out allowed). Returns the
 // number of elements satisfying pred. flags/pos: n scratch entries each.
-template <class Pred>
+template <int BS, class Pred>
 __device__ uint32_t cta_partition(const uint32_t* in, uint32_t* out, uint32_t n, Pred pred, uint8_t* flags,
                                   uint32_t* pos, uint32_t* sh)
 {
     const int tid = threadIdx.x;
     uint32_t c = 0;
-    for (uint32_t i = tid; i < n; i += SBLK)
+    for (uint32_t i = tid; i < n; i += BS)
     {
         const uint8_t f = pred(in[i]) ? 1 : 0;
         flags[i] = f;
         c += f;
     }
-    const uint32_t m = block_sum<SBLK>(c, sh);
+    const uint32_t m = block_sum<BS>(c, sh);
     // satisfying elements right of the split point, in ascending order
     uint32_t run = 0;
-    for (uint32_t base = m; base < n; base += SBLK)
+    for (uint32_t base = m; base < n; base += BS)
     {
         const uint32_t i = base + tid;
         const uint32_t f = (i < n) ? flags[i] : 0u;
         uint32_t tot;
-        const uint32_t e = block_excl_scan<SBLK>(f, sh, &tot);
+        const uint32_t e = block_excl_scan<BS>(f, sh, &tot);
         if (f) { pos[run + e] = i; }
         run += tot;
     }
@@ -164,12 +164,12 @@ __device__ uint32_t cta_partition(const uint32_t* in, uint32_t* out, uint32_t n,
     const uint32_t tr = run;  // equals the failing elements left of the split point
     // exchange the k-th failing element from the left with the k-th satisfying one from the right
     uint32_t k0 = 0;
-    for (uint32_t base = 0; base < m; base += SBLK)
+    for (uint32_t base = 0; base < m; base += BS)
     {
         const uint32_t i = base + tid;
         const uint32_t f = (i < m) ? (flags[i] ? 0u : 1u) : 0u;
         uint32_t tot;
-        const uint32_t e = block_excl_scan<SBLK>(f, sh, &tot);
+        const uint32_t e = block_excl_scan<BS>(f, sh, &tot);
         if (i < m)
         {
             if (f)
@@ -185,7 +185,7 @@ __device__ uint32_t cta_partition(const uint32_t* in, uint32_t* out, uint32_t n,
     }
     if (in != out)
     {
-        for (uint32_t i = m + tid; i < n; i += SBLK)
+        for (uint32_t i = m + tid; i < n; i += BS)
         {
             if (!flags[i]) { out[i] = in[i]; }
         }
@@ -193,6 +193,78 @@ __device__ uint32_t cta_partition(const uint32_t* in, uint32_t* out, uint32_t n,
     __syncthreads();
     return m;
 }
+
+// The best candidate so far, in the reference's evaluation order.
+struct Best
+{
+    float cost, cmin, scale, node_min, sscale;
+    int   axis, bin, spatial;
+};
+
+// Object-split candidates of one axis (bvh_sah.cpp:88-126): sweeps from both sides over the
+// centroid bins, bins b = nb-1 .. 1, strict improvement only.
+__device__ __noinline__ void eval_object_axis(const uint32_t* cnt, const SBox* bins, int nb, int axis, float cmin, float scale,
+                                              float parent_inv_area, const Ctx& C, Best& B)
+{
+    box3 lbox[SAH_MAX_BINS];
+    uint32_t lcnt[SAH_MAX_BINS];
+    box3 la = box_empty();
+    uint32_t lc = 0;
+    for (int b = 0; b < nb - 1; b++)
+    {
+        if (cnt[b]) { box_box(la, sbox_get(bins[b])); }
+        lc += cnt[b];
+        lbox[b] = la; lcnt[b] = lc;
+    }
+    box3 ra = box_empty();
+    uint32_t rc = 0;
+    for (int b = nb - 1; b >= 1; b--)
+    {
+        if (cnt[b]) { box_box(ra, sbox_get(bins[b])); }
+        rc += cnt[b];
+        const uint32_t lc2 = lcnt[b - 1];
+        if (lc2 == 0 || rc == 0) { continue; }
+        const float cost = C.c_trav + C.c_isect *
+            (box_half_area(lbox[b - 1]) * (float)lc2 + box_half_area(ra) * (float)rc) * parent_inv_area;
+        if (cost < B.cost) { B.cost = cost; B.axis = axis; B.bin = b; B.cmin = cmin; B.scale = scale; }
+    }
+}
+
+// Spatial-split candidates of one axis (bvh_sah.cpp:198-243): entry counts from the left,
+// exit counts from the right, boxes of the clipped triangles.
+__device__ __noinline__ void eval_spatial_axis(const uint32_t* cin, const uint32_t* cout, const SBox* bins, int nb, int axis,
+                                               float node_min, float sscale, float parent_inv_area, const Ctx& C, Best& B)
+{
+    box3 lbox[SAH_MAX_BINS];
+    uint32_t lcnt[SAH_MAX_BINS];
+    box3 la = box_empty();
+    uint32_t lc = 0;
+    for (int b = 0; b < nb - 1; b++)
+    {
+        box_box(la, sbox_result(bins[b]));
+        lc += cin[b];
+        lbox[b] = la; lcnt[b] = lc;
+    }
+    box3 ra = box_empty();
+    uint32_t rc = 0;
+    for (int b = nb - 1; b >= 1; b--)
+    {
+        box_box(ra, sbox_result(bins[b]));
+        rc += cout[b];
+        const uint32_t lc2 = lcnt[b - 1];
+        if (lc2 == 0 || rc == 0) { continue; }
+        const float cost = C.c_trav + C.c_isect *
+            (box_half_area(lbox[b - 1]) * (float)lc2 + box_half_area(ra) * (float)rc) * parent_inv_area;
+        if (cost < B.cost)
+        {
+            B.cost = cost; B.axis = axis; B.bin = b; B.spatial = 1; B.node_min = node_min; B.sscale = sscale;
+        }
+    }
+}
+
+// Nodes with more references than this are evaluated and partitioned by many blocks (the
+// wide kernels below); the rest by one block each.
+constexpr uint32_t WIDE_MIN = 16384;
 
 // One block per node: evaluates every object and spatial candidate in the reference's order
 // and writes the decision with the side counts of its partitions.
@@ -203,8 +275,7 @@ k_sah_eval(const LvlNode* __restrict__ lv, const uint32_t* __restrict__ refs, Ct
     __shared__ SBox bins[SAH_MAX_BINS];
     __shared__ uint32_t s_red[SBLK / 32 + 1];
     __shared__ uint32_t s_cm, s_cM;
-    __shared__ float best_cost, best_cmin, best_scale, best_node_min, best_sscale;
-    __shared__ int best_axis, best_bin, is_spatial;
+    __shared__ Best sB;
     __shared__ int o_axis, o_bin;
     __shared__ float o_cmin, o_scale;
 
@@ -220,15 +291,15 @@ k_sah_eval(const LvlNode* __restrict__ lv, const uint32_t* __restrict__ refs, Ct
         if (tid == 0) { d.kind = K_LEAF; dec[blockIdx.x] = d; }
         return;
     }
+    if (n > WIDE_MIN) { return; }  // the wide kernels decide this node
     const int nb = std_clampi((int)n / 4, (int)C.bins_min, (int)C.bins_max);
     box3 nbox;
     for (int k = 0; k < 3; k++) { nbox.mn[k] = nd.box[k]; nbox.mx[k] = nd.box[3 + k]; }
     const float parent_inv_area = 1.0f / box_half_area(nbox);
     if (tid == 0)
     {
-        best_cost = C.c_isect * (float)n;  // leaf cost, bvh_sah.cpp:32
-        best_axis = -1; best_bin = -1; best_cmin = 0.f; best_scale = 0.f; is_spatial = 0;
-        best_node_min = 0.f; best_sscale = 0.f;
+        sB.cost = C.c_isect * (float)n;  // leaf cost, bvh_sah.cpp:32
+        sB.axis = -1; sB.bin = -1; sB.cmin = 0.f; sB.scale = 0.f; sB.spatial = 0; sB.node_min = 0.f; sB.sscale = 0.f;
     }
 
     // phase 1: centroid-binned object split (bvh_sah.cpp:52-126)
@@ -247,6 +318,7 @@ k_sah_eval(const LvlNode* __restrict__ lv, const uint32_t* __restrict__ refs, Ct
         // std::min / std::max folds starting from +FLT_MAX / -FLT_MAX (bvh_sah.cpp:54-61)
         const float cmin = std_min(3.402823466e38f, ord2f(s_cm));
         const float cmax = std_max(-3.402823466e38f, ord2f(s_cM));
+        __syncthreads();  // everyone has read s_cm / s_cM before the next axis resets them
         if (cmax - cmin < C.centroid_eps) { continue; }
         const float scale = (float)nb / (cmax - cmin);
         if (tid < nb) { cnt[tid] = 0u; sbox_clear(bins[tid]); }
@@ -259,37 +331,10 @@ k_sah_eval(const LvlNode* __restrict__ lv, const uint32_t* __restrict__ refs, Ct
             sbox_add(bins[b], tri_box(C, t));
         }
         __syncthreads();
-        if (tid == 0)
-        {
-            box3 lbox[SAH_MAX_BINS];
-            uint32_t lcnt[SAH_MAX_BINS];
-            box3 la = box_empty();
-            uint32_t lc = 0;
-            for (int b = 0; b < nb - 1; b++)
-            {
-                if (cnt[b]) { box_box(la, sbox_get(bins[b])); }
-                lc += cnt[b];
-                lbox[b] = la; lcnt[b] = lc;
-            }
-            box3 ra = box_empty();
-            uint32_t rc = 0;
-            for (int b = nb - 1; b >= 1; b--)
-            {
-                if (cnt[b]) { box_box(ra, sbox_get(bins[b])); }
-                rc += cnt[b];
-                const uint32_t lc2 = lcnt[b - 1];
-                if (lc2 == 0 || rc == 0) { continue; }
-                const float cost = C.c_trav + C.c_isect *
-                    (box_half_area(lbox[b - 1]) * (float)lc2 + box_half_area(ra) * (float)rc) * parent_inv_area;
-                if (cost < best_cost)
-                {
-                    best_cost = cost; best_axis = axis; best_bin = b; best_cmin = cmin; best_scale = scale;
-                }
-            }
-        }
+        if (tid == 0) { eval_object_axis(cnt, bins, nb, axis, cmin, scale, parent_inv_area, C, sB); }
         __syncthreads();
     }
-    if (tid == 0) { o_axis = best_axis; o_bin = best_bin; o_cmin = best_cmin; o_scale = best_scale; }
+    if (tid == 0) { o_axis = sB.axis; o_bin = sB.bin; o_cmin = sB.cmin; o_scale = sB.scale; }
     __syncthreads();
 
     // phase 2: spatial bins over the node box, triangles clipped per bin (bvh_sah.cpp:135-243)
@@ -322,60 +367,33 @@ k_sah_eval(const LvlNode* __restrict__ lv, const uint32_t* __restrict__ refs, Ct
             }
         }
         __syncthreads();
-        if (tid == 0)
-        {
-            box3 lbox[SAH_MAX_BINS];
-            uint32_t lcnt[SAH_MAX_BINS];
-            box3 la = box_empty();
-            uint32_t lc = 0;
-            for (int b = 0; b < nb - 1; b++)
-            {
-                box_box(la, sbox_result(bins[b]));
-                lc += cin[b];
-                lbox[b] = la; lcnt[b] = lc;
-            }
-            box3 ra = box_empty();
-            uint32_t rc = 0;
-            for (int b = nb - 1; b >= 1; b--)
-            {
-                box_box(ra, sbox_result(bins[b]));
-                rc += cout[b];
-                const uint32_t lc2 = lcnt[b - 1];
-                if (lc2 == 0 || rc == 0) { continue; }
-                const float cost = C.c_trav + C.c_isect *
-                    (box_half_area(lbox[b - 1]) * (float)lc2 + box_half_area(ra) * (float)rc) * parent_inv_area;
-                if (cost < best_cost)
-                {
-                    best_cost = cost; best_axis = axis; best_bin = b; is_spatial = 1;
-                    best_node_min = node_min; best_sscale = sscale;
-                }
-            }
-        }
+        if (tid == 0) { eval_spatial_axis(cin, cout, bins, nb, axis, node_min, sscale, parent_inv_area, C, sB); }
         __syncthreads();
     }
 
     // decision and partition side counts (bvh_sah.cpp:249-394)
+    const Best B = sB;
     d.nb = nb;
     d.oaxis = o_axis; d.obin = o_bin; d.ocmin = o_cmin; d.oscale = o_scale;
-    if (best_axis == -1)
+    if (B.axis == -1)
     {
         d.kind = K_LEAF;
     }
-    else if (!is_spatial)
+    else if (!B.spatial)
     {
         uint32_t l = 0;
         for (uint32_t i = tid; i < n; i += SBLK)
         {
-            l += obj_bin(centroid(C, R[i], best_axis), best_cmin, best_scale, nb) < best_bin ? 1u : 0u;
+            l += obj_bin(centroid(C, R[i], B.axis), B.cmin, B.scale, nb) < B.bin ? 1u : 0u;
         }
         l = block_sum<SBLK>(l, s_red);
         d.kind = (l == 0 || l == n) ? K_LEAF : K_OBJECT;
-        d.axis = best_axis; d.bin = best_bin; d.cmin = best_cmin; d.scale = best_scale;
+        d.axis = B.axis; d.bin = B.bin; d.cmin = B.cmin; d.scale = B.scale;
     }
     else
     {
-        const float plane = best_node_min + (float)best_bin / best_sscale;
-        const int axis = best_axis;
+        const float plane = B.node_min + (float)B.bin / B.sscale;
+        const int axis = B.axis;
         const int oa = o_axis, ob = o_bin;
         const float oc = o_cmin, os = o_scale;
         uint32_t lo_ = 0, st_ = 0, ol = 0;
@@ -405,6 +423,356 @@ k_sah_eval(const LvlNode* __restrict__ lv, const uint32_t* __restrict__ refs, Ct
         }
     }
     if (tid == 0) { dec[blockIdx.x] = d; }
+}
+
+// ---- the wide path: nodes with more than WIDE_MIN references ----
+// The top levels of a large build hold a few nodes with up to millions of references. Their
+// candidates are binned by many blocks at once (WIDE_CH references each) into per-node bins in
+// global memory -- counts by atomic adds, boxes by atomic min / max on the order-preserving
+// encoding, which are the same values the one-block path accumulates in shared memory -- and
+// then evaluated by one thread per node with the same serial code, so the decisions are the
+// ones the one-block path makes.
+constexpr uint32_t WIDE_CH = 4096;
+
+struct WideAcc
+{
+    uint32_t cm[3], cM[3];
+    uint32_t ocnt[3][SAH_MAX_BINS];
+    SBox     obox[3][SAH_MAX_BINS];
+    uint32_t cin[3][SAH_MAX_BINS], cout[3][SAH_MAX_BINS];
+    SBox     sbox[3][SAH_MAX_BINS];
+    uint32_t cnt[4];
+    Best     B;
+    int      o_axis, o_bin;
+    float    o_cmin, o_scale;
+};
+
+// The wide nodes of a level in level order (wl) with their first block (wco, exclusive prefix
+// of ceil(count / WIDE_CH)); io[8] = wide nodes, io[9] = blocks.
+__global__ void __launch_bounds__(1024)
+k_wide_list(const LvlNode* __restrict__ lv, uint32_t n_lvl, uint32_t* __restrict__ wl, uint32_t* __restrict__ wco,
+            uint32_t max_wide, uint32_t* __restrict__ io)
+{
+    __shared__ uint32_t sh[33];
+    uint32_t nw = 0, nch = 0;
+    for (uint32_t base = 0; base < n_lvl; base += 1024)
+    {
+        const uint32_t i = base + threadIdx.x;
+        const uint32_t n = i < n_lvl ? lv[i].count : 0u;
+        const uint32_t f = n > WIDE_MIN ? 1u : 0u;
+        const uint32_t c = f ? (n + WIDE_CH - 1) / WIDE_CH : 0u;
+        uint32_t tf, tc;
+        const uint32_t ef = block_excl_scan<1024>(f, sh, &tf);
+        const uint32_t ec = block_excl_scan<1024>(c, sh, &tc);
+        if (f && nw + ef < max_wide) { wl[nw + ef] = i; wco[nw + ef] = nch + ec; }
+        nw += tf;
+        nch += tc;
+    }
+    if (threadIdx.x == 0)
+    {
+        if (nw <= max_wide) { wco[nw] = nch; }
+        io[8] = nw;
+        io[9] = nch;
+    }
+}
+
+// wide node k and chunk c of block g
+__device__ __forceinline__ uint32_t wide_item(const uint32_t* __restrict__ wco, uint32_t nw, uint32_t g, uint32_t& c)
+{
+    uint32_t lo = 0, hi = nw;  // wco[lo] <= g < wco[hi]
+    while (hi - lo > 1)
+    {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (wco[mid] <= g) { lo = mid; } else { hi = mid; }
+    }
+    c = g - wco[lo];
+    return lo;
+}
+
+__global__ void __launch_bounds__(SBLK) k_wide_init(WideAcc* __restrict__ acc)
+{
+    WideAcc& A = acc[blockIdx.x];
+    uint32_t* w = reinterpret_cast<uint32_t*>(&A);
+    // counts 0, box minima ~0: the SBox members are written below
+    for (uint32_t i = threadIdx.x; i < sizeof(WideAcc) / 4; i += SBLK) { w[i] = 0u; }
+    __syncthreads();
+    if (threadIdx.x < 3) { A.cm[threadIdx.x] = 0xffffffffu; A.cM[threadIdx.x] = 0u; }
+    for (uint32_t j = threadIdx.x; j < 3 * SAH_MAX_BINS; j += SBLK)
+    {
+        sbox_clear(A.obox[j / SAH_MAX_BINS][j % SAH_MAX_BINS]);
+        sbox_clear(A.sbox[j / SAH_MAX_BINS][j % SAH_MAX_BINS]);
+    }
+}
+
+__device__ __forceinline__ void chunk_range(uint32_t n, uint32_t c, uint32_t& b, uint32_t& e)
+{
+    b = c * WIDE_CH;
+    e = min(n, b + WIDE_CH);
+}
+
+// centroid bounds per axis
+__global__ void __launch_bounds__(SBLK)
+k_wide_bounds(const LvlNode* __restrict__ lv, const uint32_t* __restrict__ refs, Ctx C, const uint32_t* __restrict__ wl,
+              const uint32_t* __restrict__ wco, uint32_t nw, WideAcc* __restrict__ acc)
+{
+    __shared__ uint32_t sm[3], sM[3];
+    uint32_t c;
+    const uint32_t k = wide_item(wco, nw, blockIdx.x, c);
+    const LvlNode nd = lv[wl[k]];
+    const uint32_t* R = refs + nd.ref_off;
+    uint32_t b, e;
+    chunk_range(nd.count, c, b, e);
+    if (threadIdx.x < 3) { sm[threadIdx.x] = 0xffffffffu; sM[threadIdx.x] = 0u; }
+    __syncthreads();
+    uint32_t m[3] = { 0xffffffffu, 0xffffffffu, 0xffffffffu }, M[3] = { 0u, 0u, 0u };
+    for (uint32_t i = b + threadIdx.x; i < e; i += SBLK)
+    {
+        const uint32_t t = R[i];
+        for (int a = 0; a < 3; a++)
+        {
+            const uint32_t o = f2ord(centroid(C, t, a));
+            m[a] = min(m[a], o); M[a] = max(M[a], o);
+        }
+    }
+    for (int a = 0; a < 3; a++)
+    {
+        for (int o = 16; o > 0; o >>= 1)
+        {
+            m[a] = min(m[a], __shfl_xor_sync(0xffffffffu, m[a], o));
+            M[a] = max(M[a], __shfl_xor_sync(0xffffffffu, M[a], o));
+        }
+        if ((threadIdx.x & 31) == 0) { atomicMin(&sm[a], m[a]); atomicMax(&sM[a], M[a]); }
+    }
+    __syncthreads();
+    if (threadIdx.x < 3)
+    {
+        atomicMin(&acc[k].cm[threadIdx.x], sm[threadIdx.x]);
+        atomicMax(&acc[k].cM[threadIdx.x], sM[threadIdx.x]);
+    }
+}
+
+__device__ __forceinline__ void wide_axis_scale(const WideAcc& A, int axis, int nb, const Ctx& C, float& cmin, float& scale)
+{
+    // std::min / std::max folds starting from +FLT_MAX / -FLT_MAX (bvh_sah.cpp:54-61)
+    cmin = std_min(3.402823466e38f, ord2f(A.cm[axis]));
+    const float cmax = std_max(-3.402823466e38f, ord2f(A.cM[axis]));
+    scale = (cmax - cmin < C.centroid_eps) ? 0.f : (float)nb / (cmax - cmin);
+}
+
+__device__ __forceinline__ void sbox_merge_global(SBox& g, const SBox& s)
+{
+    if (s.m[0] == 0xffffffffu && s.M[0] == 0u) { return; }  // nothing added
+    for (int k = 0; k < 3; k++) { atomicMin(&g.m[k], s.m[k]); atomicMax(&g.M[k], s.M[k]); }
+}
+
+// object bins of the three axes and spatial bins with clipping, one chunk per block
+__global__ void __launch_bounds__(SBLK)
+k_wide_bins(const LvlNode* __restrict__ lv, const uint32_t* __restrict__ refs, Ctx C, const uint32_t* __restrict__ wl,
+            const uint32_t* __restrict__ wco, uint32_t nw, WideAcc* __restrict__ acc)
+{
+    __shared__ uint32_t ocnt[3][SAH_MAX_BINS], cin[3][SAH_MAX_BINS], cout[3][SAH_MAX_BINS];
+    __shared__ SBox obox[3][SAH_MAX_BINS], sbx[3][SAH_MAX_BINS];
+    uint32_t c;
+    const uint32_t k = wide_item(wco, nw, blockIdx.x, c);
+    const LvlNode nd = lv[wl[k]];
+    const uint32_t n = nd.count;
+    const uint32_t* R = refs + nd.ref_off;
+    uint32_t b0, e0;
+    chunk_range(n, c, b0, e0);
+    const int nb = std_clampi((int)n / 4, (int)C.bins_min, (int)C.bins_max);
+    WideAcc& A = acc[k];
+    float cmin[3], scale[3], node_min[3], sscale[3];
+    box3 nbox;
+    for (int a = 0; a < 3; a++)
+    {
+        wide_axis_scale(A, a, nb, C, cmin[a], scale[a]);
+        nbox.mn[a] = nd.box[a]; nbox.mx[a] = nd.box[3 + a];
+        node_min[a] = nd.box[a];
+        const float node_max = nd.box[3 + a];
+        sscale[a] = (node_max - node_min[a] < C.spatial_eps) ? 0.f : (float)nb / (node_max - node_min[a]);
+    }
+    for (uint32_t j = threadIdx.x; j < 3 * SAH_MAX_BINS; j += SBLK)
+    {
+        const uint32_t a = j / SAH_MAX_BINS, bb = j % SAH_MAX_BINS;
+        ocnt[a][bb] = 0u; cin[a][bb] = 0u; cout[a][bb] = 0u;
+        sbox_clear(obox[a][bb]); sbox_clear(sbx[a][bb]);
+    }
+    __syncthreads();
+    for (uint32_t i = b0 + threadIdx.x; i < e0; i += SBLK)
+    {
+        const uint32_t t = R[i];
+        const box3 tb = tri_box(C, t);
+        for (int a = 0; a < 3; a++)
+        {
+            if (scale[a] == 0.f) { continue; }
+            const int b = obj_bin(centroid(C, t, a), cmin[a], scale[a], nb);
+            atomicAdd(&ocnt[a][b], 1u);
+            sbox_add(obox[a][b], tb);
+        }
+        f3 v0, v1, v2;
+        bool have_v = false;
+        for (int a = 0; a < 3; a++)
+        {
+            if (sscale[a] == 0.f) { continue; }
+            const int bmin = std_clampi(x86_f2i((tri_lo(C, t, a) - node_min[a]) * sscale[a]), 0, nb - 1);
+            const int bmax = std_clampi(x86_f2i((tri_hi(C, t, a) - node_min[a]) * sscale[a]), 0, nb - 1);
+            atomicAdd(&cin[a][bmin], 1u);
+            atomicAdd(&cout[a][bmax], 1u);
+            if (bmin <= bmax)
+            {
+                if (!have_v) { tri_verts(C, t, v0, v1, v2); have_v = true; }
+                box3 region = nbox;
+                for (int b = bmin; b <= bmax; b++)
+                {
+                    region.mn[a] = node_min[a] + (float)b / sscale[a];
+                    region.mx[a] = node_min[a] + (float)(b + 1) / sscale[a];
+                    const box3 cl = clip_triangle(v0, v1, v2, region);
+                    if (box_valid(cl)) { sbox_add(sbx[a][b], cl); }
+                }
+            }
+        }
+    }
+    __syncthreads();
+    for (uint32_t j = threadIdx.x; j < 3 * SAH_MAX_BINS; j += SBLK)
+    {
+        const uint32_t a = j / SAH_MAX_BINS, bb = j % SAH_MAX_BINS;
+        if (ocnt[a][bb]) { atomicAdd(&A.ocnt[a][bb], ocnt[a][bb]); }
+        if (cin[a][bb]) { atomicAdd(&A.cin[a][bb], cin[a][bb]); }
+        if (cout[a][bb]) { atomicAdd(&A.cout[a][bb], cout[a][bb]); }
+        sbox_merge_global(A.obox[a][bb], obox[a][bb]);
+        sbox_merge_global(A.sbox[a][bb], sbx[a][bb]);
+    }
+}
+
+// the reference's serial candidate evaluation over the accumulated bins, one thread per node
+__global__ void k_wide_decide(const LvlNode* __restrict__ lv, Ctx C, const uint32_t* __restrict__ wl, uint32_t nw,
+                              WideAcc* __restrict__ acc)
+{
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= nw) { return; }
+    const LvlNode nd = lv[wl[k]];
+    const uint32_t n = nd.count;
+    WideAcc& A = acc[k];
+    const int nb = std_clampi((int)n / 4, (int)C.bins_min, (int)C.bins_max);
+    box3 nbox;
+    for (int a = 0; a < 3; a++) { nbox.mn[a] = nd.box[a]; nbox.mx[a] = nd.box[3 + a]; }
+    const float parent_inv_area = 1.0f / box_half_area(nbox);
+    Best B;
+    B.cost = C.c_isect * (float)n;  // leaf cost, bvh_sah.cpp:32
+    B.axis = -1; B.bin = -1; B.cmin = 0.f; B.scale = 0.f; B.spatial = 0; B.node_min = 0.f; B.sscale = 0.f;
+    for (int a = 0; a < 3; a++)
+    {
+        float cmin, scale;
+        wide_axis_scale(A, a, nb, C, cmin, scale);
+        if (scale == 0.f) { continue; }
+        eval_object_axis(A.ocnt[a], A.obox[a], nb, a, cmin, scale, parent_inv_area, C, B);
+    }
+    A.o_axis = B.axis; A.o_bin = B.bin; A.o_cmin = B.cmin; A.o_scale = B.scale;
+    for (int a = 0; a < 3; a++)
+    {
+        const float node_min = nbox.mn[a], node_max = nbox.mx[a];
+        if (node_max - node_min < C.spatial_eps) { continue; }
+        const float sscale = (float)nb / (node_max - node_min);
+        eval_spatial_axis(A.cin[a], A.cout[a], A.sbox[a], nb, a, node_min, sscale, parent_inv_area, C, B);
+    }
+    A.B = B;
+}
+
+// partition side counts of the chosen candidate
+__global__ void __launch_bounds__(SBLK)
+k_wide_counts(const LvlNode* __restrict__ lv, const uint32_t* __restrict__ refs, Ctx C, const uint32_t* __restrict__ wl,
+              const uint32_t* __restrict__ wco, uint32_t nw, WideAcc* __restrict__ acc)
+{
+    __shared__ uint32_t sh[SBLK / 32 + 1];
+    uint32_t c;
+    const uint32_t k = wide_item(wco, nw, blockIdx.x, c);
+    const LvlNode nd = lv[wl[k]];
+    const uint32_t n = nd.count;
+    const uint32_t* R = refs + nd.ref_off;
+    WideAcc& A = acc[k];
+    const Best B = A.B;
+    if (B.axis == -1) { return; }
+    uint32_t b0, e0;
+    chunk_range(n, c, b0, e0);
+    const int nb = std_clampi((int)n / 4, (int)C.bins_min, (int)C.bins_max);
+    if (!B.spatial)
+    {
+        uint32_t l = 0;
+        for (uint32_t i = b0 + threadIdx.x; i < e0; i += SBLK)
+        {
+            l += obj_bin(centroid(C, R[i], B.axis), B.cmin, B.scale, nb) < B.bin ? 1u : 0u;
+        }
+        l = block_sum<SBLK>(l, sh);
+        if (threadIdx.x == 0 && l) { atomicAdd(&A.cnt[0], l); }
+        return;
+    }
+    const float plane = B.node_min + (float)B.bin / B.sscale;
+    const int axis = B.axis;
+    const int oa = A.o_axis, ob = A.o_bin;
+    const float oc = A.o_cmin, os = A.o_scale;
+    uint32_t lo_ = 0, st_ = 0, ol = 0;
+    for (uint32_t i = b0 + threadIdx.x; i < e0; i += SBLK)
+    {
+        const uint32_t t = R[i];
+        if (tri_hi(C, t, axis) <= plane) { lo_++; }
+        else if (tri_lo(C, t, axis) < plane) { st_++; }
+        if (oa != -1) { ol += obj_bin(centroid(C, t, oa), oc, os, nb) < ob ? 1u : 0u; }
+    }
+    lo_ = block_sum<SBLK>(lo_, sh);
+    st_ = block_sum<SBLK>(st_, sh);
+    ol = block_sum<SBLK>(ol, sh);
+    if (threadIdx.x == 0)
+    {
+        if (lo_) { atomicAdd(&A.cnt[0], lo_); }
+        if (st_) { atomicAdd(&A.cnt[1], st_); }
+        if (ol) { atomicAdd(&A.cnt[2], ol); }
+    }
+}
+
+// the decision record, as the one-block path writes it (bvh_sah.cpp:249-394)
+__global__ void k_wide_final(const LvlNode* __restrict__ lv, Ctx C, const uint32_t* __restrict__ wl, uint32_t nw,
+                             const WideAcc* __restrict__ acc, Dec* __restrict__ dec)
+{
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= nw) { return; }
+    const uint32_t node = wl[k];
+    const uint32_t n = lv[node].count;
+    const WideAcc& A = acc[k];
+    const Best B = A.B;
+    Dec d;
+    memset(&d, 0, sizeof(d));
+    d.n = n;
+    d.nb = std_clampi((int)n / 4, (int)C.bins_min, (int)C.bins_max);
+    d.oaxis = A.o_axis; d.obin = A.o_bin; d.ocmin = A.o_cmin; d.oscale = A.o_scale;
+    if (B.axis == -1)
+    {
+        d.kind = K_LEAF;
+    }
+    else if (!B.spatial)
+    {
+        const uint32_t l = A.cnt[0];
+        d.kind = (l == 0 || l == n) ? K_LEAF : K_OBJECT;
+        d.axis = B.axis; d.bin = B.bin; d.cmin = B.cmin; d.scale = B.scale;
+    }
+    else
+    {
+        const uint32_t lo_ = A.cnt[0], st_ = A.cnt[1], ol = A.cnt[2];
+        const uint32_t ri = n - lo_ - st_;
+        const int fb = (A.o_axis == -1 || ol == 0 || ol == n) ? K_LEAF : K_OBJECT;
+        d.sp_axis = B.axis; d.plane = B.node_min + (float)B.bin / B.sscale; d.straddle = st_; d.right = ri; d.fb_kind = fb;
+        if ((lo_ + st_ == 0) || (st_ + ri == 0))
+        {
+            // the saved object split, applied after the spatial partitions (bvh_sah.cpp:331-333)
+            d.kind = fb; d.pre_spatial = 1;
+            d.axis = A.o_axis; d.bin = A.o_bin; d.cmin = A.o_cmin; d.scale = A.o_scale;
+        }
+        else
+        {
+            d.kind = K_SPATIAL;
+            d.axis = B.axis;
+        }
+    }
+    dec[node] = d;
 }
 
 // One block: grants the spatial-split reference budget in queue order, then allocates child
@@ -448,30 +816,76 @@ k_sah_resolve(Dec* __restrict__ dec, const LvlNode* __restrict__ lv, const SahRo
         for (uint32_t k = tid; k < n_scenes; k += 1024) { used[k] = (uint32_t)(used[k] + s_need[k]); }
         if (tid == 0) { io[1] += nsp; }
     }
-    else if (tid == 0)
+    else
     {
-        for (uint32_t i = 0; i < n_lvl; i++)
+        // The grants are sequential (a refused request leaves the budget to later, smaller
+        // ones), so one thread walks the spatial candidates in queue order -- compacted first,
+        // and with one scene it stops as soon as even the smallest request no longer fits;
+        // the rest are refused in parallel. leaf_off serves as the candidate list here (it is
+        // filled only further down).
+        __shared__ uint32_t s_ns, s_stop, s_minneed;
+        uint32_t ns = 0, mn = 0xffffffffu;
+        for (uint32_t base = 0; base < n_lvl; base += 1024)
         {
-            Dec d = dec[i];
-            if (d.kind != K_SPATIAL) { continue; }
-            const uint32_t sc = min(roots[lv[i].root].scene, n_scenes - 1u);
-            const uint32_t nd = d.right + d.straddle;
-            if ((unsigned long long)used[sc] + nd > (unsigned long long)cap[sc])
+            const uint32_t i = base + tid;
+            uint32_t f = 0;
+            if (i < n_lvl)
             {
-                d.kind = d.fb_kind; d.pre_spatial = 1;
-                d.axis = d.oaxis; d.bin = d.obin; d.cmin = d.ocmin; d.scale = d.oscale;
-                dec[i] = d;
-                io[2]++;
+                const Dec d = dec[i];
+                if (d.kind == K_SPATIAL) { f = 1; mn = min(mn, d.right + d.straddle); }
             }
-            else
-            {
-                used[sc] += nd;
-                io[1]++;
-            }
+            uint32_t tot;
+            const uint32_t e = block_excl_scan<1024>(f, sh, &tot);
+            if (f) { leaf_off[ns + e] = i; }
+            ns += tot;
         }
+        for (int o = 16; o > 0; o >>= 1) { mn = min(mn, __shfl_xor_sync(0xffffffffu, mn, o)); }
+        if (tid == 0) { s_minneed = 0xffffffffu; s_ns = ns; }
+        __syncthreads();
+        if ((tid & 31) == 0) { atomicMin(&s_minneed, mn); }
+        __syncthreads();
+        if (tid == 0)
+        {
+            const uint32_t min_need = s_minneed;
+            uint32_t j = 0;
+            for (; j < s_ns; j++)
+            {
+                if (n_scenes == 1 && (unsigned long long)used[0] + min_need > (unsigned long long)cap[0]) { break; }
+                const uint32_t i = leaf_off[j];
+                Dec d = dec[i];
+                const uint32_t sc = min(roots[lv[i].root].scene, n_scenes - 1u);
+                const uint32_t nd = d.right + d.straddle;
+                if ((unsigned long long)used[sc] + nd > (unsigned long long)cap[sc])
+                {
+                    d.kind = d.fb_kind; d.pre_spatial = 1;
+                    d.axis = d.oaxis; d.bin = d.obin; d.cmin = d.ocmin; d.scale = d.oscale;
+                    dec[i] = d;
+                    io[2]++;
+                }
+                else
+                {
+                    used[sc] += nd;
+                    io[1]++;
+                }
+            }
+            s_stop = j;
+        }
+        __syncthreads();
+        uint32_t refused = 0;
+        for (uint32_t j = s_stop + tid; j < s_ns; j += 1024)
+        {
+            const uint32_t i = leaf_off[j];
+            Dec d = dec[i];
+            d.kind = d.fb_kind; d.pre_spatial = 1;
+            d.axis = d.oaxis; d.bin = d.obin; d.cmin = d.ocmin; d.scale = d.oscale;
+            dec[i] = d;
+            refused++;
+        }
+        refused = block_sum<1024>(refused, sh);
+        if (tid == 0) { io[2] += refused; }
     }
     __syncthreads();
-    uint32_t c0 = 0, c1 = 0, c2 = 0, nleaf = 0;
+    uint32_t c0 = 0, c1 = 0, c2 = 0, nleaf = 0, bmax = 0;
     for (uint32_t base = 0; base < n_lvl; base += 1024)
     {
         const uint32_t i = base + tid;
@@ -480,7 +894,7 @@ k_sah_resolve(Dec* __restrict__ dec, const LvlNode* __restrict__ lv, const SahRo
         {
             const Dec d = dec[i];
             if (d.kind == K_LEAF) { c = d.n; nleaf++; }
-            else { a = 2; b = d.kind == K_OBJECT ? d.n : d.n + d.straddle; }
+            else { a = 2; b = d.kind == K_OBJECT ? d.n : d.n + d.straddle; bmax = max(bmax, b); }
         }
         uint32_t ta, tb, tc;
         const uint32_t ea = block_excl_scan<1024>(a, sh, &ta);
@@ -490,6 +904,11 @@ k_sah_resolve(Dec* __restrict__ dec, const LvlNode* __restrict__ lv, const SahRo
         c0 += ta; c1 += tb; c2 += tc;
     }
     nleaf = block_sum<1024>(nleaf, sh);
+    // an upper bound of the largest next-level node (its parent's references)
+    for (int o = 16; o > 0; o >>= 1) { bmax = max(bmax, __shfl_xor_sync(0xffffffffu, bmax, o)); }
+    if (tid == 0) { io[10] = 0u; }
+    __syncthreads();
+    if ((tid & 31) == 0) { atomicMax(&io[10], bmax); }
     if (tid == 0) { io[3] = c0; io[4] = c1; io[5] = c2; io[6] += nleaf; }
 }
 
@@ -510,17 +929,23 @@ __device__ __forceinline__ void set_out_child(OutNode& o, const box3& b, uint32_
 // One block per node: applies the decision -- the reference's partitions in its order, the
 // children's reference lists and boxes (computeRangeAABB for object splits, the union of
 // the triangles clipped to each side for spatial splits, bvh_sah.cpp:426-444).
-__global__ void __launch_bounds__(SBLK)
+// node_list: the level nodes this launch covers (the wide nodes, with BS = 1024), or nullptr
+// for one block per level node, which then leaves the wide nodes out.
+template <int BS>
+__global__ void __launch_bounds__(BS)
 k_sah_split(const LvlNode* __restrict__ lv, const uint32_t* __restrict__ refs, const Dec* __restrict__ dec,
             const uint32_t* __restrict__ child_slot, const uint32_t* __restrict__ ref_off,
             const uint32_t* __restrict__ leaf_off, Ctx C, uint32_t* __restrict__ tmp, uint32_t* __restrict__ pos,
             uint8_t* __restrict__ flags, LvlNode* __restrict__ lv_next, uint32_t* __restrict__ refs_next,
-            OutNode* __restrict__ out, uint32_t out_base, uint32_t leaf_base, uint32_t* __restrict__ leaf_refs)
+            OutNode* __restrict__ out, uint32_t out_base, uint32_t leaf_base, uint32_t* __restrict__ leaf_refs,
+            const uint32_t* __restrict__ node_list)
 {
-    __shared__ uint32_t sh[SBLK / 32 + 1];
+    __shared__ uint32_t sh[BS / 32 + 1];
     __shared__ SBox sb[2];
-    const LvlNode nd = lv[blockIdx.x];
-    const Dec d = dec[blockIdx.x];
+    const uint32_t ni = node_list ? node_list[blockIdx.x] : blockIdx.x;
+    const LvlNode nd = lv[ni];
+    if (!node_list && nd.count > WIDE_MIN) { return; }
+    const Dec d = dec[ni];
     const uint32_t n = nd.count;
     const uint32_t* R = refs + nd.ref_off;
     uint32_t* T = tmp + nd.ref_off;
@@ -533,8 +958,8 @@ k_sah_split(const LvlNode* __restrict__ lv, const uint32_t* __restrict__ refs, c
     {
         const int ax = d.sp_axis;
         const float plane = d.plane;
-        left_end = cta_partition(R, T, n, [&](uint32_t t) { return tri_hi(C, t, ax) <= plane; }, F, P, sh);
-        straddle_end = left_end + cta_partition(T + left_end, T + left_end, n - left_end,
+        left_end = cta_partition<BS>(R, T, n, [&](uint32_t t) { return tri_hi(C, t, ax) <= plane; }, F, P, sh);
+        straddle_end = left_end + cta_partition<BS>(T + left_end, T + left_end, n - left_end,
                                                 [&](uint32_t t) { return tri_lo(C, t, ax) < plane; }, F + left_end,
                                                 P + left_end, sh);
         W = T;
@@ -542,13 +967,13 @@ k_sah_split(const LvlNode* __restrict__ lv, const uint32_t* __restrict__ refs, c
     OutNode* o = &out[nd.out];
     if (d.kind == K_LEAF)
     {
-        const uint32_t lo = leaf_base + leaf_off[blockIdx.x];
-        for (uint32_t i = tid; i < n; i += SBLK) { leaf_refs[lo + i] = W[i]; }
+        const uint32_t lo = leaf_base + leaf_off[ni];
+        for (uint32_t i = tid; i < n; i += BS) { leaf_refs[lo + i] = W[i]; }
         if (tid == 0) { o->is_leaf = 1; o->a = lo; o->b = n; }
         return;
     }
-    const uint32_t slot = child_slot[blockIdx.x];
-    const uint32_t roff = ref_off[blockIdx.x];
+    const uint32_t slot = child_slot[ni];
+    const uint32_t roff = ref_off[ni];
     const uint32_t lid = out_base + slot, rid = lid + 1;
     uint32_t* Q = refs_next + roff;
     if (tid < 2) { sbox_clear(sb[tid]); }
@@ -558,19 +983,19 @@ k_sah_split(const LvlNode* __restrict__ lv, const uint32_t* __restrict__ refs, c
     {
         const int ax = d.axis, bin = d.bin, nb = d.nb;
         const float cmin = d.cmin, scale = d.scale;
-        const uint32_t m = cta_partition(W, Q, n, [&](uint32_t t) { return obj_bin(centroid(C, t, ax), cmin, scale, nb) < bin; },
+        const uint32_t m = cta_partition<BS>(W, Q, n, [&](uint32_t t) { return obj_bin(centroid(C, t, ax), cmin, scale, nb) < bin; },
                                          F, P, sh);
         lsz = m; rsz = n - m;
-        for (uint32_t i = tid; i < n; i += SBLK) { sbox_add(sb[i < m ? 0 : 1], tri_box(C, Q[i])); }
+        for (uint32_t i = tid; i < n; i += BS) { sbox_add(sb[i < m ? 0 : 1], tri_box(C, Q[i])); }
     }
     else
     {
         const uint32_t st = straddle_end - left_end, rc = n - straddle_end;
         lsz = left_end + st;
         rsz = rc + st;
-        for (uint32_t i = tid; i < lsz; i += SBLK) { Q[i] = W[i]; }
-        for (uint32_t i = tid; i < rc; i += SBLK) { Q[lsz + i] = W[straddle_end + i]; }
-        for (uint32_t i = tid; i < st; i += SBLK) { Q[lsz + rc + i] = W[left_end + i]; }
+        for (uint32_t i = tid; i < lsz; i += BS) { Q[i] = W[i]; }
+        for (uint32_t i = tid; i < rc; i += BS) { Q[lsz + i] = W[straddle_end + i]; }
+        for (uint32_t i = tid; i < st; i += BS) { Q[lsz + rc + i] = W[left_end + i]; }
         const int ax = d.axis;
         box3 nbox;
         for (int k = 0; k < 3; k++) { nbox.mn[k] = nd.box[k]; nbox.mx[k] = nd.box[3 + k]; }
@@ -578,7 +1003,7 @@ k_sah_split(const LvlNode* __restrict__ lv, const uint32_t* __restrict__ refs, c
         lclip.mx[ax] = d.plane;
         rclip.mn[ax] = d.plane;
         __syncthreads();
-        for (uint32_t i = tid; i < lsz + rsz; i += SBLK)
+        for (uint32_t i = tid; i < lsz + rsz; i += BS)
         {
             f3 v0, v1, v2;
             tri_verts(C, Q[i], v0, v1, v2);
@@ -755,8 +1180,15 @@ int sah_build(rt_bvh* B, const rt_build_cfg& cfg, const SahInput& in, cudaStream
     uint32_t* root_out = leaf_offs + cap;
     uint32_t* new_off = root_out + nr;
     uint32_t* io = new_off + nr;
-    uint32_t io_h[8] = { in.n, 0, 0, 0, 0, 0, 0, 0 };
-    RT_CUDA(cudaMemcpyAsync(io, io_h, 32, cudaMemcpyHostToDevice, st));
+    uint32_t io_h[16] = { in.n, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0 };
+    RT_CUDA(cudaMemcpyAsync(io, io_h, 64, cudaMemcpyHostToDevice, st));
+    // wide-node scratch: at most cap / WIDE_MIN nodes of a level have more than WIDE_MIN references
+    const uint32_t max_wide = cap / WIDE_MIN + 2;
+    if (S.sah_wide.ensure((size_t)max_wide * sizeof(WideAcc) + (size_t)(2 * max_wide + 2) * 4)) { return RT_E_CUDA; }
+    WideAcc* wacc = S.sah_wide.as<WideAcc>();
+    uint32_t* wl = reinterpret_cast<uint32_t*>(wacc + max_wide);
+    uint32_t* wco = wl + max_wide;
+    uint32_t next_bound = 0;  // upper bound of the largest node of the coming level
     const uint32_t n_budget = (uint32_t)in.budget_used.size();
     if (n_budget == 0 || n_budget > MAX_BUDGET_SCENES || in.budget_cap.size() != n_budget)
     {
@@ -793,6 +1225,7 @@ int sah_build(rt_bvh* B, const rt_build_cfg& cfg, const SahInput& in, cudaStream
         {
             new_off_h[ri + m] = r_cur + add;
             add += roots[ri + m].count;
+            next_bound = std::max(next_bound, roots[ri + m].count);
             m++;
         }
         const uint32_t lvl_begin = out_total - n_cur;
@@ -820,22 +1253,54 @@ int sah_build(rt_bvh* B, const rt_build_cfg& cfg, const SahInput& in, cudaStream
             continue;
         }
         levels.emplace_back(lvl_begin, out_total);
+        uint32_t nw = 0, nch = 0;
+        if (next_bound > WIDE_MIN)
+        {
+            k_wide_list<<<1, 1024, 0, st>>>(lv_cur, n_cur, wl, wco, max_wide, io);
+            count_launch();
+            RT_CUDA(cudaMemcpyAsync(io_h + 8, io + 8, 8, cudaMemcpyDeviceToHost, st));
+            RT_CUDA(cudaStreamSynchronize(st));
+            nw = io_h[8];
+            nch = io_h[9];
+            if (nw > max_wide) { return fail(RT_E_CAPACITY, "SAH builder: too many wide nodes"); }
+        }
         k_sah_eval<<<n_cur, SBLK, 0, st>>>(lv_cur, refs_cur, C, S.sah_dec.as<Dec>());
+        count_launch();
+        if (nw > 0)
+        {
+            k_wide_init<<<nw, SBLK, 0, st>>>(wacc);
+            k_wide_bounds<<<nch, SBLK, 0, st>>>(lv_cur, refs_cur, C, wl, wco, nw, wacc);
+            k_wide_bins<<<nch, SBLK, 0, st>>>(lv_cur, refs_cur, C, wl, wco, nw, wacc);
+            k_wide_decide<<<(nw + 31) / 32, 32, 0, st>>>(lv_cur, C, wl, nw, wacc);
+            k_wide_counts<<<nch, SBLK, 0, st>>>(lv_cur, refs_cur, C, wl, wco, nw, wacc);
+            k_wide_final<<<(nw + 31) / 32, 32, 0, st>>>(lv_cur, C, wl, nw, wacc, S.sah_dec.as<Dec>());
+            count_launch(6);
+        }
         k_sah_resolve<<<1, 1024, 0, st>>>(S.sah_dec.as<Dec>(), lv_cur, d_roots, n_cur, n_budget, d_used, d_used + n_budget,
                                           io, child_slot, ref_offs, leaf_offs);
-        count_launch(2);
+        count_launch();
         if (int e = check_launch("sah eval")) { return e; }
-        RT_CUDA(cudaMemcpyAsync(io_h, io, 32, cudaMemcpyDeviceToHost, st));
+        RT_CUDA(cudaMemcpyAsync(io_h, io, 64, cudaMemcpyDeviceToHost, st));
         RT_CUDA(cudaStreamSynchronize(st));
         const uint32_t n_next = io_h[3], r_next = io_h[4], leaf_lvl = io_h[5];
         if (n_next > cap || r_next > cap || (uint64_t)out_total + n_next > 2ull * cap || (uint64_t)leaf_total + leaf_lvl > cap)
         {
             return fail(RT_E_CAPACITY, "SAH builder: capacity exceeded");
         }
-        k_sah_split<<<n_cur, SBLK, 0, st>>>(lv_cur, refs_cur, S.sah_dec.as<Dec>(), child_slot, ref_offs, leaf_offs, C,
-                                            S.sah_tmp.as<uint32_t>(), S.sah_pos.as<uint32_t>(), S.sah_scan_in.as<uint8_t>(),
-                                            lv_next, refs_next, out, out_total, leaf_total, S.sah_leaf_refs.as<uint32_t>());
+        k_sah_split<SBLK><<<n_cur, SBLK, 0, st>>>(lv_cur, refs_cur, S.sah_dec.as<Dec>(), child_slot, ref_offs, leaf_offs, C,
+                                                  S.sah_tmp.as<uint32_t>(), S.sah_pos.as<uint32_t>(),
+                                                  S.sah_scan_in.as<uint8_t>(), lv_next, refs_next, out, out_total, leaf_total,
+                                                  S.sah_leaf_refs.as<uint32_t>(), nullptr);
         count_launch();
+        if (nw > 0)
+        {
+            k_sah_split<1024><<<nw, 1024, 0, st>>>(lv_cur, refs_cur, S.sah_dec.as<Dec>(), child_slot, ref_offs, leaf_offs, C,
+                                                   S.sah_tmp.as<uint32_t>(), S.sah_pos.as<uint32_t>(),
+                                                   S.sah_scan_in.as<uint8_t>(), lv_next, refs_next, out, out_total,
+                                                   leaf_total, S.sah_leaf_refs.as<uint32_t>(), wl);
+            count_launch();
+        }
+        next_bound = io_h[10];
         if (int e = check_launch("sah split")) { return e; }
         out_total += n_next;
         leaf_total += leaf_lvl;

@@ -94,14 +94,17 @@ def test_errors_are_reported():
     assert e.value.code == 8  # RT_E_EMPTY
 
 
-@pytest.mark.parametrize("preset", ["lbvh63", "lbvh30", "hybrid"])
+@pytest.mark.parametrize("preset", ["lbvh63", "lbvh30", "hybrid", "sah4", "sah16"])
 def test_large_odd_soup_matches_oracle(orc, preset):
     """262,147 triangles: 257 tiles of the local tree phase (the last one partial), frontier
-    nodes on every tile edge, and the large-input tile shape of the radix sort."""
+    nodes on every tile edge; for the SAH presets the top levels' nodes above 16,384
+    references, which many blocks evaluate at once."""
     v, t = scenes.soup(262147, seed=77)
     ref = orc.build(v, t, orc_cfg(preset))
     b = rtb200.Bvh.build(v, t, preset)
     assert_same_tree(b.download(), ref, f"soup262147/{preset}")
+    st = b.stats()
+    assert st["spatial_taken"] == int(ref.stats[0]) and st["spatial_refused"] == int(ref.stats[1])
 
 
 def test_sort_tile_shapes_agree(orc):
