@@ -120,6 +120,27 @@ __device__ __forceinline__ void sbox_add(SBox& s, const box3& b)
 {
     for (int k = 0; k < 3; k++) { atomicMin(&s.m[k], f2ord(b.mn[k])); atomicMax(&s.M[k], f2ord(b.mx[k])); }
 }
+// A thread's own accumulation in the same encoding, merged into a shared SBox once per warp
+// (min / max of the encoded values are exact and order-free, so the result is the same as
+// adding every box to the SBox directly).
+struct OBox { uint32_t m[3], M[3]; };
+__device__ __forceinline__ void obox_clear(OBox& o) { for (int k = 0; k < 3; k++) { o.m[k] = 0xffffffffu; o.M[k] = 0u; } }
+__device__ __forceinline__ void obox_add(OBox& o, const box3& b)
+{
+    for (int k = 0; k < 3; k++) { o.m[k] = min(o.m[k], f2ord(b.mn[k])); o.M[k] = max(o.M[k], f2ord(b.mx[k])); }
+}
+__device__ __forceinline__ void obox_flush_warp(OBox o, SBox& s)
+{
+    for (int k = 0; k < 3; k++)
+    {
+        o.m[k] = __reduce_min_sync(0xffffffffu, o.m[k]);
+        o.M[k] = __reduce_max_sync(0xffffffffu, o.M[k]);
+    }
+    if ((threadIdx.x & 31) == 0 && !(o.m[0] == 0xffffffffu && o.M[0] == 0u))
+    {
+        for (int k = 0; k < 3; k++) { atomicMin(&s.m[k], o.m[k]); atomicMax(&s.M[k], o.M[k]); }
+    }
+}
 __device__ __forceinline__ box3 sbox_get(const SBox& s)
 {
     box3 b;
@@ -201,70 +222,273 @@ struct Best
     int   axis, bin, spatial;
 };
 
-// Object-split candidates of one axis (bvh_sah.cpp:88-126): sweeps from both sides over the
-// centroid bins, bins b = nb-1 .. 1, strict improvement only.
-__device__ __noinline__ void eval_object_axis(const uint32_t* cnt, const SBox* bins, int nb, int axis, float cmin, float scale,
-                                              float parent_inv_area, const Ctx& C, Best& B)
+// The candidate sweeps of bvh_sah.cpp:88-126 (object splits: centroid bins, counts from both
+// sides) and :198-243 (spatial splits: entry counts from the left, exit counts from the right,
+// clipped boxes), bins b = nb-1 .. 1, strict improvement only -- across one warp: lane b holds
+// bin b; the left and right unions are
+// inclusive scans of the order-preserving box encoding (min / max are exact there, so the
+// decoded boxes -- and the costs -- equal the serial ones: the serial union of float boxes
+// differs only in the sign of zero bounds, which leaves extents and areas unchanged), and the
+// winner is the candidate the serial loop keeps: the lowest cost, on ties the first in its
+// order (bins b = nb-1 .. 1), taken only if strictly below the best so far. All 32 lanes call
+// these with the same B and return the same B.
+__device__ __forceinline__ void warp_box_scan_up(uint32_t (&m)[3], uint32_t (&M)[3], uint32_t& c, int lane)
 {
-    box3 lbox[SAH_MAX_BINS];
-    uint32_t lcnt[SAH_MAX_BINS];
-    box3 la = box_empty();
-    uint32_t lc = 0;
-    for (int b = 0; b < nb - 1; b++)
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1)
     {
-        if (cnt[b]) { box_box(la, sbox_get(bins[b])); }
-        lc += cnt[b];
-        lbox[b] = la; lcnt[b] = lc;
+        uint32_t tm[3], tM[3];
+        for (int k = 0; k < 3; k++) { tm[k] = __shfl_up_sync(0xffffffffu, m[k], o); tM[k] = __shfl_up_sync(0xffffffffu, M[k], o); }
+        const uint32_t tc = __shfl_up_sync(0xffffffffu, c, o);
+        if (lane >= o)
+        {
+            for (int k = 0; k < 3; k++) { m[k] = min(m[k], tm[k]); M[k] = max(M[k], tM[k]); }
+            c += tc;
+        }
     }
-    box3 ra = box_empty();
-    uint32_t rc = 0;
-    for (int b = nb - 1; b >= 1; b--)
+}
+__device__ __forceinline__ void warp_box_scan_down(uint32_t (&m)[3], uint32_t (&M)[3], uint32_t& c, int lane)
+{
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1)
     {
-        if (cnt[b]) { box_box(ra, sbox_get(bins[b])); }
-        rc += cnt[b];
-        const uint32_t lc2 = lcnt[b - 1];
-        if (lc2 == 0 || rc == 0) { continue; }
-        const float cost = C.c_trav + C.c_isect *
-            (box_half_area(lbox[b - 1]) * (float)lc2 + box_half_area(ra) * (float)rc) * parent_inv_area;
-        if (cost < B.cost) { B.cost = cost; B.axis = axis; B.bin = b; B.cmin = cmin; B.scale = scale; }
+        uint32_t tm[3], tM[3];
+        for (int k = 0; k < 3; k++) { tm[k] = __shfl_down_sync(0xffffffffu, m[k], o); tM[k] = __shfl_down_sync(0xffffffffu, M[k], o); }
+        const uint32_t tc = __shfl_down_sync(0xffffffffu, c, o);
+        if (lane + o < 32)
+        {
+            for (int k = 0; k < 3; k++) { m[k] = min(m[k], tm[k]); M[k] = max(M[k], tM[k]); }
+            c += tc;
+        }
+    }
+}
+__device__ __forceinline__ box3 ord_box(const uint32_t (&m)[3], const uint32_t (&M)[3])
+{
+    box3 b = box_empty();
+    if (m[0] != 0xffffffffu) { for (int k = 0; k < 3; k++) { b.mn[k] = ord2f(m[k]); b.mx[k] = ord2f(M[k]); } }
+    return b;
+}
+
+// cl / cr: the counts that enter the left / right sweeps (object: the bin count for both;
+// spatial: entries and exits); has_box(b): whether bin b's box joins the unions.
+__device__ __forceinline__ bool warp_sweep(const uint32_t* cl, const uint32_t* cr, const SBox* bins, bool object, int nb,
+                                           float parent_inv_area, const Ctx& C, float& best_cost, int& best_bin)
+{
+    const int lane = threadIdx.x & 31;
+    uint32_t lm[3], lM[3], rm[3], rM[3], lc = 0, rc = 0;
+    for (int k = 0; k < 3; k++) { lm[k] = rm[k] = 0xffffffffu; lM[k] = rM[k] = 0u; }
+    if (lane < nb)
+    {
+        const SBox& sb = bins[lane];
+        const bool use = object ? (cl[lane] != 0u) : true;
+        if (use) { for (int k = 0; k < 3; k++) { lm[k] = rm[k] = sb.m[k]; lM[k] = rM[k] = sb.M[k]; } }
+        lc = cl[lane];
+        rc = cr[lane];
+    }
+    warp_box_scan_up(lm, lM, lc, lane);    // lane b: bins 0..b
+    warp_box_scan_down(rm, rM, rc, lane);  // lane b: bins b..31 (empty beyond nb)
+    // candidate b pairs the left union up to b-1 with the right union from b
+    uint32_t pm[3], pM[3];
+    for (int k = 0; k < 3; k++) { pm[k] = __shfl_up_sync(0xffffffffu, lm[k], 1); pM[k] = __shfl_up_sync(0xffffffffu, lM[k], 1); }
+    const uint32_t pc = __shfl_up_sync(0xffffffffu, lc, 1);
+    float cost = __int_as_float(0x7f800000);
+    if (lane >= 1 && lane < nb && pc != 0u && rc != 0u)
+    {
+        const box3 lb = ord_box(pm, pM), rb = ord_box(rm, rM);
+        cost = C.c_trav + C.c_isect * (box_half_area(lb) * (float)pc + box_half_area(rb) * (float)rc) * parent_inv_area;
+        if (!(cost <= 3.402823466e38f)) { cost = __int_as_float(0x7f800000); }  // a NaN never wins, as in the serial loop
+    }
+    // lowest cost; ties to the larger bin (visited first by the serial loop)
+    float bc = cost;
+    int bb = lane;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1)
+    {
+        const float oc = __shfl_xor_sync(0xffffffffu, bc, o);
+        const int obb = __shfl_xor_sync(0xffffffffu, bb, o);
+        if (oc < bc || (oc == bc && obb > bb)) { bc = oc; bb = obb; }
+    }
+    if (bc < best_cost) { best_cost = bc; best_bin = bb; return true; }
+    return false;
+}
+
+__device__ __forceinline__ void warp_eval_object_axis(const uint32_t* cnt, const SBox* bins, int nb, int axis, float cmin,
+                                                      float scale, float parent_inv_area, const Ctx& C, Best& B)
+{
+    int bin = -1;
+    if (warp_sweep(cnt, cnt, bins, true, nb, parent_inv_area, C, B.cost, bin))
+    {
+        B.axis = axis; B.bin = bin; B.cmin = cmin; B.scale = scale;
     }
 }
 
-// Spatial-split candidates of one axis (bvh_sah.cpp:198-243): entry counts from the left,
-// exit counts from the right, boxes of the clipped triangles.
-__device__ __noinline__ void eval_spatial_axis(const uint32_t* cin, const uint32_t* cout, const SBox* bins, int nb, int axis,
-                                               float node_min, float sscale, float parent_inv_area, const Ctx& C, Best& B)
+__device__ __forceinline__ void warp_eval_spatial_axis(const uint32_t* cin, const uint32_t* cout, const SBox* bins, int nb,
+                                                       int axis, float node_min, float sscale, float parent_inv_area,
+                                                       const Ctx& C, Best& B)
 {
-    box3 lbox[SAH_MAX_BINS];
-    uint32_t lcnt[SAH_MAX_BINS];
-    box3 la = box_empty();
-    uint32_t lc = 0;
-    for (int b = 0; b < nb - 1; b++)
+    int bin = -1;
+    if (warp_sweep(cin, cout, bins, false, nb, parent_inv_area, C, B.cost, bin))
     {
-        box_box(la, sbox_result(bins[b]));
-        lc += cin[b];
-        lbox[b] = la; lcnt[b] = lc;
-    }
-    box3 ra = box_empty();
-    uint32_t rc = 0;
-    for (int b = nb - 1; b >= 1; b--)
-    {
-        box_box(ra, sbox_result(bins[b]));
-        rc += cout[b];
-        const uint32_t lc2 = lcnt[b - 1];
-        if (lc2 == 0 || rc == 0) { continue; }
-        const float cost = C.c_trav + C.c_isect *
-            (box_half_area(lbox[b - 1]) * (float)lc2 + box_half_area(ra) * (float)rc) * parent_inv_area;
-        if (cost < B.cost)
-        {
-            B.cost = cost; B.axis = axis; B.bin = b; B.spatial = 1; B.node_min = node_min; B.sscale = sscale;
-        }
+        B.axis = axis; B.bin = bin; B.spatial = 1; B.node_min = node_min; B.sscale = sscale;
     }
 }
 
 // Nodes with more references than this are evaluated and partitioned by many blocks (the
-// wide kernels below); the rest by one block each.
+// wide kernels below); nodes with at most WARP_MAX references are evaluated by one warp each
+// (k_sah_eval_warp); the rest by one block each.
 constexpr uint32_t WIDE_MIN = 16384;
+constexpr uint32_t WARP_MAX = 512;
+constexpr int      EVAL_WPB = 8;  // warps (nodes) per block of k_sah_eval_warp
+
+// The evaluation of k_sah_eval below for one small node per warp: the same candidates, bins
+// and serial sweeps (lane 0), with warp reductions in place of block ones.
+__global__ void __launch_bounds__(EVAL_WPB * 32)
+k_sah_eval_warp(const LvlNode* __restrict__ lv, const uint32_t* __restrict__ refs, Ctx C, Dec* __restrict__ dec,
+                uint32_t n_lvl)
+{
+    struct WS
+    {
+        uint32_t cnt[SAH_MAX_BINS], cin[SAH_MAX_BINS], cout[SAH_MAX_BINS];
+        SBox     bins[SAH_MAX_BINS];
+    };
+    __shared__ WS ws[EVAL_WPB];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t node = blockIdx.x * EVAL_WPB + (uint32_t)w;
+    if (node >= n_lvl) { return; }
+    const LvlNode nd = lv[node];
+    const uint32_t n = nd.count;
+    if (n > WARP_MAX) { return; }  // a block or the wide kernels decide this node
+    WS& S = ws[w];
+    const uint32_t* R = refs + nd.ref_off;
+    Dec d;
+    memset(&d, 0, sizeof(d));
+    d.n = n;
+    if (n <= C.max_leaf)
+    {
+        if (lane == 0) { d.kind = K_LEAF; dec[node] = d; }
+        return;
+    }
+    const int nb = std_clampi((int)n / 4, (int)C.bins_min, (int)C.bins_max);
+    box3 nbox;
+    for (int k = 0; k < 3; k++) { nbox.mn[k] = nd.box[k]; nbox.mx[k] = nd.box[3 + k]; }
+    const float parent_inv_area = 1.0f / box_half_area(nbox);
+    Best Bw;  // identical in every lane
+    Bw.cost = C.c_isect * (float)n;  // leaf cost, bvh_sah.cpp:32
+    Bw.axis = -1; Bw.bin = -1; Bw.cmin = 0.f; Bw.scale = 0.f; Bw.spatial = 0; Bw.node_min = 0.f; Bw.sscale = 0.f;
+    // phase 1: centroid-binned object split (bvh_sah.cpp:52-126)
+    for (int axis = 0; axis < 3; axis++)
+    {
+        uint32_t m = 0xffffffffu, M = 0u;
+        for (uint32_t i = lane; i < n; i += 32)
+        {
+            const uint32_t o = f2ord(centroid(C, R[i], axis));
+            m = min(m, o); M = max(M, o);
+        }
+        m = __reduce_min_sync(0xffffffffu, m);
+        M = __reduce_max_sync(0xffffffffu, M);
+        const float cmin = std_min(3.402823466e38f, ord2f(m));
+        const float cmax = std_max(-3.402823466e38f, ord2f(M));
+        if (cmax - cmin < C.centroid_eps) { continue; }
+        const float scale = (float)nb / (cmax - cmin);
+        for (int b = lane; b < nb; b += 32) { S.cnt[b] = 0u; sbox_clear(S.bins[b]); }
+        __syncwarp();
+        for (uint32_t i = lane; i < n; i += 32)
+        {
+            const uint32_t t = R[i];
+            const int b = obj_bin(centroid(C, t, axis), cmin, scale, nb);
+            atomicAdd(&S.cnt[b], 1u);
+            sbox_add(S.bins[b], tri_box(C, t));
+        }
+        __syncwarp();
+        warp_eval_object_axis(S.cnt, S.bins, nb, axis, cmin, scale, parent_inv_area, C, Bw);
+        __syncwarp();
+    }
+    const int oa = Bw.axis, ob = Bw.bin;
+    const float oc = Bw.cmin, os = Bw.scale;
+    // phase 2: spatial bins over the node box, triangles clipped per bin (bvh_sah.cpp:135-243)
+    for (int axis = 0; axis < 3; axis++)
+    {
+        const float node_min = nbox.mn[axis], node_max = nbox.mx[axis];
+        if (node_max - node_min < C.spatial_eps) { continue; }
+        const float sscale = (float)nb / (node_max - node_min);
+        for (int b = lane; b < nb; b += 32) { S.cin[b] = 0u; S.cout[b] = 0u; sbox_clear(S.bins[b]); }
+        __syncwarp();
+        for (uint32_t i = lane; i < n; i += 32)
+        {
+            const uint32_t t = R[i];
+            const int bmin = std_clampi(x86_f2i((tri_lo(C, t, axis) - node_min) * sscale), 0, nb - 1);
+            const int bmax = std_clampi(x86_f2i((tri_hi(C, t, axis) - node_min) * sscale), 0, nb - 1);
+            atomicAdd(&S.cin[bmin], 1u);
+            atomicAdd(&S.cout[bmax], 1u);
+            if (bmin <= bmax)
+            {
+                f3 v0, v1, v2;
+                tri_verts(C, t, v0, v1, v2);
+                box3 region = nbox;
+                for (int b = bmin; b <= bmax; b++)
+                {
+                    region.mn[axis] = node_min + (float)b / sscale;
+                    region.mx[axis] = node_min + (float)(b + 1) / sscale;
+                    const box3 cl = clip_triangle(v0, v1, v2, region);
+                    if (box_valid(cl)) { sbox_add(S.bins[b], cl); }
+                }
+            }
+        }
+        __syncwarp();
+        warp_eval_spatial_axis(S.cin, S.cout, S.bins, nb, axis, node_min, sscale, parent_inv_area, C, Bw);
+        __syncwarp();
+    }
+    // decision and partition side counts (bvh_sah.cpp:249-394)
+    const Best B = Bw;
+    d.nb = nb;
+    d.oaxis = oa; d.obin = ob; d.ocmin = oc; d.oscale = os;
+    if (B.axis == -1)
+    {
+        d.kind = K_LEAF;
+    }
+    else if (!B.spatial)
+    {
+        uint32_t l = 0;
+        for (uint32_t i = lane; i < n; i += 32)
+        {
+            l += obj_bin(centroid(C, R[i], B.axis), B.cmin, B.scale, nb) < B.bin ? 1u : 0u;
+        }
+        l = __reduce_add_sync(0xffffffffu, l);
+        d.kind = (l == 0 || l == n) ? K_LEAF : K_OBJECT;
+        d.axis = B.axis; d.bin = B.bin; d.cmin = B.cmin; d.scale = B.scale;
+    }
+    else
+    {
+        const float plane = B.node_min + (float)B.bin / B.sscale;
+        const int axis = B.axis;
+        uint32_t lo_ = 0, st_ = 0, ol = 0;
+        for (uint32_t i = lane; i < n; i += 32)
+        {
+            const uint32_t t = R[i];
+            if (tri_hi(C, t, axis) <= plane) { lo_++; }
+            else if (tri_lo(C, t, axis) < plane) { st_++; }
+            if (oa != -1) { ol += obj_bin(centroid(C, t, oa), oc, os, nb) < ob ? 1u : 0u; }
+        }
+        lo_ = __reduce_add_sync(0xffffffffu, lo_);
+        st_ = __reduce_add_sync(0xffffffffu, st_);
+        ol = __reduce_add_sync(0xffffffffu, ol);
+        const uint32_t ri = n - lo_ - st_;
+        const int fb = (oa == -1 || ol == 0 || ol == n) ? K_LEAF : K_OBJECT;
+        d.sp_axis = axis; d.plane = plane; d.straddle = st_; d.right = ri; d.fb_kind = fb;
+        if ((lo_ + st_ == 0) || (st_ + ri == 0))
+        {
+            // the saved object split, applied after the spatial partitions (bvh_sah.cpp:331-333)
+            d.kind = fb; d.pre_spatial = 1;
+            d.axis = oa; d.bin = ob; d.cmin = oc; d.scale = os;
+        }
+        else
+        {
+            d.kind = K_SPATIAL;
+            d.axis = axis;
+        }
+    }
+    if (lane == 0) { dec[node] = d; }
+}
 
 // One block per node: evaluates every object and spatial candidate in the reference's order
 // and writes the decision with the side counts of its partitions.
@@ -286,12 +510,12 @@ k_sah_eval(const LvlNode* __restrict__ lv, const uint32_t* __restrict__ refs, Ct
     Dec d;
     memset(&d, 0, sizeof(d));
     d.n = n;
+    if (n <= WARP_MAX || n > WIDE_MIN) { return; }  // k_sah_eval_warp or the wide kernels decide this node
     if (n <= C.max_leaf)
     {
         if (tid == 0) { d.kind = K_LEAF; dec[blockIdx.x] = d; }
         return;
     }
-    if (n > WIDE_MIN) { return; }  // the wide kernels decide this node
     const int nb = std_clampi((int)n / 4, (int)C.bins_min, (int)C.bins_max);
     box3 nbox;
     for (int k = 0; k < 3; k++) { nbox.mn[k] = nd.box[k]; nbox.mx[k] = nd.box[3 + k]; }
@@ -331,7 +555,12 @@ k_sah_eval(const LvlNode* __restrict__ lv, const uint32_t* __restrict__ refs, Ct
             sbox_add(bins[b], tri_box(C, t));
         }
         __syncthreads();
-        if (tid == 0) { eval_object_axis(cnt, bins, nb, axis, cmin, scale, parent_inv_area, C, sB); }
+        if (tid < 32)
+        {
+            Best b = sB;
+            warp_eval_object_axis(cnt, bins, nb, axis, cmin, scale, parent_inv_area, C, b);
+            if (tid == 0) { sB = b; }
+        }
         __syncthreads();
     }
     if (tid == 0) { o_axis = sB.axis; o_bin = sB.bin; o_cmin = sB.cmin; o_scale = sB.scale; }
@@ -367,7 +596,12 @@ k_sah_eval(const LvlNode* __restrict__ lv, const uint32_t* __restrict__ refs, Ct
             }
         }
         __syncthreads();
-        if (tid == 0) { eval_spatial_axis(cin, cout, bins, nb, axis, node_min, sscale, parent_inv_area, C, sB); }
+        if (tid < 32)
+        {
+            Best b = sB;
+            warp_eval_spatial_axis(cin, cout, bins, nb, axis, node_min, sscale, parent_inv_area, C, b);
+            if (tid == 0) { sB = b; }
+        }
         __syncthreads();
     }
 
@@ -644,11 +878,11 @@ k_wide_bins(const LvlNode* __restrict__ lv, const uint32_t* __restrict__ refs, C
     }
 }
 
-// the reference's serial candidate evaluation over the accumulated bins, one thread per node
-__global__ void k_wide_decide(const LvlNode* __restrict__ lv, Ctx C, const uint32_t* __restrict__ wl, uint32_t nw,
-                              WideAcc* __restrict__ acc)
+// the candidate evaluation over the accumulated bins, one warp per node
+__global__ void __launch_bounds__(32) k_wide_decide(const LvlNode* __restrict__ lv, Ctx C, const uint32_t* __restrict__ wl,
+                                                    uint32_t nw, WideAcc* __restrict__ acc)
 {
-    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t k = blockIdx.x;
     if (k >= nw) { return; }
     const LvlNode nd = lv[wl[k]];
     const uint32_t n = nd.count;
@@ -665,17 +899,17 @@ __global__ void k_wide_decide(const LvlNode* __restrict__ lv, Ctx C, const uint3
         float cmin, scale;
         wide_axis_scale(A, a, nb, C, cmin, scale);
         if (scale == 0.f) { continue; }
-        eval_object_axis(A.ocnt[a], A.obox[a], nb, a, cmin, scale, parent_inv_area, C, B);
+        warp_eval_object_axis(A.ocnt[a], A.obox[a], nb, a, cmin, scale, parent_inv_area, C, B);
     }
-    A.o_axis = B.axis; A.o_bin = B.bin; A.o_cmin = B.cmin; A.o_scale = B.scale;
+    if (threadIdx.x == 0) { A.o_axis = B.axis; A.o_bin = B.bin; A.o_cmin = B.cmin; A.o_scale = B.scale; }
     for (int a = 0; a < 3; a++)
     {
         const float node_min = nbox.mn[a], node_max = nbox.mx[a];
         if (node_max - node_min < C.spatial_eps) { continue; }
         const float sscale = (float)nb / (node_max - node_min);
-        eval_spatial_axis(A.cin[a], A.cout[a], A.sbox[a], nb, a, node_min, sscale, parent_inv_area, C, B);
+        warp_eval_spatial_axis(A.cin[a], A.cout[a], A.sbox[a], nb, a, node_min, sscale, parent_inv_area, C, B);
     }
-    A.B = B;
+    if (threadIdx.x == 0) { A.B = B; }
 }
 
 // partition side counts of the chosen candidate
@@ -986,7 +1220,11 @@ k_sah_split(const LvlNode* __restrict__ lv, const uint32_t* __restrict__ refs, c
         const uint32_t m = cta_partition<BS>(W, Q, n, [&](uint32_t t) { return obj_bin(centroid(C, t, ax), cmin, scale, nb) < bin; },
                                          F, P, sh);
         lsz = m; rsz = n - m;
-        for (uint32_t i = tid; i < n; i += BS) { sbox_add(sb[i < m ? 0 : 1], tri_box(C, Q[i])); }
+        OBox ob[2];
+        obox_clear(ob[0]); obox_clear(ob[1]);
+        for (uint32_t i = tid; i < n; i += BS) { obox_add(ob[i < m ? 0 : 1], tri_box(C, Q[i])); }
+        obox_flush_warp(ob[0], sb[0]);
+        obox_flush_warp(ob[1], sb[1]);
     }
     else
     {
@@ -1003,13 +1241,17 @@ k_sah_split(const LvlNode* __restrict__ lv, const uint32_t* __restrict__ refs, c
         lclip.mx[ax] = d.plane;
         rclip.mn[ax] = d.plane;
         __syncthreads();
+        OBox ob[2];
+        obox_clear(ob[0]); obox_clear(ob[1]);
         for (uint32_t i = tid; i < lsz + rsz; i += BS)
         {
             f3 v0, v1, v2;
             tri_verts(C, Q[i], v0, v1, v2);
             const box3 cl = clip_triangle(v0, v1, v2, i < lsz ? lclip : rclip);
-            if (box_valid(cl)) { sbox_add(sb[i < lsz ? 0 : 1], cl); }
+            if (box_valid(cl)) { obox_add(ob[i < lsz ? 0 : 1], cl); }
         }
+        obox_flush_warp(ob[0], sb[0]);
+        obox_flush_warp(ob[1], sb[1]);
     }
     __syncthreads();
     if (tid == 0)
@@ -1264,14 +1506,20 @@ int sah_build(rt_bvh* B, const rt_build_cfg& cfg, const SahInput& in, cudaStream
             nch = io_h[9];
             if (nw > max_wide) { return fail(RT_E_CAPACITY, "SAH builder: too many wide nodes"); }
         }
-        k_sah_eval<<<n_cur, SBLK, 0, st>>>(lv_cur, refs_cur, C, S.sah_dec.as<Dec>());
+        k_sah_eval_warp<<<(n_cur + EVAL_WPB - 1) / EVAL_WPB, EVAL_WPB * 32, 0, st>>>(lv_cur, refs_cur, C, S.sah_dec.as<Dec>(),
+                                                                                       n_cur);
         count_launch();
+        if (next_bound > WARP_MAX)
+        {
+            k_sah_eval<<<n_cur, SBLK, 0, st>>>(lv_cur, refs_cur, C, S.sah_dec.as<Dec>());
+            count_launch();
+        }
         if (nw > 0)
         {
             k_wide_init<<<nw, SBLK, 0, st>>>(wacc);
             k_wide_bounds<<<nch, SBLK, 0, st>>>(lv_cur, refs_cur, C, wl, wco, nw, wacc);
             k_wide_bins<<<nch, SBLK, 0, st>>>(lv_cur, refs_cur, C, wl, wco, nw, wacc);
-            k_wide_decide<<<(nw + 31) / 32, 32, 0, st>>>(lv_cur, C, wl, nw, wacc);
+            k_wide_decide<<<nw, 32, 0, st>>>(lv_cur, C, wl, nw, wacc);
             k_wide_counts<<<nch, SBLK, 0, st>>>(lv_cur, refs_cur, C, wl, wco, nw, wacc);
             k_wide_final<<<(nw + 31) / 32, 32, 0, st>>>(lv_cur, C, wl, nw, wacc, S.sah_dec.as<Dec>());
             count_launch(6);
