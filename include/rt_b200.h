@@ -127,6 +127,13 @@ void rt_bvh_free(rt_bvh* bvh);
 #define RT_TRACE_ANY_HIT     1u  /* stop at the first accepted triangle */
 #define RT_TRACE_WATERTIGHT  2u  /* watertight test (Woop, Benthin, Wald 2013), no culling */
 
+/* Traversal loop form of a handle (no counterpart in the reference): 0 the one-loop form of
+ * traverse() (bvh_traverse.cpp:91-178), 1 the while-while form (lanes of a warp walk inner
+ * nodes, then test leaves, together), -1 the default: while-while when leaves hold 6 or more
+ * triangles on average. Both visit the same nodes in the same order and give identical hits;
+ * only their speed differs. */
+int rt_bvh_trace_loop(rt_bvh* bvh, int form);
+
 /* Traces n rays; rays and hits are device pointers. Returns RT_E_STACK if any ray
  * overflowed its 64-entry stack (those hits carry RT_HIT_FLAG_OVERFLOW). */
 int rt_trace(const rt_bvh* bvh, const rt_ray* rays, rt_hit* hits, uint64_t n, uint32_t flags, void* stream);

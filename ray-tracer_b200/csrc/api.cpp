@@ -326,12 +326,15 @@ int rt_bvh_from_arrays(const rt_bvh_node* nodes, uint32_t n_nodes, const rt_tria
     if (n_nodes == 0) { return fail(RT_E_FORMAT, "BVH without nodes"); }
     if (int e = require_device()) { return e; }
     // structural checks before any device pointer chasing: child and triangle indices
+    uint64_t n_leaves = 0, leaf_tris = 0;
     for (uint32_t i = 0; i < n_nodes; i++)
     {
         const rt_bvh_node& nd = nodes[i];
         if (nd.is_leaf)
         {
             if ((uint64_t)nd.a + nd.b > n_tris) { return fail(RT_E_FORMAT, "leaf triangle range outside the triangle array"); }
+            n_leaves++;
+            leaf_tris += nd.b;
         }
         else if (nd.a >= n_nodes || nd.b >= n_nodes || nd.a <= i || nd.b <= i)
         {
@@ -364,6 +367,7 @@ int rt_bvh_from_arrays(const rt_bvh_node* nodes, uint32_t n_nodes, const rt_tria
     b->n_tris = n_tris;
     b->n_verts = n_verts;
     b->has_prim = false;
+    b->trace_ww = prefer_while_while(leaf_tris, n_leaves);
     if (int e = make_traversal_layout(b, st)) { return bail(e); }
     *out = b;
     return RT_OK;
@@ -405,6 +409,25 @@ int rt_load_bvh(const char* path, rt_bvh** out)
     int e = rt_bvh_from_arrays(nodes.data(), hdr[1], tris.data(), hdr[2], verts.data(), hdr[3], out);
     if (e) { return e; }
     std::fprintf(stdout, "BVH loaded: %s  (%u nodes, %u tris, %u verts)\n", path, hdr[1], hdr[2], hdr[3]);
+    return RT_OK;
+}
+
+int rt_bvh_trace_loop(rt_bvh* b, int form)
+{
+    if (!b) { return fail(RT_E_NOT_LOADED, "BVH not loaded"); }
+    if (form < -1 || form > 1) { return fail(RT_E_INVALID, "form must be -1, 0 or 1"); }
+    if (form == -1)
+    {
+        uint32_t leaves = b->stats[4];
+        if (leaves == 0)  // a loaded tree: count its leaves
+        {
+            std::vector<rt_bvh_node> nodes(b->n_nodes);
+            RT_CUDA(cudaMemcpy(nodes.data(), b->nodes.p, nodes.size() * sizeof(rt_bvh_node), cudaMemcpyDeviceToHost));
+            for (const rt_bvh_node& nd : nodes) { leaves += nd.is_leaf ? 1u : 0u; }
+        }
+        b->trace_ww = prefer_while_while(b->n_tris, leaves);
+    }
+    else { b->trace_ww = form == 1; }
     return RT_OK;
 }
 

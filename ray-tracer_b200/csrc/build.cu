@@ -952,6 +952,7 @@ int build_typed(rt_bvh* B, const rt_vertex* d_verts, uint32_t V, const rt_triang
     }
     B->stats[4] = res[1] + sah.leaves;
     B->stats[3] = B->n_nodes - B->stats[4];
+    B->trace_ww = prefer_while_while(B->n_tris, B->stats[4]);
     return RT_OK;
 }
 

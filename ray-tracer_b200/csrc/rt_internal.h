@@ -136,6 +136,7 @@ struct rt_bvh
     rtb::DevBuf  scene_info, scene_roots;
     std::vector<uint32_t> scene_info_host;
     uint32_t     depth = 0;                 // tree depth (computed on demand; 0 = unknown)
+    bool         trace_ww = true;           // traversal loop form: while-while for large leaves
     uint32_t     stats[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     BuildScratch s;
     rtb::DevBuf  trace_status, trace_rays, trace_hits;
@@ -156,6 +157,10 @@ struct rt_bvh
 
 namespace rtb
 {
+// The traversal loop form for a tree with n_tris triangles in n_leaves leaves: the
+// while-while loop pays off when leaves hold 6 or more triangles on average.
+inline bool prefer_while_while(uint64_t n_tris, uint64_t n_leaves) { return n_tris >= 6 * n_leaves; }
+
 // Records the boundary event of stage `i` (0 = build start) when profiling is on.
 inline void prof_mark(rt_bvh* b, int i, cudaStream_t st)
 {

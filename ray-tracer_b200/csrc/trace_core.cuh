@@ -93,6 +93,7 @@ struct TraceCtx
     const rt_triangle* tris;
     const rt_vertex*   verts;
     const TraceRoot*   root;  // device record written by the layout kernel
+    uint32_t           ww;    // 1: while-while loop (leaves of 6 or more triangles on average)
 };
 
 struct THit
@@ -102,13 +103,13 @@ struct THit
     bool     hit, overflow;
 };
 
-// Closest hit (MODE bit 0 clear) or first accepted hit (bit 0 set); bit 1 selects the
-// watertight triangle test. Reproduces the reference's visiting order exactly. STK entries of
-// stack: the loop holds at most one entry per level of the tree plus one, so a stack deeper
-// than the tree never overflows (overflow is reported, never silent). R: the subtree to trace.
-template <int MODE, int STK = STACK>
-__device__ __forceinline__ THit trace_ray(const TraceCtx& T, const TraceRoot& R, rtd::f3 o, rtd::f3 d, float tmin,
-                                          float tmax)
+// The one-loop form of the reference's traverse() (bvh_traverse.cpp:91-178): pop a node,
+// re-test its entry distance against the best t, then test a leaf's triangles or push both
+// children, farther first. Used for trees with small leaves, where the while-while form's
+// meeting points cost more than they save.
+template <int MODE, int STK>
+__device__ __forceinline__ THit trace_ray_oneloop(const TraceCtx& T, const TraceRoot& R, rtd::f3 o, rtd::f3 d, float tmin,
+                                                  float tmax)
 {
     using namespace rtd;
     uint32_t sref[STK], scnt[STK];
@@ -175,6 +176,106 @@ __device__ __forceinline__ THit trace_ray(const TraceCtx& T, const TraceRoot& R,
     }
     H.t = best;
     return H;
+}
+
+// The while-while form (Aila & Laine, HPG 2009): an inner loop walks inner nodes
+// until the current node is a leaf, then the leaf's triangles are tested; lanes of a warp meet
+// after each phase, so they test leaves together instead of interleaving leaf and inner-node
+// steps. The node the reference would pop next after pushing both children -- the nearer one --
+// is kept in registers instead of being pushed and popped; a stack entry is one 16-byte record
+// {reference, count, entry distance}. The visiting order, the pop-time test "entry distance >=
+// best t" and the points where a 64-entry stack would overflow (the held node counts as its
+// stack entry) are those of the one-loop form of the reference's traverse().
+template <int MODE, int STK>
+__device__ __forceinline__ THit trace_ray_ww(const TraceCtx& T, const TraceRoot& R, rtd::f3 o, rtd::f3 d, float tmin,
+                                             float tmax)
+{
+    using namespace rtd;
+    uint4 stk[STK];
+    const f3 inv = mk3(1.f / d.x, 1.f / d.y, 1.f / d.z);
+    THit H;
+    H.t = tmax; H.u = 0.f; H.v = 0.f; H.tri = 0; H.hit = false; H.overflow = false;
+    float best = tmax;
+    int top = 0;
+    uint32_t cref = R.ref, ccnt = R.cnt;
+    const float troot = ray_box(o, inv, tmin, best, R.box[0], R.box[1], R.box[2], R.box[3], R.box[4], R.box[5]);
+    bool have = troot < best;
+    uint32_t pops = 0;
+    // the next stack entry whose entry distance is below best, or none
+    auto pop = [&]() {
+        have = false;
+        while (top > 0)
+        {
+            // A validated BVH is a DAG with children after parents; the cap only bounds the work
+            // a malformed one could cause.
+            if (++pops > MAX_POPS) { H.overflow = true; top = 0; break; }
+            const uint4 e = stk[--top];
+            if (__uint_as_float(e.z) < best) { cref = e.x; ccnt = e.y; have = true; break; }
+        }
+    };
+    while (have)
+    {
+        // inner nodes
+        while (have && !(ccnt & LEAF_BIT))
+        {
+            if (++pops > MAX_POPS) { H.overflow = true; have = false; break; }
+            const rt_gnode* g = T.gn + cref;
+            const float4 a = __ldg(&g->a), b = __ldg(&g->b), c = __ldg(&g->c);
+            const uint4 dd = __ldg(&g->d);
+            const float tl = ray_box(o, inv, tmin, best, a.x, a.y, a.z, a.w, b.x, b.y);
+            const float tr = ray_box(o, inv, tmin, best, b.z, b.w, c.x, c.y, c.z, c.w);
+            // the farther child waits on the stack, the nearer one is next; left first on ties
+            uint32_t fr, fc, nr, nc;
+            float ft, nt;
+            if (tl <= tr) { fr = dd.y; fc = dd.w; ft = tr; nr = dd.x; nc = dd.z; nt = tl; }
+            else { fr = dd.x; fc = dd.z; ft = tl; nr = dd.y; nc = dd.w; nt = tr; }
+            if (nt < best)  // (the farther child is hit only if the nearer one is)
+            {
+                if (ft < best)
+                {
+                    if (top >= STK) { H.overflow = true; have = false; break; }
+                    stk[top++] = make_uint4(fr, fc, __float_as_uint(ft), 0u);
+                }
+                if (top >= STK) { H.overflow = true; have = false; break; }
+                cref = nr; ccnt = nc;
+            }
+            else { pop(); }
+        }
+        if (!have) { break; }
+        // a leaf: its triangles in order, strict "t < best" (bvh_traverse.cpp:112-142)
+        const uint32_t cnt = ccnt & ~LEAF_BIT;
+        bool done = false;
+        for (uint32_t k = 0; k < cnt; k++)
+        {
+            const uint32_t ti = cref + k;
+            const float4 p0 = __ldg(&T.tp[3 * ti]), p1 = __ldg(&T.tp[3 * ti + 1]), p2 = __ldg(&T.tp[3 * ti + 2]);
+            const f3 v0 = mk3(p0.x, p0.y, p0.z), v1 = mk3(p0.w, p1.x, p1.y), v2 = mk3(p1.z, p1.w, p2.x);
+            float t, u, v;
+            const bool acc = (MODE & 2) ? ray_tri_watertight(o, d, tmin, tmax, v0, v1, v2, t, u, v)
+                                        : ray_tri(o, d, tmin, tmax, v0, v1, v2, t, u, v);
+            if (acc && t < best)
+            {
+                best = t; H.u = u; H.v = v; H.tri = ti; H.hit = true;
+                if (MODE & 1) { done = true; break; }
+            }
+        }
+        if (done) { break; }
+        pop();
+    }
+    H.t = best;
+    return H;
+}
+
+// Closest hit (MODE bit 0 clear) or first accepted hit (bit 0 set); bit 1 selects the
+// watertight triangle test. Reproduces the reference's visiting order exactly, in either loop
+// form (T.ww picks one per tree; both visit the same nodes in the same order). STK entries of
+// stack: the loop holds at most one entry per level of the tree plus one, so a stack deeper
+// than the tree never overflows (overflow is reported, never silent). R: the subtree to trace.
+template <int MODE, int STK = STACK>
+__device__ __forceinline__ THit trace_ray(const TraceCtx& T, const TraceRoot& R, rtd::f3 o, rtd::f3 d, float tmin,
+                                          float tmax)
+{
+    return T.ww ? trace_ray_ww<MODE, STK>(T, R, o, d, tmin, tmax) : trace_ray_oneloop<MODE, STK>(T, R, o, d, tmin, tmax);
 }
 
 // The whole tree (the handle's root record).

@@ -218,6 +218,7 @@ TraceCtx make_trace_ctx(const rt_bvh* B)
     T.tris = B->tris.as<rt_triangle>();
     T.verts = B->verts.as<rt_vertex>();
     T.root = B->rootbuf.as<TraceRoot>();
+    T.ww = B->trace_ww ? 1u : 0u;
     return T;
 }
 

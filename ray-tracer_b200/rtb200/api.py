@@ -103,6 +103,7 @@ def lib():
         L.rt_bvh_profile.argtypes = [vp, i32]
         L.rt_bvh_stage_ms.argtypes = [vp, vp]
         L.rt_trace.argtypes = [vp, vp, vp, u64, u32, vp]
+        L.rt_bvh_trace_loop.argtypes = [vp, i32]
         L.rt_trace_host.argtypes = [vp, vp, vp, u64, u32]
         L.rt_render.argtypes = [vp, vp, vp, u32, vp, i32, vp, vp, vp]
         L.rt_render_ex.argtypes = [vp, vp, vp, i32, vp, vp, vp]
@@ -337,6 +338,10 @@ class Bvh:
 
     def write(self, path: str):
         _check(lib().rt_write_bvh(self.h, path.encode()))
+
+    def trace_loop(self, form: int = -1):
+        """Traversal loop form: 0 one-loop, 1 while-while, -1 the default choice by leaf size."""
+        _check(lib().rt_bvh_trace_loop(self.h, int(form)))
 
     # -- tracing -----------------------------------------------------------------------
     def trace(self, rays, flags: int = TRACE_CLOSEST, stream=None):

@@ -39,14 +39,18 @@ def compare(hits, ref, tag):
 @pytest.mark.parametrize("preset", ["hybrid", "lbvh30", "sah4"])
 @pytest.mark.parametrize("scene", ["soup20k", "ico4", "cornell_ico", "big_small", "test_traverse", "identical100"])
 @pytest.mark.parametrize("flags", [rtb200.TRACE_CLOSEST, rtb200.TRACE_ANY_HIT])
-def test_trace_matches_oracle(orc, scene, preset, flags):
+@pytest.mark.parametrize("loop", [0, 1])
+def test_trace_matches_oracle(orc, scene, preset, flags, loop):
+    """Both traversal loop forms (one-loop, while-while) against the oracle: the any-hit mode
+    returns the first accepted triangle, so it checks the visiting order itself."""
     v, t = SCENES[scene]
     b = rtb200.Bvh.build(v, t, preset)
+    b.trace_loop(loop)
     nodes, tris, verts = b.download()
     rays = rays_for(v, 40000, seed=7)
     hits = b.trace(rays, flags)
     ref = orc.trace(Baked(nodes, tris, verts), rays, flags=flags, threads=8)
-    compare(hits, ref, f"{scene}/{preset}/{flags}")
+    compare(hits, ref, f"{scene}/{preset}/{flags}/loop{loop}")
 
 
 def test_trace_device_tensors(orc):
