@@ -270,29 +270,37 @@ def run_ours(a):
     peak, peak_kind = measured_peak_hbm()
     traffic_per_key = profiled_traffic()
 
-    # end to end through the C ABI with host buffers: H2D of the geometry, the bake, D2H of the
-    # baked .bvh arrays, every step (pinned host memory; host-synchronous calls)
+    # end to end through the C ABI with host buffers: every step uploads its geometry from pinned
+    # host memory (rt_rebuild with RT_HOST), bakes it and downloads the baked .bvh arrays into
+    # pinned host memory. Two handles on two streams alternate, so one step's download overlaps
+    # the next step's upload and bake (rt_bvh_download_async); the timed region ends after the
+    # last download has landed.
     hv = torch.from_numpy(verts).pin_memory()
     ht = torch.from_numpy(tris.view(np.int32)).pin_memory()
-    hn = torch.empty(nn * 48, dtype=torch.uint8).pin_memory()
-    htr = torch.empty(nt * 12, dtype=torch.uint8).pin_memory()
-    hvo = torch.empty(verts.nbytes, dtype=torch.uint8).pin_memory()
     L = rtb200.lib()
     import ctypes as C
+    handles = [bvh, rtb200.Bvh.build(dv, dt, cfg)]
+    streams = [torch.cuda.Stream(device=dev), torch.cuda.Stream(device=dev)]
+    outs = [(torch.empty(nn * 48, dtype=torch.uint8).pin_memory(), torch.empty(nt * 12, dtype=torch.uint8).pin_memory(),
+             torch.empty(verts.nbytes, dtype=torch.uint8).pin_memory()) for _ in range(2)]
 
-    def e2e_step():
-        bvh.rebuild(hv.numpy(), ht.numpy().view(np.uint32), cfg)
-        rtb200.api._check(L.rt_bvh_download(bvh.h, C.c_void_p(hn.data_ptr()), C.c_void_p(htr.data_ptr()),
-                                            C.c_void_p(hvo.data_ptr())))
-    for _ in range(2):
-        e2e_step()
+    def e2e_step(i):
+        b, s_, (hn, htr, hvo) = handles[i % 2], streams[i % 2], outs[i % 2]
+        b.rebuild(hv.numpy(), ht.numpy().view(np.uint32), cfg, stream=s_)
+        rtb200.api._check(L.rt_bvh_download_async(b.h, C.c_void_p(hn.data_ptr()), C.c_void_p(htr.data_ptr()),
+                                                  C.c_void_p(hvo.data_ptr()), C.c_void_p(s_.cuda_stream)))
+    for i in range(2):
+        e2e_step(i)
     torch.cuda.synchronize()
-    k_e2e = max(3, a.steps // 2)
+    k_e2e = max(4, a.steps // 2)
     t0 = time.perf_counter()
-    for _ in range(k_e2e):
-        e2e_step()
+    for i in range(k_e2e):
+        e2e_step(i)
     torch.cuda.synchronize()
-    e2e_s = max_over_ranks((time.perf_counter() - t0) / k_e2e, dist, dev)
+    e2e_wall = time.perf_counter() - t0
+    last_nodes = handles[(k_e2e - 1) % 2].download()[0]  # the pipelined copies hold the bake
+    assert np.array_equal(outs[(k_e2e - 1) % 2][0].numpy(), last_nodes.view(np.uint8)), "e2e download mismatch"
+    e2e_s = max_over_ranks(e2e_wall / k_e2e, dist, dev)
     e2e_value = world * n / e2e_s / 1e6
     h2d = verts.nbytes + tris.nbytes
     d2h = nn * 48 + nt * 12 + verts.nbytes

@@ -109,6 +109,12 @@ int rt_bvh_from_arrays(const rt_bvh_node* nodes, uint32_t n_nodes, const rt_tria
 int rt_bvh_counts(const rt_bvh* bvh, uint32_t* counts3);
 /* Copies the baked arrays to host memory in the .bvh layout; any pointer may be NULL. */
 int rt_bvh_download(const rt_bvh* bvh, rt_bvh_node* nodes, rt_triangle* tris, rt_vertex* verts);
+/* The same copies queued on `stream` without waiting (no counterpart in the reference): a
+ * caller baking a sequence of meshes downloads one bake while the next one uploads and builds
+ * on another stream (PCIe moves both directions at once). Host buffers should be pinned; they
+ * are written when the stream reaches the copies, so synchronise the stream before reading
+ * them, and order any rebuild of the handle after the copies (same stream, or a sync). */
+int rt_bvh_download_async(const rt_bvh* bvh, rt_bvh_node* nodes, rt_triangle* tris, rt_vertex* verts, void* stream);
 /* Original triangle index of each baked triangle (n = triangle count); host or device out. */
 int rt_bvh_prim_ids(const rt_bvh* bvh, uint32_t* out, int where);
 /* stats8: spatial splits taken, spatial splits refused for capacity, SAH roots,

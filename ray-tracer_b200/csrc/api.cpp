@@ -449,6 +449,16 @@ int rt_bvh_download(const rt_bvh* b, rt_bvh_node* nodes, rt_triangle* tris, rt_v
     return RT_OK;
 }
 
+int rt_bvh_download_async(const rt_bvh* b, rt_bvh_node* nodes, rt_triangle* tris, rt_vertex* verts, void* stream)
+{
+    if (!b) { return fail(RT_E_INVALID, "null handle"); }
+    cudaStream_t st = pick(stream);
+    if (nodes) { RT_CUDA(cudaMemcpyAsync(nodes, b->nodes.p, (size_t)b->n_nodes * 48, cudaMemcpyDeviceToHost, st)); }
+    if (tris && b->n_tris) { RT_CUDA(cudaMemcpyAsync(tris, b->tris.p, (size_t)b->n_tris * 12, cudaMemcpyDeviceToHost, st)); }
+    if (verts && b->n_verts) { RT_CUDA(cudaMemcpyAsync(verts, b->verts.p, (size_t)b->n_verts * 24, cudaMemcpyDeviceToHost, st)); }
+    return RT_OK;
+}
+
 int rt_bvh_prim_ids(const rt_bvh* b, uint32_t* out, int where)
 {
     if (!b || !out) { return fail(RT_E_INVALID, "null argument"); }

@@ -97,6 +97,7 @@ def lib():
         L.rt_bvh_from_arrays.argtypes = [vp, u32, vp, u32, vp, u32, vp]
         L.rt_bvh_counts.argtypes = [vp, vp]
         L.rt_bvh_download.argtypes = [vp, vp, vp, vp]
+        L.rt_bvh_download_async.argtypes = [vp, vp, vp, vp, vp]
         L.rt_bvh_prim_ids.argtypes = [vp, vp, i32]
         L.rt_bvh_stats.argtypes = [vp, vp]
         L.rt_bvh_free.argtypes = [vp]

@@ -115,3 +115,24 @@ def test_sort_tile_shapes_agree(orc):
     pid = b.prim_ids()
     # leaves of the LBVH presets hold sorted runs: the baked order is the stable Morton order
     assert np.array_equal(pid, perm)
+
+
+def test_download_async_on_a_stream(orc):
+    """rt_bvh_download_async: the .bvh arrays land in pinned host memory once the stream has
+    reached the copies, equal to the synchronous download."""
+    import ctypes as C
+    import torch
+    v, t = SCENES["soup20k"]
+    b = rtb200.Bvh.build(v, t, "lbvh63")
+    nn, nt, nv = b.counts()
+    s = torch.cuda.Stream()
+    hn = torch.empty(nn * 48, dtype=torch.uint8).pin_memory()
+    ht = torch.empty(nt * 12, dtype=torch.uint8).pin_memory()
+    hv = torch.empty(nv * 24, dtype=torch.uint8).pin_memory()
+    assert rtb200.lib().rt_bvh_download_async(b.h, C.c_void_p(hn.data_ptr()), C.c_void_p(ht.data_ptr()),
+                                              C.c_void_p(hv.data_ptr()), C.c_void_p(s.cuda_stream)) == 0
+    s.synchronize()
+    nodes, tris, verts = b.download()
+    assert np.array_equal(hn.numpy(), nodes.view(np.uint8))
+    assert np.array_equal(ht.numpy(), tris.view(np.uint8).reshape(-1))
+    assert np.array_equal(hv.numpy(), verts.view(np.uint8).reshape(-1))
