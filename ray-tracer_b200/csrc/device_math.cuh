@@ -110,6 +110,27 @@ RT_HD bool box_valid(const box3& b) { return b.mn[0] <= b.mx[0] && b.mn[1] <= b.
 // the empty box. At most 9 polygon vertices are live; 12 slots as in the reference.
 RT_HD box3 clip_triangle(f3 v0, f3 v1, f3 v2, const box3& region)
 {
+    // All three vertices inside the region: no plane removes or adds a vertex, so the clipped
+    // polygon is the triangle and its box the vertices' box (the loop below would return the
+    // same values).
+    {
+        bool inside = true;
+        const f3 vs[3] = { v0, v1, v2 };
+        for (int i = 0; i < 3; i++)
+        {
+            for (int axis = 0; axis < 3; axis++)
+            {
+                const float c = get3(vs[i], axis);
+                inside = inside && (c >= region.mn[axis]) && (c <= region.mx[axis]);
+            }
+        }
+        if (inside)
+        {
+            box3 r = box_empty();
+            box_pt(r, v0); box_pt(r, v1); box_pt(r, v2);
+            return r;
+        }
+    }
     f3 poly[12], tmp[12];
     int n = 3;
     poly[0] = v0; poly[1] = v1; poly[2] = v2;
