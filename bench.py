@@ -345,7 +345,7 @@ def secondary(a, bvh, dv, dt, verts, stream, dev, flush):
     import torch
     import rtb200
     from rtb200 import scenes
-    n = dv.shape[0]
+    n = dt.shape[0]  # triangles (dv holds three vertices per soup triangle)
     res = {}
 
     def timed(fn, reps):
