@@ -115,7 +115,7 @@ static void free_bvh(rt_bvh* b)
                        &b->s.sah_roots, &b->s.sah_refs_a, &b->s.sah_refs_b, &b->s.sah_tmp, &b->s.sah_pos,
                        &b->s.sah_lvl_a, &b->s.sah_lvl_b, &b->s.sah_dec, &b->s.sah_out, &b->s.sah_leaf_refs,
                        &b->s.sah_scan_in, &b->s.sah_scan_out, &b->s.sah_node_ids, &b->s.sah_roots_lvl,
-                       &b->s.in_verts, &b->s.in_tris, &b->s.gtris, &b->s.batch_off, &b->s.sah_budget, &b->s.sah_wide, &b->scene_info, &b->scene_roots,
+                       &b->s.in_verts, &b->s.in_tris, &b->s.gtris, &b->s.batch_off, &b->s.sah_budget, &b->s.sah_wide, &b->s.sah_tmp2, &b->s.sah_pos2, &b->scene_info, &b->scene_roots,
                        &b->wf_cams };
     for (DevBuf* x : bufs) { x->release(); }
     b->rootbuf.release();

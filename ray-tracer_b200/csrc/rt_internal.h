@@ -121,6 +121,7 @@ struct BuildScratch
     rtb::DevBuf batch_off;          // batched build: triangle and vertex offsets per scene
     rtb::DevBuf sah_budget;         // spatial-split budget per scene: used, cap
     rtb::DevBuf sah_wide;           // SAH nodes evaluated by many blocks: bins, list, block offsets
+    rtb::DevBuf sah_tmp2, sah_pos2; // their partitions' second buffer and satisfying-right positions
 };
 
 struct rt_bvh

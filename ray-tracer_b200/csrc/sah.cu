@@ -679,6 +679,9 @@ struct WideAcc
     Best     B;
     int      o_axis, o_bin;
     float    o_cmin, o_scale;
+    // the partitions (k_wp_*): per pass the satisfied count and the swapped pairs; child boxes
+    uint32_t pm[3], ftot[3];
+    SBox     cb[2];
 };
 
 // The wide nodes of a level in level order (wl) with their first block (wco, exclusive prefix
@@ -736,6 +739,7 @@ __global__ void __launch_bounds__(SBLK) k_wide_init(WideAcc* __restrict__ acc)
         sbox_clear(A.obox[j / SAH_MAX_BINS][j % SAH_MAX_BINS]);
         sbox_clear(A.sbox[j / SAH_MAX_BINS][j % SAH_MAX_BINS]);
     }
+    if (threadIdx.x < 2) { sbox_clear(A.cb[threadIdx.x]); }
 }
 
 __device__ __forceinline__ void chunk_range(uint32_t n, uint32_t c, uint32_t& b, uint32_t& e)
@@ -1268,6 +1272,292 @@ k_sah_split(const LvlNode* __restrict__ lv, const uint32_t* __restrict__ refs, c
     }
 }
 
+// ---- the wide path's partitions: the reference's std::partition (Hoare's scheme, see
+// cta_partition) over many blocks. Pass 0 splits a spatial node's references by "box max <=
+// plane" (R -> T), pass 1 the rest by "box min < plane" (T -> T2, the left part copied), pass 2
+// an object split by "centroid bin < split bin" (R or T2 -> the next level's list). Per pass:
+// flags and satisfied counts; per chunk the failing elements left of the split point and the
+// satisfying ones right of it; their ranks from the chunk prefixes; the scatter, where the
+// k-th failing element from the left and the k-th satisfying one from the right trade places.
+// Each block owns WIDE_CH consecutive references, 16 per thread.
+struct WideSplit
+{
+    const LvlNode*  lv;
+    const Dec*      dec;
+    const uint32_t* wl;
+    const uint32_t* wco;
+    uint32_t        nw;
+    WideAcc*        acc;
+    const uint32_t* refs;       // this level's references
+    uint32_t*       tmp;        // T
+    uint32_t*       tmp2;       // T2
+    uint32_t*       posf;       // failing-left positions, ascending
+    uint32_t*       poss;       // satisfying-right positions, ascending
+    uint8_t*        flags;
+    uint32_t*       chunk;      // per block: failing-left, satisfying-right counts
+    uint32_t*       refs_next;  // next level's references
+    const uint32_t* ref_off;    // next-level offset per level node
+    const uint32_t* child_slot;
+    const uint32_t* leaf_off;
+    uint32_t*       leaf_refs;
+    LvlNode*        lv_next;
+    OutNode*        out;
+    uint32_t        out_base, leaf_base;
+};
+
+__device__ __forceinline__ bool wp_applies(int pass, const Dec& d)
+{
+    return pass < 2 ? (d.pre_spatial || d.kind == K_SPATIAL) : d.kind == K_OBJECT;
+}
+__device__ __forceinline__ bool wp_pred(int pass, const Dec& d, const Ctx& C, uint32_t t)
+{
+    if (pass == 0) { return tri_hi(C, t, d.sp_axis) <= d.plane; }
+    if (pass == 1) { return tri_lo(C, t, d.sp_axis) < d.plane; }
+    return obj_bin(centroid(C, t, d.axis), d.cmin, d.scale, d.nb) < d.bin;
+}
+__device__ __forceinline__ const uint32_t* wp_in(int pass, const WideSplit& W, const LvlNode& nd, const Dec& d)
+{
+    if (pass == 0) { return W.refs + nd.ref_off; }
+    if (pass == 1) { return W.tmp + nd.ref_off; }
+    return (d.pre_spatial ? W.tmp2 : W.refs) + nd.ref_off;
+}
+
+// block and thread ranges of chunk c: the block's [c0, c1), this thread's [t0, t1)
+struct WpItem
+{
+    uint32_t k, g, node, c0, c1, t0, t1, n;
+};
+__device__ __forceinline__ WpItem wp_item(const WideSplit& W)
+{
+    WpItem it;
+    uint32_t c;
+    it.k = wide_item(W.wco, W.nw, blockIdx.x, c);
+    it.g = blockIdx.x;
+    it.node = W.wl[it.k];
+    it.n = W.lv[it.node].count;
+    it.c0 = c * WIDE_CH;
+    it.c1 = min(it.n, it.c0 + WIDE_CH);
+    it.t0 = min(it.c1, it.c0 + threadIdx.x * 16u);
+    it.t1 = min(it.c1, it.t0 + 16u);
+    return it;
+}
+
+template <int PASS>
+__global__ void __launch_bounds__(SBLK) k_wp_flags(WideSplit W, Ctx C)
+{
+    __shared__ uint32_t sh[SBLK / 32 + 1];
+    const WpItem it = wp_item(W);
+    const Dec d = W.dec[it.node];
+    if (!wp_applies(PASS, d)) { return; }
+    const LvlNode nd = W.lv[it.node];
+    WideAcc& A = W.acc[it.k];
+    const uint32_t b0 = PASS == 1 ? A.pm[0] : 0u;
+    const uint32_t* in = wp_in(PASS, W, nd, d);
+    uint8_t* F = W.flags + nd.ref_off;
+    uint32_t cnt = 0;
+    for (uint32_t i = max(it.t0, b0); i < it.t1; i++)
+    {
+        const uint8_t f = wp_pred(PASS, d, C, in[i]) ? 1 : 0;
+        F[i] = f;
+        cnt += f;
+    }
+    cnt = block_sum<SBLK>(cnt, sh);
+    if (threadIdx.x == 0 && cnt) { atomicAdd(&A.pm[PASS], cnt); }
+}
+
+template <int PASS>
+__global__ void __launch_bounds__(SBLK) k_wp_sides(WideSplit W)
+{
+    __shared__ uint32_t sh[SBLK / 32 + 1];
+    const WpItem it = wp_item(W);
+    const Dec d = W.dec[it.node];
+    if (!wp_applies(PASS, d)) { return; }
+    const LvlNode nd = W.lv[it.node];
+    WideAcc& A = W.acc[it.k];
+    const uint32_t b0 = PASS == 1 ? A.pm[0] : 0u;
+    const uint32_t m = b0 + A.pm[PASS];  // the split point
+    const uint8_t* F = W.flags + nd.ref_off;
+    uint32_t fl = 0, sr = 0;
+    for (uint32_t i = max(it.t0, b0); i < it.t1; i++)
+    {
+        if (i < m) { fl += F[i] ? 0u : 1u; } else { sr += F[i]; }
+    }
+    fl = block_sum<SBLK>(fl, sh);
+    sr = block_sum<SBLK>(sr, sh);
+    if (threadIdx.x == 0)
+    {
+        W.chunk[2 * it.g] = fl;
+        W.chunk[2 * it.g + 1] = sr;
+        if (fl) { atomicAdd(&A.ftot[PASS], fl); }
+    }
+}
+
+// Ranks of this thread's failing-left / satisfying-right elements: the counts of the node's
+// earlier chunks plus the block's exclusive scan.
+template <int PASS>
+__device__ __forceinline__ void wp_ranks(const WideSplit& W, const WpItem& it, const uint8_t* F, uint32_t b0, uint32_t m,
+                                         uint32_t* sh, uint32_t& rf, uint32_t& rs)
+{
+    const uint32_t g0 = W.wco[it.k];
+    uint32_t pf = 0, ps = 0;
+    for (uint32_t g = g0 + threadIdx.x; g < it.g; g += SBLK) { pf += W.chunk[2 * g]; ps += W.chunk[2 * g + 1]; }
+    pf = block_sum<SBLK>(pf, sh);
+    ps = block_sum<SBLK>(ps, sh);
+    uint32_t fl = 0, sr = 0;
+    for (uint32_t i = max(it.t0, b0); i < it.t1; i++)
+    {
+        if (i < m) { fl += F[i] ? 0u : 1u; } else { sr += F[i]; }
+    }
+    rf = pf + block_excl_scan<SBLK>(fl, sh, nullptr);
+    rs = ps + block_excl_scan<SBLK>(sr, sh, nullptr);
+}
+
+template <int PASS>
+__global__ void __launch_bounds__(SBLK) k_wp_pos(WideSplit W)
+{
+    __shared__ uint32_t sh[SBLK / 32 + 1];
+    const WpItem it = wp_item(W);
+    const Dec d = W.dec[it.node];
+    if (!wp_applies(PASS, d)) { return; }
+    const LvlNode nd = W.lv[it.node];
+    const WideAcc& A = W.acc[it.k];
+    const uint32_t b0 = PASS == 1 ? A.pm[0] : 0u;
+    const uint32_t m = b0 + A.pm[PASS];
+    const uint8_t* F = W.flags + nd.ref_off;
+    uint32_t rf, rs;
+    wp_ranks<PASS>(W, it, F, b0, m, sh, rf, rs);
+    uint32_t* PF = W.posf + nd.ref_off;
+    uint32_t* PS = W.poss + nd.ref_off;
+    for (uint32_t i = max(it.t0, b0); i < it.t1; i++)
+    {
+        if (i < m) { if (!F[i]) { PF[rf++] = i; } }
+        else if (F[i]) { PS[rs++] = i; }
+    }
+}
+
+template <int PASS>
+__global__ void __launch_bounds__(SBLK) k_wp_scatter(WideSplit W)
+{
+    __shared__ uint32_t sh[SBLK / 32 + 1];
+    const WpItem it = wp_item(W);
+    const Dec d = W.dec[it.node];
+    if (!wp_applies(PASS, d)) { return; }
+    const LvlNode nd = W.lv[it.node];
+    const WideAcc& A = W.acc[it.k];
+    const uint32_t b0 = PASS == 1 ? A.pm[0] : 0u;
+    const uint32_t m = b0 + A.pm[PASS];
+    const uint32_t tot = A.ftot[PASS];
+    const uint8_t* F = W.flags + nd.ref_off;
+    uint32_t rf, rs;
+    wp_ranks<PASS>(W, it, F, b0, m, sh, rf, rs);
+    const uint32_t* in = wp_in(PASS, W, nd, d);
+    uint32_t* out = PASS == 0 ? W.tmp + nd.ref_off : (PASS == 1 ? W.tmp2 + nd.ref_off : W.refs_next + W.ref_off[it.node]);
+    const uint32_t* PF = W.posf + nd.ref_off;
+    const uint32_t* PS = W.poss + nd.ref_off;
+    if (PASS == 1)
+    {
+        for (uint32_t i = it.t0; i < min(it.t1, b0); i++) { out[i] = in[i]; }  // the left part, unchanged
+    }
+    for (uint32_t i = max(it.t0, b0); i < it.t1; i++)
+    {
+        uint32_t src = i;
+        if (i < m) { if (!F[i]) { src = PS[tot - 1u - rf]; rf++; } }
+        else if (F[i]) { src = PF[tot - 1u - rs]; rs++; }
+        out[i] = in[src];
+    }
+}
+
+// the node's references in their final places (leaf store, or the children's lists) and the
+// children's boxes (computeRangeAABB for object splits, clipped triangles for spatial ones)
+__global__ void __launch_bounds__(SBLK) k_wp_place(WideSplit W, Ctx C)
+{
+    const WpItem it = wp_item(W);
+    const Dec d = W.dec[it.node];
+    const LvlNode nd = W.lv[it.node];
+    WideAcc& A = W.acc[it.k];
+    const uint32_t n = it.n;
+    const uint32_t* Wr = (d.pre_spatial || d.kind == K_SPATIAL ? W.tmp2 : W.refs) + nd.ref_off;
+    if (d.kind == K_LEAF)
+    {
+        const uint32_t lo = W.leaf_base + W.leaf_off[it.node];
+        for (uint32_t i = it.t0; i < it.t1; i++) { W.leaf_refs[lo + i] = Wr[i]; }
+        return;
+    }
+    uint32_t* Q = W.refs_next + W.ref_off[it.node];
+    OBox ob[2];
+    obox_clear(ob[0]); obox_clear(ob[1]);
+    if (d.kind == K_OBJECT)
+    {
+        const uint32_t m = A.pm[2];
+        for (uint32_t i = it.t0; i < it.t1; i++) { obox_add(ob[i < m ? 0 : 1], tri_box(C, Q[i])); }
+    }
+    else
+    {
+        const uint32_t le = A.pm[0], se = le + A.pm[1];
+        const uint32_t st = se - le, rc = n - se, lsz = le + st, tot = n + st;
+        box3 nbox;
+        for (int k = 0; k < 3; k++) { nbox.mn[k] = nd.box[k]; nbox.mx[k] = nd.box[3 + k]; }
+        box3 lclip = nbox, rclip = nbox;
+        lclip.mx[d.axis] = d.plane;
+        rclip.mn[d.axis] = d.plane;
+        // this block's destination slots: [c0, c1) and the duplicates' [n + c0, n + c1)
+        for (int part = 0; part < 2; part++)
+        {
+            const uint32_t j0 = part ? n + it.t0 : it.t0, j1 = part ? min(n + it.t1, tot) : it.t1;
+            for (uint32_t j = j0; j < j1; j++)
+            {
+                const uint32_t src = j < lsz ? j : (j < lsz + rc ? se + (j - lsz) : le + (j - lsz - rc));
+                const uint32_t t = Wr[src];
+                Q[j] = t;
+                f3 v0, v1, v2;
+                tri_verts(C, t, v0, v1, v2);
+                const box3 cl = clip_triangle(v0, v1, v2, j < lsz ? lclip : rclip);
+                if (box_valid(cl)) { obox_add(ob[j < lsz ? 0 : 1], cl); }
+            }
+        }
+    }
+    obox_flush_warp(ob[0], A.cb[0]);
+    obox_flush_warp(ob[1], A.cb[1]);
+}
+
+// the children's records (the tail of k_sah_split), one thread per wide node
+__global__ void k_wp_final(WideSplit W)
+{
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= W.nw) { return; }
+    const uint32_t ni = W.wl[k];
+    const LvlNode nd = W.lv[ni];
+    const Dec d = W.dec[ni];
+    const WideAcc& A = W.acc[k];
+    const uint32_t n = nd.count;
+    OutNode* o = &W.out[nd.out];
+    if (d.kind == K_LEAF)
+    {
+        o->is_leaf = 1; o->a = W.leaf_base + W.leaf_off[ni]; o->b = n;
+        return;
+    }
+    uint32_t lsz, rsz;
+    if (d.kind == K_OBJECT) { lsz = A.pm[2]; rsz = n - lsz; }
+    else
+    {
+        const uint32_t st = A.pm[1], rc = n - A.pm[0] - A.pm[1];
+        lsz = A.pm[0] + st;
+        rsz = rc + st;
+    }
+    const uint32_t slot = W.child_slot[ni];
+    const uint32_t roff = W.ref_off[ni];
+    const uint32_t lid = W.out_base + slot, rid = lid + 1;
+    const box3 lb = sbox_result(A.cb[0]), rb = sbox_result(A.cb[1]);
+    LvlNode L, Rn;
+    set_node(L, roff, lsz, lid, nd.root, nd.root_first, lb);
+    set_node(Rn, roff + lsz, rsz, rid, nd.root, nd.root_first, rb);
+    W.lv_next[slot] = L;
+    W.lv_next[slot + 1] = Rn;
+    set_out_child(W.out[lid], lb, nd.root);
+    set_out_child(W.out[rid], rb, nd.root);
+    o->is_leaf = 0; o->a = lid; o->b = rid;
+}
+
 // Copies the Morton-sorted triangles of new subtree roots into the level's reference list.
 __global__ void __launch_bounds__(SBLK)
 k_sah_root_refs(const SahRoot* __restrict__ roots, const uint32_t* __restrict__ new_off, const uint32_t* __restrict__ perm,
@@ -1426,10 +1716,16 @@ int sah_build(rt_bvh* B, const rt_build_cfg& cfg, const SahInput& in, cudaStream
     RT_CUDA(cudaMemcpyAsync(io, io_h, 64, cudaMemcpyHostToDevice, st));
     // wide-node scratch: at most cap / WIDE_MIN nodes of a level have more than WIDE_MIN references
     const uint32_t max_wide = cap / WIDE_MIN + 2;
-    if (S.sah_wide.ensure((size_t)max_wide * sizeof(WideAcc) + (size_t)(2 * max_wide + 2) * 4)) { return RT_E_CUDA; }
+    const uint32_t max_chunks = cap / WIDE_CH + max_wide + 1;
+    if (S.sah_wide.ensure((size_t)max_wide * sizeof(WideAcc) + (size_t)(2 * max_wide + 2) * 4 + (size_t)max_chunks * 8) ||
+        S.sah_tmp2.ensure((size_t)cap * 4) || S.sah_pos2.ensure((size_t)cap * 4))
+    {
+        return RT_E_CUDA;
+    }
     WideAcc* wacc = S.sah_wide.as<WideAcc>();
     uint32_t* wl = reinterpret_cast<uint32_t*>(wacc + max_wide);
     uint32_t* wco = wl + max_wide;
+    uint32_t* wchunk = wco + max_wide + 2;
     uint32_t next_bound = 0;  // upper bound of the largest node of the coming level
     const uint32_t n_budget = (uint32_t)in.budget_used.size();
     if (n_budget == 0 || n_budget > MAX_BUDGET_SCENES || in.budget_cap.size() != n_budget)
@@ -1542,11 +1838,28 @@ int sah_build(rt_bvh* B, const rt_build_cfg& cfg, const SahInput& in, cudaStream
         count_launch();
         if (nw > 0)
         {
-            k_sah_split<1024><<<nw, 1024, 0, st>>>(lv_cur, refs_cur, S.sah_dec.as<Dec>(), child_slot, ref_offs, leaf_offs, C,
-                                                   S.sah_tmp.as<uint32_t>(), S.sah_pos.as<uint32_t>(),
-                                                   S.sah_scan_in.as<uint8_t>(), lv_next, refs_next, out, out_total,
-                                                   leaf_total, S.sah_leaf_refs.as<uint32_t>(), wl);
-            count_launch();
+            WideSplit W;
+            W.lv = lv_cur; W.dec = S.sah_dec.as<Dec>(); W.wl = wl; W.wco = wco; W.nw = nw; W.acc = wacc;
+            W.refs = refs_cur; W.tmp = S.sah_tmp.as<uint32_t>(); W.tmp2 = S.sah_tmp2.as<uint32_t>();
+            W.posf = S.sah_pos.as<uint32_t>(); W.poss = S.sah_pos2.as<uint32_t>(); W.flags = S.sah_scan_in.as<uint8_t>();
+            W.chunk = wchunk; W.refs_next = refs_next; W.ref_off = ref_offs; W.child_slot = child_slot;
+            W.leaf_off = leaf_offs; W.leaf_refs = S.sah_leaf_refs.as<uint32_t>(); W.lv_next = lv_next; W.out = out;
+            W.out_base = out_total; W.leaf_base = leaf_total;
+            k_wp_flags<0><<<nch, SBLK, 0, st>>>(W, C);
+            k_wp_sides<0><<<nch, SBLK, 0, st>>>(W);
+            k_wp_pos<0><<<nch, SBLK, 0, st>>>(W);
+            k_wp_scatter<0><<<nch, SBLK, 0, st>>>(W);
+            k_wp_flags<1><<<nch, SBLK, 0, st>>>(W, C);
+            k_wp_sides<1><<<nch, SBLK, 0, st>>>(W);
+            k_wp_pos<1><<<nch, SBLK, 0, st>>>(W);
+            k_wp_scatter<1><<<nch, SBLK, 0, st>>>(W);
+            k_wp_flags<2><<<nch, SBLK, 0, st>>>(W, C);
+            k_wp_sides<2><<<nch, SBLK, 0, st>>>(W);
+            k_wp_pos<2><<<nch, SBLK, 0, st>>>(W);
+            k_wp_scatter<2><<<nch, SBLK, 0, st>>>(W);
+            k_wp_place<<<nch, SBLK, 0, st>>>(W, C);
+            k_wp_final<<<(nw + 31) / 32, 32, 0, st>>>(W);
+            count_launch(14);
         }
         next_bound = io_h[10];
         if (int e = check_launch("sah split")) { return e; }
