@@ -9,7 +9,7 @@ Mtri/s over all ranks (weak scaling: every rank bakes its own soup; no data-path
 
 Also reported: the same build end to end through the C ABI with host buffers (e2e), the other
 build presets, closest-hit / any-hit traversal of 16,777,216 incoherent rays and of 1920x1080
-pinhole rays (Mray/s), the roofline of the dominant kernel (the radix-sort pass), the
+pinhole rays (Mray/s), the roofline of the bake (all its launches as one unit), the
 reference's own CPU bake timed on this host, and under "render" the path-loop workloads:
 plain path tracing (256x256, 16 spp, depth 4, Cornell box + 20,480-triangle icosphere + two
 spheres; plain vs wavefront, and the CPU restatement on all host cores), the batched workload
@@ -40,7 +40,16 @@ N_TRIS = 1 << 20
 N_RAYS = 1 << 24
 METRIC = "BVH Mtri/s"
 WORKLOAD = "BVH build microbenchmark: 1,048,576-triangle soup, LBVH 63-bit Morton codes, leaf 16"
-SORT_BYTES_PER_KEY = (20 + 7 * 24) / 8.0  # per onesweep pass: 8 B key + 4 B value in/out (first pass: no value read)
+# Algorithmic bytes of one LBVH 63-bit bake per triangle (V = 3N vertices; each array counted
+# once per read and once per write, per kernel): clear 30, vertex renormalisation 144, triangle
+# prep 84, Morton codes 20, radix tree with boxes 100, boundary 40, scans 24, .bvh nodes and
+# triangles 93, traversal layout 158; plus the sort: 44 up to 2^21 keys (top-digit onesweep
+# pass 20 + per-bucket pass 24), else 188 (eight onesweep passes).
+BAKE_BYTES_PER_TRI_EXCL_SORT = 30 + 144 + 84 + 20 + 100 + 40 + 24 + 93 + 158
+
+
+def bake_bytes_per_tri(n: int) -> int:
+    return BAKE_BYTES_PER_TRI_EXCL_SORT + (44 if n <= (1 << 21) else 188)
 
 
 def parse_args():
@@ -119,11 +128,12 @@ def measured_peak_hbm():
 
 
 def profiled_traffic():
-    """DRAM bytes per onesweep launch per key from the committed ncu summary, if present."""
-    path = os.path.join(HERE, "profiles", "onesweep_soup1m_traffic.txt")
+    """DRAM bytes per triangle of one 1M-triangle LBVH bake (all its launches) from the
+    committed ncu summary, if present."""
+    path = os.path.join(HERE, "profiles", "lbvh_bake_soup1m_traffic.md")
     try:
         for line in open(path):
-            if line.startswith("dram_bytes_per_key_per_launch"):
+            if line.startswith("dram_bytes_per_tri_per_bake"):
                 return float(line.split("=")[1])
     except Exception:
         pass
@@ -262,13 +272,12 @@ def run_ours(a):
     st = {k: statistics.mean(s[k] for s in stages) for k in stages[0]}
     nn, nt, _ = bvh.counts()
 
-    # roofline of the dominant kernel: the onesweep radix-sort pass (8 launches per step)
-    passes = (3 * cfg.morton_bits + 7) // 8
-    sort_launch_ms = st["sort"] / passes
-    alg_bytes = SORT_BYTES_PER_KEY * n
-    achieved = alg_bytes / (sort_launch_ms * 1e-3) / 1e9
+    # roofline of the bake as one unit (no single kernel dominates it: the largest takes about
+    # 15 % of the step): algorithmic bytes per bake over the device time per bake
+    alg_bytes = bake_bytes_per_tri(n) * n
+    achieved = alg_bytes / (ms_step * 1e-3) / 1e9
     peak, peak_kind = measured_peak_hbm()
-    traffic_per_key = profiled_traffic()
+    traffic_per_tri = profiled_traffic() if n == N_TRIS and a.preset == "lbvh63" else None
 
     # end to end through the C ABI with host buffers: every step uploads its geometry from pinned
     # host memory (rt_rebuild with RT_HOST), bakes it and downloads the baked .bvh arrays into
@@ -324,10 +333,11 @@ def run_ours(a):
                        "d2h_bytes_per_step": int(d2h)},
                "gpu_launches": int(launches),
                "stage_ms": {k: round(v, 4) for k, v in st.items()},
-               "roofline": {"bound": "hbm", "kernel": "k_onesweep (radix sort pass)", "achieved": round(achieved, 1),
-                            "peak": peak, "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4),
-                            "traffic": (round(traffic_per_key * n) if traffic_per_key else None),
-                            "algorithmic_bytes_per_launch": int(alg_bytes), "launch_ms": round(sort_launch_ms, 5)},
+               "roofline": {"bound": "hbm", "kernel": f"LBVH bake, all {launches // a.steps} launches of one rebuild",
+                            "achieved": round(achieved, 1), "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
+                            "frac": round(achieved / peak, 4),
+                            "traffic": (round(traffic_per_tri * n) if traffic_per_tri else None),
+                            "algorithmic_bytes_per_launch": int(alg_bytes), "launch_ms": round(ms_step, 5)},
                "cpu_baseline": {"value": round(cpu_v, 4), "unit": "Mtri/s", "cores": 1, "kind": cpu_kind,
                                 "sample": "bvh::bakeBVH of a 131,072-triangle soup of the same generator, LBVH "
                                           "constants, 2 timed repetitions, 1 thread (the bake is single-threaded)"},

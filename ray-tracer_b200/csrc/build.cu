@@ -217,18 +217,20 @@ k_tri_prep(const rt_triangle* __restrict__ tris, uint32_t N, const rt_vertex* __
     }
 }
 
-// Morton code per triangle (input order) and the 8-bit digit histograms of all sort passes.
+// Morton code per triangle (input order) and the 8-bit digit histograms of all sort passes
+// (hist[256 p + d], digit d of bits 8p .. 8p+7); with msd_shift >= 0 also the histogram of
+// bits msd_shift .. msd_shift+7 (the key's top digit) in hist[8 * 256 + d].
 template <typename K, bool BATCH = false>
 __global__ void __launch_bounds__(BLK)
 k_morton(const float4* __restrict__ lo, const float4* __restrict__ hi, const float* __restrict__ cz, uint32_t N,
          const uint32_t* __restrict__ scene, uint32_t bits, int passes, K* __restrict__ keys, uint32_t* __restrict__ hist,
-         Batch bt = Batch{ 0u, nullptr, nullptr, 63u, nullptr })
+         int msd_shift = -1, Batch bt = Batch{ 0u, nullptr, nullptr, 63u, nullptr })
 {
     // grid-stride: the block histograms are flushed to global memory once per block, so the
     // launch uses a few blocks per SM rather than one block per 256 triangles
-    __shared__ uint32_t h[8 * 256];
+    __shared__ uint32_t h[9 * 256];
     __shared__ uint32_t soff[BATCH ? MAX_BATCH_SCENES + 1 : 1];
-    for (int t = threadIdx.x; t < passes * 256; t += BLK) { h[t] = 0u; }
+    for (int t = threadIdx.x; t < 9 * 256; t += BLK) { h[t] = 0u; }
     if (BATCH)
     {
         for (uint32_t k = threadIdx.x; k <= bt.S; k += BLK) { soff[k] = bt.toff[k]; }
@@ -262,11 +264,13 @@ k_morton(const float4* __restrict__ lo, const float4* __restrict__ hi, const flo
         if (BATCH) { code |= (uint64_t)sc << bt.sshift; }
         keys[i] = (K)code;
         for (int p = 0; p < passes; p++) { atomicAdd(&h[p * 256 + (uint32_t)((code >> (8 * p)) & 255u)], 1u); }
+        if (msd_shift >= 0) { atomicAdd(&h[8 * 256 + (uint32_t)((code >> msd_shift) & 255u)], 1u); }
     }
     __syncthreads();
-    for (int t = threadIdx.x; t < passes * 256; t += BLK)
+    for (int t = threadIdx.x; t < 9 * 256; t += BLK)
     {
-        if (h[t]) { atomicAdd(&hist[t], h[t]); }
+        const bool used = t < passes * 256 || (msd_shift >= 0 && t >= 8 * 256);  // hist may hold 8 x 256 words only
+        if (used && h[t]) { atomicAdd(&hist[t], h[t]); }
     }
 }
 
@@ -732,7 +736,7 @@ k_clear(uint32_t n, uint32_t* __restrict__ parent, unsigned long long* __restric
     if (blockIdx.x == 0)
     {
         const int t = threadIdx.x;
-        for (int k = t; k < 8 * 256; k += BLK) { hist[k] = 0u; }
+        for (int k = t; k < 9 * 256; k += BLK) { hist[k] = 0u; }
         if (t < 16) { counters[t] = 0u; }
         if (t == 0) { *status = 0u; }
     }
@@ -748,9 +752,10 @@ int build_typed(rt_bvh* B, const rt_vertex* d_verts, uint32_t V, const rt_triang
     const int key_bits = batch ? (int)bt.sshift + (int)scene_bits(bt.S) : 3 * (int)cfg.morton_bits;
     const uint32_t sshift = batch ? bt.sshift : 63u;
     const int passes = sort_passes(key_bits);
+    const int msd_shift = key_bits > 8 ? key_bits - 8 : -1;  // top digit, for the sort's MSD path
     const uint32_t nk = 2 * N - 1;  // Karras nodes
     if (S.tri_lo.ensure((size_t)N * 16) || S.tri_hi.ensure((size_t)N * 16) || S.tri_cz.ensure((size_t)N * 4) ||
-        S.keys.ensure((size_t)N * sizeof(K)) || S.vals.ensure((size_t)N * 4) || S.hist.ensure(8 * 256 * 4) ||
+        S.keys.ensure((size_t)N * sizeof(K)) || S.vals.ensure((size_t)N * 4) || S.hist.ensure(9 * 256 * 4) ||
         S.scene.ensure((size_t)n_boxes * 24 + 64) || S.status.ensure(64) || S.counters.ensure(64) ||
         (batch && (S.gtris.ensure((size_t)N * sizeof(rt_triangle)) || B->scene_info.ensure((size_t)bt.S * 16) ||
                    B->scene_roots.ensure((size_t)bt.S * 32))) ||
@@ -781,7 +786,7 @@ int build_typed(rt_bvh* B, const rt_vertex* d_verts, uint32_t V, const rt_triang
         d_tris = S.gtris.as<rt_triangle>();  // vertex indices of the concatenated array from here on
         k_morton<K, true><<<morton_blocks, BLK, 0, st>>>(S.tri_lo.as<float4>(), S.tri_hi.as<float4>(), S.tri_cz.as<float>(),
                                                          N, S.scene.as<uint32_t>(), cfg.morton_bits, passes,
-                                                         S.keys.as<K>(), S.hist.as<uint32_t>(), bt);
+                                                         S.keys.as<K>(), S.hist.as<uint32_t>(), msd_shift, bt);
     }
     else
     {
@@ -790,7 +795,7 @@ int build_typed(rt_bvh* B, const rt_vertex* d_verts, uint32_t V, const rt_triang
                                                           nullptr);
         k_morton<K><<<morton_blocks, BLK, 0, st>>>(S.tri_lo.as<float4>(), S.tri_hi.as<float4>(), S.tri_cz.as<float>(), N,
                                                    S.scene.as<uint32_t>(), cfg.morton_bits, passes, S.keys.as<K>(),
-                                                   S.hist.as<uint32_t>());
+                                                   S.hist.as<uint32_t>(), msd_shift);
     }
     count_launch(2);
     if (int e = check_launch("morton")) { return e; }
@@ -799,7 +804,8 @@ int build_typed(rt_bvh* B, const rt_vertex* d_verts, uint32_t V, const rt_triang
     K* skeys = nullptr;
     uint32_t* perm = nullptr;
     if (int e = radix_sort_pairs<K>(S.keys.as<K>(), S.vals.as<uint32_t>(), true, N, key_bits, S.hist.as<uint32_t>(),
-                                    S.sort, status, st, &skeys, &perm))
+                                    msd_shift >= 0 ? S.hist.as<uint32_t>() + 8 * 256 : nullptr, S.sort, status, st,
+                                    &skeys, &perm))
     {
         return e;
     }

@@ -60,12 +60,34 @@ __device__ __forceinline__ uint32_t block_excl_scan_256(uint32_t v, uint32_t* wa
     return r;
 }
 
+// Lanes of the warp holding the same 8-bit digit as this one (d = 0xffffffff: no key; such
+// lanes match only each other): the set __match_any_sync returns, built from one ballot per
+// digit bit plus one for the key's presence. The per-bucket sort below ranks with it (faster
+// there than the match instruction; the onesweep passes keep the instruction, which is faster
+// for them at 16M keys).
+__device__ __forceinline__ uint32_t match_digit8(uint32_t d)
+{
+    const bool valid = d != 0xffffffffu;
+    const uint32_t vm = __ballot_sync(0xffffffffu, valid);
+    uint32_t m = valid ? vm : ~vm;
+#pragma unroll
+    for (int b = 0; b < 8; b++)
+    {
+        const bool bit = (d >> b) & 1u;
+        const uint32_t bm = __ballot_sync(0xffffffffu, bit);
+        m &= bit ? bm : ~bm;
+    }
+    return m;
+}
+
 template <typename K, int RS_IPT, int MINB>
 __global__ void __launch_bounds__(RS_BLOCK, MINB)
 k_onesweep(const K* __restrict__ kin, const uint32_t* __restrict__ vin, int vals_identity, K* __restrict__ kout,
            uint32_t* __restrict__ vout, uint32_t n, uint32_t tiles, int shift, const uint32_t* __restrict__ hist,
-           uint32_t* __restrict__ tile_counter, uint32_t* __restrict__ lookback, uint32_t* __restrict__ status)
+           uint32_t* __restrict__ tile_counter, uint32_t* __restrict__ lookback, uint32_t* __restrict__ status,
+           const uint32_t* __restrict__ skip, uint32_t skip_if)
 {
+    if (skip && *skip == skip_if) { return; }  // the other sort path runs (radix_sort_pairs)
     constexpr int RS_TILE = RS_BLOCK * RS_IPT;
     extern __shared__ __align__(16) unsigned char smem[];
     K*        sk     = reinterpret_cast<K*>(smem);
@@ -215,11 +237,12 @@ constexpr size_t onesweep_smem()
     return (size_t)RS_BLOCK * IPT * sizeof(K) + (size_t)RS_BLOCK * IPT * 4 + (size_t)RS_WARPS * 256 * 4 + 2 * 256 * 4;
 }
 
-// All passes of one tile shape on the given scratch.
+// All passes of one tile shape on the given scratch. skip (device, optional): the passes do
+// nothing when *skip == skip_if (the MSD path of radix_sort_pairs sorted the keys instead).
 template <typename K, int IPT, int MINB>
 int onesweep_passes(K* keys, uint32_t* vals, bool vals_identity, uint32_t n, int passes, const uint32_t* hist, K* keys_alt,
                     uint32_t* vals_alt, uint32_t* lookback, uint32_t* tile_counters, uint32_t* status, cudaStream_t st,
-                    K** keys_out, uint32_t** vals_out)
+                    K** keys_out, uint32_t** vals_out, const uint32_t* skip = nullptr, uint32_t skip_if = 0)
 {
     constexpr uint32_t tile = RS_BLOCK * IPT;
     const uint32_t tiles = (n + tile - 1) / tile;
@@ -240,7 +263,7 @@ int onesweep_passes(K* keys, uint32_t* vals, bool vals_identity, uint32_t n, int
     {
         k_onesweep<K, IPT, MINB><<<tiles, RS_BLOCK, smem, st>>>(kin, vin, (vals_identity && p == 0) ? 1 : 0, kalt, valt, n,
                                                                 tiles, 8 * p, hist + 256 * p, tile_counters + p,
-                                                                lookback + (size_t)p * tiles * 256, status);
+                                                                lookback + (size_t)p * tiles * 256, status, skip, skip_if);
         count_launch();
         if (int e = check_launch("onesweep")) { return e; }
         K* tk = kin; kin = kalt; kalt = tk;
@@ -249,6 +272,172 @@ int onesweep_passes(K* keys, uint32_t* vals, bool vals_identity, uint32_t n, int
     *keys_out = kin;
     *vals_out = vin;
     return RT_OK;
+}
+
+// ---- MSD path: one onesweep pass on the most significant digit, then every bucket of that
+// digit sorted by the lower digits inside one block's shared memory. Used when no bucket holds
+// more keys than one block takes (decided on the device from the top digit's histogram, which
+// the key producer already built); otherwise those kernels return at once and the LSD passes
+// run. Both paths are stable and give the same order.
+// Per-bucket block shapes: LB threads x LI keys (capacity LB * LI keys per bucket).
+constexpr int LS_SMALL_B = 256, LS_SMALL_I = 18;  // 4,608 keys, two blocks per SM
+constexpr int LS_LARGE_B = 512, LS_LARGE_I = 16;  // 8,192 keys, one block per SM
+
+// bstart[d] = first position of top digit d (exclusive scan of its histogram), bstart[256] = n;
+// *flag = 1 when a bucket exceeds cap (the LSD passes must run), else 0.
+__global__ void __launch_bounds__(256)
+k_msd_check(const uint32_t* __restrict__ hist_top, uint32_t n, uint32_t cap, uint32_t* __restrict__ bstart,
+            uint32_t* __restrict__ flag)
+{
+    __shared__ uint32_t ws[RS_WARPS];
+    __shared__ uint32_t s_big;
+    const uint32_t h = hist_top[threadIdx.x];
+    if (threadIdx.x == 0) { s_big = 0u; }
+    __syncthreads();
+    if (h > cap) { atomicOr(&s_big, 1u); }
+    const uint32_t ex = block_excl_scan_256(h, ws, nullptr);
+    bstart[threadIdx.x] = ex;
+    if (threadIdx.x == 0) { bstart[256] = n; *flag = s_big; }
+}
+
+template <typename K, int LB, int LI>
+constexpr size_t local_sort_smem()
+{
+    return (size_t)LB * LI * sizeof(K) + (size_t)LB * LI * 4 + (size_t)(LB / 32) * 256 * 4 + 256 * 4;
+}
+
+// One block per bucket of the top digit: keys[bstart[b], bstart[b+1]) sorted stably by the
+// digits below the top one (npass 8-bit passes, ranked as in k_onesweep), kin/vin -> kout/vout
+// (may be the same buffers: the block holds its bucket in registers and shared memory before
+// writing).
+template <typename K, int LB, int LI, int MINB>
+__global__ void __launch_bounds__(LB, MINB)
+k_local_sort(const K* kin, const uint32_t* vin, K* kout, uint32_t* vout, const uint32_t* __restrict__ bstart,
+             const uint32_t* __restrict__ flag, int npass)
+{
+    constexpr uint32_t CAP = (uint32_t)LB * LI;
+    if (*flag) { return; }
+    extern __shared__ __align__(16) unsigned char smem[];
+    K*        sk     = reinterpret_cast<K*>(smem);
+    uint32_t* sv     = reinterpret_cast<uint32_t*>(sk + CAP);
+    uint32_t* whist  = sv + CAP;                 // [warp][digit]
+    uint32_t* tstart = whist + (LB / 32) * 256;  // block-local digit start
+    __shared__ uint32_t s_warp_sums[8];
+    const uint32_t b0 = bstart[blockIdx.x], m = bstart[blockIdx.x + 1] - b0;
+    if (m == 0) { return; }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int nw = (int)((m + 32u * LI - 1) / (32u * LI));  // warps holding keys
+    // element (warp, j, lane) = warp * 32 * LI + j * 32 + lane, so that order is input order
+    K        key[LI];
+    uint32_t val[LI];
+#pragma unroll
+    for (int j = 0; j < LI; j++)
+    {
+        const uint32_t e = (uint32_t)warp * (32u * LI) + (uint32_t)j * 32u + (uint32_t)lane;
+        if (e < m) { key[j] = kin[b0 + e]; val[j] = vin[b0 + e]; } else { key[j] = 0; val[j] = 0; }
+    }
+    const uint32_t lt = (1u << lane) - 1u;
+    for (int p = 0; p < npass; p++)
+    {
+        const int shift = 8 * p;
+        for (int i = threadIdx.x; i < nw * 256; i += LB) { whist[i] = 0u; }
+        __syncthreads();
+        uint32_t* wh = whist + warp * 256;
+        uint32_t dig[LI], off[LI];
+#pragma unroll
+        for (int j = 0; j < LI; j++) { dig[j] = 0xffffffffu; }
+        if (warp < nw)  // warps wholly past the bucket's end have nothing to rank
+        {
+#pragma unroll
+            for (int j = 0; j < LI; j++)
+            {
+                const uint32_t e = (uint32_t)warp * (32u * LI) + (uint32_t)j * 32u + (uint32_t)lane;
+                const bool valid = e < m;
+                const uint32_t d = valid ? (uint32_t)(key[j] >> shift) & 255u : 0xffffffffu;
+                dig[j] = d;
+                const uint32_t peers = match_digit8(d);
+                const uint32_t before = __popc(peers & lt);
+                uint32_t cnt = valid ? wh[d] : 0u;
+                __syncwarp();
+                if (valid && before == 0u) { wh[d] = cnt + __popc(peers); }
+                __syncwarp();
+                off[j] = cnt + before;
+            }
+        }
+        __syncthreads();
+        // per digit (threads 0..255): warps' exclusive offsets and the digit's total
+        uint32_t total = 0u;
+        if (threadIdx.x < 256)
+        {
+            for (int w = 0; w < nw; w++)
+            {
+                const uint32_t c = whist[w * 256 + threadIdx.x];
+                whist[w * 256 + threadIdx.x] = total;
+                total += c;
+            }
+        }
+        __syncthreads();
+        // exclusive scan of the 256 digit totals (warps 0..7 hold them; the others scan zeros)
+        uint32_t x = total;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1)
+        {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) { x += y; }
+        }
+        if (lane == 31 && warp < 8) { s_warp_sums[warp] = x; }
+        __syncthreads();
+        if (warp == 0)
+        {
+            uint32_t w = lane < 8 ? s_warp_sums[lane] : 0u;
+#pragma unroll
+            for (int o = 1; o < 8; o <<= 1)
+            {
+                const uint32_t y = __shfl_up_sync(0xffffffffu, w, o);
+                if (lane >= o) { w += y; }
+            }
+            if (lane < 8) { s_warp_sums[lane] = w; }
+        }
+        __syncthreads();
+        if (threadIdx.x < 256) { tstart[threadIdx.x] = (warp > 0 ? s_warp_sums[warp - 1] : 0u) + x - total; }
+        __syncthreads();
+#pragma unroll
+        for (int j = 0; j < LI; j++)
+        {
+            if (dig[j] != 0xffffffffu)
+            {
+                const uint32_t pos = tstart[dig[j]] + whist[warp * 256 + dig[j]] + off[j];
+                sk[pos] = key[j];
+                sv[pos] = val[j];
+            }
+        }
+        __syncthreads();
+        if (p + 1 < npass)
+        {
+#pragma unroll
+            for (int j = 0; j < LI; j++)
+            {
+                const uint32_t e = (uint32_t)warp * (32u * LI) + (uint32_t)j * 32u + (uint32_t)lane;
+                if (e < m) { key[j] = sk[e]; val[j] = sv[e]; }
+            }
+            __syncthreads();
+        }
+    }
+    if (npass == 0)  // nothing below the top digit: the bucket as it is
+    {
+#pragma unroll
+        for (int j = 0; j < LI; j++)
+        {
+            const uint32_t e = (uint32_t)warp * (32u * LI) + (uint32_t)j * 32u + (uint32_t)lane;
+            if (e < m) { sk[e] = key[j]; sv[e] = val[j]; }
+        }
+        __syncthreads();
+    }
+    for (uint32_t i = threadIdx.x; i < m; i += LB)
+    {
+        kout[b0 + i] = sk[i];
+        vout[b0 + i] = sv[i];
+    }
 }
 
 } // namespace
@@ -262,7 +451,8 @@ size_t sort_lookback_words(uint32_t n, int passes)
 
 template <typename K>
 int radix_sort_pairs(K* keys, uint32_t* vals, bool vals_identity, uint32_t n, int key_bits, const uint32_t* hist,
-                     SortScratch& s, uint32_t* status, cudaStream_t st, K** keys_out, uint32_t** vals_out)
+                     const uint32_t* msd_hist, SortScratch& s, uint32_t* status, cudaStream_t st, K** keys_out,
+                     uint32_t** vals_out)
 {
     *keys_out = keys;
     *vals_out = vals;
@@ -270,25 +460,75 @@ int radix_sort_pairs(K* keys, uint32_t* vals, bool vals_identity, uint32_t n, in
     if (n > LB_VAL) { return fail(RT_E_CAPACITY, "radix sort: more than 2^30 keys"); }
     const int passes = sort_passes(key_bits);
     const size_t lbw = sort_lookback_words(n, passes);
+    // tile_counters: 64 pass counters, then the MSD path's 257 bucket starts and its flag
     if (s.keys_alt.ensure((size_t)n * sizeof(K)) || s.vals_alt.ensure((size_t)n * 4) || s.lookback.ensure(lbw * 4) ||
-        s.tile_counters.ensure(64 * 4))
+        s.tile_counters.ensure((64 + 260) * 4))
     {
         return RT_E_CUDA;
     }
     if (n <= RS_SMALL_MAX)
     {
+        // per-bucket shape: the smaller one while an even spread leaves it 8% headroom
+        constexpr uint32_t cap_small = (uint32_t)LS_SMALL_B * LS_SMALL_I, cap_large = (uint32_t)LS_LARGE_B * LS_LARGE_I;
+        const bool msd = msd_hist != nullptr && key_bits > 8 && n <= 256u * cap_large;
+        const bool small = (uint64_t)n * 108 <= (uint64_t)256 * cap_small * 100;
+        uint32_t* bstart = s.tile_counters.as<uint32_t>() + 64;
+        uint32_t* flag = bstart + 257;
+        if (msd)
+        {
+            // top digit (bits key_bits-8 .. key_bits-1) by one onesweep pass keys -> alt, then the
+            // buckets by the lower digits in shared memory, alt -> the buffer the LSD passes end in
+            constexpr uint32_t tile = RS_BLOCK * 16;
+            const uint32_t tiles = (n + tile - 1) / tile;
+            constexpr size_t smem = onesweep_smem<K, 16>();
+            constexpr size_t sm_small = local_sort_smem<K, LS_SMALL_B, LS_SMALL_I>();
+            constexpr size_t sm_large = local_sort_smem<K, LS_LARGE_B, LS_LARGE_I>();
+            static bool attr_set = false;  // per key type
+            if (!attr_set)
+            {
+                RT_CUDA(cudaFuncSetAttribute(k_onesweep<K, 16, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+                RT_CUDA(cudaFuncSetAttribute(k_local_sort<K, LS_SMALL_B, LS_SMALL_I, 2>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_small));
+                RT_CUDA(cudaFuncSetAttribute(k_local_sort<K, LS_LARGE_B, LS_LARGE_I, 1>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_large));
+                attr_set = true;
+            }
+            K* kalt = s.keys_alt.as<K>();
+            uint32_t* valt = s.vals_alt.as<uint32_t>();
+            K* kfin = (passes & 1) ? kalt : keys;
+            uint32_t* vfin = (passes & 1) ? valt : vals;
+            const int npass = sort_passes(key_bits - 8);
+            RT_CUDA(cudaMemsetAsync(s.lookback.as<uint32_t>(), 0, (size_t)tiles * 256 * 4, st));
+            RT_CUDA(cudaMemsetAsync(s.tile_counters.as<uint32_t>() + 63, 0, 4, st));
+            k_msd_check<<<1, 256, 0, st>>>(msd_hist, n, small ? cap_small : cap_large, bstart, flag);
+            k_onesweep<K, 16, 2><<<tiles, RS_BLOCK, smem, st>>>(keys, vals, vals_identity ? 1 : 0, kalt, valt, n, tiles,
+                                                                key_bits - 8, msd_hist, s.tile_counters.as<uint32_t>() + 63,
+                                                                s.lookback.as<uint32_t>(), status, flag, 1u);
+            if (small)
+            {
+                k_local_sort<K, LS_SMALL_B, LS_SMALL_I, 2><<<256, LS_SMALL_B, sm_small, st>>>(kalt, valt, kfin, vfin, bstart,
+                                                                                           flag, npass);
+            }
+            else
+            {
+                k_local_sort<K, LS_LARGE_B, LS_LARGE_I, 1><<<256, LS_LARGE_B, sm_large, st>>>(kalt, valt, kfin, vfin, bstart,
+                                                                                           flag, npass);
+            }
+            count_launch(3);
+            RT_CUDA(cudaGetLastError());
+        }
         return onesweep_passes<K, 16, 2>(keys, vals, vals_identity, n, passes, hist, s.keys_alt.as<K>(), s.vals_alt.as<uint32_t>(),
                                          s.lookback.as<uint32_t>(), s.tile_counters.as<uint32_t>(), status, st, keys_out,
-                                         vals_out);
+                                         vals_out, msd ? flag : nullptr, 0u);
     }
     return onesweep_passes<K, 8, 5>(keys, vals, vals_identity, n, passes, hist, s.keys_alt.as<K>(), s.vals_alt.as<uint32_t>(),
                                     s.lookback.as<uint32_t>(), s.tile_counters.as<uint32_t>(), status, st, keys_out, vals_out);
 }
 
-template int radix_sort_pairs<uint64_t>(uint64_t*, uint32_t*, bool, uint32_t, int, const uint32_t*, SortScratch&,
-                                        uint32_t*, cudaStream_t, uint64_t**, uint32_t**);
-template int radix_sort_pairs<uint32_t>(uint32_t*, uint32_t*, bool, uint32_t, int, const uint32_t*, SortScratch&,
-                                        uint32_t*, cudaStream_t, uint32_t**, uint32_t**);
+template int radix_sort_pairs<uint64_t>(uint64_t*, uint32_t*, bool, uint32_t, int, const uint32_t*, const uint32_t*,
+                                        SortScratch&, uint32_t*, cudaStream_t, uint64_t**, uint32_t**);
+template int radix_sort_pairs<uint32_t>(uint32_t*, uint32_t*, bool, uint32_t, int, const uint32_t*, const uint32_t*,
+                                        SortScratch&, uint32_t*, cudaStream_t, uint32_t**, uint32_t**);
 
 } // namespace rtb
 

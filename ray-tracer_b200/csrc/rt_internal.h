@@ -64,10 +64,12 @@ struct SortScratch
 {
     DevBuf keys_alt, vals_alt, lookback, tile_counters;
 };
+// hist: the counts of every LSD digit (256 per pass); msd_hist (optional): the counts of the
+// key's top digit, bits key_bits-8 .. key_bits-1, which enables the MSD + per-bucket path.
 template <typename K>
 int radix_sort_pairs(K* keys, uint32_t* vals, bool vals_identity, uint32_t n, int key_bits,
-                     const uint32_t* hist, SortScratch& s, uint32_t* status, cudaStream_t st,
-                     K** keys_out, uint32_t** vals_out);
+                     const uint32_t* hist, const uint32_t* msd_hist, SortScratch& s, uint32_t* status,
+                     cudaStream_t st, K** keys_out, uint32_t** vals_out);
 // The same sort on caller-provided scratch; allocates nothing.
 template <typename K>
 int radix_sort_pairs_raw(K* keys, uint32_t* vals, uint32_t n, int key_bits, const uint32_t* hist, K* keys_alt,

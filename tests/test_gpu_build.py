@@ -117,6 +117,37 @@ def test_sort_tile_shapes_agree(orc):
     assert np.array_equal(pid, perm)
 
 
+def clustered_soup(n, seed):
+    """90% of the triangles inside 5% of the box: the top Morton digit's first bucket holds far
+    more than one block's worth of keys."""
+    v, t = scenes.soup(n, seed=seed)
+    v = v.copy()
+    v[: 3 * (9 * n // 10), :3] *= 0.05
+    return v, t
+
+
+@pytest.mark.parametrize("case", ["uniform1m", "uniform1500k", "uniform3k", "clustered200k"])
+@pytest.mark.parametrize("preset", ["lbvh63", "lbvh30"])
+def test_sort_msd_and_lsd_paths_agree(orc, case, preset):
+    """Uniform soups take the sort's MSD + per-bucket path (every top-digit bucket fits one
+    block: 4,608-key blocks up to about 1.09M keys, 8,192-key blocks above), the clustered one
+    its LSD passes; all give the oracle's stable Morton order."""
+    if case == "uniform1m":
+        v, t = scenes.soup(1_000_003, seed=81)
+    elif case == "uniform1500k":
+        v, t = scenes.soup(1_500_001, seed=84)
+    elif case == "uniform3k":
+        v, t = scenes.soup(3001, seed=82)
+    else:
+        v, t = clustered_soup(200_000, seed=83)
+    codes, perm, _ = orc.morton(v, t, orc_cfg(preset))
+    if case == "clustered200k":
+        top = np.asarray(codes, np.uint64) >> np.uint64(55 if preset == "lbvh63" else 22)  # bits key_bits-8 ..
+        assert np.bincount(top.astype(np.int64)).max() > 8192
+    pid = rtb200.Bvh.build(v, t, preset).prim_ids()
+    assert np.array_equal(pid, perm)
+
+
 def test_download_async_on_a_stream(orc):
     """rt_bvh_download_async: the .bvh arrays land in pinned host memory once the stream has
     reached the copies, equal to the synchronous download."""
