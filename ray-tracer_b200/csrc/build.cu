@@ -21,6 +21,7 @@
 //               (bvh_bake.cpp:75-149): a node's pre-order index is the number of nodes whose
 //               key range starts before its own plus its depth on its left spine, so every
 //               node finds its output slot from two prefix sums without a tree walk.
+#include <atomic>
 #include "rt_internal.h"
 #include "device_math.cuh"
 #include "cta_utils.cuh"
@@ -406,6 +407,14 @@ __device__ __forceinline__ bool split_lower(const K* __restrict__ keys, uint32_t
 constexpr int CL_T = 1024;
 constexpr unsigned long long CL_DONE = ~0ull - 1ull;
 
+// Shared memory of k_climb_local: exchange slots, boxes of the tile's inner nodes and leaves
+// (float4 pairs), and the tile's keys with one key of halo on either side.
+template <typename K>
+constexpr size_t climb_local_smem()
+{
+    return (size_t)CL_T * 8 + (size_t)4 * CL_T * 16 + (size_t)(CL_T + 2) * sizeof(K);
+}
+
 template <typename K>
 __global__ void __launch_bounds__(CL_T)
 k_climb_local(const K* __restrict__ keys, const uint32_t* __restrict__ perm, uint32_t n, const float4* __restrict__ lo,
@@ -413,22 +422,47 @@ k_climb_local(const K* __restrict__ keys, const uint32_t* __restrict__ perm, uin
               unsigned long long* __restrict__ other, float4* __restrict__ kbox, uint32_t* __restrict__ frontier,
               uint32_t* __restrict__ n_frontier, uint32_t* __restrict__ status)
 {
-    __shared__ unsigned long long s_other[CL_T];  // slot of split p at p - t0
-    __shared__ float4 s_box[2 * CL_T];            // box of inner node p at 2 (p - t0)
+    // the climb inside a tile touches only the tile's keys (and one on either side) and boxes of
+    // its own leaves and inner nodes: all are staged in shared memory first, so that the
+    // dependent chain of a climb does not wait on gathers from global memory
+    extern __shared__ __align__(16) unsigned char cl_smem[];
+    unsigned long long* s_other = reinterpret_cast<unsigned long long*>(cl_smem);  // slot of split p at p - t0
+    float4* s_box = reinterpret_cast<float4*>(s_other + CL_T);                     // inner node p at 2 (p - t0)
+    float4* s_leaf = s_box + 2 * CL_T;                                             // leaf k at 2 (k - t0)
+    K* s_key = reinterpret_cast<K*>(s_leaf + 2 * CL_T);                            // key t0 - 1 + i at i
     const uint32_t t0 = blockIdx.x * (uint32_t)CL_T;
     const uint32_t t1 = min(t0 + (uint32_t)CL_T, n);
-    for (int i = threadIdx.x; i < CL_T; i += CL_T) { s_other[i] = ~0ull; }
-    __syncthreads();
     const uint32_t k = t0 + threadIdx.x;
+    s_other[threadIdx.x] = ~0ull;
+    float4 mn = make_float4(0.f, 0.f, 0.f, 0.f), mx = mn;
+    if (k < n)
+    {
+        const uint32_t t = perm[k];
+        mn = lo[t];
+        mx = hi[t];
+        s_leaf[2 * threadIdx.x] = mn;
+        s_leaf[2 * threadIdx.x + 1] = mx;
+    }
+    for (uint32_t i = threadIdx.x; i < (uint32_t)CL_T + 2u; i += CL_T)
+    {
+        const uint32_t g = t0 + i;  // key g - 1
+        if (g >= 1 && g - 1 < n) { s_key[i] = keys[g - 1]; }
+    }
+    __syncthreads();
+    // split_lower on the staged keys: key j sits at s_key[j - t0 + 1]
+    auto lower = [&](uint32_t a, uint32_t b) -> bool {
+        const K xa = s_key[a - t0 + 1] ^ s_key[a - t0 + 2], xb = s_key[b - t0 + 1] ^ s_key[b - t0 + 2];
+        if (xa != xb) { return xa < xb; }
+        return (a ^ (a + 1)) < (b ^ (b + 1));
+    };
     if (k < n && n >= 2)
     {
         uint32_t L = k, R = k, id = n - 1 + k;
-        const uint32_t t = perm[k];
-        float4 mn = lo[t], mx = hi[t];
         for (uint32_t guard = 0;; guard++)
         {
             if (guard > MAX_DEPTH) { atomicOr(status, ST_CAPACITY); break; }
-            const bool go_right = (L == 0) || (R != n - 1 && split_lower<K>(keys, R, L - 1));
+            // L >= t0 and R < t1 here, so keys R, R + 1, L - 1 and L are staged
+            const bool go_right = (L == 0) || (R != n - 1 && lower(R, L - 1));
             const uint32_t p = go_right ? R : L - 1;
             parent[id] = p;
             if (p < t0 || p + 1 >= t1)
@@ -442,9 +476,9 @@ k_climb_local(const K* __restrict__ keys, const uint32_t* __restrict__ perm, uin
             if (prev == ~0ull) { break; }  // first arrival
             __threadfence_block();
             const uint32_t sid = (uint32_t)prev;
-            float4 smn, smx;
-            if (sid < n - 1) { smn = s_box[2 * (sid - t0)]; smx = s_box[2 * (sid - t0) + 1]; }  // completed in this block
-            else { const uint32_t st = perm[sid - (n - 1)]; smn = lo[st]; smx = hi[st]; }
+            // the sibling was completed or started in this block: its box is staged
+            const float4* sb = sid < n - 1 ? &s_box[2 * (sid - t0)] : &s_leaf[2 * (sid - (n - 1) - t0)];
+            const float4 smn = sb[0], smx = sb[1];
             if (go_right) { R = (uint32_t)(prev >> 32); } else { L = (uint32_t)(prev >> 32); }
             mn = make_float4(sse_min(mn.x, smn.x), sse_min(mn.y, smn.y), sse_min(mn.z, smn.z), 0.f);
             mx = make_float4(sse_max(mx.x, smx.x), sse_max(mx.y, smx.y), sse_max(mx.z, smx.z), 0.f);
@@ -814,7 +848,14 @@ int build_typed(rt_bvh* B, const rt_vertex* d_verts, uint32_t V, const rt_triang
     {
         // the frontier list lives in the rank array, which k_boundary fills only afterwards
         uint32_t* frontier = S.rank.as<uint32_t>();
-        k_climb_local<K><<<blocks_for(N, CL_T), CL_T, 0, st>>>(skeys, perm, N, S.tri_lo.as<float4>(), S.tri_hi.as<float4>(),
+        static std::atomic<bool> cl_attr{ false };  // per key type (bakes may run on several host threads)
+        if (!cl_attr)
+        {
+            RT_CUDA(cudaFuncSetAttribute(k_climb_local<K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)climb_local_smem<K>()));
+            cl_attr = true;
+        }
+        k_climb_local<K><<<blocks_for(N, CL_T), CL_T, climb_local_smem<K>(), st>>>(skeys, perm, N, S.tri_lo.as<float4>(), S.tri_hi.as<float4>(),
                                                                S.knode.as<uint4>(), S.parent.as<uint32_t>(),
                                                                S.visit.as<unsigned long long>(), S.kbox.as<float4>(),
                                                                frontier, counters + 8, status);

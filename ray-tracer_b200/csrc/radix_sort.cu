@@ -6,6 +6,7 @@
 //
 // This replaces the reference's serial 8-pass LSD sort (src/bvh/bvh_morton.cpp:109-159);
 // stability keeps equal Morton codes in ascending triangle order, as there.
+#include <atomic>
 #include "rt_internal.h"
 
 namespace rtb
@@ -249,7 +250,7 @@ int onesweep_passes(K* keys, uint32_t* vals, bool vals_identity, uint32_t n, int
     RT_CUDA(cudaMemsetAsync(lookback, 0, (size_t)passes * tiles * 256 * 4, st));
     RT_CUDA(cudaMemsetAsync(tile_counters, 0, 64 * 4, st));
     constexpr size_t smem = onesweep_smem<K, IPT>();
-    static bool attr_set = false;  // per instantiation
+    static std::atomic<bool> attr_set{ false };  // per instantiation (bakes may run on several host threads)
     if (!attr_set)
     {
         RT_CUDA(cudaFuncSetAttribute(k_onesweep<K, IPT, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -483,7 +484,7 @@ int radix_sort_pairs(K* keys, uint32_t* vals, bool vals_identity, uint32_t n, in
             constexpr size_t smem = onesweep_smem<K, 16>();
             constexpr size_t sm_small = local_sort_smem<K, LS_SMALL_B, LS_SMALL_I>();
             constexpr size_t sm_large = local_sort_smem<K, LS_LARGE_B, LS_LARGE_I>();
-            static bool attr_set = false;  // per key type
+            static std::atomic<bool> attr_set{ false };  // per key type
             if (!attr_set)
             {
                 RT_CUDA(cudaFuncSetAttribute(k_onesweep<K, 16, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
