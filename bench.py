@@ -239,7 +239,6 @@ def run_ours(a):
     dt = torch.from_numpy(tris.view(np.int32)).to(dev)
     cfg = rtb200.make_cfg(a.preset)
     bvh = rtb200.Bvh.build(dv, dt, cfg, stream=stream)
-    bvh.profile(True)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)  # 256 MiB > 126 MB L2
     for _ in range(max(a.warmup, 3)):
         bvh.rebuild(dv, dt, cfg, stream=stream)
@@ -251,7 +250,6 @@ def run_ours(a):
     clk.start()
     l0 = rtb200.kernel_launches()
     evs = []
-    stages = []
     for _ in range(a.steps):
         flush.zero_()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -259,7 +257,6 @@ def run_ours(a):
         bvh.rebuild(dv, dt, cfg, stream=stream)
         e1.record(stream)
         evs.append((e0, e1))
-        stages.append(bvh.stage_ms())
     torch.cuda.synchronize()
     if dist:
         dist.barrier()
@@ -269,6 +266,15 @@ def run_ours(a):
     total_ms = max_over_ranks(sum(e0.elapsed_time(e1) for e0, e1 in evs), dist, dev)
     ms_step = total_ms / a.steps
     value = world * n / (ms_step * 1e-3) / 1e6
+    # stage split from three more bakes with the stage events on (outside the timed region: the
+    # event records add host work between the launches)
+    bvh.profile(True)
+    stages = []
+    for _ in range(3):
+        flush.zero_()
+        bvh.rebuild(dv, dt, cfg, stream=stream)
+        stages.append(bvh.stage_ms())
+    bvh.profile(False)
     st = {k: statistics.mean(s[k] for s in stages) for k in stages[0]}
     nn, nt, _ = bvh.counts()
 
