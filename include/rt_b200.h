@@ -137,8 +137,19 @@ void rt_bvh_free(rt_bvh* bvh);
  * traverse() (bvh_traverse.cpp:91-178), 1 the while-while form (lanes of a warp walk inner
  * nodes, then test leaves, together), -1 the default: while-while when leaves hold 6 or more
  * triangles on average. Both visit the same nodes in the same order and give identical hits;
- * only their speed differs. */
+ * only their speed differs. 2: the 8-wide layout (128-byte nodes of up to eight children with
+ * 8-bit quantised, conservative child boxes), built now and again after every rebuild of the
+ * handle; rt_trace and the wavefront path tracer's trace stage use it (the plain per-pixel
+ * renderer keeps the binary loop). It is not the reference's visiting
+ * order: the closest hit's distance is the same, but on an exact tie in distance the reported
+ * triangle may differ, and a triangle that an exact box test loses by rounding at a box face
+ * may be found. */
 int rt_bvh_trace_loop(rt_bvh* bvh, int form);
+/* The wide layout of a handle in form 2 (no counterpart in the reference): *n_wide nodes of
+ * 128 bytes each -- {float p[3]; uint32 meta (x / y / z scale exponents in bits 0-23, inner-
+ * child mask in 24-31); uint32 ref[8]; uint16 cnt[8]; uint8 qlo[3][8], qhi[3][8]; 16 bytes
+ * zero} -- into out (host memory; out = NULL only reports the count). */
+int rt_bvh_wide_download(const rt_bvh* bvh, void* out, uint32_t* n_wide);
 
 /* Traces n rays; rays and hits are device pointers. Returns RT_E_STACK if any ray
  * overflowed its 64-entry stack (those hits carry RT_HIT_FLAG_OVERFLOW). */

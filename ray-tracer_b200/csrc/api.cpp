@@ -115,7 +115,7 @@ static void free_bvh(rt_bvh* b)
                        &b->s.sah_roots, &b->s.sah_refs_a, &b->s.sah_refs_b, &b->s.sah_tmp, &b->s.sah_pos,
                        &b->s.sah_lvl_a, &b->s.sah_lvl_b, &b->s.sah_dec, &b->s.sah_out, &b->s.sah_leaf_refs,
                        &b->s.sah_scan_in, &b->s.sah_scan_out, &b->s.sah_node_ids, &b->s.sah_roots_lvl,
-                       &b->s.in_verts, &b->s.in_tris, &b->s.gtris, &b->s.batch_off, &b->s.sah_budget, &b->s.sah_wide, &b->s.sah_tmp2, &b->s.sah_pos2, &b->scene_info, &b->scene_roots,
+                       &b->s.in_verts, &b->s.in_tris, &b->s.gtris, &b->s.batch_off, &b->s.sah_budget, &b->s.sah_wide, &b->s.sah_tmp2, &b->s.sah_pos2, &b->s.wide_flag, &b->s.wide_par, &b->wnodes, &b->wid, &b->scene_info, &b->scene_roots,
                        &b->wf_cams };
     for (DevBuf* x : bufs) { x->release(); }
     b->rootbuf.release();
@@ -203,7 +203,8 @@ int rt_rebuild(rt_bvh* b, const void* verts, uint32_t n_verts, const void* tris,
     }
     else if (where != RT_DEVICE) { return fail(RT_E_INVALID, "where must be RT_HOST or RT_DEVICE"); }
     b->depth = 0;
-    return build_bvh(b, dv, n_verts, dt, n_tris, c, st);
+    if (int e = build_bvh(b, dv, n_verts, dt, n_tris, c, st)) { return e; }
+    return b->trace_wide ? make_wide_layout(b, st) : RT_OK;  // the wide layout follows the tree
 }
 
 int rt_rebuild_batch(rt_bvh* b, const void* verts, const uint32_t* vert_offsets, const void* tris, const uint32_t* tri_offsets,
@@ -250,7 +251,8 @@ int rt_rebuild_batch(rt_bvh* b, const void* verts, const uint32_t* vert_offsets,
         dt = b->s.in_tris.as<rt_triangle>();
     }
     else if (where != RT_DEVICE) { return bail(fail(RT_E_INVALID, "where must be RT_HOST or RT_DEVICE")); }
-    return build_bvh_batch(b, dv, V, dt, N, c, st, n_scenes, d_toff, d_voff, tri_offsets);
+    if (int e = build_bvh_batch(b, dv, V, dt, N, c, st, n_scenes, d_toff, d_voff, tri_offsets)) { return e; }
+    return b->trace_wide ? make_wide_layout(b, st) : RT_OK;
 }
 
 int rt_build_batch(const void* verts, const uint32_t* vert_offsets, const void* tris, const uint32_t* tri_offsets,
@@ -415,7 +417,15 @@ int rt_load_bvh(const char* path, rt_bvh** out)
 int rt_bvh_trace_loop(rt_bvh* b, int form)
 {
     if (!b) { return fail(RT_E_NOT_LOADED, "BVH not loaded"); }
-    if (form < -1 || form > 1) { return fail(RT_E_INVALID, "form must be -1, 0 or 1"); }
+    if (form < -1 || form > 2) { return fail(RT_E_INVALID, "form must be -1, 0, 1 or 2"); }
+    if (form == 2)
+    {
+        if (int e = require_device()) { return e; }
+        if (int e = make_wide_layout(b, default_stream())) { return e; }
+        b->trace_wide = true;
+        return RT_OK;
+    }
+    b->trace_wide = false;
     if (form == -1)
     {
         uint32_t leaves = b->stats[4];
@@ -446,6 +456,15 @@ int rt_bvh_download(const rt_bvh* b, rt_bvh_node* nodes, rt_triangle* tris, rt_v
     if (tris && b->n_tris) { RT_CUDA(cudaMemcpyAsync(tris, b->tris.p, (size_t)b->n_tris * 12, cudaMemcpyDeviceToHost, st)); }
     if (verts && b->n_verts) { RT_CUDA(cudaMemcpyAsync(verts, b->verts.p, (size_t)b->n_verts * 24, cudaMemcpyDeviceToHost, st)); }
     RT_CUDA(cudaStreamSynchronize(st));
+    return RT_OK;
+}
+
+int rt_bvh_wide_download(const rt_bvh* b, void* out, uint32_t* n_wide)
+{
+    if (!b || !n_wide) { return fail(RT_E_INVALID, "null argument"); }
+    if (!b->trace_wide) { return fail(RT_E_INVALID, "the handle has no wide layout (rt_bvh_trace_loop form 2)"); }
+    *n_wide = b->n_wide;
+    if (out && b->n_wide) { RT_CUDA(cudaMemcpy(out, b->wnodes.p, (size_t)b->n_wide * sizeof(rt_wnode), cudaMemcpyDeviceToHost)); }
     return RT_OK;
 }
 

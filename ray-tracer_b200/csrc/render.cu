@@ -555,14 +555,17 @@ int wf_run_graph(rt_bvh* B, const WfJob& J, const rt_wavefront_params& W, cudaSt
 {
     if (int e = wf_buffers(B, J, W)) { return e; }
     // the graph bakes in kernel arguments and buffer addresses: all of them form its key
-    std::vector<unsigned char> key(sizeof(WfJob) + sizeof(W) + 16 * sizeof(void*));
+    // (and the traversal form: binary one-loop / while-while, or the 8-wide layout)
+    const void* ptrs[] = { B->wf_rays[0].p, B->wf_rays[1].p, B->wf_state[0].p, B->wf_state[1].p, B->wf_scene[0].p,
+                           B->wf_scene[1].p, B->wf_hits.p, B->wf_acc.p, B->wf_ctr.p, B->trace_status.p, B->gnodes.p,
+                           B->tripos.p, B->tris.p, B->verts.p, B->rootbuf.p, B->scene_roots.p, B->wnodes.p, B->wid.p };
+    const uint32_t form[2] = { B->trace_ww ? 1u : 0u, B->trace_wide ? 1u : 0u };
+    std::vector<unsigned char> key(sizeof(WfJob) + sizeof(W) + sizeof(ptrs) + sizeof(form));
     std::memset(key.data(), 0, key.size());
     std::memcpy(key.data(), &J, sizeof(WfJob));
     std::memcpy(key.data() + sizeof(WfJob), &W, sizeof(W));
-    const void* ptrs[] = { B->wf_rays[0].p, B->wf_rays[1].p, B->wf_state[0].p, B->wf_state[1].p, B->wf_scene[0].p,
-                           B->wf_scene[1].p, B->wf_hits.p, B->wf_acc.p, B->wf_ctr.p, B->trace_status.p, B->gnodes.p,
-                           B->tripos.p, B->tris.p, B->verts.p, B->rootbuf.p, B->scene_roots.p };
     std::memcpy(key.data() + sizeof(WfJob) + sizeof(W), ptrs, sizeof(ptrs));
+    std::memcpy(key.data() + sizeof(WfJob) + sizeof(W) + sizeof(ptrs), form, sizeof(form));
     if (!B->wf_stream)
     {
         RT_CUDA(cudaStreamCreateWithFlags(&B->wf_stream, cudaStreamNonBlocking));

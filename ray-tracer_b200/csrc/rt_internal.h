@@ -100,6 +100,20 @@ struct rt_gnode
     uint4  d;  // l.ref   r.ref   l.cnt   r.cnt
 };
 
+// 128-byte node of the 8-wide traversal layout (wide.cu): child c's box is
+// [p + qlo * 2^e, p + qhi * 2^e] per axis, conservative.
+struct rt_wnode
+{
+    float    p[3];       // quantisation origin
+    uint32_t meta;       // bits 0-7 / 8-15 / 16-23: biased exponents of the x / y / z scales; 24-31: inner-child mask
+    uint32_t ref[8];     // inner child: wide node index; leaf child: first triangle
+    uint16_t cnt[8];     // leaf child: triangle count; inner child: 1; 0: an empty slot
+    uint8_t  qlo[3][8];  // lower planes, per axis and child
+    uint8_t  qhi[3][8];  // upper planes
+    uint32_t pad[4];
+};
+static_assert(sizeof(rt_wnode) == 128, "rt_wnode is one 128-byte line");
+
 struct BuildScratch
 {
     rtb::DevBuf tri_lo, tri_hi, tri_cz, keys, vals, hist, scene, status;
@@ -124,6 +138,7 @@ struct BuildScratch
     rtb::DevBuf sah_budget;         // spatial-split budget per scene: used, cap
     rtb::DevBuf sah_wide;           // SAH nodes evaluated by many blocks: bins, list, block offsets
     rtb::DevBuf sah_tmp2, sah_pos2; // their partitions' second buffer and satisfying-right positions
+    rtb::DevBuf wide_flag, wide_par;  // wide layout: which binary nodes are wide nodes; parents
 };
 
 struct rt_bvh
@@ -140,6 +155,9 @@ struct rt_bvh
     std::vector<uint32_t> scene_info_host;
     uint32_t     depth = 0;                 // tree depth (computed on demand; 0 = unknown)
     bool         trace_ww = true;           // traversal loop form: while-while for large leaves
+    bool         trace_wide = false;        // traverse the 8-wide layout (rebuilt after every rebuild)
+    rtb::DevBuf  wnodes, wid;               // wide layout and the wide index of each binary node
+    uint32_t     n_wide = 0;
     uint32_t     stats[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     BuildScratch s;
     rtb::DevBuf  trace_status, trace_rays, trace_hits;
@@ -183,6 +201,8 @@ int build_bvh_batch(rt_bvh* b, const rt_vertex* d_verts, uint32_t n_verts, const
                     const uint32_t* d_voff, const uint32_t* h_toff);
 // traverse.cu: the traversal entry record of every scene root of a batched build
 int launch_scene_roots(rt_bvh* b, uint32_t n_scenes, const uint32_t* d_counts, uint32_t* status, cudaStream_t st);
+// wide.cu: the 8-wide traversal layout of the handle's tree (synchronises the stream)
+int make_wide_layout(rt_bvh* b, cudaStream_t st);
 // traverse.cu: depth of the tree (levels of inner nodes above the deepest leaf), cached in b->depth
 int tree_depth(rt_bvh* b, cudaStream_t st, uint32_t* depth);
 // traverse.cu: (re)creates the traversal layout from the .bvh-layout arrays on the device

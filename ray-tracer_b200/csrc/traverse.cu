@@ -132,7 +132,7 @@ __global__ void k_depth(const rt_bvh_node* __restrict__ nodes, uint32_t n, const
 // rt_ray records in, rt_hit records out (two 128-bit accesses each). n_dev, when set, holds
 // the ray count on the device (the wavefront path tracer's queue length). ROOTS: ray i
 // traces the subtree roots[rscene[i]] (a scene of a batched build).
-template <int MODE, int STK, bool ROOTS>
+template <int MODE, int STK, bool ROOTS, bool WIDE = false>
 __global__ void __launch_bounds__(256)
 k_trace(TraceCtx T, const float4* __restrict__ rays, float4* __restrict__ hits, uint64_t n, const uint32_t* __restrict__ n_dev,
         unsigned long long* __restrict__ counter, uint32_t* __restrict__ status, const TraceRoot* __restrict__ roots,
@@ -151,8 +151,11 @@ k_trace(TraceCtx T, const float4* __restrict__ rays, float4* __restrict__ hits, 
         const uint64_t ri = base + (uint64_t)lane;
         if (ri >= n) { continue; }
         const float4 r0 = rays[2 * ri], r1 = rays[2 * ri + 1];
-        const THit H = trace_ray<MODE, STK>(T, ROOTS ? roots[rscene[ri]] : R0, mk3(r0.x, r0.y, r0.z), mk3(r1.x, r1.y, r1.z),
-                                            r0.w, r1.w);
+        const TraceRoot& R = ROOTS ? roots[rscene[ri]] : R0;
+        const f3 o = mk3(r0.x, r0.y, r0.z), d = mk3(r1.x, r1.y, r1.z);
+        THit H;
+        if constexpr (WIDE) { H = trace_ray_wide<MODE, 2 * STK>(T, R, o, d, r0.w, r1.w); }  // up to 7 entries per level
+        else { H = trace_ray<MODE, STK>(T, R, o, d, r0.w, r1.w); }
         float4 h0 = make_float4(0.f, 0.f, 0.f, 0.f), h1 = make_float4(0.f, 0.f, 0.f, 0.f);
         uint32_t flags = 0;
         if (H.hit)
@@ -172,8 +175,19 @@ k_trace(TraceCtx T, const float4* __restrict__ rays, float4* __restrict__ hits, 
 using TraceFn = void (*)(TraceCtx, const float4*, float4*, uint64_t, const uint32_t*, unsigned long long*, uint32_t*,
                          const TraceRoot*, const uint32_t*);
 
-TraceFn trace_fn(uint32_t flags, int stack, bool roots)
+TraceFn trace_fn(uint32_t flags, int stack, bool roots, bool wide)
 {
+    if (wide)
+    {
+        if (roots) { return (flags & 3u) == 0 ? k_trace<0, STACK, true, true> : nullptr; }
+        switch (flags & 3u)
+        {
+        case 0: return k_trace<0, STACK, false, true>;
+        case 1: return k_trace<1, STACK, false, true>;
+        case 2: return k_trace<2, STACK, false, true>;
+        default: return k_trace<3, STACK, false, true>;
+        }
+    }
     if (stack <= 32)
     {
         if (roots) { return k_trace<0, 32, true>; }
@@ -219,6 +233,8 @@ TraceCtx make_trace_ctx(const rt_bvh* B)
     T.verts = B->verts.as<rt_vertex>();
     T.root = B->rootbuf.as<TraceRoot>();
     T.ww = B->trace_ww ? 1u : 0u;
+    T.wn = B->wnodes.as<rt_wnode>();
+    T.wid = B->wid.as<uint32_t>();
     return T;
 }
 
@@ -259,7 +275,7 @@ int make_traversal_layout(rt_bvh* B, cudaStream_t st)
 int trace_launch(const rt_bvh* B, const void* d_rays, void* d_hits, uint64_t n, const uint32_t* n_dev, uint32_t flags,
                  cudaStream_t st, uint32_t* d_status, unsigned long long* d_counter, const TraceLaunch& opt)
 {
-    const TraceFn fn = trace_fn(flags, opt.stack, opt.roots != nullptr);
+    const TraceFn fn = trace_fn(flags, opt.stack, opt.roots != nullptr, B->trace_wide);
     if (!fn) { return fail(RT_E_INVALID, "no trace kernel for this mode and stack depth"); }
     const int block = opt.block > 0 ? opt.block : TBLK;
     if (block % 32 || block > 256) { return fail(RT_E_INVALID, "trace block must be a multiple of 32, at most 256"); }

@@ -26,6 +26,9 @@ STATUS = {0: "RT_OK", 1: "RT_E_INVALID", 2: "RT_E_IO", 3: "RT_E_FORMAT", 4: "RT_
 
 NODE_DTYPE = np.dtype([("bmin", "<f4", 4), ("bmax", "<f4", 4), ("is_leaf", "u1"), ("pad0", "u1", 3),
                        ("a", "<u4"), ("b", "<u4"), ("pad1", "<u4")])
+# one node of the 8-wide traversal layout (rt_bvh_wide_download)
+WIDE_NODE_DTYPE = np.dtype([("p", "<f4", 3), ("meta", "<u4"), ("ref", "<u4", 8), ("cnt", "<u2", 8), ("qlo", "u1", (3, 8)),
+                            ("qhi", "u1", (3, 8)), ("pad", "<u4", 4)])
 HIT_DTYPE = np.dtype([("t", "<f4"), ("u", "<f4"), ("v", "<f4"), ("tri", "<u4"), ("n", "<f4", 3), ("flags", "<u4")])
 assert NODE_DTYPE.itemsize == 48 and HIT_DTYPE.itemsize == 32
 
@@ -98,6 +101,7 @@ def lib():
         L.rt_bvh_counts.argtypes = [vp, vp]
         L.rt_bvh_download.argtypes = [vp, vp, vp, vp]
         L.rt_bvh_download_async.argtypes = [vp, vp, vp, vp, vp]
+        L.rt_bvh_wide_download.argtypes = [vp, vp, vp]
         L.rt_bvh_prim_ids.argtypes = [vp, vp, i32]
         L.rt_bvh_stats.argtypes = [vp, vp]
         L.rt_bvh_free.argtypes = [vp]
@@ -341,8 +345,18 @@ class Bvh:
         _check(lib().rt_write_bvh(self.h, path.encode()))
 
     def trace_loop(self, form: int = -1):
-        """Traversal loop form: 0 one-loop, 1 while-while, -1 the default choice by leaf size."""
+        """Traversal form: 0 one-loop, 1 while-while, -1 the default choice by leaf size (all three
+        the reference's visiting order); 2 the 8-wide layout (same closest distance, ties may
+        report another triangle; kept up to date across rebuilds)."""
         _check(lib().rt_bvh_trace_loop(self.h, int(form)))
+
+    def wide_nodes(self):
+        """The 8-wide layout (after trace_loop(2)) as a WIDE_NODE_DTYPE array."""
+        n = C.c_uint32(0)
+        _check(lib().rt_bvh_wide_download(self.h, None, C.byref(n)))
+        out = np.zeros(n.value, WIDE_NODE_DTYPE)
+        _check(lib().rt_bvh_wide_download(self.h, _ptr(out), C.byref(n)))
+        return out
 
     # -- tracing -----------------------------------------------------------------------
     def trace(self, rays, flags: int = TRACE_CLOSEST, stream=None):
