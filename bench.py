@@ -411,6 +411,11 @@ def secondary(a, bvh, dv, dt, verts, stream, dev, flush):
             for fl, fname in ((rtb200.TRACE_CLOSEST, "closest"), (rtb200.TRACE_ANY_HIT, "anyhit")):
                 ms = timed(lambda: b.trace(r, fl, stream=stream), 3)
                 res[f"trace_{preset}_{name}_{fname}_mray_s"] = round(r.shape[0] / (ms * 1e-3) / 1e6, 1)
+        # the 8-wide layout (opt-in form: same closest distances, ties may name another triangle)
+        b.trace_loop(2)
+        for name, r in (("incoherent16M", rays), ("primary1080p", prim)):
+            ms = timed(lambda: b.trace(r, rtb200.TRACE_CLOSEST, stream=stream), 3)
+            res[f"trace_{preset}_wide8_{name}_closest_mray_s"] = round(r.shape[0] / (ms * 1e-3) / 1e6, 1)
         b.free()
     return res
 

@@ -268,119 +268,103 @@ __device__ __forceinline__ THit trace_ray_ww(const TraceCtx& T, const TraceRoot&
     return H;
 }
 
-// Traversal of the 8-wide layout (wide.cu): pop an entry, skip it if its entry distance is
-// not below the best t, test a leaf's triangles in order or decode a wide node's child boxes
-// and push the children that are hit, farthest first (a sorting network over the eight entry
-// distances), so the nearest pops next. The closest hit's distance is that of the binary
+// Traversal of the 8-wide layout (wide.cu). A visited wide node's eight child boxes are decoded
+// and tested at once; the node goes on the stack as one entry {node, mask of the children hit}
+// with the mask in the ray's visiting order -- the builder puts children in octant slots, and a
+// ray whose direction has the signs o visits slot s as its (s ^ o)-th, near to far along each
+// axis -- and each step takes the next child from the top entry: a leaf's triangles are tested
+// in order, an inner child is visited. The closest hit's distance is that of the binary
 // traversal; on an exact tie in distance the triangle found first may differ, since the
 // visiting order differs, and the conservative child boxes may admit a triangle that an exact
-// box test rejects by rounding at a face. Not the reference's order: an opt-in fast form.
+// box test rejects by rounding at a face. Not the reference's order: an opt-in form.
 template <int MODE, int STK>
 __device__ __forceinline__ THit trace_ray_wide(const TraceCtx& T, const TraceRoot& R, rtd::f3 o, rtd::f3 d, float tmin,
                                                float tmax)
 {
     using namespace rtd;
-    uint32_t sref[STK], scnt[STK];
-    float stn[STK];
+    uint2 stk[STK];  // {wide node, remaining children hit, in visiting order}
     const f3 inv = mk3(1.f / d.x, 1.f / d.y, 1.f / d.z);
+    const uint32_t oct = (d.x < 0.f ? 1u : 0u) | (d.y < 0.f ? 2u : 0u) | (d.z < 0.f ? 4u : 0u);
     THit H;
     H.t = tmax; H.u = 0.f; H.v = 0.f; H.tri = 0; H.hit = false; H.overflow = false;
     float best = tmax;
     int top = 0;
     const float troot = ray_box(o, inv, tmin, best, R.box[0], R.box[1], R.box[2], R.box[3], R.box[4], R.box[5]);
-    if (troot < best)
-    {
-        sref[0] = (R.cnt & LEAF_BIT) ? R.ref : __ldg(&T.wid[R.ref]);
-        scnt[0] = R.cnt;  // 0: a wide node
-        stn[0] = troot;
-        top = 1;
-    }
+    if (!(troot < best)) { return H; }
+    // the entry to visit: a wide node (cnt 0) or a leaf's triangle range
+    uint32_t cref = (R.cnt & LEAF_BIT) ? R.ref : __ldg(&T.wid[R.ref]);
+    uint32_t ccnt = R.cnt;
+    bool have = true;
     uint32_t pops = 0;
-    while (top > 0)
+    for (;;)
     {
         if (++pops > MAX_POPS) { H.overflow = true; break; }
-        --top;
-        if (stn[top] >= best) { continue; }
-        const uint32_t ref = sref[top], cnt = scnt[top];
-        if (cnt & LEAF_BIT)
+        if (have)
         {
-            const uint32_t c = cnt & ~LEAF_BIT;
-            bool done = false;
-            for (uint32_t k = 0; k < c; k++)
+            have = false;
+            if (ccnt & LEAF_BIT)
             {
-                const uint32_t ti = ref + k;
-                const float4 p0 = __ldg(&T.tp[3 * ti]), p1 = __ldg(&T.tp[3 * ti + 1]), p2 = __ldg(&T.tp[3 * ti + 2]);
-                const f3 v0 = mk3(p0.x, p0.y, p0.z), v1 = mk3(p0.w, p1.x, p1.y), v2 = mk3(p1.z, p1.w, p2.x);
-                float t, u, v;
-                const bool acc = (MODE & 2) ? ray_tri_watertight(o, d, tmin, tmax, v0, v1, v2, t, u, v)
-                                            : ray_tri(o, d, tmin, tmax, v0, v1, v2, t, u, v);
-                if (acc && t < best)
+                const uint32_t c = ccnt & ~LEAF_BIT;
+                bool done = false;
+                for (uint32_t k = 0; k < c; k++)
                 {
-                    best = t; H.u = u; H.v = v; H.tri = ti; H.hit = true;
-                    if (MODE & 1) { done = true; break; }
+                    const uint32_t ti = cref + k;
+                    const float4 p0 = __ldg(&T.tp[3 * ti]), p1 = __ldg(&T.tp[3 * ti + 1]), p2 = __ldg(&T.tp[3 * ti + 2]);
+                    const f3 v0 = mk3(p0.x, p0.y, p0.z), v1 = mk3(p0.w, p1.x, p1.y), v2 = mk3(p1.z, p1.w, p2.x);
+                    float t, u, v;
+                    const bool acc = (MODE & 2) ? ray_tri_watertight(o, d, tmin, tmax, v0, v1, v2, t, u, v)
+                                                : ray_tri(o, d, tmin, tmax, v0, v1, v2, t, u, v);
+                    if (acc && t < best)
+                    {
+                        best = t; H.u = u; H.v = v; H.tri = ti; H.hit = true;
+                        if (MODE & 1) { done = true; break; }
+                    }
+                }
+                if (done) { break; }
+            }
+            else
+            {
+                const uint4* g = reinterpret_cast<const uint4*>(T.wn + cref);
+                const uint4 w0 = __ldg(g), w3 = __ldg(g + 3), w4 = __ldg(g + 4), w5 = __ldg(g + 5), w6 = __ldg(g + 6);
+                const float px = __uint_as_float(w0.x), py = __uint_as_float(w0.y), pz = __uint_as_float(w0.z);
+                const float sx = __uint_as_float((w0.w & 0xffu) << 23), sy = __uint_as_float(((w0.w >> 8) & 0xffu) << 23),
+                            sz = __uint_as_float(((w0.w >> 16) & 0xffu) << 23);
+                const uint32_t cn[4] = { w3.x, w3.y, w3.z, w3.w };  // two 16-bit counts per word
+                uint32_t mask = 0;
+#pragma unroll
+                for (int c = 0; c < 8; c++)
+                {
+                    const uint32_t cc = (cn[c >> 1] >> (16 * (c & 1))) & 0xffffu;
+                    const int sb = 8 * (c & 3);
+                    const uint32_t lx = ((c < 4 ? w4.x : w4.y) >> sb) & 0xffu, ly = ((c < 4 ? w4.z : w4.w) >> sb) & 0xffu;
+                    const uint32_t lz = ((c < 4 ? w5.x : w5.y) >> sb) & 0xffu, hx = ((c < 4 ? w5.z : w5.w) >> sb) & 0xffu;
+                    const uint32_t hy = ((c < 4 ? w6.x : w6.y) >> sb) & 0xffu, hz = ((c < 4 ? w6.z : w6.w) >> sb) & 0xffu;
+                    // the decoded planes (the layout builder checks these very operations are conservative)
+                    const float bx0 = __fadd_rn(px, __fmul_rn((float)lx, sx)), bx1 = __fadd_rn(px, __fmul_rn((float)hx, sx));
+                    const float by0 = __fadd_rn(py, __fmul_rn((float)ly, sy)), by1 = __fadd_rn(py, __fmul_rn((float)hy, sy));
+                    const float bz0 = __fadd_rn(pz, __fmul_rn((float)lz, sz)), bz1 = __fadd_rn(pz, __fmul_rn((float)hz, sz));
+                    const float t = ray_box(o, inv, tmin, best, bx0, by0, bz0, bx1, by1, bz1);
+                    if (cc != 0u && t < best) { mask |= 1u << ((uint32_t)c ^ oct); }
+                }
+                if (mask)
+                {
+                    if (top >= STK) { H.overflow = true; break; }
+                    stk[top++] = make_uint2(cref, mask);
                 }
             }
-            if (done) { break; }
-            continue;
         }
-        const uint4* g = reinterpret_cast<const uint4*>(T.wn + ref);
-        const uint4 w0 = __ldg(g), w1 = __ldg(g + 1), w2 = __ldg(g + 2), w3 = __ldg(g + 3);
-        const uint4 w4 = __ldg(g + 4), w5 = __ldg(g + 5), w6 = __ldg(g + 6);
-        const float px = __uint_as_float(w0.x), py = __uint_as_float(w0.y), pz = __uint_as_float(w0.z);
-        const float sx = __uint_as_float((w0.w & 0xffu) << 23), sy = __uint_as_float(((w0.w >> 8) & 0xffu) << 23),
-                    sz = __uint_as_float(((w0.w >> 16) & 0xffu) << 23);
-        const uint32_t imask = w0.w >> 24;
-        const uint32_t refs[8] = { w1.x, w1.y, w1.z, w1.w, w2.x, w2.y, w2.z, w2.w };
-        const uint32_t cn[4] = { w3.x, w3.y, w3.z, w3.w };  // two 16-bit counts per word
-        // planes: qlo x (w4.x, w4.y), y (w4.z, w4.w), z (w5.x, w5.y); qhi x (w5.z, w5.w), y (w6.x, w6.y), z (w6.z, w6.w)
-        float tn[8];
-        uint32_t ord[8];
-#pragma unroll
-        for (int c = 0; c < 8; c++)
-        {
-            ord[c] = (uint32_t)c;
-            const uint32_t cc = (cn[c >> 1] >> (16 * (c & 1))) & 0xffffu;
-            const int sb = 8 * (c & 3);
-            const uint32_t lx = ((c < 4 ? w4.x : w4.y) >> sb) & 0xffu, ly = ((c < 4 ? w4.z : w4.w) >> sb) & 0xffu;
-            const uint32_t lz = ((c < 4 ? w5.x : w5.y) >> sb) & 0xffu, hx = ((c < 4 ? w5.z : w5.w) >> sb) & 0xffu;
-            const uint32_t hy = ((c < 4 ? w6.x : w6.y) >> sb) & 0xffu, hz = ((c < 4 ? w6.z : w6.w) >> sb) & 0xffu;
-            // the decoded planes (the layout builder checks these very operations are conservative)
-            const float bx0 = __fadd_rn(px, __fmul_rn((float)lx, sx)), bx1 = __fadd_rn(px, __fmul_rn((float)hx, sx));
-            const float by0 = __fadd_rn(py, __fmul_rn((float)ly, sy)), by1 = __fadd_rn(py, __fmul_rn((float)hy, sy));
-            const float bz0 = __fadd_rn(pz, __fmul_rn((float)lz, sz)), bz1 = __fadd_rn(pz, __fmul_rn((float)hz, sz));
-            const float t = ray_box(o, inv, tmin, best, bx0, by0, bz0, bx1, by1, bz1);
-            tn[c] = cc != 0u ? t : bits2f(0x7f800000u);
-        }
-        // descending entry distance (Batcher's odd-even merge network for eight keys)
-        auto cas = [&](int a, int b) {
-            if (tn[a] < tn[b])
-            {
-                const float tt = tn[a]; tn[a] = tn[b]; tn[b] = tt;
-                const uint32_t oo = ord[a]; ord[a] = ord[b]; ord[b] = oo;
-            }
-        };
-        cas(0, 1); cas(2, 3); cas(4, 5); cas(6, 7);
-        cas(0, 2); cas(1, 3); cas(4, 6); cas(5, 7);
-        cas(1, 2); cas(5, 6);
-        cas(0, 4); cas(1, 5); cas(2, 6); cas(3, 7);
-        cas(2, 4); cas(3, 5);
-        cas(1, 2); cas(3, 4); cas(5, 6);
-        bool ovf = false;
-#pragma unroll
-        for (int k = 0; k < 8; k++)
-        {
-            if (tn[k] < best)
-            {
-                if (top >= STK) { ovf = true; break; }
-                const uint32_t c = ord[k];
-                const uint32_t cc = (cn[c >> 1] >> (16 * (c & 1))) & 0xffffu;
-                sref[top] = refs[c];
-                scnt[top] = ((imask >> c) & 1u) ? 0u : (LEAF_BIT | cc);
-                stn[top] = tn[k];
-                top++;
-            }
-        }
-        if (ovf) { H.overflow = true; break; }
+        if (top == 0) { break; }
+        // the next child of the top entry
+        uint2& e = stk[top - 1];
+        const uint32_t k = (uint32_t)__ffs((int)e.y) - 1u;
+        const uint32_t node = e.x;
+        e.y &= e.y - 1u;
+        if (e.y == 0u) { --top; }
+        const uint32_t c = k ^ oct;
+        const rt_wnode* wn = T.wn + node;
+        cref = __ldg(&wn->ref[c]);
+        ccnt = ((__ldg(&wn->meta) >> (24 + c)) & 1u) ? 0u : (LEAF_BIT | (uint32_t)__ldg(&wn->cnt[c]));
+        have = true;
     }
     H.t = best;
     return H;

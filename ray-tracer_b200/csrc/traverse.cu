@@ -154,7 +154,7 @@ k_trace(TraceCtx T, const float4* __restrict__ rays, float4* __restrict__ hits, 
         const TraceRoot& R = ROOTS ? roots[rscene[ri]] : R0;
         const f3 o = mk3(r0.x, r0.y, r0.z), d = mk3(r1.x, r1.y, r1.z);
         THit H;
-        if constexpr (WIDE) { H = trace_ray_wide<MODE, 2 * STK>(T, R, o, d, r0.w, r1.w); }  // up to 7 entries per level
+        if constexpr (WIDE) { H = trace_ray_wide<MODE, STK>(T, R, o, d, r0.w, r1.w); }  // one entry per wide level
         else { H = trace_ray<MODE, STK>(T, R, o, d, r0.w, r1.w); }
         float4 h0 = make_float4(0.f, 0.f, 0.f, 0.f), h1 = make_float4(0.f, 0.f, 0.f, 0.f);
         uint32_t flags = 0;

@@ -124,6 +124,41 @@ __global__ void k_wide_build(const rt_bvh_node* __restrict__ nodes, uint32_t n, 
         }
         any = true;
     }
+    // slots by octant: child c goes to a slot s whose octant (bit a set: the positive side of
+    // axis a) matches the offset of its box centre from the node's centre, greedily by the
+    // smallest cost; a ray whose direction has the signs o (bit a set: negative) visits slot s
+    // as its (s ^ o)-th, near to far along each axis
+    int slot[8];
+    bool used[8];
+    float off[8][3];
+    float ctr[3];
+    for (int a = 0; a < 3; a++) { ctr[a] = __fmul_rn(__fadd_rn(lo3[a], hi3[a]), 0.5f); }
+    int npres = 0;
+    for (int c = 0; c < 8; c++) { slot[c] = -1; used[c] = false; }
+    for (int c = 0; c < cnt; c++)
+    {
+        if (!present[c]) { continue; }
+        npres++;
+        for (int a = 0; a < 3; a++) { off[c][a] = __fsub_rn(__fmul_rn(__fadd_rn(cn[c].bmin[a], cn[c].bmax[a]), 0.5f), ctr[a]); }
+    }
+    for (int r = 0; r < npres; r++)
+    {
+        float bv = 0.f;
+        int bc = -1, bs = -1;
+        for (int c = 0; c < cnt; c++)
+        {
+            if (!present[c] || slot[c] >= 0) { continue; }
+            for (int sl = 0; sl < 8; sl++)
+            {
+                if (used[sl]) { continue; }
+                const float v = __fadd_rn(__fadd_rn((sl & 1) ? -off[c][0] : off[c][0], (sl & 2) ? -off[c][1] : off[c][1]),
+                                          (sl & 4) ? -off[c][2] : off[c][2]);
+                if (bc < 0 || v < bv) { bv = v; bc = c; bs = sl; }
+            }
+        }
+        slot[bc] = bs;
+        used[bs] = true;
+    }
     rt_wnode w;
     uint32_t e[3];
     for (int a = 0; a < 3; a++) { w.p[a] = lo3[a]; e[a] = wexponent(lo3[a], hi3[a]); }
@@ -133,19 +168,20 @@ __global__ void k_wide_build(const rt_bvh_node* __restrict__ nodes, uint32_t n, 
         w.ref[c] = 0u; w.cnt[c] = 0u;
         for (int a = 0; a < 3; a++) { w.qlo[a][c] = 0u; w.qhi[a][c] = 0u; }
     }
-    for (int c = 0; c < cnt; c++)
+    for (int c0 = 0; c0 < cnt; c0++)
     {
-        if (!present[c]) { continue; }
-        if (cn[c].is_leaf)
+        if (!present[c0]) { continue; }
+        const int c = slot[c0];  // written to its slot; cn / list stay indexed by c0
+        if (cn[c0].is_leaf)
         {
-            if (cn[c].b > 0xffffu) { atomicOr(status, ST_CAPACITY); return; }
-            w.ref[c] = cn[c].a;
-            w.cnt[c] = (uint16_t)cn[c].b;
+            if (cn[c0].b > 0xffffu) { atomicOr(status, ST_CAPACITY); return; }
+            w.ref[c] = cn[c0].a;
+            w.cnt[c] = (uint16_t)cn[c0].b;
         }
         else
         {
-            if (!flag[list[c]]) { atomicOr(status, ST_CAPACITY); return; }
-            w.ref[c] = wid[list[c]];
+            if (!flag[list[c0]]) { atomicOr(status, ST_CAPACITY); return; }
+            w.ref[c] = wid[list[c0]];
             w.cnt[c] = 1u;
             imask |= 1u << c;
         }
@@ -153,12 +189,12 @@ __global__ void k_wide_build(const rt_bvh_node* __restrict__ nodes, uint32_t n, 
         {
             const float s = __uint_as_float(e[a] << 23);
             const float p = lo3[a];
-            const double ql = floor(((double)cn[c].bmin[a] - (double)p) / (double)s);
-            const double qh = ceil(((double)cn[c].bmax[a] - (double)p) / (double)s);
+            const double ql = floor(((double)cn[c0].bmin[a] - (double)p) / (double)s);
+            const double qh = ceil(((double)cn[c0].bmax[a] - (double)p) / (double)s);
             uint32_t lo = (uint32_t)fmin(fmax(ql, 0.0), 255.0), hi = (uint32_t)fmin(fmax(qh, 0.0), 255.0);
-            while (lo > 0u && wdecode(p, lo, s) > cn[c].bmin[a]) { lo--; }
-            while (hi < 255u && wdecode(p, hi, s) < cn[c].bmax[a]) { hi++; }
-            if (wdecode(p, lo, s) > cn[c].bmin[a] || wdecode(p, hi, s) < cn[c].bmax[a]) { atomicOr(status, ST_CAPACITY); }
+            while (lo > 0u && wdecode(p, lo, s) > cn[c0].bmin[a]) { lo--; }
+            while (hi < 255u && wdecode(p, hi, s) < cn[c0].bmax[a]) { hi++; }
+            if (wdecode(p, lo, s) > cn[c0].bmin[a] || wdecode(p, hi, s) < cn[c0].bmax[a]) { atomicOr(status, ST_CAPACITY); }
             w.qlo[a][c] = (uint8_t)lo;
             w.qhi[a][c] = (uint8_t)hi;
         }

@@ -61,12 +61,33 @@ def wide_restatement(nodes, scene_roots=()):
         lo3 = [min(nodes["bmin"][c][a] for c, ok in zip(lst, pres) if ok) for a in range(3)]
         hi3 = [max(nodes["bmax"][c][a] for c, ok in zip(lst, pres) if ok) for a in range(3)]
         e = [_exponent(lo3[a], hi3[a]) for a in range(3)]
+        # octant slots, greedily by the smallest cost (the first minimal pair wins)
+        f32 = np.float32
+        ctr = [f32(f32(f32(lo3[a]) + f32(hi3[a])) * f32(0.5)) for a in range(3)]
+        off = {k: [f32(f32(f32(f32(nodes["bmin"][c][a]) + f32(nodes["bmax"][c][a])) * f32(0.5)) - ctr[a])
+                   for a in range(3)] for k, (c, ok) in enumerate(zip(lst, pres)) if ok}
+        slot, used = {}, set()
+        for _ in range(len(off)):
+            best = None
+            for k in range(len(lst)):
+                if k not in off or k in slot:
+                    continue
+                for sl in range(8):
+                    if sl in used:
+                        continue
+                    o = off[k]
+                    v = f32(f32((-o[0] if sl & 1 else o[0]) + (-o[1] if sl & 2 else o[1])) + (-o[2] if sl & 4 else o[2]))
+                    if best is None or v < best[0]:
+                        best = (v, k, sl)
+            slot[best[1]] = best[2]
+            used.add(best[2])
         w = out[wid[i]]
         w["p"] = lo3
         imask = 0
-        for k, (c, ok) in enumerate(zip(lst, pres)):
+        for k0, (c, ok) in enumerate(zip(lst, pres)):
             if not ok:
                 continue
+            k = slot[k0]
             if leaf[c]:
                 w["ref"][k], w["cnt"][k] = nodes["a"][c], nodes["b"][c]
             else:
