@@ -622,14 +622,24 @@ k_emit(const K* __restrict__ keys, uint32_t n, const uint4* __restrict__ knode, 
 __global__ void __launch_bounds__(BLK)
 k_emit_tris(const uint32_t* __restrict__ perm, const uint8_t* __restrict__ kpos, const uint32_t* __restrict__ stri,
             uint32_t n, const rt_triangle* __restrict__ tris, rt_triangle* __restrict__ out, uint32_t* __restrict__ prim,
-            uint32_t max_tris, uint32_t* __restrict__ status)
+            uint32_t max_tris, const rt_vertex* __restrict__ verts, float4* __restrict__ tp, uint32_t* __restrict__ status)
 {
     const uint32_t k = blockIdx.x * BLK + threadIdx.x;
     if (k >= n || !kpos[k]) { return; }
     const uint32_t t = perm[k], at = stri[k];
     if (at >= max_tris) { atomicOr(status, ST_CAPACITY); return; }
-    out[at] = tris[t];
+    const rt_triangle tr = tris[t];
+    out[at] = tr;
     prim[at] = t;
+    if (tp)  // the traversal layout's position record of the baked triangle (k_make_tripos)
+    {
+        const rt_vertex& a = verts[tr.v[0]];
+        const rt_vertex& b = verts[tr.v[1]];
+        const rt_vertex& c = verts[tr.v[2]];
+        tp[3 * at + 0] = make_float4(a.x, a.y, a.z, b.x);
+        tp[3 * at + 1] = make_float4(b.y, b.z, c.x, c.y);
+        tp[3 * at + 2] = make_float4(c.z, 0.f, 0.f, 0.f);
+    }
 }
 
 // ---- device-wide exclusive scan (reduce, scan of partials, apply) ----
@@ -925,8 +935,11 @@ int build_typed(rt_bvh* B, const rt_vertex* d_verts, uint32_t V, const rt_triang
                                                   S.stri.as<uint32_t>(), B->nodes.as<rt_bvh_node>(), 2 * cap - 1,
                                                   batch ? B->scene_info.as<uint32_t>() : nullptr, status);
         count_launch();
+        // without SAH subtrees every triangle passes here: its traversal record is written too
+        // (input positions: the renormalisation changes only normals)
         k_emit_tris<<<blocks_for(N), BLK, 0, st>>>(perm, S.bnd.as<uint8_t>(), S.stri.as<uint32_t>(), N, d_tris,
-                                                    B->tris.as<rt_triangle>(), B->prim.as<uint32_t>(), cap, status);
+                                                    B->tris.as<rt_triangle>(), B->prim.as<uint32_t>(), cap, d_verts,
+                                                    n_roots == 0 ? B->tripos.as<float4>() : nullptr, status);
         count_launch();
         if (n_roots > 0)
         {
@@ -965,7 +978,7 @@ int build_typed(rt_bvh* B, const rt_vertex* d_verts, uint32_t V, const rt_triang
         if (int e = emit_all()) { return e; }
         prof_mark(B, 5, st);
         // traversal layout from the device-side counts: the build's only host round trip follows
-        if (int e = launch_traversal_layout(B, st, 2 * cap - 1, cap, counters + 4, status)) { return e; }
+        if (int e = launch_traversal_layout(B, st, 2 * cap - 1, cap, counters + 4, status, n_roots == 0)) { return e; }
         if (batch)
         {
             if (int e = launch_scene_roots(B, bt.S, counters + 4, status, st)) { return e; }
@@ -1037,7 +1050,8 @@ int build_bvh_batch(rt_bvh* B, const rt_vertex* d_verts, uint32_t V, const rt_tr
     uint32_t cap = (uint32_t)((float)N * cfg.spatial_mult);  // bvh_morton.cpp:46-47
     if (cap < N) { cap = N; }
     const size_t max_nodes = (size_t)cap * 2 - 1;  // bvh_bfs.cpp:58
-    if (B->nodes.ensure(max_nodes * sizeof(rt_bvh_node)) || B->tris.ensure((size_t)cap * sizeof(rt_triangle)) ||
+    if (B->tripos.ensure((size_t)cap * 48) ||  // written by k_emit_tris in builds without SAH subtrees
+        B->nodes.ensure(max_nodes * sizeof(rt_bvh_node)) || B->tris.ensure((size_t)cap * sizeof(rt_triangle)) ||
         B->prim.ensure((size_t)cap * 4) || B->verts.ensure((size_t)V * sizeof(rt_vertex)))
     {
         return RT_E_CUDA;
