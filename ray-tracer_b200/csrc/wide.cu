@@ -1,7 +1,8 @@
 // wide.cu -- the 8-wide traversal layout: the baked binary tree collapsed into 128-byte nodes
-// of up to eight children with child boxes quantised to 8 bits per plane against the node's
-// own box (the compressed wide BVH of Ylitie, Karras and Laine, HPG 2017, in a simpler form:
-// explicit child references, no octant slot order).
+// of up to eight children with child boxes quantised to 8 bits per plane against the union of
+// the children's boxes, children placed in octant slots (after the compressed wide BVH of
+// Ylitie, Karras and Laine, HPG 2017, in a simpler form: explicit child references, a greedy
+// slot assignment).
 //
 // Which binary nodes become wide nodes: the root, every inner node whose depth is a multiple
 // of three, and every scene root of a batched build. A wide node's children are found by
