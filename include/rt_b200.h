@@ -142,8 +142,9 @@ void rt_bvh_free(rt_bvh* bvh);
  * handle; rt_trace and the wavefront path tracer's trace stage use it (the plain per-pixel
  * renderer keeps the binary loop). It is not the reference's visiting
  * order: the closest hit's distance is the same, but on an exact tie in distance the reported
- * triangle may differ, and a triangle that an exact box test loses by rounding at a box face
- * may be found. */
+ * triangle may differ, and a triangle that the binary boxes cull -- one an exact box test
+ * loses by rounding at a face, or, in trees with spatial splits, one outside a collapsed
+ * intermediate node's box -- may be found. */
 int rt_bvh_trace_loop(rt_bvh* bvh, int form);
 /* The wide layout of a handle in form 2 (no counterpart in the reference): *n_wide nodes of
  * 128 bytes each -- {float p[3]; uint32 meta (x / y / z scale exponents in bits 0-23, inner-
