@@ -275,8 +275,10 @@ __device__ __forceinline__ THit trace_ray_ww(const TraceCtx& T, const TraceRoot&
 // axis -- and each step takes the next child from the top entry: a leaf's triangles are tested
 // in order, an inner child is visited. The closest hit's distance is that of the binary
 // traversal; on an exact tie in distance the triangle found first may differ, since the
-// visiting order differs, and the conservative child boxes may admit a triangle that an exact
-// box test rejects by rounding at a face. Not the reference's order: an opt-in form.
+// visiting order differs, and a triangle the binary boxes cull may be found: the conservative
+// child boxes admit one an exact box test rejects by rounding at a face, and the boxes of the
+// collapsed binary levels are not tested (with spatial splits they need not contain their
+// children's). Not the reference's order: an opt-in form.
 template <int MODE, int STK>
 __device__ __forceinline__ THit trace_ray_wide(const TraceCtx& T, const TraceRoot& R, rtd::f3 o, rtd::f3 d, float tmin,
                                                float tmax)
