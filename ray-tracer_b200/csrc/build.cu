@@ -770,9 +770,12 @@ __global__ void __launch_bounds__(256) k_scan2_apply(Scan2 S, uint32_t n, const 
 __global__ void __launch_bounds__(BLK)
 k_clear(uint32_t n, uint32_t* __restrict__ parent, unsigned long long* __restrict__ visit, uint32_t* __restrict__ wnode,
         uint32_t* __restrict__ wtri, uint8_t* __restrict__ kpos, uint32_t* __restrict__ scene, uint32_t n_scene_boxes,
-        uint32_t* __restrict__ hist, uint32_t* __restrict__ counters, uint32_t* __restrict__ status)
+        uint32_t* __restrict__ hist, uint32_t* __restrict__ counters, uint32_t* __restrict__ status,
+        uint32_t* __restrict__ lookback, uint32_t n_lookback, uint32_t* __restrict__ tile_counters)
 {
     const uint32_t i = blockIdx.x * BLK + threadIdx.x;
+    if (i < n_lookback) { lookback[i] = 0u; }  // the radix sort's look-back words (all its passes)
+    if (i < 64) { tile_counters[i] = 0u; }
     if (i < 2 * n - 1) { parent[i] = NONE; }
     if (i < n) { visit[i] = ~0ull; kpos[i] = 0u; }
     if (i <= n) { wnode[i] = 0u; wtri[i] = 0u; }
@@ -811,13 +814,17 @@ int build_typed(rt_bvh* B, const rt_vertex* d_verts, uint32_t V, const rt_triang
     {
         return RT_E_CUDA;
     }
-    uint32_t* status = S.status.as<uint32_t>();
     uint32_t* counters = S.counters.as<uint32_t>();
+    uint32_t* status = counters + 15;  // read back with the counters in one copy
+    // the sort's scratch, zeroed by k_clear below (radix_sort_pairs then skips its memsets)
+    const size_t n_lookback = sort_lookback_words(N, passes);
+    if (S.sort.lookback.ensure(n_lookback * 4) || S.sort.tile_counters.ensure((64 + 260) * 4)) { return RT_E_CUDA; }
 
     prof_mark(B, 0, st);
-    k_clear<<<blocks_for(std::max<uint32_t>(nk + 1, 6 * n_boxes)), BLK, 0, st>>>(
+    k_clear<<<blocks_for(std::max<uint32_t>(std::max<uint32_t>(nk + 1, 6 * n_boxes), (uint32_t)n_lookback)), BLK, 0, st>>>(
         N, S.parent.as<uint32_t>(), S.visit.as<unsigned long long>(), S.wnode.as<uint32_t>(), S.wtri.as<uint32_t>(),
-        S.bnd.as<uint8_t>(), S.scene.as<uint32_t>(), n_boxes, S.hist.as<uint32_t>(), counters, status);
+        S.bnd.as<uint8_t>(), S.scene.as<uint32_t>(), n_boxes, S.hist.as<uint32_t>(), counters, status,
+        S.sort.lookback.as<uint32_t>(), (uint32_t)n_lookback, S.sort.tile_counters.as<uint32_t>());
     count_launch();
     k_vertices<<<blocks_for(V), BLK, 0, st>>>(d_verts, B->verts.as<rt_vertex>(), V);
     count_launch();
@@ -849,7 +856,7 @@ int build_typed(rt_bvh* B, const rt_vertex* d_verts, uint32_t V, const rt_triang
     uint32_t* perm = nullptr;
     if (int e = radix_sort_pairs<K>(S.keys.as<K>(), S.vals.as<uint32_t>(), true, N, key_bits, S.hist.as<uint32_t>(),
                                     msd_shift >= 0 ? S.hist.as<uint32_t>() + 8 * 256 : nullptr, S.sort, status, st,
-                                    &skeys, &perm))
+                                    &skeys, &perm, true))
     {
         return e;
     }
@@ -957,7 +964,7 @@ int build_typed(rt_bvh* B, const rt_vertex* d_verts, uint32_t V, const rt_triang
     // and redone in the rare case such runs exist, which saves a host round trip.
     const bool expect_sah = cfg.lbvh_threshold > cfg.max_leaf;
     if (batch) { RT_CUDA(cudaMemsetAsync(B->scene_info.p, 0xff, (size_t)bt.S * 16, st)); }
-    uint32_t res[8];
+    uint32_t res[16];  // counters[0..15]; [15] is the status word
     uint32_t stat = 0;
     for (int attempt = 0; attempt < 2; attempt++)
     {
@@ -986,9 +993,9 @@ int build_typed(rt_bvh* B, const rt_vertex* d_verts, uint32_t V, const rt_triang
             RT_CUDA(cudaMemcpyAsync(B->scene_info_host.data(), B->scene_info.p, (size_t)bt.S * 16, cudaMemcpyDeviceToHost, st));
         }
         prof_mark(B, 6, st);
-        RT_CUDA(cudaMemcpyAsync(res, counters, 32, cudaMemcpyDeviceToHost, st));
-        RT_CUDA(cudaMemcpyAsync(&stat, status, 4, cudaMemcpyDeviceToHost, st));
+        RT_CUDA(cudaMemcpyAsync(res, counters, 64, cudaMemcpyDeviceToHost, st));
         RT_CUDA(cudaStreamSynchronize(st));
+        stat = res[15];
         if (expect_sah || res[0] == 0) { break; }
         n_roots = res[0];  // identical-code runs found: build their SAH subtrees and emit again
     }

@@ -243,12 +243,16 @@ constexpr size_t onesweep_smem()
 template <typename K, int IPT, int MINB>
 int onesweep_passes(K* keys, uint32_t* vals, bool vals_identity, uint32_t n, int passes, const uint32_t* hist, K* keys_alt,
                     uint32_t* vals_alt, uint32_t* lookback, uint32_t* tile_counters, uint32_t* status, cudaStream_t st,
-                    K** keys_out, uint32_t** vals_out, const uint32_t* skip = nullptr, uint32_t skip_if = 0)
+                    K** keys_out, uint32_t** vals_out, const uint32_t* skip = nullptr, uint32_t skip_if = 0,
+                    bool zeroed = false)
 {
     constexpr uint32_t tile = RS_BLOCK * IPT;
     const uint32_t tiles = (n + tile - 1) / tile;
-    RT_CUDA(cudaMemsetAsync(lookback, 0, (size_t)passes * tiles * 256 * 4, st));
-    RT_CUDA(cudaMemsetAsync(tile_counters, 0, 64 * 4, st));
+    if (!zeroed)
+    {
+        RT_CUDA(cudaMemsetAsync(lookback, 0, (size_t)passes * tiles * 256 * 4, st));
+        RT_CUDA(cudaMemsetAsync(tile_counters, 0, 64 * 4, st));
+    }
     constexpr size_t smem = onesweep_smem<K, IPT>();
     static std::atomic<bool> attr_set{ false };  // per instantiation (bakes may run on several host threads)
     if (!attr_set)
@@ -453,7 +457,7 @@ size_t sort_lookback_words(uint32_t n, int passes)
 template <typename K>
 int radix_sort_pairs(K* keys, uint32_t* vals, bool vals_identity, uint32_t n, int key_bits, const uint32_t* hist,
                      const uint32_t* msd_hist, SortScratch& s, uint32_t* status, cudaStream_t st, K** keys_out,
-                     uint32_t** vals_out)
+                     uint32_t** vals_out, bool scratch_zeroed)
 {
     *keys_out = keys;
     *vals_out = vals;
@@ -499,8 +503,13 @@ int radix_sort_pairs(K* keys, uint32_t* vals, bool vals_identity, uint32_t n, in
             K* kfin = (passes & 1) ? kalt : keys;
             uint32_t* vfin = (passes & 1) ? valt : vals;
             const int npass = sort_passes(key_bits - 8);
-            RT_CUDA(cudaMemsetAsync(s.lookback.as<uint32_t>(), 0, (size_t)tiles * 256 * 4, st));
-            RT_CUDA(cudaMemsetAsync(s.tile_counters.as<uint32_t>() + 63, 0, 4, st));
+            // either this pass or the LSD passes use the look-back words (the flag picks one), so
+            // one zeroing serves both
+            if (!scratch_zeroed)
+            {
+                RT_CUDA(cudaMemsetAsync(s.lookback.as<uint32_t>(), 0, (size_t)tiles * 256 * 4, st));
+                RT_CUDA(cudaMemsetAsync(s.tile_counters.as<uint32_t>() + 63, 0, 4, st));
+            }
             k_msd_check<<<1, 256, 0, st>>>(msd_hist, n, small ? cap_small : cap_large, bstart, flag);
             k_onesweep<K, 16, 2><<<tiles, RS_BLOCK, smem, st>>>(keys, vals, vals_identity ? 1 : 0, kalt, valt, n, tiles,
                                                                 key_bits - 8, msd_hist, s.tile_counters.as<uint32_t>() + 63,
@@ -520,16 +529,17 @@ int radix_sort_pairs(K* keys, uint32_t* vals, bool vals_identity, uint32_t n, in
         }
         return onesweep_passes<K, 16, 2>(keys, vals, vals_identity, n, passes, hist, s.keys_alt.as<K>(), s.vals_alt.as<uint32_t>(),
                                          s.lookback.as<uint32_t>(), s.tile_counters.as<uint32_t>(), status, st, keys_out,
-                                         vals_out, msd ? flag : nullptr, 0u);
+                                         vals_out, msd ? flag : nullptr, 0u, scratch_zeroed);
     }
     return onesweep_passes<K, 8, 5>(keys, vals, vals_identity, n, passes, hist, s.keys_alt.as<K>(), s.vals_alt.as<uint32_t>(),
-                                    s.lookback.as<uint32_t>(), s.tile_counters.as<uint32_t>(), status, st, keys_out, vals_out);
+                                    s.lookback.as<uint32_t>(), s.tile_counters.as<uint32_t>(), status, st, keys_out, vals_out,
+                                    nullptr, 0u, scratch_zeroed);
 }
 
 template int radix_sort_pairs<uint64_t>(uint64_t*, uint32_t*, bool, uint32_t, int, const uint32_t*, const uint32_t*,
-                                        SortScratch&, uint32_t*, cudaStream_t, uint64_t**, uint32_t**);
+                                        SortScratch&, uint32_t*, cudaStream_t, uint64_t**, uint32_t**, bool);
 template int radix_sort_pairs<uint32_t>(uint32_t*, uint32_t*, bool, uint32_t, int, const uint32_t*, const uint32_t*,
-                                        SortScratch&, uint32_t*, cudaStream_t, uint32_t**, uint32_t**);
+                                        SortScratch&, uint32_t*, cudaStream_t, uint32_t**, uint32_t**, bool);
 
 } // namespace rtb
 
