@@ -27,7 +27,13 @@ int fail(int code, const std::string& msg)
     g_err = msg;
     return code;
 }
-void count_launch(uint64_t n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+static thread_local uint64_t t_launches = 0;
+void count_launch(uint64_t n)
+{
+    g_launches.fetch_add(n, std::memory_order_relaxed);
+    t_launches += n;
+}
+uint64_t thread_launches() { return t_launches; }
 int check_launch(const char* what)
 {
     cudaError_t e = cudaGetLastError();
@@ -127,6 +133,12 @@ static void free_bvh(rt_bvh* b)
         if (e) { cudaEventDestroy(e); e = nullptr; }
     }
     if (b->wf_stream) { cudaStreamDestroy(b->wf_stream); b->wf_stream = nullptr; }
+    if (b->bake_exec) { cudaGraphExecDestroy(b->bake_exec); b->bake_exec = nullptr; }
+    for (cudaEvent_t& e : b->bake_ev)
+    {
+        if (e) { cudaEventDestroy(e); e = nullptr; }
+    }
+    if (b->bake_stream) { cudaStreamDestroy(b->bake_stream); b->bake_stream = nullptr; }
     for (cudaEvent_t& e : b->ev)
     {
         if (e) { cudaEventDestroy(e); e = nullptr; }

@@ -28,6 +28,7 @@ int  fail(int code, const std::string& msg);
 
 // Counts this library's kernel launches (rt_kernel_launches()).
 void count_launch(uint64_t n = 1);
+uint64_t thread_launches();  // launches counted by the calling host thread
 // Checks the last launch; returns RT_OK or RT_E_CUDA.
 int  check_launch(const char* what);
 
@@ -167,6 +168,16 @@ struct rt_bvh
     rtb::DevBuf  wf_scene[2], wf_cams;      // scene of each queued ray; per-scene cameras
     cudaStream_t wf_stream = nullptr;       // the graph replays here, fenced by wf_ev
     cudaEvent_t  wf_ev[2] = { nullptr, nullptr };
+    // an LBVH bake's launch sequence, captured on the second call with the same key (sizes,
+    // settings, inputs, buffer addresses) and replayed on bake_stream (fenced with the caller's
+    // stream by bake_ev); its key, and the key the last plain bake left
+    cudaGraphExec_t bake_exec = nullptr;
+    std::vector<unsigned char> bake_key, bake_seen;
+    uint64_t     bake_kernels = 0;
+    void*        bake_skeys = nullptr;      // where the captured sort left keys and permutation
+    uint32_t*    bake_perm = nullptr;
+    cudaStream_t bake_stream = nullptr;
+    cudaEvent_t  bake_ev[2] = { nullptr, nullptr };
     cudaGraphExec_t wf_exec = nullptr;      // the captured launch sequence and its key
     std::vector<unsigned char> wf_key;
     uint32_t     wf_kernels = 0;
