@@ -82,6 +82,24 @@ def test_rebuild_reuses_handle(orc):
         assert_same_tree(b.download(), orc.build(v, t, orc_cfg("lbvh63")), f"rebuild {name}")
 
 
+def test_rebuild_replays_with_new_contents(orc):
+    """Bakes of one size from the same device buffers replay a captured launch graph from the
+    third bake on; new contents in those buffers give the new tree every time."""
+    import torch
+    (v1, t1), (v2, t2) = scenes.soup(20000, seed=91), scenes.soup(20000, seed=92)
+    dv = torch.from_numpy(v1).cuda()
+    dt = torch.from_numpy(t1.view(np.int32)).cuda()
+    b = rtb200.Bvh.build(dv, dt, "lbvh63")
+    for k in range(5):
+        v, t = (v1, t1) if k % 2 == 0 else (v2, t2)
+        dv.copy_(torch.from_numpy(v))
+        dt.copy_(torch.from_numpy(t.view(np.int32)))
+        torch.cuda.synchronize()
+        b.rebuild(dv, dt, "lbvh63")
+        assert_same_tree(b.download(), orc.build(v, t, orc_cfg("lbvh63")), f"bake {k}")
+        assert np.array_equal(t[b.prim_ids()], b.download()[1])
+
+
 def test_errors_are_reported():
     v, t = SCENES["soup2k"]
     bad = t.copy()
