@@ -404,7 +404,7 @@ __device__ __forceinline__ bool split_lower(const K* __restrict__ keys, uint32_t
 //  k_climb_global  one thread per frontier node continues with global slots and device-scope
 //                  release / acquire fences (about depth x tiles nodes instead of all n - 1).
 // Both phases take the same parent for every node, so the tree is the one-pass tree.
-constexpr int CL_T = 1024;
+constexpr int CL_T = 256;
 constexpr unsigned long long CL_DONE = ~0ull - 1ull;
 
 // Shared memory of k_climb_local: exchange slots, boxes of the tile's inner nodes and leaves
