@@ -114,7 +114,7 @@ def test_errors_are_reported():
 
 @pytest.mark.parametrize("preset", ["lbvh63", "lbvh30", "hybrid", "sah4", "sah16"])
 def test_large_odd_soup_matches_oracle(orc, preset):
-    """262,147 triangles: 257 tiles of the local tree phase (the last one partial), frontier
+    """262,147 triangles: 1,025 tiles of the local tree phase (the last one partial), frontier
     nodes on every tile edge; for the SAH presets the top levels' nodes above 16,384
     references, which many blocks evaluate at once."""
     v, t = scenes.soup(262147, seed=77)
