@@ -203,7 +203,7 @@ def run_reference(a):
     import multiprocessing as mp
     cores = os.cpu_count() or 1
     sample = 1 << 17
-    per = max(1, (a.steps + cores - 1) // cores)
+    per = max(3, (a.steps + cores - 1) // cores)  # bakes per process
     # one process per host core (the bake's state is process-global); the timed bakes of all
     # processes start together after their set-up, and the slowest one's time is the wall
     ctx = mp.get_context("spawn")
