@@ -823,6 +823,9 @@ int build_typed(rt_bvh* B, const rt_vertex* d_verts, uint32_t V, const rt_triang
     K* skeys = nullptr;
     uint32_t* perm = nullptr;
     const uint32_t tm = std::max(cfg.max_leaf, cfg.lbvh_threshold);
+    // a captured bake leaves the sort's LSD fallback out and reports in counters[14] whether it
+    // was needed (a top-digit bucket over one block); such a bake is then done again plainly
+    bool msd_only = false;
     // everything up to the boundary nodes, enqueued on st
     auto front = [&]() -> int {
         prof_mark(B, 0, st);
@@ -859,7 +862,7 @@ int build_typed(rt_bvh* B, const rt_vertex* d_verts, uint32_t V, const rt_triang
         prof_mark(B, 1, st);
         if (int e = radix_sort_pairs<K>(S.keys.as<K>(), S.vals.as<uint32_t>(), true, N, key_bits, S.hist.as<uint32_t>(),
                                         msd_shift >= 0 ? S.hist.as<uint32_t>() + 8 * 256 : nullptr, S.sort, status, st,
-                                        &skeys, &perm, true))
+                                        &skeys, &perm, true, msd_only ? counters + 14 : nullptr))
         {
             return e;
         }
@@ -1024,8 +1027,10 @@ int build_typed(rt_bvh* B, const rt_vertex* d_verts, uint32_t V, const rt_triang
                 st = B->bake_stream;  // the lambdas enqueue on st
                 RT_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
                 const uint64_t l0 = thread_launches();
+                msd_only = true;
                 int e = front();
                 if (!e) { e = tail(); }
+                msd_only = false;
                 cudaGraph_t g = nullptr;
                 const cudaError_t ce = cudaStreamEndCapture(st, &g);
                 st = caller;
@@ -1082,6 +1087,15 @@ int build_typed(rt_bvh* B, const rt_vertex* d_verts, uint32_t V, const rt_triang
         }
         RT_CUDA(cudaMemcpyAsync(res, counters, 64, cudaMemcpyDeviceToHost, st));
         RT_CUDA(cudaStreamSynchronize(st));
+        if (attempt == 0 && enq0 && res[14] != 0u)
+        {
+            // the replayed launches have no LSD fallback and a bucket overflowed: bake plainly
+            enq0 = false;
+            if (int e = front()) { return e; }
+            if (int e = tail()) { return e; }
+            RT_CUDA(cudaMemcpyAsync(res, counters, 64, cudaMemcpyDeviceToHost, st));
+            RT_CUDA(cudaStreamSynchronize(st));
+        }
         stat = res[15];
         if (graph_path && attempt == 0 && !enq0) { B->bake_seen = bake_key(); }  // with this bake's buffers
         if (expect_sah || res[0] == 0) { break; }

@@ -292,7 +292,7 @@ constexpr int LS_LARGE_B = 512, LS_LARGE_I = 16;  // 8,192 keys, one block per S
 // *flag = 1 when a bucket exceeds cap (the LSD passes must run), else 0.
 __global__ void __launch_bounds__(256)
 k_msd_check(const uint32_t* __restrict__ hist_top, uint32_t n, uint32_t cap, uint32_t* __restrict__ bstart,
-            uint32_t* __restrict__ flag)
+            uint32_t* __restrict__ flag, uint32_t* __restrict__ flag_copy)
 {
     __shared__ uint32_t ws[RS_WARPS];
     __shared__ uint32_t s_big;
@@ -302,7 +302,12 @@ k_msd_check(const uint32_t* __restrict__ hist_top, uint32_t n, uint32_t cap, uin
     if (h > cap) { atomicOr(&s_big, 1u); }
     const uint32_t ex = block_excl_scan_256(h, ws, nullptr);
     bstart[threadIdx.x] = ex;
-    if (threadIdx.x == 0) { bstart[256] = n; *flag = s_big; }
+    if (threadIdx.x == 0)
+    {
+        bstart[256] = n;
+        *flag = s_big;
+        if (flag_copy) { *flag_copy = s_big; }
+    }
 }
 
 template <typename K, int LB, int LI>
@@ -457,7 +462,7 @@ size_t sort_lookback_words(uint32_t n, int passes)
 template <typename K>
 int radix_sort_pairs(K* keys, uint32_t* vals, bool vals_identity, uint32_t n, int key_bits, const uint32_t* hist,
                      const uint32_t* msd_hist, SortScratch& s, uint32_t* status, cudaStream_t st, K** keys_out,
-                     uint32_t** vals_out, bool scratch_zeroed)
+                     uint32_t** vals_out, bool scratch_zeroed, uint32_t* msd_only_flag)
 {
     *keys_out = keys;
     *vals_out = vals;
@@ -510,7 +515,7 @@ int radix_sort_pairs(K* keys, uint32_t* vals, bool vals_identity, uint32_t n, in
                 RT_CUDA(cudaMemsetAsync(s.lookback.as<uint32_t>(), 0, (size_t)tiles * 256 * 4, st));
                 RT_CUDA(cudaMemsetAsync(s.tile_counters.as<uint32_t>() + 63, 0, 4, st));
             }
-            k_msd_check<<<1, 256, 0, st>>>(msd_hist, n, small ? cap_small : cap_large, bstart, flag);
+            k_msd_check<<<1, 256, 0, st>>>(msd_hist, n, small ? cap_small : cap_large, bstart, flag, msd_only_flag);
             k_onesweep<K, 16, 2><<<tiles, RS_BLOCK, smem, st>>>(keys, vals, vals_identity ? 1 : 0, kalt, valt, n, tiles,
                                                                 key_bits - 8, msd_hist, s.tile_counters.as<uint32_t>() + 63,
                                                                 s.lookback.as<uint32_t>(), status, flag, 1u);
@@ -526,6 +531,12 @@ int radix_sort_pairs(K* keys, uint32_t* vals, bool vals_identity, uint32_t n, in
             }
             count_launch(3);
             RT_CUDA(cudaGetLastError());
+            if (msd_only_flag)  // no LSD fallback: the caller reads *msd_only_flag and sorts again if set
+            {
+                *keys_out = kfin;
+                *vals_out = vfin;
+                return RT_OK;
+            }
         }
         return onesweep_passes<K, 16, 2>(keys, vals, vals_identity, n, passes, hist, s.keys_alt.as<K>(), s.vals_alt.as<uint32_t>(),
                                          s.lookback.as<uint32_t>(), s.tile_counters.as<uint32_t>(), status, st, keys_out,
@@ -537,9 +548,9 @@ int radix_sort_pairs(K* keys, uint32_t* vals, bool vals_identity, uint32_t n, in
 }
 
 template int radix_sort_pairs<uint64_t>(uint64_t*, uint32_t*, bool, uint32_t, int, const uint32_t*, const uint32_t*,
-                                        SortScratch&, uint32_t*, cudaStream_t, uint64_t**, uint32_t**, bool);
+                                        SortScratch&, uint32_t*, cudaStream_t, uint64_t**, uint32_t**, bool, uint32_t*);
 template int radix_sort_pairs<uint32_t>(uint32_t*, uint32_t*, bool, uint32_t, int, const uint32_t*, const uint32_t*,
-                                        SortScratch&, uint32_t*, cudaStream_t, uint32_t**, uint32_t**, bool);
+                                        SortScratch&, uint32_t*, cudaStream_t, uint32_t**, uint32_t**, bool, uint32_t*);
 
 } // namespace rtb
 

@@ -100,6 +100,25 @@ def test_rebuild_replays_with_new_contents(orc):
         assert np.array_equal(t[b.prim_ids()], b.download()[1])
 
 
+def test_replayed_bake_sorts_clustered_keys(orc):
+    """A replayed bake leaves the sort's LSD fallback out; when new contents put more keys in a
+    top-digit bucket than one block sorts, the bake is done again launch by launch, so the tree
+    is still the oracle's."""
+    import torch
+    n = 200_000
+    vu, tu = scenes.soup(n, seed=93)
+    vc, tc = clustered_soup(n, seed=94)
+    dv = torch.from_numpy(vu).cuda()
+    dt = torch.from_numpy(tu.view(np.int32)).cuda()
+    b = rtb200.Bvh.build(dv, dt, "lbvh63")
+    for k, (v, t) in enumerate([(vu, tu)] * 3 + [(vc, tc), (vu, tu), (vc, tc)]):
+        dv.copy_(torch.from_numpy(v))
+        dt.copy_(torch.from_numpy(t.view(np.int32)))
+        torch.cuda.synchronize()
+        b.rebuild(dv, dt, "lbvh63")
+        assert_same_tree(b.download(), orc.build(v, t, orc_cfg("lbvh63")), f"bake {k}")
+
+
 def test_errors_are_reported():
     v, t = SCENES["soup2k"]
     bad = t.copy()
