@@ -57,10 +57,11 @@ cudaStream_t default_stream();
 int          device_sm_count();
 
 // ---- radix sort (radix_sort.cu) ---------------------------------------------------------
-// Stable LSD onesweep sort of `n` keys with uint32 values by their low `key_bits` bits.
-// Histograms of all digit passes must already be in `hist` (256 counters per pass, built
-// by the producer of the keys). keys/vals are ping-ponged: the sorted result ends in the
-// buffer returned through *keys_out / *vals_out.
+// Stable sort of `n` keys with uint32 values by their low `key_bits` bits: onesweep LSD
+// passes, or up to 2^21 keys an MSD pass on the top digit and a per-bucket sort in shared
+// memory (radix_sort_pairs). Histograms of all digit passes must already be in `hist` (256
+// counters per pass, built by the producer of the keys). keys/vals are ping-ponged: the
+// sorted result ends in the buffer returned through *keys_out / *vals_out.
 struct SortScratch
 {
     DevBuf keys_alt, vals_alt, lookback, tile_counters;
