@@ -289,7 +289,9 @@ int rt_autotune_wavefront(rt_bvh* bvh, const rt_render_cfg* cfgs, uint32_t n_sce
  *   RT_E_CAPACITY; use rt_build). The first call on a device looks up the scratch array's
  *   device address (cudaGetSymbolAddress); make that first call before any stream capture.
  *   Every call shares the one scratch array, so calls whose work overlaps on the GPU
- *   (different streams or threads at once) race and must be serialised by the caller. */
+ *   (different streams or threads at once) race and must be serialised by the caller. Each
+ *   call reads the kernels' status word back and synchronises `stream` before returning, so
+ *   perm_out is complete when it returns RT_OK. */
 #define RT_NOALLOC_MAX_TRIS 65536u
 int rt_morton_order_noalloc(const rt_vertex* verts, uint32_t n_verts, const rt_triangle* tris, uint32_t n_tris,
                             uint32_t morton_bits, uint32_t* perm_out, void* stream);
@@ -331,6 +333,9 @@ const char* rt_last_error(void);     /* thread-local text of the last failure */
 const char* rt_version(void);
 /* Number of this library's kernels launched so far in this process (all devices). */
 uint64_t    rt_kernel_launches(void);
+/* Number of device allocations (cudaMalloc) this library has made so far in this process (all
+ * devices): handles grow their buffers on demand, so a steady-state rebuild adds none. */
+uint64_t    rt_device_allocations(void);
 int         rt_device_sync(void* stream);
 
 #ifdef __cplusplus

@@ -20,6 +20,7 @@ namespace rtb
 {
 static thread_local std::string g_err;
 static std::atomic<uint64_t> g_launches{ 0 };
+static std::atomic<uint64_t> g_allocs{ 0 };
 
 void set_error(const std::string& msg) { g_err = msg; }
 int fail(int code, const std::string& msg)
@@ -34,6 +35,7 @@ void count_launch(uint64_t n)
     t_launches += n;
 }
 uint64_t thread_launches() { return t_launches; }
+void count_alloc() { g_allocs.fetch_add(1, std::memory_order_relaxed); }
 int check_launch(const char* what)
 {
     cudaError_t e = cudaGetLastError();
@@ -54,6 +56,7 @@ int DevBuf::ensure(size_t n)
         return RT_E_CUDA;
     }
     bytes = want;
+    count_alloc();
     return 0;
 }
 void DevBuf::release()
@@ -182,6 +185,7 @@ void rt_build_cfg_default(rt_build_cfg* c)
 const char* rt_last_error(void) { return g_err.c_str(); }
 const char* rt_version(void) { return "rt_b200 1.0 (sm_100a)"; }
 uint64_t rt_kernel_launches(void) { return g_launches.load(); }
+uint64_t rt_device_allocations(void) { return g_allocs.load(); }
 
 int rt_device_sync(void* stream)
 {

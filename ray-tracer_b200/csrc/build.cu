@@ -871,12 +871,14 @@ int build_typed(rt_bvh* B, const rt_vertex* d_verts, uint32_t V, const rt_triang
         {
             // the frontier list lives in the rank array, which k_boundary fills only afterwards
             uint32_t* frontier = S.rank.as<uint32_t>();
-            static std::atomic<bool> cl_attr{ false };  // per key type (bakes may run on several host threads)
-            if (!cl_attr)
+            static PerDeviceOnce cl_attr;  // per key type and device (bakes may run on several host threads and GPUs)
+            if (int e = cl_attr.once([] {
+                    RT_CUDA(cudaFuncSetAttribute(k_climb_local<K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                 (int)climb_local_smem<K>()));
+                    return (int)RT_OK;
+                }))
             {
-                RT_CUDA(cudaFuncSetAttribute(k_climb_local<K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)climb_local_smem<K>()));
-                cl_attr = true;
+                return e;
             }
             k_climb_local<K><<<blocks_for(N, CL_T), CL_T, climb_local_smem<K>(), st>>>(skeys, perm, N, S.tri_lo.as<float4>(), S.tri_hi.as<float4>(),
                                                                    S.knode.as<uint4>(), S.parent.as<uint32_t>(),
@@ -1199,7 +1201,7 @@ namespace
 {
 
 constexpr uint32_t NA_MAX_TRIS = RT_NOALLOC_MAX_TRIS;
-constexpr uint32_t NA_TILES = (NA_MAX_TRIS + 4095) / 4096;  // onesweep tiles of 4096 keys
+constexpr uint32_t NA_TILES = (NA_MAX_TRIS + rtb::RS_SMALL_TILE_KEYS - 1) / rtb::RS_SMALL_TILE_KEYS;  // onesweep tiles
 constexpr size_t NA_OFF_LO = 0;
 constexpr size_t NA_OFF_HI = NA_OFF_LO + 16ull * NA_MAX_TRIS;
 constexpr size_t NA_OFF_CZ = NA_OFF_HI + 16ull * NA_MAX_TRIS;
@@ -1211,6 +1213,9 @@ constexpr size_t NA_OFF_LB = NA_OFF_HIST + 8ull * 256 * 4;
 constexpr size_t NA_OFF_TILE = NA_OFF_LB + 8ull * NA_TILES * 256 * 4;
 constexpr size_t NA_OFF_SMALL = NA_OFF_TILE + 64 * 4;  // scene box, counters, status
 constexpr size_t NA_BYTES = NA_OFF_SMALL + 256;
+static_assert(NA_MAX_TRIS <= rtb::RS_SMALL_MAX_KEYS, "the fixed-scratch sort takes at most RS_SMALL_MAX_KEYS keys");
+static_assert(NA_OFF_TILE - NA_OFF_LB >= 4 * rtb::sort_raw_lookback_words(NA_MAX_TRIS, 8),
+              "look-back region too small for the sort's tiles");
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[NA_BYTES];
 

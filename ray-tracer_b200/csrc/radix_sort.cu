@@ -19,7 +19,7 @@ constexpr int      RS_WARPS   = RS_BLOCK / 32;
 // Two tile shapes: up to 2^21 keys, tiles of 16 keys per thread (4096) with 2 resident blocks
 // per SM; above, 8 keys per thread (2048) with 5 resident blocks per SM (48 registers), whose
 // extra occupancy hides the memory latency of the long passes.
-constexpr uint32_t RS_SMALL_MAX = 1u << 21;
+constexpr uint32_t RS_SMALL_MAX = RS_SMALL_MAX_KEYS;
 constexpr uint32_t LB_AGG     = 1u << 30;           // tile aggregate published
 constexpr uint32_t LB_PRE     = 2u << 30;           // inclusive prefix published
 constexpr uint32_t LB_VAL     = (1u << 30) - 1u;
@@ -254,11 +254,13 @@ int onesweep_passes(K* keys, uint32_t* vals, bool vals_identity, uint32_t n, int
         RT_CUDA(cudaMemsetAsync(tile_counters, 0, 64 * 4, st));
     }
     constexpr size_t smem = onesweep_smem<K, IPT>();
-    static std::atomic<bool> attr_set{ false };  // per instantiation (bakes may run on several host threads)
-    if (!attr_set)
+    static PerDeviceOnce attr;  // per instantiation and device (bakes may run on several host threads and GPUs)
+    if (int e = attr.once([] {
+            RT_CUDA(cudaFuncSetAttribute(k_onesweep<K, IPT, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            return (int)RT_OK;
+        }))
     {
-        RT_CUDA(cudaFuncSetAttribute(k_onesweep<K, IPT, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        attr_set = true;
+        return e;
     }
     K* kin = keys;
     K* kalt = keys_alt;
@@ -493,15 +495,17 @@ int radix_sort_pairs(K* keys, uint32_t* vals, bool vals_identity, uint32_t n, in
             constexpr size_t smem = onesweep_smem<K, 16>();
             constexpr size_t sm_small = local_sort_smem<K, LS_SMALL_B, LS_SMALL_I>();
             constexpr size_t sm_large = local_sort_smem<K, LS_LARGE_B, LS_LARGE_I>();
-            static std::atomic<bool> attr_set{ false };  // per key type
-            if (!attr_set)
+            static PerDeviceOnce attr;  // per key type and device
+            if (int e = attr.once([] {
+                    RT_CUDA(cudaFuncSetAttribute(k_onesweep<K, 16, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+                    RT_CUDA(cudaFuncSetAttribute(k_local_sort<K, LS_SMALL_B, LS_SMALL_I, 2>,
+                                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_small));
+                    RT_CUDA(cudaFuncSetAttribute(k_local_sort<K, LS_LARGE_B, LS_LARGE_I, 1>,
+                                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_large));
+                    return (int)RT_OK;
+                }))
             {
-                RT_CUDA(cudaFuncSetAttribute(k_onesweep<K, 16, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-                RT_CUDA(cudaFuncSetAttribute(k_local_sort<K, LS_SMALL_B, LS_SMALL_I, 2>,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_small));
-                RT_CUDA(cudaFuncSetAttribute(k_local_sort<K, LS_LARGE_B, LS_LARGE_I, 1>,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_large));
-                attr_set = true;
+                return e;
             }
             K* kalt = s.keys_alt.as<K>();
             uint32_t* valt = s.vals_alt.as<uint32_t>();
@@ -570,6 +574,7 @@ int radix_sort_pairs_raw(K* keys, uint32_t* vals, uint32_t n, int key_bits, cons
     if (n == 0) { return RT_OK; }
     const int passes = sort_passes(key_bits);
     if (n > RS_SMALL_MAX) { return fail(RT_E_CAPACITY, "radix sort on fixed scratch: at most 2^21 keys"); }
+    static_assert(RS_BLOCK * 16 == RS_SMALL_TILE_KEYS, "fixed-scratch callers size the look-back words by this tile");
     return onesweep_passes<K, 16, 2>(keys, vals, true, n, passes, hist, keys_alt, vals_alt, lookback, tile_counters, status, st,
                                      keys_out, vals_out);
 }

@@ -1,6 +1,7 @@
 // rt_internal.h -- internal declarations shared by the librt_b200 translation units.
 #pragma once
 
+#include <atomic>
 #include <cstddef>
 #include <cstdint>
 #include <string>
@@ -26,8 +27,33 @@ int  fail(int code, const std::string& msg);
         }                                                                                    \
     } while (0)
 
+// A setting made once per device. Function attributes (the dynamic shared-memory limit of a
+// kernel above 48 KB, for one) belong to the context of the device that was current when they
+// were set, so a process driving several GPUs sets them on each. once(f) runs f the first time
+// it is reached with a given current device (devices 64 and up: every time) and records the
+// device when f returns RT_OK; two host threads may both run f for the same device, which is
+// harmless for idempotent settings.
+class PerDeviceOnce
+{
+    std::atomic<uint64_t> done_{ 0 };
+
+public:
+    template <typename F> int once(F&& f)
+    {
+        int dev = 0;
+        RT_CUDA(cudaGetDevice(&dev));
+        const bool tracked = dev >= 0 && dev < 64;
+        if (tracked && ((done_.load(std::memory_order_acquire) >> dev) & 1ull)) { return RT_OK; }
+        if (int e = f()) { return e; }
+        if (tracked) { done_.fetch_or(1ull << dev, std::memory_order_acq_rel); }
+        return RT_OK;
+    }
+};
+
 // Counts this library's kernel launches (rt_kernel_launches()).
 void count_launch(uint64_t n = 1);
+// Counts this library's device allocations (rt_device_allocations()).
+void count_alloc();
 uint64_t thread_launches();  // launches counted by the calling host thread
 // Checks the last launch; returns RT_OK or RT_E_CUDA.
 int  check_launch(const char* what);
@@ -86,6 +112,15 @@ int radix_sort_pairs_raw(K* keys, uint32_t* vals, uint32_t n, int key_bits, cons
 inline int sort_passes(int key_bits) { return (key_bits + 7) / 8; }
 // Look-back words (passes x tiles x 256) a sort of n keys uses.
 size_t sort_lookback_words(uint32_t n, int passes);
+// Keys per tile of the onesweep passes up to RS_SMALL_MAX_KEYS keys (256 threads x 16 keys),
+// the shape radix_sort_pairs_raw always uses; above that size the tile is half as large.
+constexpr uint32_t RS_SMALL_TILE_KEYS = 4096;
+constexpr uint32_t RS_SMALL_MAX_KEYS = 1u << 21;
+// Look-back words of a radix_sort_pairs_raw sort of n keys (n <= RS_SMALL_MAX_KEYS).
+constexpr size_t sort_raw_lookback_words(uint32_t n, int passes)
+{
+    return (size_t)passes * ((n + RS_SMALL_TILE_KEYS - 1) / RS_SMALL_TILE_KEYS) * 256;
+}
 
 // Device-wide exclusive scan of uint32 (scan.cu is in build.cu); returns total through *d_total.
 struct ScanScratch { DevBuf partials; };

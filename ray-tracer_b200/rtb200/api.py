@@ -139,6 +139,7 @@ def lib():
         L.rt_last_error.restype = C.c_char_p
         L.rt_version.restype = C.c_char_p
         L.rt_kernel_launches.restype = u64
+        L.rt_device_allocations.restype = u64
         L.rt_device_sync.argtypes = [vp]
         L.rt_morton_order_noalloc.argtypes = [vp, u32, vp, u32, u32, vp, vp]
         _lib = L
@@ -163,6 +164,11 @@ def last_error() -> str:
 
 def kernel_launches() -> int:
     return int(lib().rt_kernel_launches())
+
+
+def device_allocations() -> int:
+    """Device allocations (cudaMalloc) the library has made so far in this process."""
+    return int(lib().rt_device_allocations())
 
 
 def make_cfg(preset: str = "hybrid", **kw) -> BuildCfg:

@@ -204,3 +204,18 @@ def test_download_async_on_a_stream(orc):
     assert np.array_equal(hn.numpy(), nodes.view(np.uint8))
     assert np.array_equal(ht.numpy(), tris.view(np.uint8).reshape(-1))
     assert np.array_equal(hv.numpy(), verts.view(np.uint8).reshape(-1))
+
+
+def test_build_on_every_visible_device(orc):
+    """Kernel attributes (the sort's and the climb's shared-memory limits above 48 KB) are
+    per-device settings: a bake on device 1 after device 0 in the same process must launch with
+    them set there too. Needs two visible GPUs."""
+    import torch
+    if torch.cuda.device_count() < 2:
+        pytest.skip("one visible GPU")
+    v, t = scenes.soup(300000, seed=41)  # MSD sort path with 63-bit keys, climb with its shared-memory tiles
+    ref = orc.build(v, t, orc_cfg("lbvh63"))
+    for dev in range(torch.cuda.device_count()):
+        with torch.cuda.device(dev):
+            b = rtb200.Bvh.build(torch.from_numpy(v).cuda(), torch.from_numpy(t.view(np.int32)).cuda(), "lbvh63")
+            assert_same_tree(b.download(), ref, f"device {dev}")
