@@ -40,11 +40,19 @@ N_TRIS = 1 << 20
 N_RAYS = 1 << 24
 METRIC = "BVH Mtri/s"
 WORKLOAD = "BVH build microbenchmark: 1,048,576-triangle soup, LBVH 63-bit Morton codes, leaf 16"
-# Algorithmic bytes of one LBVH 63-bit bake per triangle (V = 3N vertices; each array counted
-# once per read and once per write, per kernel): clear 30, vertex renormalisation 144, triangle
+# Algorithmic bytes per triangle of a minimal LBVH bake, the roofline's numerator: read the
+# triangles and positions once for the Morton codes (12 + 36 in, 8 + 4 out = 60), eight onesweep
+# passes over (key, index) pairs plus their histograms (8 x 24 + 8 = 200), the radix-tree
+# topology (8 key + 12 links = 20) and the box refit (48 triangle + 2 x 24 child + 24 out = 120):
+# 400 for 63-bit codes; with 30-bit codes the Morton step writes 4-byte keys (56) and the sort
+# takes four passes over 16-byte pairs (68), with a 16-byte topology: 260.
+ROOFLINE_BYTES_PER_TRI = {21: 400, 10: 260}
+# What this library's bake moves per triangle by its own count (each array once per read and
+# once per write, per kernel; V = 3N vertices): clear 30, vertex renormalisation 144, triangle
 # prep 84, Morton codes 20, radix tree with boxes 100, boundary 40, scans 24, .bvh nodes and
 # triangles 93, traversal layout 158; plus the sort: 44 up to 2^21 keys (top-digit onesweep
-# pass 20 + per-bucket pass 24), else 188 (eight onesweep passes).
+# pass 20 + per-bucket pass 24), else 188 (eight onesweep passes). It includes the outputs the
+# minimal count leaves out (renormalised normals, the .bvh layout, the traversal layout).
 BAKE_BYTES_PER_TRI_EXCL_SORT = 30 + 144 + 84 + 20 + 100 + 40 + 24 + 93 + 158
 
 
@@ -183,50 +191,56 @@ def cpu_reference_bake(n_tris: int, seed: int, reps: int):
     return n_tris / dt / 1e6, kind, dt
 
 
-def _ref_process(n, seed, reps, barrier, queue):
-    """One host core's share of the reference arm: set up (sample, library, one untimed bake),
-    wait for every process to be ready, then time `reps` bakes."""
+def _ref_process(n, seed, warmup, steps, barrier, queue):
+    """One host core's share of the reference arm: set up (soup, library), `warmup` untimed
+    bakes, wait for every process to be ready, then time `steps` bakes."""
     with quiet_stdout():
         fn, kind = _reference_bake_fn(n, seed)
-        fn()
-        barrier.wait(timeout=900)
+        for _ in range(warmup):
+            fn()
+        barrier.wait(timeout=1800)
         t0 = time.perf_counter()
-        for _ in range(reps):
+        for _ in range(steps):
             fn()
         queue.put((time.perf_counter() - t0, kind))
 
 
 def run_reference(a):
+    """The reference's own bake (bvh::bakeBVH with its LBVH constants, compiled from its sources
+    into oracle/_ref/lbvh63) of the same 1,048,576-triangle soup as this arm's N=1 line, on every
+    host core: one process per core, since the bake keeps its state in process globals and is
+    single-threaded. One step = one bake in every process at once; the wall time of the steps is
+    the slowest process's."""
     rank, world, _ = env_rank()
     if rank != 0:
         return 0
     import multiprocessing as mp
+    from rtb200 import scenes
     cores = os.cpu_count() or 1
-    sample = 1 << 17
-    per = max(3, (a.steps + cores - 1) // cores)  # bakes per process
-    # one process per host core (the bake's state is process-global); the timed bakes of all
-    # processes start together after their set-up, and the slowest one's time is the wall
+    n = a.n_tris
     ctx = mp.get_context("spawn")
     barrier, queue = ctx.Barrier(cores), ctx.Queue()
-    procs = [ctx.Process(target=_ref_process, args=(sample, 20261204 + i, per, barrier, queue)) for i in range(cores)]
+    procs = [ctx.Process(target=_ref_process, args=(n, scenes.BASE_SEED + 1, a.warmup, a.steps, barrier, queue))
+             for _ in range(cores)]
     for p_ in procs:
         p_.start()
-    res = [queue.get(timeout=1800) for _ in procs]
+    res = [queue.get(timeout=3600) for _ in procs]
     for p_ in procs:
         p_.join()
     wall = max(r[0] for r in res)
     kind = res[0][1]
-    total = sample * per * cores
-    value = total / wall / 1e6
+    value = n * a.steps * cores / wall / 1e6
     out = {"metric": METRIC, "value": round(value, 4), "unit": "Mtri/s", "impl": "reference", "n_gpus": a.gpus,
-           "steps": a.steps, "warmup": a.warmup, "ms_per_step": round(wall / (per) * 1e3, 3), "higher_is_better": True,
+           "steps": a.steps, "warmup": a.warmup, "ms_per_step": round(wall / a.steps * 1e3, 3), "higher_is_better": True,
            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded soup)",
-           "config": {"workload": WORKLOAD, "n_tris_sample": sample, "preset": "lbvh63 (reference constants patched: "
-                      "BVH_LBVH_THRESHOLD=0)", "processes": cores},
+           "config": {"workload": WORKLOAD, "n_tris": n, "same_config": True,
+                      "preset": "lbvh63 (reference constants patched: BVH_LBVH_THRESHOLD=0)", "processes": cores,
+                      "bakes_timed": a.steps * cores,
+                      "step": f"one bake of the {n:,}-triangle soup in each of {cores} processes at once"},
            "cpu_baseline": {"value": round(value, 4), "unit": "Mtri/s", "cores": cores, "kind": kind,
-                            "sample": f"{cores} processes, each timing {per} bake(s) of its own {sample}-triangle "
-                                      f"soup after set-up (the reference bake is single-threaded); wall = the "
-                                      f"slowest process"},
+                            "sample": f"{cores} processes, each timing {a.steps} bake(s) of the {n:,}-triangle soup "
+                                      f"after {a.warmup} untimed one(s) (the reference bake is single-threaded); "
+                                      f"wall = the slowest process"},
            "e2e": {"value": round(value, 4), "unit": "Mtri/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(out), flush=True)
     return 0
@@ -297,8 +311,9 @@ def run_ours(a):
 
     # roofline of the bake as one unit (no single kernel dominates it: the largest takes about
     # 15 % of the step): algorithmic bytes per bake over the device time per bake
-    alg_bytes = bake_bytes_per_tri(n) * n
+    alg_bytes = ROOFLINE_BYTES_PER_TRI.get(int(cfg.morton_bits), 400) * n
     achieved = alg_bytes / (ms_step * 1e-3) / 1e9
+    own_bytes = bake_bytes_per_tri(n) * n
     peak, peak_kind = measured_peak_hbm()
     traffic_per_tri = profiled_traffic() if n == N_TRIS and a.preset == "lbvh63" else None
 
@@ -365,7 +380,7 @@ def run_ours(a):
     out = None
     if rank == 0:
         with quiet_stdout():
-            cpu_v, cpu_kind, cpu_dt = cpu_reference_bake(1 << 17, 20261204, 2)
+            cpu_v, cpu_kind, cpu_dt = cpu_reference_bake(n, scenes.BASE_SEED + 1, 3)
         out = {"metric": METRIC, "value": round(value, 3), "unit": "Mtri/s", "n_gpus": world, "steps": a.steps,
                "warmup": a.warmup, "ms_per_step": round(ms_step, 4), "higher_is_better": True, "scaling": "weak",
                "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded soup, per-rank seed)",
@@ -379,10 +394,12 @@ def run_ours(a):
                             "achieved": round(achieved, 1), "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
                             "frac": round(achieved / peak, 4),
                             "traffic": (round(traffic_per_tri * n) if traffic_per_tri else None),
-                            "algorithmic_bytes_per_launch": int(alg_bytes), "launch_ms": round(ms_step, 5)},
+                            "algorithmic_bytes_per_launch": int(alg_bytes), "launch_ms": round(ms_step, 5),
+                            "builder_bytes_per_launch": int(own_bytes),
+                            "builder_frac": round(own_bytes / (ms_step * 1e-3) / 1e9 / peak, 4)},
                "cpu_baseline": {"value": round(cpu_v, 4), "unit": "Mtri/s", "cores": 1, "kind": cpu_kind,
-                                "sample": "bvh::bakeBVH of a 131,072-triangle soup of the same generator, LBVH "
-                                          "constants, 2 timed repetitions, 1 thread (the bake is single-threaded)"},
+                                "sample": f"bvh::bakeBVH of the same {n:,}-triangle soup, LBVH constants, 3 timed "
+                                          f"repetitions after one untimed, 1 thread (the bake is single-threaded)"},
                "clocks": clocks, "extra": extra, "render": render}
         print(json.dumps(out), flush=True)
     if dist:

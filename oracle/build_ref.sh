@@ -1,6 +1,7 @@
 #!/bin/sh
 # Builds the reference's own BVH sources, read in place from the reference tree, into
-# oracle/_ref/<variant>/libref.so (test oracle only; nothing here is shipped).
+# oracle/_ref/<variant>/libref.so (test oracle only; nothing here is shipped), together with
+# the reference's path loop, src/main.cpp, reached through oracle/ref_main_harness.cpp.
 #
 # The reference fixes its build parameters as constexpr values in
 # src/bvh/bvh_defines.hpp, included with quotes from the same directory. Each variant
@@ -8,7 +9,9 @@
 # '-I-' switch stops the compiler from searching the including file's own directory
 # first, so the reference sources pick up the patched header without being copied.
 #
-# usage: oracle/build_ref.sh [reference-root]     (default /root/reference)
+# usage: oracle/build_ref.sh [reference-root]
+# The reference tree is the first argument, else $RT_REFERENCE_ROOT, else the read-only
+# checkout this build environment mounts; without its sources the script builds nothing.
 set -e
 REF=${1:-${RT_REFERENCE_ROOT:-/root/reference}}
 HERE=$(cd "$(dirname "$0")" && pwd)
@@ -31,13 +34,13 @@ build_variant() {
     mkdir -p "$OUT/$name"
     sed "$@" "$DEFS" > "$OUT/$name/bvh_defines.hpp.new"
     if ! cmp -s "$OUT/$name/bvh_defines.hpp.new" "$OUT/$name/bvh_defines.hpp" 2>/dev/null || [ ! -f "$OUT/$name/libref.so" ] \
-        || [ "$HERE/ref_harness.cpp" -nt "$OUT/$name/libref.so" ]; then
+        || [ "$HERE/ref_harness.cpp" -nt "$OUT/$name/libref.so" ] || [ "$HERE/ref_main_harness.cpp" -nt "$OUT/$name/libref.so" ]; then
         mv "$OUT/$name/bvh_defines.hpp.new" "$OUT/$name/bvh_defines.hpp"
         # Same language level and optimisation as the reference Makefile (-std=c++2b -O2),
         # plain x86-64 (SSE, no FMA contraction), as the reference is built.
         g++ -std=c++2b -O2 -fPIC -shared -w -Wno-deprecated \
             -I"$OUT/$name" -I- -I"$HERE/stubs" -I"$REF/src/bvh" -I"$REF/src/math" -I"$REF/src" -I"$CXXINC/pstl" \
-            -o "$OUT/$name/libref.so" $SRCS "$HERE/ref_harness.cpp" -lpthread
+            -o "$OUT/$name/libref.so" $SRCS "$HERE/ref_harness.cpp" "$HERE/ref_main_harness.cpp" -lpthread
         echo "built oracle/_ref/$name/libref.so"
     else
         rm -f "$OUT/$name/bvh_defines.hpp.new"

@@ -117,6 +117,9 @@ class Restatement:
         L.orc_render_ex.argtypes = [vp, vp, vp, u32, vp, vp, vp, u32, u32, u32, u32, vp, vp, C.c_int]
         L.orc_adjoint.argtypes = [vp, vp, vp, u32, vp, vp, vp, vp, vp, C.c_int]
         L.orc_philox.argtypes = [u32, u32, u32, u32, u32, u32, vp]
+        L.orc_primary_rays.argtypes = [vp, u64, vp, vp, vp, vp, vp]
+        L.orc_cosine_dirs.argtypes = [u64, vp, vp, vp, vp]
+        L.orc_ibl_lookup.argtypes = [vp, u32, u32, u64, vp, vp]
 
     def morton(self, verts, tris, cfg: OrcCfg):
         verts = np.ascontiguousarray(verts, np.float32); tris = np.ascontiguousarray(tris, np.uint32)
@@ -210,6 +213,26 @@ class Restatement:
         self.L.orc_free(hnd)
         return g_alb, g_em
 
+    def primary_rays(self, rcfg: OrcRenderCfg, px, py, jx, jy):
+        px = np.ascontiguousarray(px, np.int32); py = np.ascontiguousarray(py, np.int32)
+        jx = np.ascontiguousarray(jx, np.float32); jy = np.ascontiguousarray(jy, np.float32)
+        out = np.zeros((px.shape[0], 8), np.float32)
+        self.L.orc_primary_rays(C.byref(rcfg), px.shape[0], _p(px), _p(py), _p(jx), _p(jy), _p(out))
+        return out
+
+    def cosine_dirs(self, u1, u2, normals):
+        u1 = np.ascontiguousarray(u1, np.float32); u2 = np.ascontiguousarray(u2, np.float32)
+        nrm = np.ascontiguousarray(normals, np.float32)
+        out = np.zeros((u1.shape[0], 3), np.float32)
+        self.L.orc_cosine_dirs(u1.shape[0], _p(u1), _p(u2), _p(nrm), _p(out))
+        return out
+
+    def ibl_lookup(self, env_map, dirs):
+        em = np.ascontiguousarray(env_map, np.float32); d = np.ascontiguousarray(dirs, np.float32)
+        out = np.zeros((d.shape[0], 3), np.float32)
+        self.L.orc_ibl_lookup(_p(em), em.shape[1], em.shape[0], d.shape[0], _p(d), _p(out))
+        return out
+
     def philox(self, c, k):
         out = np.zeros(4, np.uint32)
         self.L.orc_philox(*[int(x) for x in c], *[int(x) for x in k], _p(out))
@@ -236,6 +259,15 @@ class Reference:
         L.ref_load.argtypes = [C.c_char_p]
         L.ref_trace.argtypes = [vp, u64, vp, vp, vp, C.c_int]
         L.ref_clip_triangle.argtypes = [vp, vp, vp]
+        # the path loop of src/main.cpp (oracle/ref_main_harness.cpp)
+        i32 = C.c_int
+        L.ref_scene_config.argtypes = [C.c_char_p, vp, vp, vp]
+        L.ref_camera_lookat.argtypes = [vp, vp, C.c_float, vp]
+        L.ref_camera_quat.argtypes = [vp, vp, C.c_float, vp]
+        L.ref_primary_rays.argtypes = [vp, i32, i32, u64, vp, vp, vp, vp, vp]
+        L.ref_cosine_dirs.argtypes = [u64, vp, vp, vp, vp]
+        L.ref_ibl_lookup.argtypes = [vp, i32, i32, u64, vp, vp]
+        L.ref_path_render.argtypes = [vp, i32, i32, i32, i32, u32, vp, i32, i32, i32, i32, vp, vp, i32]
 
     @staticmethod
     def available(variant: str = "hybrid") -> bool:
@@ -290,6 +322,69 @@ class Reference:
         out = np.zeros(6, np.float32)
         self.L.ref_clip_triangle(_p(v9), _p(box6), _p(out))
         return out
+
+    # ---- the path loop of src/main.cpp ----
+    def scene_config(self, scn_path):
+        """parseSceneConfig (main.cpp:218-285): (width, height), camera (13 floats: pos, fwd,
+        right, up, tanHalfFovY), ambient, whether an ibl line named a map."""
+        wh = np.zeros(2, np.int32); cam = np.zeros(13, np.float32); amb = np.zeros(3, np.float32)
+        has_ibl = self.L.ref_scene_config(scn_path.encode(), _p(wh), _p(cam), _p(amb))
+        return (int(wh[0]), int(wh[1])), cam, amb, bool(has_ibl)
+
+    def camera_lookat(self, pos, target, fov_deg):
+        cam = np.zeros(13, np.float32)
+        self.L.ref_camera_lookat(_p(np.asarray(pos, np.float32)), _p(np.asarray(target, np.float32)),
+                                 float(fov_deg), _p(cam))
+        return cam
+
+    def camera_quat(self, pos, q_wxyz, focal):
+        cam = np.zeros(13, np.float32)
+        self.L.ref_camera_quat(_p(np.asarray(pos, np.float32)), _p(np.asarray(q_wxyz, np.float32)), float(focal),
+                               _p(cam))
+        return cam
+
+    def primary_rays(self, cam13, W, H, px, py, jx, jy):
+        """primaryRay (main.cpp:69-83): (n, 8) rays = origin, tmin, dir, tmax."""
+        px = np.ascontiguousarray(px, np.int32); py = np.ascontiguousarray(py, np.int32)
+        jx = np.ascontiguousarray(jx, np.float32); jy = np.ascontiguousarray(jy, np.float32)
+        out = np.zeros((px.shape[0], 8), np.float32)
+        self.L.ref_primary_rays(_p(np.ascontiguousarray(cam13, np.float32)), int(W), int(H), px.shape[0], _p(px),
+                                _p(py), _p(jx), _p(jy), _p(out))
+        return out
+
+    def cosine_dirs(self, u1, u2, normals):
+        """toWorld(sampleCosineHemisphere(u1, u2), n) (main.cpp:123-141)."""
+        u1 = np.ascontiguousarray(u1, np.float32); u2 = np.ascontiguousarray(u2, np.float32)
+        nrm = np.ascontiguousarray(normals, np.float32)
+        out = np.zeros((u1.shape[0], 3), np.float32)
+        self.L.ref_cosine_dirs(u1.shape[0], _p(u1), _p(u2), _p(nrm), _p(out))
+        return out
+
+    def ibl_lookup(self, env_map, dirs):
+        """IBL::sample (main.cpp:107-117) of an (h, w, 3) map."""
+        em = np.ascontiguousarray(env_map, np.float32); d = np.ascontiguousarray(dirs, np.float32)
+        out = np.zeros((d.shape[0], 3), np.float32)
+        self.L.ref_ibl_lookup(_p(em), em.shape[1], em.shape[0], d.shape[0], _p(d), _p(out))
+        return out
+
+    def path_render(self, baked: Baked, cam13, W, H, spp, max_bounce=8, seed=1, env_map=None, rows=None,
+                    threads: int = 1):
+        """The reference's pixel loop and pathTrace (main.cpp:145-204, 339-365) over `baked`
+        (loaded with the reference's loadBVH), one std::mt19937 per pixel. Returns the per-pixel
+        mean and mean of squares, (rows, W, 3) float64, row 0 at the bottom."""
+        with tempfile.TemporaryDirectory() as d:
+            path = os.path.join(d, "r.bvh")
+            write_bvh(path, baked)
+            assert self.L.ref_load(path.encode())
+        r0, r1 = rows if rows is not None else (0, H)
+        mean = np.zeros((r1 - r0, W, 3), np.float64); sq = np.zeros_like(mean)
+        em = np.ascontiguousarray(env_map, np.float32) if env_map is not None else None
+        eh, ew = (em.shape[0], em.shape[1]) if em is not None else (0, 0)
+        ok = self.L.ref_path_render(_p(np.ascontiguousarray(cam13, np.float32)), int(W), int(H), int(spp),
+                                    int(max_bounce), int(seed), _p(em), ew, eh, r0, r1 - r0, _p(mean), _p(sq),
+                                    int(threads))
+        assert ok
+        return mean, sq
 
 
 def write_bvh(path, baked: Baked):

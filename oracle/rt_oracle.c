@@ -993,28 +993,81 @@ static void surface(const render_ctx* R, uint32_t tri, v3* albedo, v3* emission,
     if (R->talb) { const float* a = R->talb + 3 * (size_t)tri; *albedo = mk3(a[0], a[1], a[2]); }
 }
 
-/* primaryRay + pathTrace (src/main.cpp:69-83, 145-204) for one sample of one pixel; rec
- * (optional) receives the vertices of the path. */
-static v3 path_sample(const render_ctx* R, uint32_t x, uint32_t y, uint32_t sidx, path_rec* rec)
+/* primaryRay (src/main.cpp:69-83): the ray through pixel (x, y) at jitter (jx, jy). */
+static oray primary_ray(const orc_render_cfg* C, uint32_t x, uint32_t y, float jx, float jy)
 {
-    const orc_render_cfg* C = R->C;
-    const uint32_t W = C->width, H = C->height, pix = y * W + x;
+    const uint32_t W = C->width, H = C->height;
     const float aspect = (float)W / (float)H;
     const v3 pos = mk3(C->cam_pos[0], C->cam_pos[1], C->cam_pos[2]);
     const v3 fwd = mk3(C->cam_fwd[0], C->cam_fwd[1], C->cam_fwd[2]);
     const v3 rgt = mk3(C->cam_right[0], C->cam_right[1], C->cam_right[2]);
     const v3 up  = mk3(C->cam_up[0], C->cam_up[1], C->cam_up[2]);
     const float th = C->tan_half_fov_y;
-    if (rec) { rec->n = 0; rec->missed = 0; }
-    uint32_t r4[4];
-    orc_philox(pix, sidx, 0u, 0u, C->seed, 0x5EEDu, r4);
-    float u = (((float)x + u01(r4[0])) / (float)W * 2.f - 1.f) * aspect;
-    float v = ((float)y + u01(r4[1])) / (float)H * 2.f - 1.f;
+    float u = (((float)x + jx) / (float)W * 2.f - 1.f) * aspect;
+    float v = ((float)y + jy) / (float)H * 2.f - 1.f;
     oray ray;
     ray.o = pos;
     ray.d = norm3(add3(add3(fwd, muls(rgt, u * th)), muls(up, v * th)));
     ray.tmin = 1e-3f;
     ray.tmax = INFINITY;
+    return ray;
+}
+
+/* toWorld(sampleCosineHemisphere(u1, u2), n) (src/main.cpp:123-141). */
+static v3 cosine_dir(float u1, float u2, v3 n)
+{
+    float rr = sqrtf(u1);
+    float theta = 2.f * ORC_PI * u2;
+    v3 ld = mk3(rr * cosf(theta), sqrtf(std_max(0.f, 1.f - u1)), rr * sinf(theta));
+    v3 axis = fabsf(n.x) < 0.9f ? mk3(1.f, 0.f, 0.f) : mk3(0.f, 1.f, 0.f);
+    v3 t = norm3(cross3(n, axis));
+    v3 b = cross3(n, t);
+    return add3(add3(muls(t, ld.x), muls(n, ld.y)), muls(b, ld.z));
+}
+
+void orc_primary_rays(const orc_render_cfg* C, uint64_t n, const int32_t* px, const int32_t* py, const float* jx,
+                      const float* jy, float* rays8)
+{
+    for (uint64_t i = 0; i < n; i++)
+    {
+        oray r = primary_ray(C, (uint32_t)px[i], (uint32_t)py[i], jx[i], jy[i]);
+        float* o = rays8 + 8 * i;
+        o[0] = r.o.x; o[1] = r.o.y; o[2] = r.o.z; o[3] = r.tmin;
+        o[4] = r.d.x; o[5] = r.d.y; o[6] = r.d.z; o[7] = r.tmax;
+    }
+}
+
+void orc_cosine_dirs(uint64_t n, const float* u1, const float* u2, const float* nrm3, float* out3)
+{
+    for (uint64_t i = 0; i < n; i++)
+    {
+        v3 w = cosine_dir(u1[i], u2[i], mk3(nrm3[3 * i], nrm3[3 * i + 1], nrm3[3 * i + 2]));
+        out3[3 * i] = w.x; out3[3 * i + 1] = w.y; out3[3 * i + 2] = w.z;
+    }
+}
+
+void orc_ibl_lookup(const float* map, uint32_t w, uint32_t h, uint64_t n, const float* dirs3, float* out3)
+{
+    render_ctx R;
+    memset(&R, 0, sizeof(R));
+    R.env_map = map; R.env_w = w; R.env_h = h;
+    for (uint64_t i = 0; i < n; i++)
+    {
+        v3 c = ibl_sample(&R, mk3(dirs3[3 * i], dirs3[3 * i + 1], dirs3[3 * i + 2]));
+        out3[3 * i] = c.x; out3[3 * i + 1] = c.y; out3[3 * i + 2] = c.z;
+    }
+}
+
+/* primaryRay + pathTrace (src/main.cpp:69-83, 145-204) for one sample of one pixel; rec
+ * (optional) receives the vertices of the path. */
+static v3 path_sample(const render_ctx* R, uint32_t x, uint32_t y, uint32_t sidx, path_rec* rec)
+{
+    const orc_render_cfg* C = R->C;
+    const uint32_t W = C->width, pix = y * W + x;
+    if (rec) { rec->n = 0; rec->missed = 0; }
+    uint32_t r4[4];
+    orc_philox(pix, sidx, 0u, 0u, C->seed, 0x5EEDu, r4);
+    oray ray = primary_ray(C, x, y, u01(r4[0]), u01(r4[1]));
     v3 tp = mk3(1.f, 1.f, 1.f), L = mk3(0.f, 0.f, 0.f);
     for (uint32_t bounce = 0; bounce <= C->max_bounce; bounce++)
     {
@@ -1052,15 +1105,7 @@ static v3 path_sample(const render_ctx* R, uint32_t x, uint32_t y, uint32_t sidx
         }
         else
         {
-            /* sampleCosineHemisphere + toWorld, src/main.cpp:123-141 */
-            float u1 = u01(r4[0]), u2 = u01(r4[1]);
-            float rr = sqrtf(u1);
-            float theta = 2.f * ORC_PI * u2;
-            v3 ld = mk3(rr * cosf(theta), sqrtf(std_max(0.f, 1.f - u1)), rr * sinf(theta));
-            v3 axis = fabsf(h.n.x) < 0.9f ? mk3(1.f, 0.f, 0.f) : mk3(0.f, 1.f, 0.f);
-            v3 t = norm3(cross3(h.n, axis));
-            v3 b = cross3(h.n, t);
-            wdir = add3(add3(muls(t, ld.x), muls(h.n, ld.y)), muls(b, ld.z));
+            wdir = cosine_dir(u01(r4[0]), u01(r4[1]), h.n);  /* sampleCosineHemisphere + toWorld */
         }
         tp = mul3(tp, albedo);
         if (C->rr_after >= 0 && (int32_t)bounce > C->rr_after)

@@ -131,6 +131,15 @@ void orc_adjoint(const orc_bvh* b, const orc_render_cfg* cfg, const orc_material
                  const uint32_t* mat_of_tri, const float* tri_albedo, const float* d_rgb, double* grad_albedo,
                  double* grad_emission, int nthreads);
 
+/* The pieces of the path loop, for bit-level checks against the reference's own functions:
+ * primaryRay (src/main.cpp:69-83) for n (pixel, jitter) pairs with cfg's camera and size
+ * (rays8 = origin, tmin, dir, tmax); toWorld(sampleCosineHemisphere(u1, u2), n)
+ * (main.cpp:123-141); IBL::sample (main.cpp:107-117) of an h x w RGB map. */
+void orc_primary_rays(const orc_render_cfg* cfg, uint64_t n, const int32_t* px, const int32_t* py, const float* jx,
+                      const float* jy, float* rays8);
+void orc_cosine_dirs(uint64_t n, const float* u1, const float* u2, const float* nrm3, float* out3);
+void orc_ibl_lookup(const float* map, uint32_t w, uint32_t h, uint64_t n, const float* dirs3, float* out3);
+
 /* Counter-based RNG shared with the device code: Philox4x32-10 (Salmon et al., SC'11). */
 void orc_philox(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3, uint32_t k0, uint32_t k1,
                 uint32_t* out4);
