@@ -66,6 +66,13 @@ build_variant sah4ns   -e 's/BVH_LBVH_THRESHOLD   = 64/BVH_LBVH_THRESHOLD   = 21
                        -e 's/BVH_SPATIAL_EPS      = 1e-6f/BVH_SPATIAL_EPS      = 3.0e38f/' &
 wait
 
+# The reference's own mesh files (bunny.ply: extra vertex properties; letterX / letterY.ply:
+# quads), copied for the mesh-ingestion tests, which also run where the reference tree is absent.
+mkdir -p "$OUT/meshes"
+for m in bunny.ply letterX.ply letterY.ply; do
+    if [ -f "$REF/$m" ]; then cp -f "$REF/$m" "$OUT/meshes/$m"; fi
+done
+
 # The reference's own unit and integration tests, read in place and compiled unchanged against
 # this repository's drop-in headers (include/bvh, include/math) and librt_b200.so: the proof that
 # code written for the reference's bake/load/trace/AABB interface builds and links against the

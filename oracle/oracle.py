@@ -21,6 +21,8 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_LIB = os.path.join(HERE, "lib", "liboracle.so")
 REF_DIR = os.path.join(HERE, "_ref")
+# the reference's own mesh files, copied next to its build by oracle/build_ref.sh
+REF_MESH_DIR = os.path.join(REF_DIR, "meshes")
 
 # Build parameter sets: the reference's compile-time constants of each oracle/_ref variant
 # (oracle/build_ref.sh) as runtime values.
@@ -259,6 +261,7 @@ class Reference:
         L.ref_load.argtypes = [C.c_char_p]
         L.ref_trace.argtypes = [vp, u64, vp, vp, vp, C.c_int]
         L.ref_clip_triangle.argtypes = [vp, vp, vp]
+        L.ref_mesh_transform.argtypes = [vp, C.c_float, vp, u64, vp, vp, vp]
         # the path loop of src/main.cpp (oracle/ref_main_harness.cpp)
         i32 = C.c_int
         L.ref_scene_config.argtypes = [C.c_char_p, vp, vp, vp]
@@ -321,6 +324,15 @@ class Reference:
         v9 = np.ascontiguousarray(v9, np.float32); box6 = np.ascontiguousarray(box6, np.float32)
         out = np.zeros(6, np.float32)
         self.L.ref_clip_triangle(_p(v9), _p(box6), _p(out))
+        return out
+
+    def mesh_transform(self, translate, scale, q_wxyz, pos, nrm):
+        """loadMesh's transform of imported positions and normals (bvh_IO.cpp:24-70, 221-224):
+        (n, 6) float32 = x, y, z, nx, ny, nz."""
+        pos = np.ascontiguousarray(pos, np.float32); nrm = np.ascontiguousarray(nrm, np.float32)
+        out = np.zeros((pos.shape[0], 6), np.float32)
+        self.L.ref_mesh_transform(_p(np.asarray(translate, np.float32)), float(scale),
+                                  _p(np.asarray(q_wxyz, np.float32)), pos.shape[0], _p(pos), _p(nrm), _p(out))
         return out
 
     # ---- the path loop of src/main.cpp ----

@@ -219,6 +219,27 @@ void ref_trace(const float* rays8, uint64_t n, float* out6, uint32_t* tri, uint8
     for (auto& x : th) { x.join(); }
 }
 
+// The transform loadMesh applies to an imported mesh (src/bvh/bvh_IO.cpp:24-70 with the matrix
+// readScene builds at bvh_IO.cpp:221-224): positions by translate * scale * toMat4(q),
+// normals by transpose(inverse(that)), in the reference's own math library. q_wxyz as the
+// .scn line gives it after reordering (w, x, y, z). pos3 / nrm3: n points and normals;
+// out6: transformed x, y, z, nx, ny, nz (normals not renormalised, as loadMesh leaves them).
+void ref_mesh_transform(const float* t3, float scale, const float* q_wxyz, uint64_t n, const float* pos3,
+                        const float* nrm3, float* out6)
+{
+    math::mat4 transform = math::translate(math::mat4(1.f), math::vec3(t3[0], t3[1], t3[2])) *
+                           math::scale(math::mat4(1.f), math::vec3(scale)) *
+                           math::toMat4(math::quat(q_wxyz[0], q_wxyz[1], q_wxyz[2], q_wxyz[3]));
+    math::mat4 normalTransform = math::transpose(math::inverse(transform));
+    for (uint64_t i = 0; i < n; i++)
+    {
+        math::vec4 tp = transform * math::vec4(pos3[3 * i], pos3[3 * i + 1], pos3[3 * i + 2], 1.0f);
+        math::vec4 tn = normalTransform * math::vec4(nrm3[3 * i], nrm3[3 * i + 1], nrm3[3 * i + 2], 0.0f);
+        float* o = out6 + 6 * i;
+        o[0] = tp.x; o[1] = tp.y; o[2] = tp.z; o[3] = tn.x; o[4] = tn.y; o[5] = tn.z;
+    }
+}
+
 // clipTriangleToAABB (src/bvh/AABB.cpp:86-171): v9 = three vertices, box6 = min, max.
 // out6 = min, max of the clipped polygon (the empty box is +inf / -inf).
 void ref_clip_triangle(const float* v9, const float* box6, float* out6)
