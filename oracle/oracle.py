@@ -120,6 +120,7 @@ class Restatement:
         L.orc_adjoint.argtypes = [vp, vp, vp, u32, vp, vp, vp, vp, vp, C.c_int]
         L.orc_philox.argtypes = [u32, u32, u32, u32, u32, u32, vp]
         L.orc_primary_rays.argtypes = [vp, u64, vp, vp, vp, vp, vp]
+        L.orc_trace_brute.argtypes = [vp, vp, u32, vp, u64, u32, vp, vp, vp]
         L.orc_cosine_dirs.argtypes = [u64, vp, vp, vp, vp]
         L.orc_ibl_lookup.argtypes = [vp, u32, u32, u64, vp, vp]
 
@@ -214,6 +215,15 @@ class Restatement:
                            _p(g_alb), _p(g_em), threads)
         self.L.orc_free(hnd)
         return g_alb, g_em
+
+    def trace_brute(self, verts, tris, rays, flags: int = 0):
+        """Every ray against every triangle (no BVH): hit, (n, 3) t / u / v, triangle."""
+        verts = np.ascontiguousarray(verts, np.float32); tris = np.ascontiguousarray(tris, np.uint32)
+        rays = np.ascontiguousarray(rays, np.float32)
+        n = rays.shape[0]
+        out = np.zeros((n, 3), np.float32); tri = np.zeros(n, np.uint32); hit = np.zeros(n, np.uint8)
+        self.L.orc_trace_brute(_p(verts), _p(tris), tris.shape[0], _p(rays), n, flags, _p(out), _p(tri), _p(hit))
+        return hit, out, tri
 
     def primary_rays(self, rcfg: OrcRenderCfg, px, py, jx, jy):
         px = np.ascontiguousarray(px, np.int32); py = np.ascontiguousarray(py, np.int32)

@@ -800,6 +800,98 @@ static inline int ray_tri(const oray* r, v3 v0, v3 v1, v3 v2, float* t, float* u
     return 1;
 }
 
+static inline float flip_sign(float x, uint32_t sign_bit)
+{
+    uint32_t b;
+    memcpy(&b, &x, 4);
+    b ^= sign_bit;
+    memcpy(&x, &b, 4);
+    return x;
+}
+
+/* Watertight ray/triangle intersection after Woop, Benthin and Wald, "Watertight Ray/Triangle
+ * Intersection", Journal of Computer Graphics Techniques 2(1), 2013, section 3 and its
+ * listing, without back-face culling. Not in the reference (its rayTriangle culls back faces
+ * and is not watertight); the test of the library's RT_TRACE_WATERTIGHT mode. Steps:
+ *  1. kz = the axis of the largest |dir| component, kx = kz + 1, ky = kx + 1 (mod 3), kx and
+ *     ky swapped when dir[kz] < 0 so the winding is kept;
+ *  2. shear constants Sx = dir[kx] / dir[kz], Sy = dir[ky] / dir[kz], Sz = 1 / dir[kz];
+ *  3. vertices relative to the origin, sheared: A = v0 - org, Ax = A[kx] - Sx * A[kz], ...;
+ *  4. scaled barycentrics U = Cx * By - Cy * Bx, V = Ax * Cy - Ay * Cx, W = Bx * Ay - By * Ax,
+ *     all three recomputed in double precision when any is exactly zero (edge hits);
+ *  5. miss when the signs of U, V, W differ; det = U + V + W, miss when det = 0;
+ *  6. scaled distance T = U * (Sz A[kz]) + V * (Sz B[kz]) + W * (Sz C[kz]), tested against the
+ *     ray's [tmin, tmax] scaled by |det| with det's sign taken off T (no division yet);
+ *  7. t = T / det and the barycentrics of v1 and v2 (V / det, W / det) through one reciprocal.
+ * The paper's lower distance bound of 0 is the ray's tmin here, its upper bound the ray's tmax
+ * (the reference's rayTriangle tests the ray's own range; traverse keeps the nearest). */
+static inline int ray_tri_watertight(const oray* r, v3 v0, v3 v1, v3 v2, float* t, float* u, float* v)
+{
+    const float adx = fabsf(r->d.x), ady = fabsf(r->d.y), adz = fabsf(r->d.z);
+    int kz = (adx > ady) ? (adx > adz ? 0 : 2) : (ady > adz ? 1 : 2);
+    int kx = (kz + 1) % 3, ky = (kx + 1) % 3;
+    const float dz = v3_get(r->d, kz);
+    if (dz < 0.f) { int sw = kx; kx = ky; ky = sw; }
+    const float Sx = v3_get(r->d, kx) / dz, Sy = v3_get(r->d, ky) / dz, Sz = 1.f / dz;
+    const v3 A = sub3(v0, r->o), B = sub3(v1, r->o), C = sub3(v2, r->o);
+    const float Ax = v3_get(A, kx) - Sx * v3_get(A, kz), Ay = v3_get(A, ky) - Sy * v3_get(A, kz);
+    const float Bx = v3_get(B, kx) - Sx * v3_get(B, kz), By = v3_get(B, ky) - Sy * v3_get(B, kz);
+    const float Cx = v3_get(C, kx) - Sx * v3_get(C, kz), Cy = v3_get(C, ky) - Sy * v3_get(C, kz);
+    float U = Cx * By - Cy * Bx, V = Ax * Cy - Ay * Cx, W = Bx * Ay - By * Ax;
+    if (U == 0.f || V == 0.f || W == 0.f)
+    {
+        const double CxBy = (double)Cx * (double)By, CyBx = (double)Cy * (double)Bx;
+        const double AxCy = (double)Ax * (double)Cy, AyCx = (double)Ay * (double)Cx;
+        const double BxAy = (double)Bx * (double)Ay, ByAx = (double)By * (double)Ax;
+        U = (float)(CxBy - CyBx);
+        V = (float)(AxCy - AyCx);
+        W = (float)(BxAy - ByAx);
+    }
+    if ((U < 0.f || V < 0.f || W < 0.f) && (U > 0.f || V > 0.f || W > 0.f)) { return 0; }
+    const float det = U + V + W;
+    if (det == 0.f) { return 0; }
+    const float Az = Sz * v3_get(A, kz), Bz = Sz * v3_get(B, kz), Cz = Sz * v3_get(C, kz);
+    const float T = U * Az + V * Bz + W * Cz;
+    uint32_t db;
+    memcpy(&db, &det, 4);
+    const uint32_t sign_bit = db & 0x80000000u;
+    const float Ts = flip_sign(T, sign_bit), Ds = flip_sign(det, sign_bit);
+    if (!(Ts >= r->tmin * Ds && Ts <= r->tmax * Ds)) { return 0; }
+    const float rcp = 1.f / det;
+    *t = T * rcp; *u = V * rcp; *v = W * rcp;
+    return 1;
+}
+
+/* Every ray against every triangle (no BVH), nearest accepted hit: isolates the triangle
+ * tests from the box tests of the traversal. out3 = t, u, v. */
+void orc_trace_brute(const float* verts6, const uint32_t* tris3, uint32_t n_tris, const float* rays8, uint64_t n,
+                     uint32_t flags, float* out3, uint32_t* tri, uint8_t* hit)
+{
+    for (uint64_t i = 0; i < n; i++)
+    {
+        const float* rp = rays8 + 8 * i;
+        oray r;
+        r.o = mk3(rp[0], rp[1], rp[2]); r.tmin = rp[3];
+        r.d = mk3(rp[4], rp[5], rp[6]); r.tmax = rp[7];
+        float best = r.tmax;
+        hit[i] = 0; tri[i] = 0; out3[3 * i] = 0.f; out3[3 * i + 1] = 0.f; out3[3 * i + 2] = 0.f;
+        for (uint32_t k = 0; k < n_tris; k++)
+        {
+            const uint32_t* tv = tris3 + 3 * (size_t)k;
+            v3 p0 = vpos(verts6, tv[0]), p1 = vpos(verts6, tv[1]), p2 = vpos(verts6, tv[2]);
+            float t = INFINITY, u = 0.f, v = 0.f;
+            const int acc = (flags & ORC_TRACE_WATERTIGHT) ? ray_tri_watertight(&r, p0, p1, p2, &t, &u, &v)
+                                                           : ray_tri(&r, p0, p1, p2, &t, &u, &v);
+            if (acc && t < best)
+            {
+                best = t;
+                hit[i] = 1; tri[i] = k; out3[3 * i] = t; out3[3 * i + 1] = u; out3[3 * i + 2] = v;
+                if (flags & ORC_TRACE_ANY_HIT) { break; }
+            }
+        }
+    }
+}
+
 /* traverse, bvh_traverse.cpp:91-178. Returns 1 if the 64-entry stack would overflow. */
 static int traverse(const orc_bvh* B, const oray* r, uint32_t flags, ohit* best, uint32_t* ctr)
 {
@@ -825,7 +917,9 @@ static int traverse(const orc_bvh* B, const oray* r, uint32_t flags, ohit* best,
                 v3 p0 = vpos(B->verts, tv[0]), p1 = vpos(B->verts, tv[1]), p2 = vpos(B->verts, tv[2]);
                 float t = INFINITY, u = 0.f, v = 0.f;
                 tested++;
-                if (!ray_tri(r, p0, p1, p2, &t, &u, &v)) { t = INFINITY; }
+                const int acc = (flags & ORC_TRACE_WATERTIGHT) ? ray_tri_watertight(r, p0, p1, p2, &t, &u, &v)
+                                                               : ray_tri(r, p0, p1, p2, &t, &u, &v);
+                if (!acc) { t = INFINITY; }
                 if (t < best_t)
                 {
                     best_t = t;

@@ -77,6 +77,7 @@ void orc_clip_triangle(const float* v9, const float* box6, float* out6);
 
 /* Trace flags */
 #define ORC_TRACE_ANY_HIT 1u /* stop at the first accepted triangle */
+#define ORC_TRACE_WATERTIGHT 2u /* watertight triangle test (Woop, Benthin, Wald 2013), both faces */
 
 /* Closest-hit trace of n rays (o.xyz, tmin, d.xyz, tmax) through a BVH
  * (src/bvh/bvh_traverse.cpp:22-178). out6 = t,u,v,n.xyz; counters (optional, 3 per
@@ -139,6 +140,11 @@ void orc_primary_rays(const orc_render_cfg* cfg, uint64_t n, const int32_t* px, 
                       const float* jy, float* rays8);
 void orc_cosine_dirs(uint64_t n, const float* u1, const float* u2, const float* nrm3, float* out3);
 void orc_ibl_lookup(const float* map, uint32_t w, uint32_t h, uint64_t n, const float* dirs3, float* out3);
+
+/* Every ray against every triangle, no BVH (the triangle tests alone): nearest accepted hit,
+ * out3 = t, u, v; flags as orc_trace. */
+void orc_trace_brute(const float* verts6, const uint32_t* tris3, uint32_t n_tris, const float* rays8, uint64_t n,
+                     uint32_t flags, float* out3, uint32_t* tri, uint8_t* hit);
 
 /* Counter-based RNG shared with the device code: Philox4x32-10 (Salmon et al., SC'11). */
 void orc_philox(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3, uint32_t k0, uint32_t k1,

@@ -46,7 +46,11 @@ __device__ __forceinline__ bool ray_tri(f3 o, f3 d, float tmin, float tmax, f3 v
     return true;
 }
 
-// Watertight ray/triangle test (Woop, Benthin, Wald, JCGT 2013), both faces, as an option.
+// Watertight ray/triangle test (Woop, Benthin, Wald, JCGT 2013), both faces, as an option:
+// shear and scale into the ray's frame, edge functions U / V / W (again in double precision
+// when one is exactly zero), the distance range tested on T against [tmin, tmax] * |det| with
+// det's sign taken off T, and the division by det only for an accepted hit. u, v are the
+// weights of v1 and v2, as in the reference's rayTriangle.
 __device__ __forceinline__ bool ray_tri_watertight(f3 o, f3 d, float tmin, float tmax, f3 v0, f3 v1, f3 v2, float& t,
                                                    float& u, float& v)
 {
@@ -73,10 +77,12 @@ __device__ __forceinline__ bool ray_tri_watertight(f3 o, f3 d, float tmin, float
     if (det == 0.f) { return false; }
     const float Az = Sz * get3(A, kz), Bz = Sz * get3(Bv, kz), Cz = Sz * get3(Cv, kz);
     const float T = U * Az + V * Bz + W * Cz;
+    const uint32_t sign_bit = __float_as_uint(det) & 0x80000000u;
+    const float Ts = __uint_as_float(__float_as_uint(T) ^ sign_bit);
+    const float Ds = __uint_as_float(__float_as_uint(det) ^ sign_bit);
+    if (!(Ts >= tmin * Ds && Ts <= tmax * Ds)) { return false; }
     const float rd = 1.f / det;
-    const float tt = T * rd;
-    if (!(tt >= tmin && tt <= tmax)) { return false; }
-    t = tt; u = V * rd; v = W * rd;
+    t = T * rd; u = V * rd; v = W * rd;
     return true;
 }
 

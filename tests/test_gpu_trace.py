@@ -38,11 +38,13 @@ def compare(hits, ref, tag):
 
 @pytest.mark.parametrize("preset", ["hybrid", "lbvh30", "sah4"])
 @pytest.mark.parametrize("scene", ["soup20k", "ico4", "cornell_ico", "big_small", "test_traverse", "identical100"])
-@pytest.mark.parametrize("flags", [rtb200.TRACE_CLOSEST, rtb200.TRACE_ANY_HIT])
+@pytest.mark.parametrize("flags", [rtb200.TRACE_CLOSEST, rtb200.TRACE_ANY_HIT, rtb200.TRACE_WATERTIGHT,
+                                   rtb200.TRACE_WATERTIGHT | rtb200.TRACE_ANY_HIT])
 @pytest.mark.parametrize("loop", [0, 1])
 def test_trace_matches_oracle(orc, scene, preset, flags, loop):
     """Both traversal loop forms (one-loop, while-while) against the oracle: the any-hit mode
-    returns the first accepted triangle, so it checks the visiting order itself."""
+    returns the first accepted triangle, so it checks the visiting order itself. The watertight
+    modes against the oracle's own restatement of Woop, Benthin and Wald (2013)."""
     v, t = SCENES[scene]
     b = rtb200.Bvh.build(v, t, preset)
     b.trace_loop(loop)
