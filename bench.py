@@ -70,6 +70,8 @@ def parse_args():
     p.add_argument("--preset", default="lbvh63")
     p.add_argument("--no-extra", action="store_true", help="skip the secondary measurements")
     p.add_argument("--no-render", action="store_true", help="skip the path-loop workloads")
+    p.add_argument("--only", choices=["trace", "sah5m", "c1", "c3", "c4", "c5"],
+                   help="run one secondary workload alone and print its figures (for profiling runs)")
     return p.parse_args()
 
 
@@ -265,6 +267,8 @@ def run_ours(a):
     dev = torch.device("cuda", local)
     stream = torch.cuda.current_stream()
     n = a.n_tris
+    if a.only:
+        return run_only(a, stream, dev)
     verts, tris = scenes.soup(n, seed=scenes.BASE_SEED + 1 + rank)
     dv = torch.from_numpy(verts).to(dev)
     dt = torch.from_numpy(tris.view(np.int32)).to(dev)
@@ -408,7 +412,34 @@ def run_ours(a):
     return 0
 
 
-def secondary(a, bvh, dv, dt, verts, stream, dev, flush):
+def run_only(a, stream, dev):
+    """One secondary workload alone (the command the committed ncu summaries were made with)."""
+    import numpy as np
+    import torch
+    import rtb200
+    from rtb200 import scenes
+    if a.only in RENDER_WORKLOADS:
+        out = render_workloads(stream, dev, a.only)
+    elif a.only == "sah5m":
+        lsc = scenes.large_scene()
+        dvl = torch.from_numpy(lsc.verts).to(dev)
+        dtl = torch.from_numpy(lsc.tris.view(np.int32)).to(dev)
+        bl = rtb200.Bvh.build(dvl, dtl, "sah4", stream=stream)
+        ms = _ev_ms(lambda: bl.rebuild(dvl, dtl, "sah4", stream=stream), stream, 1)
+        out = {"sah5m": {"workload": "binned SAH + spatial splits, leaf 4, of the large-render scene (5,000,010 "
+                                     "triangles)", "build_ms": round(ms, 1),
+                         "build_mtri_s": round(lsc.tris.shape[0] / ms / 1e3, 3)}}
+    else:
+        verts, tris = scenes.soup(a.n_tris, seed=scenes.BASE_SEED + 1)
+        dv = torch.from_numpy(verts).to(dev)
+        dt = torch.from_numpy(tris.view(np.int32)).to(dev)
+        flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+        out = {"trace": secondary(a, None, dv, dt, verts, stream, dev, flush, builds=False)}
+    print(json.dumps(out), flush=True)
+    return 0
+
+
+def secondary(a, bvh, dv, dt, verts, stream, dev, flush, builds=True):
     """Other presets' build rates and traversal rates (single measurements after warm-up)."""
     import numpy as np
     import torch
@@ -431,7 +462,7 @@ def secondary(a, bvh, dv, dt, verts, stream, dev, flush):
             ms.append(e0.elapsed_time(e1))
         return statistics.median(ms)
 
-    for preset in ("lbvh30", "hybrid", "sah4"):
+    for preset in ("lbvh30", "hybrid", "sah4") if builds else ():
         b = rtb200.Bvh.build(dv, dt, preset, stream=stream)
         ms = timed(lambda: b.rebuild(dv, dt, preset, stream=stream), 3 if preset != "sah4" else 1)
         res[f"build_{preset}_mtri_s"] = round(n / (ms * 1e-3) / 1e6, 3)
@@ -470,18 +501,74 @@ def _ev_ms(fn, stream, reps=3):
     return statistics.median(ms)
 
 
-def render_workloads(stream, dev):
-    """The path-loop workloads (GPU numbers by CUDA events on torch's stream)."""
+def _orc_cfg(orc, rc):
+    o = orc.OrcRenderCfg()
+    for name, _ in orc.OrcRenderCfg._fields_:
+        val = getattr(rc, name)
+        if hasattr(val, "__len__"):
+            getattr(o, name)[:] = list(val)
+        else:
+            setattr(o, name, val)
+    return o
+
+
+def _trace_ceiling(b, verts, stream, dev, n=1 << 22):
+    """Closest-hit rate (Mray/s, CUDA events) of n incoherent rays -- origins uniform in the
+    scene's box, directions uniform on the sphere -- through the same BVH: the traversal
+    ceiling a path loop's segments are measured against."""
+    import torch
+    from rtb200 import scenes
+    lo, hi = verts[:, :3].min(0), verts[:, :3].max(0)
+    rays = torch.from_numpy(scenes.incoherent_rays(n, lo, hi, seed=scenes.BASE_SEED + 11, tmin=1e-4)).to(dev)
+    ms = _ev_ms(lambda: b.trace(rays, 0, stream=stream), stream)
+    return n / (ms * 1e-3) / 1e6
+
+
+def profiled_render_counters(key):
+    """Issue-slot and cache figures of a path-loop kernel from the committed ncu summary
+    (profiles/render_kernels_c1.md: lines `key: name=value, ...`), if present."""
+    path = os.path.join(HERE, "profiles", "render_kernels_c1.md")
+    try:
+        for line in open(path):
+            if line.startswith(key + ":"):
+                return {kv.split("=")[0].strip(): float(kv.split("=")[1]) for kv in line.split(":", 1)[1].split(",")}
+    except Exception:
+        pass
+    return None
+
+
+def _render_roofline(counts, samples_counted, samples, ms, ceiling, kernel, counters_key=None):
+    """Traversal roofline of a path-loop workload: segments traced per second against the
+    incoherent-ray closest-hit rate on the same BVH; the traversal work per sample (nodes
+    popped and triangles tested, 48 bytes each: a node's two child boxes and references, a
+    triangle's index and positions) from the oracle's count over the same samples."""
+    seg, nodes, tris = (c / samples_counted for c in counts)
+    rate = seg * samples / (ms * 1e-3) / 1e6
+    out = {"bound": "issue (traversal)", "kernel": kernel, "achieved": round(rate, 1), "peak": round(ceiling, 1),
+           "unit": "Mray/s (segments)", "frac": round(rate / ceiling, 4),
+           "peak_kind": "closest-hit rate of 4,194,304 incoherent rays on the same BVH (rt_trace, CUDA events)",
+           "segments_per_sample": round(seg, 4), "nodes_per_segment": round(nodes / seg, 2),
+           "tri_tests_per_segment": round(tris / seg, 2),
+           "traversal_bytes_per_sample": round(48 * (nodes + tris), 1),
+           "traversal_gbs": round(48 * (nodes + tris) * samples / (ms * 1e-3) / 1e9, 1),
+           "counted_samples": int(samples_counted)}
+    if counters_key:
+        out["ncu"] = profiled_render_counters(counters_key)
+    return out
+
+
+def _mpx(n, ms):
+    return round(n / (ms * 1e-3) / 1e6, 1)
+
+
+def render_c1(stream, dev):
+    """Plain path tracing: 256 x 256, 16 spp, depth 4, no roulette; Cornell box + icosphere +
+    two spheres; plain vs wavefront; the restated path loop on all host cores as the CPU leg."""
     import numpy as np
     import torch
     import rtb200
     from rtb200 import scenes
-    sys.path.insert(0, os.path.join(HERE, "oracle"))
     import oracle as orc
-    out = {}
-    mpx = lambda n, ms: round(n / (ms * 1e-3) / 1e6, 1)  # noqa: E731
-
-    # plain path tracing
     sv, st_ = rtb200.Mesh().add_sphere((0.0, 0.0, 0.0), 0.3).arrays()
     sc = scenes.plain_scene(sphere_tris=(sv, st_))
     b = rtb200.Bvh.build(sc.verts, sc.tris, "lbvh30")
@@ -494,37 +581,45 @@ def render_workloads(stream, dev):
     ip, _ = b.render(rc, mats, mot, mode=rtb200.RENDER_PLAIN)
     iw, _ = b.render(rc, mats, mot, mode=rtb200.RENDER_WAVEFRONT)
     ip64, iw64 = ip.double(), iw.double()
-    # CPU baseline: the restated path loop (the reference's pathTrace with per-pixel counter RNG,
-    # reference traversal) over 16 rows on all host cores, scaled to the metric
     nodes, tris, vv = b.download()
     R = orc.Restatement()
-    ocfg = orc.OrcRenderCfg()
-    for name, _ in orc.OrcRenderCfg._fields_:
-        val = getattr(rc, name)
-        if hasattr(val, "__len__"):
-            getattr(ocfg, name)[:] = list(val)
-        else:
-            setattr(ocfg, name, val)
+    ocfg = _orc_cfg(orc, rc)
     cores = os.cpu_count() or 1
     rows = 16
+    baked = orc.Baked(nodes, tris, vv)
+    bmot = sc.baked_materials(b.prim_ids())
     t0 = time.perf_counter()
-    ref, _ = R.render(orc.Baked(nodes, tris, vv), ocfg, sc.mats, sc.baked_materials(b.prim_ids()), rows=(120, 120 + rows),
-                      threads=cores)
+    ref, _ = R.render(baked, ocfg, sc.mats, bmot, rows=(120, 120 + rows), threads=cores)
     cpu_s = time.perf_counter() - t0
+    _, counts = R.render_stats(baked, ocfg, sc.mats, bmot, rows=(120, 120 + rows), threads=cores)
+    ceiling = _trace_ceiling(b, sc.verts, stream, dev)
     sl = ip.cpu().numpy()[120:120 + rows].astype(np.float64)
-    out["plain_c1"] = {
+    out = {
         "workload": "256x256, 16 spp, depth 4, no roulette; Cornell box + 20,480-tri icosphere + 2 spheres (21,462 tris), "
                     "LBVH 30-bit",
-        "plain_mpx_spp_s": mpx(n, tp), "wavefront_mpx_spp_s": mpx(n, tw), "plain_ms": round(tp, 3), "wavefront_ms": round(tw, 3),
+        "plain_mpx_spp_s": _mpx(n, tp), "wavefront_mpx_spp_s": _mpx(n, tw), "plain_ms": round(tp, 3),
+        "wavefront_ms": round(tw, 3),
         "wavefront_vs_plain_max_rel_diff": float(((iw64 - ip64).abs().max() / ip64.abs().max()).item()),
-        "cpu_mpx_spp_s": round(256 * rows * 16 / cpu_s / 1e6, 4), "cpu_cores": cores,
-        "cpu_kind": "port (the oracle's restated path loop over the reference traversal)",
-        "cpu_sample": f"{rows} image rows (of 256) at 16 spp",
-        "cpu_rows_rel_mean_error": float(abs(sl.mean() - ref[120:120 + rows].astype(np.float64).mean()) /
-                                         max(ref[120:120 + rows].mean(), 1e-12))}
+        "roofline": _render_roofline(counts, 256 * rows * 16, n, min(tp, tw), ceiling,
+                                     "wavefront" if tw < tp else "plain", "c1_wavefront_trace"),
+        "cpu_baseline": {"value": round(256 * rows * 16 / cpu_s / 1e6, 4), "unit": "Mpx*spp/s", "cores": cores,
+                         "kind": "port (the oracle's restated path loop over the reference traversal)",
+                         "sample": f"{rows} image rows (of 256) at 16 spp, scaled to the metric"},
+        "cpu_rows_match_gpu_rel_mean": float(abs(sl.mean() - ref[120:120 + rows].astype(np.float64).mean()) /
+                                             max(ref[120:120 + rows].mean(), 1e-12))}
     b.free()
+    return out
 
-    # batched scenes
+
+def render_c3(stream, dev):
+    """Batched: 64 scenes of 1,000-500,000 triangles built in one launch sequence and rendered
+    at 512 x 512, 4 spp, depth 5 by the graph-replayed wavefront (autotuned) vs the plain kernel
+    per scene; CPU leg: the reference's bake plus the restated path loop per scene, on a subset."""
+    import numpy as np
+    import torch
+    import rtb200
+    from rtb200 import scenes
+    import oracle as orc
     scs = scenes.batch_scenes(64)
     v, t, vo, to = rtb200.batch_arrays([(s_.verts, s_.tris) for s_ in scs])
     dvb = torch.from_numpy(v).to(dev)
@@ -562,39 +657,92 @@ def render_workloads(stream, dev):
     for i in (0, 21, 42, 63):
         r_, _ = singles[i].render(rcs[i], smats[i], smot[i], mode=rtb200.RENDER_PLAIN)
         diffs.append(float(((img[i].double() - r_.double()).abs().max() / max(float(r_.abs().max()), 1e-12))))
-    out["batched_c3"] = {
+    # CPU leg on four scenes of the batch (spread over its size range): the reference's own
+    # single-threaded bake of each scene (oracle/_ref lbvh30) plus the restated path loop over
+    # 8 of its 512 rows on all host cores, scaled to the full image and to 64 scenes
+    cores = os.cpu_count() or 1
+    R = orc.Restatement()
+    sub = (0, 21, 42, 63)
+    bake_s, render_s, counts, ceil = 0.0, 0.0, [0, 0, 0], []
+    ref = orc.Reference("lbvh30") if orc.Reference.available("lbvh30") else None
+    for i in sub:
+        s_ = scs[i]
+        if ref is not None:
+            with quiet_stdout():
+                t0 = time.perf_counter()
+                ref.bake(s_.verts, s_.tris)
+                bake_s += time.perf_counter() - t0
+        nodes, tris, vv = singles[i].download()
+        baked = orc.Baked(nodes, tris, vv)
+        mot_i = s_.baked_materials(singles[i].prim_ids())
+        t0 = time.perf_counter()
+        R.render(baked, _orc_cfg(orc, rcs[i]), s_.mats, mot_i, rows=(252, 260), threads=cores)
+        render_s += (time.perf_counter() - t0) * 512 / 8
+        _, c = R.render_stats(baked, _orc_cfg(orc, rcs[i]), s_.mats, mot_i, rows=(252, 260), threads=cores)
+        counts = [a + b_ for a, b_ in zip(counts, c)]
+        ceil.append(_trace_ceiling(singles[i], s_.verts, stream, dev, n=1 << 20))
+    cpu_total_s = (bake_s + render_s) * 64 / len(sub)
+    out = {
         "workload": f"64 scenes, {int(to[-1])} triangles (log-uniform 1,000-500,000 per scene), 512x512, 4 spp, depth 5",
         "build_batched_ms": round(tbb, 3), "build_batched_mtri_s": round(int(to[-1]) / tbb / 1e3, 1),
         "build_64_separate_ms": round(tbs, 3),
-        "render_batched_wavefront_mpx_spp_s": mpx(nb, tbr), "render_plain_per_scene_mpx_spp_s": mpx(nb, tpa),
+        "render_batched_wavefront_mpx_spp_s": _mpx(nb, tbr), "render_plain_per_scene_mpx_spp_s": _mpx(nb, tpa),
         "render_batched_ms": round(tbr, 2), "render_plain_per_scene_ms": round(tpa, 2),
         "autotuned": tuned.as_dict(), "autotune_s": round(tune_s, 2),
-        "batched_vs_plain_max_rel_diff": max(diffs)}
+        "batched_vs_plain_max_rel_diff": max(diffs),
+        "roofline": _render_roofline(counts, len(sub) * 8 * 512 * 4, nb, tbr, statistics.mean(ceil),
+                                     "batched wavefront (autotuned)"),
+        "cpu_baseline": {"value": round(nb / cpu_total_s / 1e6, 4), "unit": "Mpx*spp/s (bake + render)", "cores": cores,
+                         "kind": "reference bake + port (the oracle's restated path loop)",
+                         "sample": f"scenes {sub}: the reference's bake of each (1 thread, {bake_s:.2f} s) and the "
+                                   f"restated path loop over rows 252-259 of 512 at 4 spp on {cores} threads, the "
+                                   f"render scaled by 64 to the full image; the sum scaled by 16 to 64 scenes",
+                         "bake_s_subset": round(bake_s, 3), "render_s_subset_scaled": round(render_s, 3)}}
     for bs in singles:
         bs.free()
     bb.free()
-    del dvb, dtb
+    return out
 
-    # differentiable rendering: adjoint / forward
-    dsc, init, _gt = scenes.diff_scene()
+
+def render_c4(stream, dev):
+    """Differentiable rendering: adjoint / forward of the L2 loss against a 1024-spp target
+    image rendered from the seeded ground-truth albedos."""
+    import numpy as np
+    import torch
+    import rtb200
+    from rtb200 import scenes
+    dsc, init, gt = scenes.diff_scene()
     bd = rtb200.Bvh.build(dsc.verts, dsc.tris, "lbvh30")
     prim = bd.prim_ids()
     dmot = torch.from_numpy(dsc.baked_materials(prim).astype(np.int32)).to(dev)
     dmats = torch.from_numpy(rtb200.materials_array(dsc.mats)).to(dev)
     talb = torch.from_numpy(init[prim]).to(dev)
+    rct = rtb200.render_cfg(512, 512, 1024, max_bounce=4, rr_after=-1, env_kind=1, seed=77, lookat=dsc.lookat)
+    target, _ = bd.render(rct, dmats, dmot, tri_albedo=torch.from_numpy(gt[prim]).to(dev))
     rcd = rtb200.render_cfg(512, 512, 32, max_bounce=4, rr_after=-1, env_kind=1, seed=9, lookat=dsc.lookat)
     fwd = _ev_ms(lambda: bd.render(rcd, dmats, dmot, tri_albedo=talb, stream=stream), stream)
     img, _ = bd.render(rcd, dmats, dmot, tri_albedo=talb)
-    dimg = (2.0 * (img - 0.5 * img.mean())).contiguous()
+    loss = float(((img.double() - target.double()) ** 2).sum().item())
+    dimg = (2.0 * (img - target)).contiguous()  # dLoss/dimage of the L2 loss
     adj = _ev_ms(lambda: bd.adjoint(rcd, dimg, dmats, dmot, tri_albedo=talb, stream=stream), stream)
-    out["adjoint_c4"] = {
-        "workload": "512x512, 32 spp, depth 4; Cornell box + 50,000-triangle icosphere; gradients of per-triangle RGB "
-                    "albedo and material emission",
+    out = {
+        "workload": "512x512, 32 spp, depth 4; Cornell box + 50,000-triangle icosphere; L2 loss against a 1024-spp "
+                    "target from seeded ground-truth albedos; gradients of per-triangle RGB albedo and material emission",
         "forward_ms": round(fwd, 2), "adjoint_ms": round(adj, 2), "adjoint_over_forward": round(adj / fwd, 3),
-        "forward_mpx_spp_s": mpx(512 * 512 * 32, fwd)}
+        "forward_mpx_spp_s": _mpx(512 * 512 * 32, fwd), "l2_loss": round(loss, 3)}
     bd.free()
+    return out
 
-    # large render
+
+def render_c5(stream, dev):
+    """Large render: 1920 x 1080, 64 spp, depth 8, roulette after bounce 2, 5,000,010 triangles,
+    binned SAH with spatial splits; plain vs wavefront (defaults and autotuned); CPU leg: the
+    restated path loop on a few rows."""
+    import numpy as np
+    import torch
+    import rtb200
+    from rtb200 import scenes
+    import oracle as orc
     lsc = scenes.large_scene()
     dvl = torch.from_numpy(lsc.verts).to(dev)
     dtl = torch.from_numpy(lsc.tris.view(np.int32)).to(dev)
@@ -606,15 +754,46 @@ def render_workloads(stream, dev):
                             lookat=lsc.lookat)
     tlp = _ev_ms(lambda: bl.render(rcl, lmats, lmot, mode=rtb200.RENDER_PLAIN, stream=stream), stream, 1)
     tlw = _ev_ms(lambda: bl.render(rcl, lmats, lmot, mode=rtb200.RENDER_WAVEFRONT, stream=stream), stream, 1)
+    tuned = bl.autotune([rcl], lmats, lmot, stream=stream)
+    tlt = _ev_ms(lambda: bl.render_batch([rcl], lmats, lmot, stream=stream), stream, 1)
     nl = 1920 * 1080 * 64
-    out["large_c5"] = {
+    # CPU leg and traversal counts: the restated path loop over 4 of the 1080 rows
+    cores = os.cpu_count() or 1
+    nodes, tris, vv = bl.download()
+    baked = orc.Baked(nodes, tris, vv)
+    R = orc.Restatement()
+    bmot = lsc.baked_materials(bl.prim_ids())
+    rows = (538, 542)
+    t0 = time.perf_counter()
+    R.render(baked, _orc_cfg(orc, rcl), lsc.mats, bmot, rows=rows, threads=cores)
+    cpu_s = time.perf_counter() - t0
+    _, counts = R.render_stats(baked, _orc_cfg(orc, rcl), lsc.mats, bmot, rows=rows, threads=cores)
+    ceiling = _trace_ceiling(bl, lsc.verts, stream, dev)
+    best = min(tlp, tlw, tlt)
+    out = {
         "workload": "1920x1080, 64 spp, depth 8, roulette after bounce 2; 400 icospheres x 12,500 triangles + floor + "
                     "4 quad lights (5,000,010 triangles), 80/20 Lambertian/mirror; binned SAH + spatial splits, leaf 4",
         "sah_build_ms": round(tsah, 1), "sah_build_mtri_s": round(lsc.tris.shape[0] / tsah / 1e3, 3),
-        "plain_mpx_spp_s": mpx(nl, tlp), "wavefront_mpx_spp_s": mpx(nl, tlw),
-        "plain_ms": round(tlp, 1), "wavefront_ms": round(tlw, 1)}
+        "plain_mpx_spp_s": _mpx(nl, tlp), "wavefront_mpx_spp_s": _mpx(nl, tlw),
+        "wavefront_tuned_mpx_spp_s": _mpx(nl, tlt), "autotuned": tuned.as_dict(),
+        "plain_ms": round(tlp, 1), "wavefront_ms": round(tlw, 1), "wavefront_tuned_ms": round(tlt, 1),
+        "roofline": _render_roofline(counts, 1920 * (rows[1] - rows[0]) * 64, nl, best, ceiling,
+                                     {tlp: "plain", tlw: "wavefront", tlt: "wavefront (autotuned)"}[best]),
+        "cpu_baseline": {"value": round(1920 * (rows[1] - rows[0]) * 64 / cpu_s / 1e6, 4), "unit": "Mpx*spp/s",
+                         "cores": cores, "kind": "port (the oracle's restated path loop over the reference traversal)",
+                         "sample": f"rows {rows[0]}-{rows[1] - 1} of 1080 at 64 spp, scaled to the metric"}}
     bl.free()
     return out
+
+
+RENDER_WORKLOADS = {"c1": render_c1, "c3": render_c3, "c4": render_c4, "c5": render_c5}
+
+
+def render_workloads(stream, dev, which=None):
+    """The path-loop workloads (GPU numbers by CUDA events on torch's stream)."""
+    sys.path.insert(0, os.path.join(HERE, "oracle"))
+    names = {"c1": "plain_c1", "c3": "batched_c3", "c4": "adjoint_c4", "c5": "large_c5"}
+    return {names[k]: fn(stream, dev) for k, fn in RENDER_WORKLOADS.items() if which is None or k == which}
 
 
 def main():

@@ -120,6 +120,7 @@ class Restatement:
         L.orc_adjoint.argtypes = [vp, vp, vp, u32, vp, vp, vp, vp, vp, C.c_int]
         L.orc_philox.argtypes = [u32, u32, u32, u32, u32, u32, vp]
         L.orc_primary_rays.argtypes = [vp, u64, vp, vp, vp, vp, vp]
+        L.orc_render_stats.argtypes = [vp, vp, vp, u32, vp, vp, vp, u32, u32, u32, u32, vp, vp, C.c_int]
         L.orc_trace_brute.argtypes = [vp, vp, u32, vp, u64, u32, vp, vp, vp]
         L.orc_cosine_dirs.argtypes = [u64, vp, vp, vp, vp]
         L.orc_ibl_lookup.argtypes = [vp, u32, u32, u64, vp, vp]
@@ -201,6 +202,24 @@ class Restatement:
                              _p(em), ew, eh, r0, r1, _p(rgb), _p(rgb2), threads)
         self.L.orc_free(hnd)
         return rgb, rgb2
+
+    def render_stats(self, baked: Baked, rcfg: OrcRenderCfg, mats=None, mat_of_tri=None, rows=None, threads: int = 1,
+                     tri_albedo=None, env_map=None):
+        """Rows [r0, r1) of render() plus its traversal work: (rgb, (segments traced, nodes
+        popped, triangles tested) summed over every sample of those rows)."""
+        W, H = rcfg.width, rcfg.height
+        rgb = np.zeros((H, W, 3), np.float32)
+        hnd = self._handle(baked)
+        r0, r1 = rows if rows is not None else (0, H)
+        mats_arr, mot = self._mats(mats, mat_of_tri)
+        ta = np.ascontiguousarray(tri_albedo, np.float32) if tri_albedo is not None else None
+        em = np.ascontiguousarray(env_map, np.float32) if env_map is not None else None
+        eh, ew = (em.shape[0], em.shape[1]) if em is not None else (0, 0)
+        counts = np.zeros(3, np.uint64)
+        self.L.orc_render_stats(hnd, C.byref(rcfg), mats_arr, len(mats) if mats is not None else 0, _p(mot), _p(ta),
+                                _p(em), ew, eh, r0, r1, _p(rgb), _p(counts), threads)
+        self.L.orc_free(hnd)
+        return rgb, tuple(int(x) for x in counts)
 
     def adjoint(self, baked: Baked, rcfg: OrcRenderCfg, d_rgb, mats=None, mat_of_tri=None, tri_albedo=None,
                 threads: int = 1):

@@ -1154,7 +1154,7 @@ void orc_ibl_lookup(const float* map, uint32_t w, uint32_t h, uint64_t n, const 
 
 /* primaryRay + pathTrace (src/main.cpp:69-83, 145-204) for one sample of one pixel; rec
  * (optional) receives the vertices of the path. */
-static v3 path_sample(const render_ctx* R, uint32_t x, uint32_t y, uint32_t sidx, path_rec* rec)
+static v3 path_sample(const render_ctx* R, uint32_t x, uint32_t y, uint32_t sidx, path_rec* rec, uint64_t* st3)
 {
     const orc_render_cfg* C = R->C;
     const uint32_t W = C->width, pix = y * W + x;
@@ -1166,7 +1166,9 @@ static v3 path_sample(const render_ctx* R, uint32_t x, uint32_t y, uint32_t sidx
     for (uint32_t bounce = 0; bounce <= C->max_bounce; bounce++)
     {
         ohit h;
-        traverse(R->B, &ray, 0u, &h, NULL);
+        uint32_t ctr[3];
+        traverse(R->B, &ray, 0u, &h, st3 ? ctr : NULL);
+        if (st3) { st3[0] += 1u; st3[1] += ctr[0]; st3[2] += ctr[1]; }
         if (!h.hit)
         {
             v3 env;
@@ -1221,6 +1223,8 @@ typedef struct
     uint32_t row0, row1; float* rgb; float* rgb2;
     /* adjoint */
     const float* dimg; double* g_alb; double* g_em;
+    /* traversal counts (orc_render_stats): segments traced, nodes popped, triangles tested */
+    int want_stats; uint64_t stats[3];
 } render_job;
 
 static void* render_worker(void* p)
@@ -1236,7 +1240,7 @@ static void* render_worker(void* p)
             v3 acc = mk3(0, 0, 0), acc2 = mk3(0, 0, 0);
             for (uint32_t s = 0; s < C->spp; s++)
             {
-                const v3 L = path_sample(J->R, x, y, C->sample_offset + s, NULL);
+                const v3 L = path_sample(J->R, x, y, C->sample_offset + s, NULL, J->want_stats ? J->stats : NULL);
                 acc = add3(acc, L);
                 acc2 = add3(acc2, mul3(L, L));
             }
@@ -1275,7 +1279,7 @@ static void* adjoint_worker(void* p)
             if (dl[0] == 0.0 && dl[1] == 0.0 && dl[2] == 0.0) { continue; }
             for (uint32_t s = 0; s < C->spp; s++)
             {
-                (void)path_sample(J->R, x, y, C->sample_offset + s, &rec);
+                (void)path_sample(J->R, x, y, C->sample_offset + s, &rec, NULL);
                 const uint32_t n = rec.n;
                 /* T[i] = prod_{j<i} w_j */
                 for (int c = 0; c < 3; c++) { T[0][c] = 1.0; }
@@ -1352,9 +1356,17 @@ static void run_rows(render_job* proto, uint32_t row0, uint32_t row1, int nthrea
         }
         jobs[used++] = J;
     }
-    if (used == 1) { fn(&jobs[0]); return; }
-    for (int t = 0; t < used; t++) { pthread_create(&th[t], NULL, fn, &jobs[t]); }
-    for (int t = 0; t < used; t++) { pthread_join(th[t], NULL); }
+    if (used == 1) { fn(&jobs[0]); }
+    else
+    {
+        for (int t = 0; t < used; t++) { pthread_create(&th[t], NULL, fn, &jobs[t]); }
+        for (int t = 0; t < used; t++) { pthread_join(th[t], NULL); }
+    }
+    if (fn == render_worker && proto->want_stats)
+    {
+        for (int t = 0; t < used; t++) { for (int k = 0; k < 3; k++) { proto->stats[k] += jobs[t].stats[k]; } }
+    }
+    if (used == 1) { return; }
     if (fn == adjoint_worker)
     {
         for (int t = 1; t < used; t++)
@@ -1371,8 +1383,19 @@ void orc_render_ex(const orc_bvh* B, const orc_render_cfg* C, const orc_material
 {
     if (row1 > C->height) { row1 = C->height; }
     render_ctx R = { B, C, mats, mot, tri_albedo, n_mats, env_map, env_w, env_h };
-    render_job P = { &R, 0, 0, rgb, rgb2, NULL, NULL, NULL };
+    render_job P = { &R, 0, 0, rgb, rgb2, NULL, NULL, NULL, 0, { 0, 0, 0 } };
     run_rows(&P, row0, row1, nthreads, render_worker, 0, 0);
+}
+
+void orc_render_stats(const orc_bvh* B, const orc_render_cfg* C, const orc_material* mats, uint32_t n_mats,
+                      const uint32_t* mot, const float* tri_albedo, const float* env_map, uint32_t env_w,
+                      uint32_t env_h, uint32_t row0, uint32_t row1, float* rgb, uint64_t* counts3, int nthreads)
+{
+    if (row1 > C->height) { row1 = C->height; }
+    render_ctx R = { B, C, mats, mot, tri_albedo, n_mats, env_map, env_w, env_h };
+    render_job P = { &R, 0, 0, rgb, NULL, NULL, NULL, NULL, 1, { 0, 0, 0 } };
+    run_rows(&P, row0, row1, nthreads, render_worker, 0, 0);
+    for (int k = 0; k < 3; k++) { counts3[k] = P.stats[k]; }
 }
 
 void orc_render(const orc_bvh* B, const orc_render_cfg* C, const orc_material* mats, const uint32_t* mot,
@@ -1386,6 +1409,6 @@ void orc_adjoint(const orc_bvh* B, const orc_render_cfg* C, const orc_material* 
                  double* grad_emission, int nthreads)
 {
     render_ctx R = { B, C, mats, mot, tri_albedo, n_mats, NULL, 0, 0 };
-    render_job P = { &R, 0, 0, NULL, NULL, d_rgb, grad_albedo, mats ? grad_emission : NULL };
+    render_job P = { &R, 0, 0, NULL, NULL, d_rgb, grad_albedo, mats ? grad_emission : NULL, 0, { 0, 0, 0 } };
     run_rows(&P, 0, C->height, nthreads, adjoint_worker, (size_t)B->n_tris * 3, (size_t)n_mats * 3);
 }

@@ -123,6 +123,13 @@ void orc_render_ex(const orc_bvh* b, const orc_render_cfg* cfg, const orc_materi
                    const uint32_t* mat_of_tri, const float* tri_albedo, const float* env_map, uint32_t env_w,
                    uint32_t env_h, uint32_t row0, uint32_t row1, float* rgb, float* rgb2, int nthreads);
 
+/* orc_render_ex (without rgb2) that also counts, over every sample of rows [row0, row1), the
+ * segments traced (trace calls of pathTrace), the BVH nodes popped and the triangles tested:
+ * counts3 = those three totals, for the path loop's algorithmic traversal work. */
+void orc_render_stats(const orc_bvh* b, const orc_render_cfg* cfg, const orc_material* mats, uint32_t n_mats,
+                      const uint32_t* mat_of_tri, const float* tri_albedo, const float* env_map, uint32_t env_w,
+                      uint32_t env_h, uint32_t row0, uint32_t row1, float* rgb, uint64_t* counts3, int nthreads);
+
 /* Gradients of sum(d_rgb * image) with respect to the per-triangle albedo (grad_albedo,
  * n_tris*3, used when tri_albedo is given or materials supply the albedo) and the material
  * emission (grad_emission, n_mats*3), accumulated in double precision into the arrays.
