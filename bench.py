@@ -70,6 +70,8 @@ def parse_args():
     p.add_argument("--preset", default="lbvh63")
     p.add_argument("--no-extra", action="store_true", help="skip the secondary measurements")
     p.add_argument("--no-render", action="store_true", help="skip the path-loop workloads")
+    p.add_argument("--kernels-only", action="store_true",
+                   help="time the device bake alone: no end-to-end or CPU legs (for profiling runs)")
     p.add_argument("--only", choices=["trace", "sah5m", "c1", "c3", "c4", "c5"],
                    help="run one secondary workload alone and print its figures (for profiling runs)")
     return p.parse_args()
@@ -327,6 +329,59 @@ def run_ours(a):
     # handles are independent; a bake call returns once its bake has finished), so that one
     # step's upload, another's bake and a third's download (rt_bvh_download_async) overlap; the
     # timed region ends after the last download has landed.
+    e2e_value = None
+    if not a.kernels_only:
+        e2e_value = end_to_end(a, bvh, dv, dt, verts, tris, cfg, nn, nt, dev, dist)
+    h2d = verts.nbytes + tris.nbytes
+    d2h = nn * 48 + nt * 12 + verts.nbytes
+
+    extra = {}
+    if not a.no_extra:
+        extra = secondary(a, bvh, dv, dt, verts, stream, dev, flush)
+    render = {}
+    if not a.no_render and rank == 0:
+        render = render_workloads(stream, dev)
+    out = None
+    if rank == 0:
+        cpu_v, cpu_kind = None, None
+        if not a.kernels_only:
+            with quiet_stdout():
+                cpu_v, cpu_kind, cpu_dt = cpu_reference_bake(n, scenes.BASE_SEED + 1, 3)
+        out = {"metric": METRIC, "value": round(value, 3), "unit": "Mtri/s", "n_gpus": world, "steps": a.steps,
+               "warmup": a.warmup, "ms_per_step": round(ms_step, 4), "higher_is_better": True, "scaling": "weak",
+               "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded soup, per-rank seed)",
+               "config": {"workload": WORKLOAD, "n_tris": n, "preset": a.preset, "nodes": nn, "baked_tris": nt,
+                          "l2": "flushed between steps (256 MiB write)", "parallelism": f"replicas x{world}"},
+               "e2e": ({"value": round(e2e_value, 3), "unit": "Mtri/s", "h2d_bytes_per_step": int(h2d),
+                        "d2h_bytes_per_step": int(d2h)} if e2e_value is not None else None),
+               "gpu_launches": int(launches),
+               "stage_ms": {k: round(v, 4) for k, v in st.items()},
+               "roofline": {"bound": "hbm", "kernel": f"LBVH bake, all {launches // a.steps} launches of one rebuild",
+                            "achieved": round(achieved, 1), "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
+                            "frac": round(achieved / peak, 4),
+                            "traffic": (round(traffic_per_tri * n) if traffic_per_tri else None),
+                            "algorithmic_bytes_per_launch": int(alg_bytes), "launch_ms": round(ms_step, 5),
+                            "builder_bytes_per_launch": int(own_bytes),
+                            "builder_frac": round(own_bytes / (ms_step * 1e-3) / 1e9 / peak, 4)},
+               "cpu_baseline": None if cpu_v is None else {"value": round(cpu_v, 4), "unit": "Mtri/s", "cores": 1, "kind": cpu_kind,
+                                "sample": f"bvh::bakeBVH of the same {n:,}-triangle soup, LBVH constants, 3 timed "
+                                          f"repetitions after one untimed, 1 thread (the bake is single-threaded)"},
+               "clocks": clocks, "extra": extra, "render": render}
+        print(json.dumps(out), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def end_to_end(a, bvh, dv, dt, verts, tris, cfg, nn, nt, dev, dist):
+    """The same bake end to end through the C ABI with host buffers (Mtri/s over all ranks)."""
+    import numpy as np
+    import torch
+    import rtb200
+    from rtb200.dist import max_over_ranks
+    rank, world, _ = env_rank()
+    n = dt.shape[0]
     import ctypes as C
     import threading
     hv = torch.from_numpy(verts).pin_memory()
@@ -371,45 +426,7 @@ def run_ours(a):
     for j in range(depth):  # the pipelined copies hold each handle's bake
         assert np.array_equal(outs[j][0].numpy(), handles[j].download()[0].view(np.uint8)), "e2e download mismatch"
     e2e_s = max_over_ranks(e2e_wall / k_e2e, dist, dev)
-    e2e_value = world * n / e2e_s / 1e6
-    h2d = verts.nbytes + tris.nbytes
-    d2h = nn * 48 + nt * 12 + verts.nbytes
-
-    extra = {}
-    if not a.no_extra:
-        extra = secondary(a, bvh, dv, dt, verts, stream, dev, flush)
-    render = {}
-    if not a.no_render and rank == 0:
-        render = render_workloads(stream, dev)
-    out = None
-    if rank == 0:
-        with quiet_stdout():
-            cpu_v, cpu_kind, cpu_dt = cpu_reference_bake(n, scenes.BASE_SEED + 1, 3)
-        out = {"metric": METRIC, "value": round(value, 3), "unit": "Mtri/s", "n_gpus": world, "steps": a.steps,
-               "warmup": a.warmup, "ms_per_step": round(ms_step, 4), "higher_is_better": True, "scaling": "weak",
-               "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded soup, per-rank seed)",
-               "config": {"workload": WORKLOAD, "n_tris": n, "preset": a.preset, "nodes": nn, "baked_tris": nt,
-                          "l2": "flushed between steps (256 MiB write)", "parallelism": f"replicas x{world}"},
-               "e2e": {"value": round(e2e_value, 3), "unit": "Mtri/s", "h2d_bytes_per_step": int(h2d),
-                       "d2h_bytes_per_step": int(d2h)},
-               "gpu_launches": int(launches),
-               "stage_ms": {k: round(v, 4) for k, v in st.items()},
-               "roofline": {"bound": "hbm", "kernel": f"LBVH bake, all {launches // a.steps} launches of one rebuild",
-                            "achieved": round(achieved, 1), "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
-                            "frac": round(achieved / peak, 4),
-                            "traffic": (round(traffic_per_tri * n) if traffic_per_tri else None),
-                            "algorithmic_bytes_per_launch": int(alg_bytes), "launch_ms": round(ms_step, 5),
-                            "builder_bytes_per_launch": int(own_bytes),
-                            "builder_frac": round(own_bytes / (ms_step * 1e-3) / 1e9 / peak, 4)},
-               "cpu_baseline": {"value": round(cpu_v, 4), "unit": "Mtri/s", "cores": 1, "kind": cpu_kind,
-                                "sample": f"bvh::bakeBVH of the same {n:,}-triangle soup, LBVH constants, 3 timed "
-                                          f"repetitions after one untimed, 1 thread (the bake is single-threaded)"},
-               "clocks": clocks, "extra": extra, "render": render}
-        print(json.dumps(out), flush=True)
-    if dist:
-        dist.barrier()
-        dist.destroy_process_group()
-    return 0
+    return world * n / e2e_s / 1e6
 
 
 def run_only(a, stream, dev):

@@ -7,11 +7,12 @@
 //  k_morton     quantisation + 3-way bit interleave (bvh_morton.cpp:19-36,61-101), and the
 //               digit histograms of every radix pass
 //  radix sort   stable onesweep LSD sort (radix_sort.cu; bvh_morton.cpp:109-159)
-//  k_climb      the binary radix tree over the sorted codes (Karras, HPG 2012), built bottom-up
-//               in one pass with every node's exact range box (Apetrei, 2014). Its split of a
-//               range whose first and last codes differ is the reference's Morton split (the
-//               first index where the highest differing bit flips, bvh_bfs.cpp:35-48,98-109),
-//               and a range box is the reference's computeRangeAABB (bvh_bfs.cpp:14-28)
+//  k_karras     the binary radix tree over the sorted codes (Karras, HPG 2012), every node
+//               found independently, and a hierarchy of block boxes over the sorted keys. Its
+//               split of a range whose first and last codes differ is the reference's Morton
+//               split (the first index where the highest differing bit flips,
+//               bvh_bfs.cpp:35-48,98-109); a node's range box, the reference's computeRangeAABB
+//               (bvh_bfs.cpp:14-28), is a union of at most 15 hierarchy blocks per level and end
 //  k_boundary   the reference stops splitting at <= BVH_MAX_LEAF_SIZE triangles and hands ranges
 //               of <= BVH_LBVH_THRESHOLD triangles or of identical codes to the binned SAH
 //               (bvh_bfs.cpp:30-33,79-107); this kernel finds those boundary nodes, marks their
@@ -276,24 +277,12 @@ k_morton(const float4* __restrict__ lo, const float4* __restrict__ hi, const flo
 }
 
 // Node ids of the binary radix tree: inner 0..n-2, leaf k -> n-1+k; knode = {first, last,
-// left, right} (built by k_climb below).
+// left, right} (built by k_karras below).
 template <typename K>
 __device__ __forceinline__ void krange(const uint4* __restrict__ knode, uint32_t n, uint32_t x, uint32_t& f, uint32_t& l)
 {
     if (x < n - 1) { const uint4 k = knode[x]; f = k.x; l = k.y; }
     else { f = l = x - (n - 1); }
-}
-
-// The reference splits a node by Morton code only if it has more triangles than both the
-// leaf size and the SAH threshold and its codes are not all equal (bvh_bfs.cpp:79-107).
-// A range over two or more scenes of a batched build is always split (at a scene boundary:
-// the scene bits are the highest key bits).
-template <typename K>
-__device__ __forceinline__ bool morton_split_node(const K* __restrict__ keys, uint32_t f, uint32_t l, uint32_t tm,
-                                                  uint32_t sshift)
-{
-    const uint64_t x = (uint64_t)(keys[f] ^ keys[l]);
-    return ((l - f + 1u) > tm && x != 0) || (x >> sshift) != 0;
 }
 
 __device__ __forceinline__ void store_box(float4* kbox, uint32_t x, const box3& b)
@@ -309,36 +298,407 @@ __device__ __forceinline__ box3 load_box(const float4* kbox, uint32_t x)
     return b;
 }
 
+// ---- the binary radix tree (Karras, "Maximizing Parallelism in the Construction of BVHs,
+// Octrees, and k-d Trees", HPG 2012) and the boxes of key ranges ----
+//
+// Inner node i (0 <= i < n - 1) of the tree over the sorted keys, each extended by its index so
+// that equal codes still differ, covers a key range with one end at i: its direction and other
+// end come from an exponential and a binary search on the length of the common prefix, its
+// split from one more binary search. Every node is found independently (no climb, no atomics).
+// The split of a range whose first and last codes differ is the reference's Morton split (the
+// first index where the highest differing bit flips, bvh_bfs.cpp:35-48,98-109).
+//
+// A node's box is the reference's computeRangeAABB (bvh_bfs.cpp:14-28): the union of the boxes
+// of the triangles in its key range. Level 0 of a hierarchy is the sorted keys, level k + 1 has
+// one element per 16 elements of level k (its box: their union, `blk`), and every element of
+// levels 0 .. top - 1 also has the union from the start of its group of 16 up to itself (`pre`)
+// and from itself to the end of the group (`suf`). A range whose ends lie in different groups
+// is then `suf` of its first element, `pre` of its last, and the same two entries one level up
+// for the groups strictly between, until both ends share a group: at most 2 loads per level plus
+// 14 at the top, all independent of one another (range_box). k_karras builds levels 0 and 1,
+// k_box_levels level 2 and, in its last block, the levels above.
+constexpr uint32_t LV_FAN = 16;
+constexpr int LV_MAX = 8;  // 16^8 = 2^32 keys
+
+// Elements of level k over n keys, and the number of levels below the first one-element level.
+__host__ __device__ __forceinline__ uint64_t lv_count(uint32_t n, int k) { return ((uint64_t)n + (1ull << (4 * k)) - 1) >> (4 * k); }
+inline int lv_top(uint32_t n)
+{
+    int k = 0;
+    while (k < LV_MAX && lv_count(n, k) > 1) { k++; }
+    return k;
+}
+// Offset (in boxes) of level k in the pre / suf arrays (levels 0 ..) and in the blk array
+// (levels 1 ..): the counts of the levels before it.
+__host__ __device__ __forceinline__ uint64_t lv_off(uint32_t n, int k, int first)
+{
+    uint64_t o = 0;
+    for (int j = first; j < k; j++) { o += lv_count(n, j); }
+    return o;
+}
+
+struct BoxLevels
+{
+    float4* pre;  // 2 float4 (min, max) per element of levels 0 .. top - 1
+    float4* suf;
+    float4* blk;  // levels 1 .. top
+    uint32_t n;
+    int top;
+};
+
+__device__ __forceinline__ void box_union(box3& b, float4 mn, float4 mx)
+{
+    b.mn[0] = sse_min(b.mn[0], mn.x); b.mn[1] = sse_min(b.mn[1], mn.y); b.mn[2] = sse_min(b.mn[2], mn.z);
+    b.mx[0] = sse_max(b.mx[0], mx.x); b.mx[1] = sse_max(b.mx[1], mx.y); b.mx[2] = sse_max(b.mx[2], mx.z);
+}
+__device__ __forceinline__ void box_union_at(box3& b, const float4* __restrict__ a, uint64_t e)
+{
+    box_union(b, __ldcg(&a[2 * e]), __ldcg(&a[2 * e + 1]));
+}
+__device__ __forceinline__ void put_box(float4* __restrict__ a, uint64_t e, float4 mn, float4 mx)
+{
+    __stcg(&a[2 * e], mn);
+    __stcg(&a[2 * e + 1], mx);
+}
+
+// Box of the triangles of sorted keys [f, l] (inclusive).
+__device__ box3 range_box(const uint32_t* __restrict__ perm, const float4* __restrict__ lo, const float4* __restrict__ hi,
+                          const BoxLevels& V, uint32_t f, uint32_t l)
+{
+    box3 b = box_empty();
+    if ((f >> 4) == (l >> 4))  // one group of 16 keys: its triangles' boxes
+    {
+#pragma unroll
+        for (uint32_t q = 0; q < LV_FAN; q++)
+        {
+            if (f + q <= l) { const uint32_t t = perm[f + q]; box_union(b, lo[t], hi[t]); }
+        }
+        return b;
+    }
+    box_union_at(b, V.suf, f);
+    box_union_at(b, V.pre, l);
+    uint64_t a = f >> 4, c = l >> 4, off_ps = V.n, off_blk = 0;
+#pragma unroll
+    for (int k = 1; k < LV_MAX; k++)
+    {
+        // elements a + 1 .. c - 1 of level k are still to be covered
+        if (a + 1 >= c) { break; }
+        if ((a >> 4) == (c >> 4))
+        {
+#pragma unroll
+            for (uint32_t q = 1; q < LV_FAN - 1; q++)
+            {
+                if (a + q < c) { box_union_at(b, V.blk, off_blk + a + q); }
+            }
+            break;
+        }
+        if ((a & 15u) != 15u) { box_union_at(b, V.suf, off_ps + a + 1); }
+        if ((c & 15u) != 0u) { box_union_at(b, V.pre, off_ps + c - 1); }
+        off_ps += lv_count(V.n, k);
+        off_blk += lv_count(V.n, k);
+        a >>= 4;
+        c >>= 4;
+    }
+    return b;
+}
+
+// Prefix and suffix unions over each group of 16 lanes of a full warp (lane 0 of a group ends
+// with the group's total as its suffix).
+__device__ __forceinline__ void group_scans(float4 mn, float4 mx, float4& pmn, float4& pmx, float4& smn, float4& smx)
+{
+    const uint32_t g = threadIdx.x & 15u;
+    pmn = mn; pmx = mx; smn = mn; smx = mx;
+#pragma unroll
+    for (int o = 1; o < 16; o <<= 1)
+    {
+        const float ax = __shfl_up_sync(0xffffffffu, pmn.x, o, 16), ay = __shfl_up_sync(0xffffffffu, pmn.y, o, 16);
+        const float az = __shfl_up_sync(0xffffffffu, pmn.z, o, 16);
+        const float bx = __shfl_up_sync(0xffffffffu, pmx.x, o, 16), by = __shfl_up_sync(0xffffffffu, pmx.y, o, 16);
+        const float bz = __shfl_up_sync(0xffffffffu, pmx.z, o, 16);
+        const float cx = __shfl_down_sync(0xffffffffu, smn.x, o, 16), cy = __shfl_down_sync(0xffffffffu, smn.y, o, 16);
+        const float cz = __shfl_down_sync(0xffffffffu, smn.z, o, 16);
+        const float dx = __shfl_down_sync(0xffffffffu, smx.x, o, 16), dy = __shfl_down_sync(0xffffffffu, smx.y, o, 16);
+        const float dz = __shfl_down_sync(0xffffffffu, smx.z, o, 16);
+        if (g >= (uint32_t)o)
+        {
+            pmn.x = sse_min(pmn.x, ax); pmn.y = sse_min(pmn.y, ay); pmn.z = sse_min(pmn.z, az);
+            pmx.x = sse_max(pmx.x, bx); pmx.y = sse_max(pmx.y, by); pmx.z = sse_max(pmx.z, bz);
+        }
+        if (g + (uint32_t)o < 16u)
+        {
+            smn.x = sse_min(smn.x, cx); smn.y = sse_min(smn.y, cy); smn.z = sse_min(smn.z, cz);
+            smx.x = sse_max(smx.x, dx); smx.y = sse_max(smx.y, dy); smx.z = sse_max(smx.z, dz);
+        }
+    }
+}
+
+__device__ __forceinline__ void empty_box4(float4& mn, float4& mx)
+{
+    const float inf = bits2f(0x7f800000u), ninf = bits2f(0xff800000u);
+    mn = make_float4(inf, inf, inf, 0.f);
+    mx = make_float4(ninf, ninf, ninf, 0.f);
+}
+
+// One level of the hierarchy from level k's element boxes, called by whole warps (element e,
+// 16-aligned groups; lanes with valid = false carry an empty box and write nothing): pre / suf
+// of every element and the blk box of every group (level k + 1).
+__device__ __forceinline__ void level_from(const BoxLevels& V, int k, uint64_t e, bool valid, float4 mn, float4 mx)
+{
+    float4 pmn, pmx, smn, smx;
+    group_scans(mn, mx, pmn, pmx, smn, smx);
+    if (!valid || e >= lv_count(V.n, k)) { return; }
+    const uint64_t o = lv_off(V.n, k, 0);
+    put_box(V.pre, o + e, pmn, pmx);
+    put_box(V.suf, o + e, smn, smx);
+    // the group's union is its first lane's suffix
+    if ((e & 15u) == 0) { put_box(V.blk, lv_off(V.n, k + 1, 1) + (e >> 4), smn, smx); }
+}
+
+// Length of the common prefix of sorted keys a and b extended by their indices; -1 when b is
+// outside the keys.
+template <typename K>
+__device__ __forceinline__ int prefix_len(const K* __restrict__ keys, uint32_t n, uint32_t a, int64_t b)
+{
+    if (b < 0 || b >= (int64_t)n) { return -1; }
+    const K x = keys[a] ^ keys[(uint32_t)b];
+    constexpr int W = 8 * (int)sizeof(K);
+    if (x == 0) { return W + __clz(a ^ (uint32_t)b); }
+    return sizeof(K) == 8 ? __clzll((unsigned long long)x) : __clz((unsigned int)x);
+}
+
+// Bucket table of the sorted keys: tab[b] = the first index whose top `tb` key bits are >= b,
+// for b = 0 .. 2^tb (tab[2^tb] = n). One thread per key writes the entries between its
+// predecessor's bucket and its own; thread n the entries past the last key.
+template <typename K>
+__global__ void __launch_bounds__(BLK)
+k_bucket_table(const K* __restrict__ keys, uint32_t n, int kshift, uint32_t tb_size, uint32_t* __restrict__ tab)
+{
+    const uint32_t i = blockIdx.x * BLK + threadIdx.x;
+    if (i > n) { return; }
+    const uint64_t b = i < n ? (uint64_t)(keys[i] >> kshift) : (uint64_t)tb_size;
+    const uint64_t b0 = i == 0 ? 0 : (uint64_t)(keys[i - 1] >> kshift) + 1u;
+    for (uint64_t q = b0; q <= b; q++) { tab[q] = i; }
+}
+
+// The reference splits a node by Morton code (it is "Morton-split") if it has more triangles
+// than the leaf size and the SAH threshold and its codes are not all equal, or if it spans
+// scenes of a batched build (bvh_bfs.cpp:79-107).
+template <typename K>
+__device__ __forceinline__ bool morton_split_keys(K kf, K kl, uint32_t size, uint32_t tm, uint32_t sshift)
+{
+    const uint64_t x = (uint64_t)(kf ^ kl);
+    return (size > tm && x != 0) || (x >> sshift) != 0;
+}
+
+// Per node flags written by the node's parent (the root's by thread 0): bit 0 kept (the parent
+// is Morton-split, or it is the root), bit 1 the node itself is Morton-split.
+constexpr uint8_t KF_KEPT = 1u, KF_MSPLIT = 2u;
+
+// One thread per sorted key i: level 0 (key i's triangle box) and level 1 of the box hierarchy;
+// inner node i ({first, last, left, right}; leaf k has id n - 1 + k), the parent of its two
+// children and their flags. The node's range is all keys sharing one more leading bit with key i
+// than its neighbour on the other side does; with the bucket table over the top `tb` key bits
+// (key_bits in all) the range, and then the split, are table lookups when that prefix is at most
+// tb bits long, and short binary searches inside one bucket otherwise; runs of equal keys
+// (split by the index bits) take the general exponential and binary searches.
+template <typename K>
+__global__ void __launch_bounds__(BLK)
+k_karras(const K* __restrict__ keys, const uint32_t* __restrict__ perm, uint32_t n, const float4* __restrict__ lo,
+         const float4* __restrict__ hi, uint4* __restrict__ knode, uint32_t* __restrict__ parent,
+         uint8_t* __restrict__ kflag, const uint32_t* __restrict__ tab, int key_bits, int tb, uint32_t tm,
+         uint32_t sshift, BoxLevels V, uint32_t* __restrict__ status)
+{
+    static_assert(BLK == LV_FAN * LV_FAN, "one block of threads covers one level-2 element");
+    __shared__ float4 s_mn[LV_FAN], s_mx[LV_FAN];
+    const uint32_t i = blockIdx.x * BLK + threadIdx.x;
+    float4 mn, mx;
+    empty_box4(mn, mx);
+    if (i < n)
+    {
+        const uint32_t t = perm[i];
+        mn = lo[t];
+        mx = hi[t];
+    }
+    {
+        float4 pmn, pmx, smn, smx;
+        group_scans(mn, mx, pmn, pmx, smn, smx);
+        if (i < n) { put_box(V.pre, i, pmn, pmx); put_box(V.suf, i, smn, smx); }
+        if ((threadIdx.x & 15u) == 0) { s_mn[threadIdx.x >> 4] = smn; s_mx[threadIdx.x >> 4] = smx; }
+    }
+    if (n >= 2 && i < n - 1)
+    {
+        constexpr int W = 8 * (int)sizeof(K);
+        const int lead = W - key_bits;  // leading bits every key has zero
+        const K ki = keys[i];
+        const int dR = prefix_len<K>(keys, n, i, (int64_t)i + 1), dL = prefix_len<K>(keys, n, i, (int64_t)i - 1);
+        const int d = dR > dL ? 1 : -1;
+        const int dmin = d > 0 ? dL : dR;
+        uint32_t f, l;
+        const int p = dmin + 1 - lead;  // key bits the range shares
+        if (dmin < W && p <= 0) { f = 0; l = n - 1; }
+        else if (dmin < W && p <= tb)
+        {
+            const uint64_t P = (uint64_t)(ki >> (key_bits - p));
+            f = tab[P << (tb - p)];
+            l = tab[(P + 1) << (tb - p)] - 1u;
+        }
+        else if (dmin < W)
+        {
+            // the range lies inside key i's bucket: the farthest key in direction d that still
+            // shares dmin + 1 bits with key i
+            const uint64_t b = (uint64_t)(ki >> (key_bits - tb));
+            const uint32_t lim = d > 0 ? tab[b + 1] - 1u - i : i - tab[b];
+            uint32_t len = 0;
+            for (uint32_t t = lim ? 1u << (31 - __clz(lim)) : 0u; t >= 1; t >>= 1)
+            {
+                if (len + t <= lim && prefix_len<K>(keys, n, i, (int64_t)i + (int64_t)(len + t) * d) > dmin) { len += t; }
+            }
+            const int64_t j = (int64_t)i + (int64_t)len * d;
+            f = (uint32_t)min((int64_t)i, j);
+            l = (uint32_t)max((int64_t)i, j);
+        }
+        else
+        {
+            uint64_t lmax = 2;
+            while (prefix_len<K>(keys, n, i, (int64_t)i + (int64_t)lmax * d) > dmin) { lmax <<= 1; }
+            uint64_t len = 0;
+            for (uint64_t t = lmax >> 1; t >= 1; t >>= 1)
+            {
+                if (prefix_len<K>(keys, n, i, (int64_t)i + (int64_t)(len + t) * d) > dmin) { len += t; }
+            }
+            const int64_t j = (int64_t)i + (int64_t)len * d;
+            f = (uint32_t)min((int64_t)i, j);
+            l = (uint32_t)max((int64_t)i, j);
+        }
+        // the split: the last key before the highest bit in which the range's ends differ flips
+        const K kf = keys[f], kl = keys[l];
+        uint32_t g;
+        if (kf == kl)
+        {
+            const int hb = 31 - __clz(f ^ l);  // a run of equal keys splits by the index bits
+            g = ((l >> hb) << hb) - 1u;
+        }
+        else
+        {
+            const int dn = prefix_len<K>(keys, n, f, (int64_t)l);
+            const int pn = dn - lead;  // key bits the whole range shares
+            if (pn + 1 <= tb)
+            {
+                const uint64_t P = pn == 0 ? 0ull : (uint64_t)(kf >> (key_bits - pn));
+                g = tab[((P << 1) | 1ull) << (tb - pn - 1)] - 1u;
+            }
+            else
+            {
+                uint32_t s = 0;
+                const uint32_t lim = l - f - 1u;
+                for (uint32_t t = lim ? 1u << (31 - __clz(lim)) : 0u; t >= 1; t >>= 1)
+                {
+                    if (s + t <= lim && prefix_len<K>(keys, n, f, (int64_t)f + s + t) > dn) { s += t; }
+                }
+                g = f + s;
+            }
+        }
+        if (g < f || g >= l || (d > 0 ? f != i : l != i)) { atomicOr(status, ST_CAPACITY); }
+        else
+        {
+            const uint32_t left = g == f ? n - 1 + g : g;
+            const uint32_t right = g + 1 == l ? n + g : g + 1;
+            knode[i] = make_uint4(f, l, left, right);
+            parent[left] = i;
+            parent[right] = i;
+            const bool ms = morton_split_keys<K>(kf, kl, l - f + 1u, tm, sshift);
+            const K kg = keys[g], kg1 = keys[g + 1];
+            const uint8_t kept = ms ? KF_KEPT : 0u;
+            kflag[left] = kept | (g > f && morton_split_keys<K>(kf, kg, g - f + 1u, tm, sshift) ? KF_MSPLIT : 0u);
+            kflag[right] = kept | (g + 1 < l && morton_split_keys<K>(kg1, kl, l - g, tm, sshift) ? KF_MSPLIT : 0u);
+            if (i == 0) { kflag[0] = KF_KEPT | (ms ? KF_MSPLIT : 0u); }  // the root (its range is all keys)
+        }
+    }
+    // level 1: the block's 16 groups of keys, in the first warp (its upper half idle)
+    __syncthreads();
+    if (threadIdx.x < 32 && V.top >= 1)
+    {
+        const bool mine = threadIdx.x < LV_FAN;
+        const uint64_t e = (uint64_t)blockIdx.x * LV_FAN + (threadIdx.x & 15u);
+        const bool valid = mine && e < lv_count(n, 1);
+        float4 a, c;
+        empty_box4(a, c);
+        if (valid)
+        {
+            a = s_mn[threadIdx.x];
+            c = s_mx[threadIdx.x];
+            put_box(V.blk, e, a, c);  // level 1 starts the blk array
+        }
+        if (V.top >= 2) { level_from(V, 1, e, valid, a, c); }
+    }
+}
+
+// Level 2 from level 1 (one thread per level-1 group), then, in the last block to finish, the
+// levels above.
+__global__ void __launch_bounds__(BLK) k_box_levels(BoxLevels V, uint32_t* __restrict__ ticket)
+{
+    __shared__ uint32_t s_last;
+    if (V.top >= 3)
+    {
+        const uint64_t e = (uint64_t)blockIdx.x * BLK + threadIdx.x;  // level-2 element
+        float4 mn, mx;
+        empty_box4(mn, mx);
+        if (e < lv_count(V.n, 2))
+        {
+            const uint64_t o = lv_off(V.n, 2, 1) + e;
+            mn = __ldcg(&V.blk[2 * o]);
+            mx = __ldcg(&V.blk[2 * o + 1]);
+        }
+        level_from(V, 2, e, true, mn, mx);
+    }
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) { s_last = atomicAdd(ticket, 1u) == gridDim.x - 1u ? 1u : 0u; }
+    __syncthreads();
+    if (!s_last) { return; }
+    __threadfence();
+    for (int k = 3; k < V.top; k++)
+    {
+        const uint64_t cnt = lv_count(V.n, k);
+        for (uint64_t e0 = 0; e0 < cnt; e0 += BLK)
+        {
+            const uint64_t e = e0 + threadIdx.x;
+            float4 mn, mx;
+            empty_box4(mn, mx);
+            if (e < cnt)
+            {
+                const uint64_t o = lv_off(V.n, k, 1) + e;
+                mn = __ldcg(&V.blk[2 * o]);
+                mx = __ldcg(&V.blk[2 * o + 1]);
+            }
+            level_from(V, k, e, true, mn, mx);
+        }
+        __threadfence_block();
+        __syncthreads();
+    }
+}
+
 // One thread per Karras node. Kept nodes (Morton-split nodes and the boundary nodes right
-// below them) record their left-spine rank; boundary nodes compute their range box, mark
-// their positions, register SAH roots, and climb to refit the Morton-split ancestors.
+// below them) record their left-spine rank and their range box; boundary nodes also mark their
+// positions and register SAH roots.
 template <typename K>
 __global__ void __launch_bounds__(BLK)
 k_boundary(const K* __restrict__ keys, const uint32_t* __restrict__ perm, uint32_t n, const uint4* __restrict__ knode,
            const uint32_t* __restrict__ parent, const float4* __restrict__ lo, const float4* __restrict__ hi,
+           BoxLevels V,
            uint32_t tm, uint32_t max_leaf, uint32_t sshift, float4* __restrict__ kbox, uint32_t* __restrict__ rank,
            uint32_t* __restrict__ wnode, uint32_t* __restrict__ wtri,
            uint8_t* __restrict__ kpos, SahRoot* __restrict__ roots, uint32_t* __restrict__ counters,
-           uint32_t* __restrict__ status)
+           const uint8_t* __restrict__ kflag, uint32_t* __restrict__ status)
 {
     const uint32_t x = blockIdx.x * BLK + threadIdx.x;
     if (x >= 2 * n - 1) { return; }
+    const uint8_t fl = kflag[x];
+    if (!(fl & KF_KEPT)) { return; }
+    const bool is_m = (fl & KF_MSPLIT) != 0;
     uint32_t f, l;
     krange<K>(knode, n, x, f, l);
-    const bool is_m = morton_split_node<K>(keys, f, l, tm, sshift);
     const uint32_t par = parent[x];
-    bool kept = is_m;
-    if (!is_m)
-    {
-        if (par == NONE) { kept = true; }
-        else
-        {
-            uint32_t pf, pl;
-            krange<K>(knode, n, par, pf, pl);
-            kept = morton_split_node<K>(keys, pf, pl, tm, sshift);
-        }
-    }
-    if (!kept) { return; }
 
     // left-spine rank: consecutive steps up while this chain is a left child
     uint32_t r = 0, cur = x, p = par;
@@ -348,14 +708,18 @@ k_boundary(const K* __restrict__ keys, const uint32_t* __restrict__ perm, uint32
         if (r > MAX_DEPTH) { atomicOr(status, ST_CAPACITY); return; }
     }
     rank[x] = r;
+    // the exact range box (computeRangeAABB): from the box hierarchy for an inner node, the
+    // triangle's own box for a single-key leaf
+    box3 b;
+    if (x < n - 1)
+    {
+        b = range_box(perm, lo, hi, V, f, l);
+        store_box(kbox, x, b);
+    }
     if (is_m) { return; }
 
-    // boundary node: its exact range box (computeRangeAABB) -- from the climb for an inner
-    // node, the triangle's own box for a single-key leaf
     const uint32_t size = l - f + 1u;
-    box3 b;
-    if (x < n - 1) { b = load_box(kbox, x); }
-    else
+    if (x >= n - 1)
     {
         const uint32_t t = perm[f];
         const float4 a = lo[t], c = hi[t];
@@ -364,208 +728,29 @@ k_boundary(const K* __restrict__ keys, const uint32_t* __restrict__ perm, uint32
     }
     if (size <= max_leaf)
     {
-        wnode[f] = r + 1u;
-        for (uint32_t k = f; k <= l; k++) { wtri[k] = 1u; kpos[k] = 1u; }
-        atomicAdd(&counters[1], 1u);
+        wnode[f] = r + 1u;  // its keys' wtri and kpos are 1 from k_clear
     }
     else
     {
+        // an SAH subtree root: its keys' triangles are counted and placed by the SAH builder
+        for (uint32_t k = f; k <= l; k++) { wtri[k] = 0u; kpos[k] = 0u; }
         uint32_t depth = 0;
         for (uint32_t q = par; q != NONE; q = parent[q])
         {
             if (++depth > MAX_DEPTH) { atomicOr(status, ST_CAPACITY); return; }
         }
-        const uint32_t slot = atomicAdd(&counters[0], 1u);
+        // one atomic per warp for the roots of its lanes
+        const unsigned m = __activemask();
+        const int lane = (int)(threadIdx.x & 31u), leader = __ffs(m) - 1;
+        uint32_t base = 0;
+        if (lane == leader) { base = atomicAdd(&counters[0], (uint32_t)__popc(m)); }
+        base = __shfl_sync(m, base, leader);
+        const uint32_t slot = base + (uint32_t)__popc(m & ((1u << lane) - 1u));
         SahRoot sr;
         sr.kid = x; sr.first = f; sr.count = size; sr.depth = depth; sr.rank = r;
         sr.scene = (uint32_t)((uint64_t)keys[f] >> sshift);
         for (int k = 0; k < 3; k++) { sr.box[k] = b.mn[k]; sr.box[3 + k] = b.mx[k]; }
         roots[slot] = sr;
-    }
-}
-
-// Whether the split after key a separates keys with a shorter common prefix than the split
-// after key b (keys extended by their index so that equal codes still differ).
-template <typename K>
-__device__ __forceinline__ bool split_lower(const K* __restrict__ keys, uint32_t a, uint32_t b)
-{
-    const K xa = keys[a] ^ keys[a + 1], xb = keys[b] ^ keys[b + 1];
-    if (xa != xb) { return xa < xb; }
-    return (a ^ (a + 1)) < (b ^ (b + 1));
-}
-
-// The climb runs in two phases so that most nodes need no device-scope fence:
-//  k_climb_local   one block per tile of CL_T sorted keys. A node whose parent split lies in
-//                  the tile (keys p and p + 1 both in it) meets its sibling through a slot in
-//                  shared memory, with boxes of the tile's inner nodes in shared memory, so only
-//                  block-scope ordering is needed. A node whose parent split is outside the
-//                  tile stops and becomes a frontier node; a slot where only one child arrived
-//                  is copied to the global slot array at the end of the block.
-//  k_climb_global  one thread per frontier node continues with global slots and device-scope
-//                  release / acquire fences (about depth x tiles nodes instead of all n - 1).
-// Both phases take the same parent for every node, so the tree is the one-pass tree.
-constexpr int CL_T = 256;
-constexpr unsigned long long CL_DONE = ~0ull - 1ull;
-
-// Shared memory of k_climb_local: exchange slots, boxes of the tile's inner nodes and leaves
-// (float4 pairs), and the tile's keys with one key of halo on either side.
-template <typename K>
-constexpr size_t climb_local_smem()
-{
-    return (size_t)CL_T * 8 + (size_t)4 * CL_T * 16 + (size_t)(CL_T + 2) * sizeof(K);
-}
-
-template <typename K>
-__global__ void __launch_bounds__(CL_T)
-k_climb_local(const K* __restrict__ keys, const uint32_t* __restrict__ perm, uint32_t n, const float4* __restrict__ lo,
-              const float4* __restrict__ hi, uint4* __restrict__ knode, uint32_t* __restrict__ parent,
-              unsigned long long* __restrict__ other, float4* __restrict__ kbox, uint32_t* __restrict__ frontier,
-              uint32_t* __restrict__ n_frontier, uint32_t* __restrict__ status)
-{
-    // the climb inside a tile touches only the tile's keys (and one on either side) and boxes of
-    // its own leaves and inner nodes: all are staged in shared memory first, so that the
-    // dependent chain of a climb does not wait on gathers from global memory
-    extern __shared__ __align__(16) unsigned char cl_smem[];
-    unsigned long long* s_other = reinterpret_cast<unsigned long long*>(cl_smem);  // slot of split p at p - t0
-    float4* s_box = reinterpret_cast<float4*>(s_other + CL_T);                     // inner node p at 2 (p - t0)
-    float4* s_leaf = s_box + 2 * CL_T;                                             // leaf k at 2 (k - t0)
-    K* s_key = reinterpret_cast<K*>(s_leaf + 2 * CL_T);                            // key t0 - 1 + i at i
-    const uint32_t t0 = blockIdx.x * (uint32_t)CL_T;
-    const uint32_t t1 = min(t0 + (uint32_t)CL_T, n);
-    const uint32_t k = t0 + threadIdx.x;
-    s_other[threadIdx.x] = ~0ull;
-    float4 mn = make_float4(0.f, 0.f, 0.f, 0.f), mx = mn;
-    if (k < n)
-    {
-        const uint32_t t = perm[k];
-        mn = lo[t];
-        mx = hi[t];
-        s_leaf[2 * threadIdx.x] = mn;
-        s_leaf[2 * threadIdx.x + 1] = mx;
-    }
-    for (uint32_t i = threadIdx.x; i < (uint32_t)CL_T + 2u; i += CL_T)
-    {
-        const uint32_t g = t0 + i;  // key g - 1
-        if (g >= 1 && g - 1 < n) { s_key[i] = keys[g - 1]; }
-    }
-    __syncthreads();
-    // split_lower on the staged keys: key j sits at s_key[j - t0 + 1]
-    auto lower = [&](uint32_t a, uint32_t b) -> bool {
-        const K xa = s_key[a - t0 + 1] ^ s_key[a - t0 + 2], xb = s_key[b - t0 + 1] ^ s_key[b - t0 + 2];
-        if (xa != xb) { return xa < xb; }
-        return (a ^ (a + 1)) < (b ^ (b + 1));
-    };
-    if (k < n && n >= 2)
-    {
-        uint32_t L = k, R = k, id = n - 1 + k;
-        for (uint32_t guard = 0;; guard++)
-        {
-            if (guard > MAX_DEPTH) { atomicOr(status, ST_CAPACITY); break; }
-            // L >= t0 and R < t1 here, so keys R, R + 1, L - 1 and L are staged
-            const bool go_right = (L == 0) || (R != n - 1 && lower(R, L - 1));
-            const uint32_t p = go_right ? R : L - 1;
-            parent[id] = p;
-            if (p < t0 || p + 1 >= t1)
-            {
-                frontier[atomicAdd(n_frontier, 1u)] = id;  // parent split outside the tile
-                break;
-            }
-            if (id < n - 1) { __threadfence_block(); }  // this node's box (s_box) before the exchange
-            const unsigned long long mine = ((unsigned long long)(go_right ? L : R) << 32) | id;
-            const unsigned long long prev = atomicExch(&s_other[p - t0], mine);
-            if (prev == ~0ull) { break; }  // first arrival
-            __threadfence_block();
-            const uint32_t sid = (uint32_t)prev;
-            // the sibling was completed or started in this block: its box is staged
-            const float4* sb = sid < n - 1 ? &s_box[2 * (sid - t0)] : &s_leaf[2 * (sid - (n - 1) - t0)];
-            const float4 smn = sb[0], smx = sb[1];
-            if (go_right) { R = (uint32_t)(prev >> 32); } else { L = (uint32_t)(prev >> 32); }
-            mn = make_float4(sse_min(mn.x, smn.x), sse_min(mn.y, smn.y), sse_min(mn.z, smn.z), 0.f);
-            mx = make_float4(sse_max(mx.x, smx.x), sse_max(mx.y, smx.y), sse_max(mx.z, smx.z), 0.f);
-            knode[p] = make_uint4(L, R, go_right ? id : sid, go_right ? sid : id);
-            __stcg(&kbox[2 * p], mn);
-            __stcg(&kbox[2 * p + 1], mx);
-            s_box[2 * (p - t0)] = mn;
-            s_box[2 * (p - t0) + 1] = mx;
-            s_other[p - t0] = CL_DONE;
-            id = p;
-            if (L == 0 && R == n - 1) { break; }  // the root
-        }
-    }
-    __syncthreads();
-    // slots with one arrival continue in the global phase
-    for (uint32_t i = threadIdx.x; t0 + i + 1 < t1; i += CL_T)
-    {
-        const unsigned long long v = s_other[i];
-        if (v != ~0ull && v != CL_DONE) { other[t0 + i] = v; }
-    }
-}
-
-// Bottom-up construction of the binary radix tree with boxes (Apetrei, "Fast and Simple
-// Agglomerative LBVH Construction", 2014), from the frontier nodes of k_climb_local: a node
-// covering keys [L, R] becomes a child of the split at R (right boundary) or at L-1 (left
-// boundary), whichever separates keys with the longer common prefix; the second child to
-// arrive completes the parent. Keys are extended by their index so equal codes split as in
-// the Karras tree; the tree is that same binary radix tree. Inner node p is the split between
-// keys p and p+1: it covers [L, R] with children [L, p] and [p+1, R]; its record is
-// {L, R, left id, right id} (leaf k has id n-1+k). other[p] (initially ~0) takes the first
-// arrival's outer bound and id in one exchange; its box is then in kbox (an inner node,
-// written before the release) or is its triangle's box (a leaf).
-template <typename K>
-__global__ void __launch_bounds__(BLK)
-k_climb_global(const K* __restrict__ keys, const uint32_t* __restrict__ perm, uint32_t n, const float4* __restrict__ lo,
-               const float4* __restrict__ hi, uint4* __restrict__ knode, uint32_t* __restrict__ parent,
-               unsigned long long* __restrict__ other, float4* __restrict__ kbox, const uint32_t* __restrict__ frontier,
-               const uint32_t* __restrict__ n_frontier, uint32_t* __restrict__ status)
-{
-    const uint32_t nf = *n_frontier;
-    for (uint32_t f = blockIdx.x * BLK + threadIdx.x; f < nf; f += gridDim.x * BLK)
-    {
-        uint32_t id = frontier[f], L, R;
-        float4 mn, mx;
-        if (id < n - 1)
-        {
-            const uint4 kn = __ldcg(&knode[id]);  // completed by the local phase
-            L = kn.x; R = kn.y;
-            mn = __ldcg(&kbox[2 * id]); mx = __ldcg(&kbox[2 * id + 1]);
-        }
-        else
-        {
-            L = R = id - (n - 1);
-            const uint32_t t = perm[L];
-            mn = lo[t]; mx = hi[t];
-        }
-        for (uint32_t guard = 0;; guard++)
-        {
-            if (guard > MAX_DEPTH) { atomicOr(status, ST_CAPACITY); break; }
-            const bool go_right = (L == 0) || (R != n - 1 && split_lower<K>(keys, R, L - 1));
-            const uint32_t p = go_right ? R : L - 1;  // go_right: this node is p's left child
-            parent[id] = p;
-            // an inner node's box was just written: release it before the exchange; a leaf's box
-            // lives in arrays written by an earlier kernel and needs no ordering
-            if (id < n - 1) { cuda::atomic_thread_fence(cuda::memory_order_release, cuda::thread_scope_device); }
-            cuda::atomic_ref<unsigned long long, cuda::thread_scope_device> ex(other[p]);
-            const unsigned long long mine = ((unsigned long long)(go_right ? L : R) << 32) | id;
-            const unsigned long long prev = ex.exchange(mine, cuda::memory_order_relaxed);
-            if (prev == ~0ull) { break; }  // first arrival: the sibling completes p
-            const uint32_t sid = (uint32_t)prev;
-            float4 smn, smx;
-            if (sid < n - 1)
-            {
-                cuda::atomic_thread_fence(cuda::memory_order_acquire, cuda::thread_scope_device);
-                smn = __ldcg(&kbox[2 * sid]);
-                smx = __ldcg(&kbox[2 * sid + 1]);
-            }
-            else { const uint32_t st = perm[sid - (n - 1)]; smn = lo[st]; smx = hi[st]; }
-            if (go_right) { R = (uint32_t)(prev >> 32); } else { L = (uint32_t)(prev >> 32); }
-            mn = make_float4(sse_min(mn.x, smn.x), sse_min(mn.y, smn.y), sse_min(mn.z, smn.z), 0.f);
-            mx = make_float4(sse_max(mx.x, smx.x), sse_max(mx.y, smx.y), sse_max(mx.z, smx.z), 0.f);
-            knode[p] = make_uint4(L, R, go_right ? id : sid, go_right ? sid : id);
-            __stcg(&kbox[2 * p], mn);
-            __stcg(&kbox[2 * p + 1], mx);
-            id = p;
-            if (L == 0 && R == n - 1) { break; }  // the root (internal node): no parent
-        }
     }
 }
 
@@ -577,20 +762,15 @@ __global__ void __launch_bounds__(BLK)
 k_emit(const K* __restrict__ keys, uint32_t n, const uint4* __restrict__ knode, const uint32_t* __restrict__ parent,
        uint32_t tm, uint32_t max_leaf, uint32_t sshift, const float4* __restrict__ kbox, const uint32_t* __restrict__ rank,
        const uint32_t* __restrict__ snode, const uint32_t* __restrict__ stri, rt_bvh_node* __restrict__ out,
-       uint32_t max_nodes, uint32_t* __restrict__ info, uint32_t* __restrict__ status)
+       uint32_t max_nodes, uint32_t* __restrict__ info, const uint8_t* __restrict__ kflag, uint32_t* __restrict__ status)
 {
     const uint32_t x = blockIdx.x * BLK + threadIdx.x;
     if (x >= 2 * n - 1) { return; }
+    const uint8_t fl = kflag[x];
+    if (!(fl & KF_KEPT)) { return; }
+    const bool is_m = (fl & KF_MSPLIT) != 0;
     uint32_t f, l;
     krange<K>(knode, n, x, f, l);
-    const bool is_m = morton_split_node<K>(keys, f, l, tm, sshift);
-    const uint32_t par = parent[x];
-    if (!is_m && par != NONE)
-    {
-        uint32_t pf, pl;
-        krange<K>(knode, n, par, pf, pl);
-        if (!morton_split_node<K>(keys, pf, pl, tm, sshift)) { return; }
-    }
     const uint32_t pre = snode[f] + rank[x];
     if (info)
     {
@@ -768,7 +948,7 @@ __global__ void __launch_bounds__(256) k_scan2_apply(Scan2 S, uint32_t n, const 
 
 // All per-build initialisation in one launch: block 0 also does k_init's work.
 __global__ void __launch_bounds__(BLK)
-k_clear(uint32_t n, uint32_t* __restrict__ parent, unsigned long long* __restrict__ visit, uint32_t* __restrict__ wnode,
+k_clear(uint32_t n, uint32_t* __restrict__ parent, uint8_t* __restrict__ kflag, uint32_t* __restrict__ wnode,
         uint32_t* __restrict__ wtri, uint8_t* __restrict__ kpos, uint32_t* __restrict__ scene, uint32_t n_scene_boxes,
         uint32_t* __restrict__ hist, uint32_t* __restrict__ counters, uint32_t* __restrict__ status,
         uint32_t* __restrict__ lookback, uint32_t n_lookback, uint32_t* __restrict__ tile_counters)
@@ -777,8 +957,10 @@ k_clear(uint32_t n, uint32_t* __restrict__ parent, unsigned long long* __restric
     if (i < n_lookback) { lookback[i] = 0u; }  // the radix sort's look-back words (all its passes)
     if (i < 64) { tile_counters[i] = 0u; }
     if (i < 2 * n - 1) { parent[i] = NONE; }
-    if (i < n) { visit[i] = ~0ull; kpos[i] = 0u; }
-    if (i <= n) { wnode[i] = 0u; wtri[i] = 0u; }
+    if (i == 0 && n == 1) { kflag[0] = KF_KEPT; }  // a single triangle: the root leaf (no k_karras)
+    // every key starts in a Morton leaf (k_boundary clears the keys of SAH subtree roots)
+    if (i < n) { kpos[i] = 1u; }
+    if (i <= n) { wnode[i] = 0u; wtri[i] = i < n ? 1u : 0u; }
     if (i < 6 * n_scene_boxes) { scene[i] = (i % 6) < 3 ? 0xffffffffu : 0u; }
     if (blockIdx.x == 0)
     {
@@ -801,13 +983,17 @@ int build_typed(rt_bvh* B, const rt_vertex* d_verts, uint32_t V, const rt_triang
     const int passes = sort_passes(key_bits);
     const int msd_shift = key_bits > 8 ? key_bits - 8 : -1;  // top digit, for the sort's MSD path
     const uint32_t nk = 2 * N - 1;  // Karras nodes
+    // the box hierarchy: pre / suf of levels 0 .. top - 1, blk of levels 1 .. top
+    const int lv_top_level = lv_top(N);
+    const uint64_t n_ps = lv_off(N, lv_top_level, 0), n_blk = lv_off(N, lv_top_level + 1, 1);
     if (S.tri_lo.ensure((size_t)N * 16) || S.tri_hi.ensure((size_t)N * 16) || S.tri_cz.ensure((size_t)N * 4) ||
         S.keys.ensure((size_t)N * sizeof(K)) || S.vals.ensure((size_t)N * 4) || S.hist.ensure(9 * 256 * 4) ||
         S.scene.ensure((size_t)n_boxes * 24 + 64) || S.status.ensure(64) || S.counters.ensure(64) ||
         (batch && (S.gtris.ensure((size_t)N * sizeof(rt_triangle)) || B->scene_info.ensure((size_t)bt.S * 16) ||
                    B->scene_roots.ensure((size_t)bt.S * 32))) ||
         S.knode.ensure((size_t)std::max<uint32_t>(N - 1, 1) * 16) || S.parent.ensure((size_t)nk * 4) ||
-        S.kbox.ensure((size_t)nk * 32) || S.visit.ensure((size_t)N * 8) || S.rank.ensure((size_t)nk * 4) ||
+        S.kbox.ensure((size_t)nk * 32) || S.lvbox.ensure((size_t)(2 * n_ps + n_blk) * 32 + 32) ||
+        S.kflag.ensure((size_t)nk + 16) || S.ktab.ensure(((size_t)1 << 16) * 4 + 16) || S.rank.ensure((size_t)nk * 4) ||
         S.wnode.ensure((size_t)(N + 1) * 4) || S.wtri.ensure((size_t)(N + 1) * 4) ||
         S.snode.ensure((size_t)(N + 1) * 4) || S.stri.ensure((size_t)(N + 1) * 4) || S.bnd.ensure((size_t)N) ||
         S.sah_roots.ensure((size_t)N * sizeof(SahRoot)))
@@ -816,6 +1002,12 @@ int build_typed(rt_bvh* B, const rt_vertex* d_verts, uint32_t V, const rt_triang
     }
     uint32_t* counters = S.counters.as<uint32_t>();
     uint32_t* status = counters + 15;  // read back with the counters in one copy
+    BoxLevels bl;
+    bl.pre = S.lvbox.as<float4>();
+    bl.suf = bl.pre + 2 * n_ps;
+    bl.blk = bl.suf + 2 * n_ps;
+    bl.n = N;
+    bl.top = lv_top_level;
     // the sort's scratch, zeroed by k_clear below (radix_sort_pairs then skips its memsets)
     const size_t n_lookback = sort_lookback_words(N, passes);
     if (S.sort.lookback.ensure(n_lookback * 4) || S.sort.tile_counters.ensure((64 + 260) * 4)) { return RT_E_CUDA; }
@@ -830,7 +1022,7 @@ int build_typed(rt_bvh* B, const rt_vertex* d_verts, uint32_t V, const rt_triang
     auto front = [&]() -> int {
         prof_mark(B, 0, st);
         k_clear<<<blocks_for(std::max<uint32_t>(std::max<uint32_t>(nk + 1, 6 * n_boxes), (uint32_t)n_lookback)), BLK, 0, st>>>(
-            N, S.parent.as<uint32_t>(), S.visit.as<unsigned long long>(), S.wnode.as<uint32_t>(), S.wtri.as<uint32_t>(),
+            N, S.parent.as<uint32_t>(), S.kflag.as<uint8_t>(), S.wnode.as<uint32_t>(), S.wtri.as<uint32_t>(),
             S.bnd.as<uint8_t>(), S.scene.as<uint32_t>(), n_boxes, S.hist.as<uint32_t>(), counters, status,
             S.sort.lookback.as<uint32_t>(), (uint32_t)n_lookback, S.sort.tile_counters.as<uint32_t>());
         count_launch();
@@ -869,31 +1061,23 @@ int build_typed(rt_bvh* B, const rt_vertex* d_verts, uint32_t V, const rt_triang
         prof_mark(B, 2, st);
         if (N >= 2)
         {
-            // the frontier list lives in the rank array, which k_boundary fills only afterwards
-            uint32_t* frontier = S.rank.as<uint32_t>();
-            static PerDeviceOnce cl_attr;  // per key type and device (bakes may run on several host threads and GPUs)
-            if (int e = cl_attr.once([] {
-                    RT_CUDA(cudaFuncSetAttribute(k_climb_local<K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                 (int)climb_local_smem<K>()));
-                    return (int)RT_OK;
-                }))
-            {
-                return e;
-            }
-            k_climb_local<K><<<blocks_for(N, CL_T), CL_T, climb_local_smem<K>(), st>>>(skeys, perm, N, S.tri_lo.as<float4>(), S.tri_hi.as<float4>(),
-                                                                   S.knode.as<uint4>(), S.parent.as<uint32_t>(),
-                                                                   S.visit.as<unsigned long long>(), S.kbox.as<float4>(),
-                                                                   frontier, counters + 8, status);
-            k_climb_global<K><<<std::min<uint32_t>(blocks_for(N), 4u * (uint32_t)device_sm_count()), BLK, 0, st>>>(
-                skeys, perm, N, S.tri_lo.as<float4>(), S.tri_hi.as<float4>(), S.knode.as<uint4>(), S.parent.as<uint32_t>(),
-                S.visit.as<unsigned long long>(), S.kbox.as<float4>(), frontier, counters + 8, status);
+            const int tb = std::min(16, key_bits);
+            k_bucket_table<K><<<blocks_for((uint64_t)N + 1), BLK, 0, st>>>(skeys, N, key_bits - tb, 1u << tb,
+                                                                         S.ktab.as<uint32_t>());
+            k_karras<K><<<blocks_for(N), BLK, 0, st>>>(skeys, perm, N, S.tri_lo.as<float4>(), S.tri_hi.as<float4>(),
+                                                       S.knode.as<uint4>(), S.parent.as<uint32_t>(), S.kflag.as<uint8_t>(),
+                                                       S.ktab.as<uint32_t>(), key_bits, tb, tm, sshift, bl, status);
+            count_launch();
+            // counters[8]: the ticket that elects the last block to build the upper levels
+            k_box_levels<<<blocks_for(lv_count(N, 2)), BLK, 0, st>>>(bl, counters + 8);
             count_launch(2);
         }
         k_boundary<K><<<blocks_for(nk), BLK, 0, st>>>(skeys, perm, N, S.knode.as<uint4>(), S.parent.as<uint32_t>(),
-                                                      S.tri_lo.as<float4>(), S.tri_hi.as<float4>(), tm, cfg.max_leaf, sshift,
+                                                      S.tri_lo.as<float4>(), S.tri_hi.as<float4>(), bl,
+                                                      tm, cfg.max_leaf, sshift,
                                                       S.kbox.as<float4>(), S.rank.as<uint32_t>(),
                                                       S.wnode.as<uint32_t>(), S.wtri.as<uint32_t>(), S.bnd.as<uint8_t>(),
-                                                      S.sah_roots.as<SahRoot>(), counters, status);
+                                                      S.sah_roots.as<SahRoot>(), counters, S.kflag.as<uint8_t>(), status);
         count_launch();
         if (int e = check_launch("boundary")) { return e; }
         prof_mark(B, 3, st);
@@ -949,7 +1133,8 @@ int build_typed(rt_bvh* B, const rt_vertex* d_verts, uint32_t V, const rt_triang
         k_emit<K><<<blocks_for(nk), BLK, 0, st>>>(skeys, N, S.knode.as<uint4>(), S.parent.as<uint32_t>(), tm, cfg.max_leaf,
                                                   sshift, S.kbox.as<float4>(), S.rank.as<uint32_t>(), S.snode.as<uint32_t>(),
                                                   S.stri.as<uint32_t>(), B->nodes.as<rt_bvh_node>(), 2 * cap - 1,
-                                                  batch ? B->scene_info.as<uint32_t>() : nullptr, status);
+                                                  batch ? B->scene_info.as<uint32_t>() : nullptr, S.kflag.as<uint8_t>(),
+                                                  status);
         count_launch();
         // without SAH subtrees every triangle passes here: its traversal record is written too
         // (input positions: the renormalisation changes only normals)
@@ -997,7 +1182,7 @@ int build_typed(rt_bvh* B, const rt_vertex* d_verts, uint32_t V, const rt_triang
     const bool graph_path = !batch && !B->prof && !expect_sah;
     auto bake_key = [&]() {
         const void* bufs[] = { S.tri_lo.p, S.tri_hi.p, S.tri_cz.p, S.keys.p, S.vals.p, S.hist.p, S.scene.p, S.counters.p,
-                               S.knode.p, S.parent.p, S.kbox.p, S.visit.p, S.rank.p, S.wnode.p, S.wtri.p, S.snode.p,
+                               S.knode.p, S.parent.p, S.kbox.p, S.lvbox.p, S.kflag.p, S.ktab.p, S.rank.p, S.wnode.p, S.wtri.p, S.snode.p,
                                S.stri.p, S.bnd.p, S.sah_roots.p, S.sort.keys_alt.p, S.sort.vals_alt.p, S.sort.lookback.p,
                                S.sort.tile_counters.p, S.scan.partials.p, B->nodes.p, B->tris.p, B->prim.p, B->verts.p,
                                B->gnodes.p, B->tripos.p, B->rootbuf.p, d_verts, d_tris };
@@ -1121,7 +1306,7 @@ int build_typed(rt_bvh* B, const rt_vertex* d_verts, uint32_t V, const rt_triang
             return fail(RT_E_CAPACITY, "batched build: a scene's root record is out of range");
         }
     }
-    B->stats[4] = res[1] + sah.leaves;
+    B->stats[4] = (B->n_nodes + 1u) / 2u;  // a full binary tree: one leaf more than inner nodes
     B->stats[3] = B->n_nodes - B->stats[4];
     B->trace_ww = prefer_while_while(B->n_tris, B->stats[4]);
     return RT_OK;

@@ -318,14 +318,108 @@ constexpr size_t local_sort_smem()
     return (size_t)LB * LI * sizeof(K) + (size_t)LB * LI * 4 + (size_t)(LB / 32) * 256 * 4 + 256 * 4;
 }
 
+// Compare-exchange partner order of the (key, position) pairs of a sub-bucket sort.
+template <typename K>
+__device__ __forceinline__ bool pair_less(K ka, uint32_t pa, K kb, uint32_t pb)
+{
+    return ka < kb || (ka == kb && pa < pb);
+}
+
+// Bitonic sort (Batcher, 1968) of one sub-bucket of cnt <= 64 keys in shared memory by one warp:
+// lane L holds elements L and L + 32 as (key, position in the sub-bucket, value); padding sorts
+// last. Ties on the key keep the position order, so the sort is stable.
+template <typename K>
+__device__ __forceinline__ void warp_sort64(K* sk, uint32_t* sv, uint32_t start, uint32_t cnt, int lane)
+{
+    K key[2];
+    uint32_t pos[2], val[2];
+#pragma unroll
+    for (int h = 0; h < 2; h++)
+    {
+        const uint32_t e = (uint32_t)lane + 32u * h;
+        const bool v = e < cnt;
+        key[h] = v ? sk[start + e] : (K)~(K)0;
+        val[h] = v ? sv[start + e] : 0u;
+        pos[h] = v ? e : 64u + e;
+    }
+#pragma unroll
+    for (int k = 2; k <= 64; k <<= 1)
+    {
+#pragma unroll
+        for (int j = k >> 1; j > 0; j >>= 1)
+        {
+            if (j == 32)
+            {
+                // elements L and L + 32 of one lane (k = 64: ascending)
+                if (pair_less<K>(key[1], pos[1], key[0], pos[0]))
+                {
+                    const K tk = key[0]; key[0] = key[1]; key[1] = tk;
+                    const uint32_t tp = pos[0]; pos[0] = pos[1]; pos[1] = tp;
+                    const uint32_t tv = val[0]; val[0] = val[1]; val[1] = tv;
+                }
+                continue;
+            }
+#pragma unroll
+            for (int h = 0; h < 2; h++)
+            {
+                const uint32_t idx = (uint32_t)lane + 32u * h;
+                const K ok = __shfl_xor_sync(0xffffffffu, key[h], j);
+                const uint32_t op = __shfl_xor_sync(0xffffffffu, pos[h], j);
+                const uint32_t ov = __shfl_xor_sync(0xffffffffu, val[h], j);
+                const bool lower = (idx & (uint32_t)j) == 0;
+                const bool asc = (idx & (uint32_t)k) == 0;
+                const bool other_less = pair_less<K>(ok, op, key[h], pos[h]);
+                // the lower index of an ascending pair (and the upper of a descending one) keeps the smaller
+                if (other_less == (lower == asc)) { key[h] = ok; pos[h] = op; val[h] = ov; }
+            }
+        }
+    }
+#pragma unroll
+    for (int h = 0; h < 2; h++)
+    {
+        const uint32_t e = (uint32_t)lane + 32u * h;
+        if (e < cnt) { sk[start + e] = key[h]; sv[start + e] = val[h]; }
+    }
+}
+
+// The same network on N = 16 or 32 elements, one per lane: the lanes of each group of N (idx =
+// lane mod N) sort the sub-bucket [start, start + cnt) they were given (cnt <= N; groups of 16
+// lanes in one warp may sort different sub-buckets).
+template <typename K, int N>
+__device__ __forceinline__ void warp_sort_n(K* sk, uint32_t* sv, uint32_t start, uint32_t cnt, uint32_t idx)
+{
+    const bool v = idx < cnt;
+    K key = v ? sk[start + idx] : (K)~(K)0;
+    uint32_t val = v ? sv[start + idx] : 0u;
+    uint32_t pos = v ? idx : 64u + idx;
+#pragma unroll
+    for (int k = 2; k <= N; k <<= 1)
+    {
+#pragma unroll
+        for (int j = k >> 1; j > 0; j >>= 1)
+        {
+            const K ok = __shfl_xor_sync(0xffffffffu, key, j);
+            const uint32_t op = __shfl_xor_sync(0xffffffffu, pos, j);
+            const uint32_t ov = __shfl_xor_sync(0xffffffffu, val, j);
+            const bool lower = (idx & (uint32_t)j) == 0;
+            const bool asc = (idx & (uint32_t)k) == 0;
+            if (pair_less<K>(ok, op, key, pos) == (lower == asc)) { key = ok; pos = op; val = ov; }
+        }
+    }
+    if (v) { sk[start + idx] = key; sv[start + idx] = val; }
+}
+
 // One block per bucket of the top digit: keys[bstart[b], bstart[b+1]) sorted stably by the
-// digits below the top one (npass 8-bit passes, ranked as in k_onesweep), kin/vin -> kout/vout
-// (may be the same buffers: the block holds its bucket in registers and shared memory before
-// writing).
+// digits below the top one, kin/vin -> kout/vout (may be the same buffers: the block holds its
+// bucket in registers and shared memory before writing). With sub_shift >= 0 the block first
+// takes one counting pass on the 8 bits below the top digit (bits sub_shift .. sub_shift + 7),
+// which splits the bucket into 256 sub-buckets, and, when none holds more than 64 keys, sorts
+// each with a warp's bitonic network on the whole key; otherwise (and with sub_shift < 0) it
+// takes npass 8-bit LSD passes, ranked as in k_onesweep.
 template <typename K, int LB, int LI, int MINB>
 __global__ void __launch_bounds__(LB, MINB)
 k_local_sort(const K* kin, const uint32_t* vin, K* kout, uint32_t* vout, const uint32_t* __restrict__ bstart,
-             const uint32_t* __restrict__ flag, int npass)
+             const uint32_t* __restrict__ flag, int npass, int sub_shift)
 {
     constexpr uint32_t CAP = (uint32_t)LB * LI;
     if (*flag) { return; }
@@ -335,6 +429,8 @@ k_local_sort(const K* kin, const uint32_t* vin, K* kout, uint32_t* vout, const u
     uint32_t* whist  = sv + CAP;                 // [warp][digit]
     uint32_t* tstart = whist + (LB / 32) * 256;  // block-local digit start
     __shared__ uint32_t s_warp_sums[8];
+    __shared__ uint32_t s_tot[256];
+    __shared__ uint32_t s_max;
     const uint32_t b0 = bstart[blockIdx.x], m = bstart[blockIdx.x + 1] - b0;
     if (m == 0) { return; }
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -342,16 +438,19 @@ k_local_sort(const K* kin, const uint32_t* vin, K* kout, uint32_t* vout, const u
     // element (warp, j, lane) = warp * 32 * LI + j * 32 + lane, so that order is input order
     K        key[LI];
     uint32_t val[LI];
+    auto load = [&]() {
 #pragma unroll
-    for (int j = 0; j < LI; j++)
-    {
-        const uint32_t e = (uint32_t)warp * (32u * LI) + (uint32_t)j * 32u + (uint32_t)lane;
-        if (e < m) { key[j] = kin[b0 + e]; val[j] = vin[b0 + e]; } else { key[j] = 0; val[j] = 0; }
-    }
+        for (int j = 0; j < LI; j++)
+        {
+            const uint32_t e = (uint32_t)warp * (32u * LI) + (uint32_t)j * 32u + (uint32_t)lane;
+            if (e < m) { key[j] = kin[b0 + e]; val[j] = vin[b0 + e]; } else { key[j] = 0; val[j] = 0; }
+        }
+    };
+    load();
     const uint32_t lt = (1u << lane) - 1u;
-    for (int p = 0; p < npass; p++)
-    {
-        const int shift = 8 * p;
+    // one stable counting pass of the registers' keys by bits shift .. shift + 7 into sk / sv;
+    // leaves the digit totals in s_tot and their exclusive scan in tstart
+    auto pass = [&](int shift) {
         for (int i = threadIdx.x; i < nw * 256; i += LB) { whist[i] = 0u; }
         __syncthreads();
         uint32_t* wh = whist + warp * 256;
@@ -387,6 +486,7 @@ k_local_sort(const K* kin, const uint32_t* vin, K* kout, uint32_t* vout, const u
                 whist[w * 256 + threadIdx.x] = total;
                 total += c;
             }
+            s_tot[threadIdx.x] = total;
         }
         __syncthreads();
         // exclusive scan of the 256 digit totals (warps 0..7 hold them; the others scan zeros)
@@ -424,26 +524,79 @@ k_local_sort(const K* kin, const uint32_t* vin, K* kout, uint32_t* vout, const u
             }
         }
         __syncthreads();
-        if (p + 1 < npass)
+    };
+    bool sorted = false;
+    if (sub_shift >= 0)
+    {
+        if (threadIdx.x == 0) { s_max = 0u; }
+        pass(sub_shift);
+        if (threadIdx.x < 256) { atomicMax(&s_max, s_tot[threadIdx.x]); }
+        __syncthreads();
+        if (s_max <= 64u)
+        {
+            // warp w owns digits w, w + LB/32, ...: one per lane; small sub-buckets two at a time
+            // with 16-lane networks, then 32- and 64-element networks for the larger ones
+            constexpr int NWARP = LB / 32;
+            const int myd = warp + NWARP * lane;
+            const uint32_t myc = myd < 256 ? s_tot[myd] : 0u;
+            uint32_t small = __ballot_sync(0xffffffffu, myc > 1u && myc <= 16u);
+            uint32_t mid = __ballot_sync(0xffffffffu, myc > 16u && myc <= 32u);
+            uint32_t big = __ballot_sync(0xffffffffu, myc > 32u);
+            while (small)
+            {
+                const int l1 = __ffs(small) - 1;
+                small &= small - 1u;
+                const int l2 = small ? __ffs(small) - 1 : -1;
+                if (l2 >= 0) { small &= small - 1u; }
+                const int mine = lane < 16 ? l1 : l2;
+                const uint32_t d = mine >= 0 ? (uint32_t)(warp + NWARP * mine) : 0u;
+                warp_sort_n<K, 16>(sk, sv, tstart[d], mine >= 0 ? s_tot[d] : 0u, (uint32_t)lane & 15u);
+            }
+            while (mid)
+            {
+                const int l1 = __ffs(mid) - 1;
+                mid &= mid - 1u;
+                const uint32_t d = (uint32_t)(warp + NWARP * l1);
+                warp_sort_n<K, 32>(sk, sv, tstart[d], s_tot[d], (uint32_t)lane);
+            }
+            while (big)
+            {
+                const int l1 = __ffs(big) - 1;
+                big &= big - 1u;
+                const uint32_t d = (uint32_t)(warp + NWARP * l1);
+                warp_sort64<K>(sk, sv, tstart[d], s_tot[d], lane);
+            }
+            __syncthreads();
+            sorted = true;
+        }
+        // else a crowded sub-bucket: the LSD passes below, from the registers (still in input order)
+    }
+    if (!sorted)
+    {
+        for (int p = 0; p < npass; p++)
+        {
+            pass(8 * p);
+            if (p + 1 < npass)
+            {
+#pragma unroll
+                for (int j = 0; j < LI; j++)
+                {
+                    const uint32_t e = (uint32_t)warp * (32u * LI) + (uint32_t)j * 32u + (uint32_t)lane;
+                    if (e < m) { key[j] = sk[e]; val[j] = sv[e]; }
+                }
+                __syncthreads();
+            }
+        }
+        if (npass == 0)  // nothing below the top digit: the bucket as it is
         {
 #pragma unroll
             for (int j = 0; j < LI; j++)
             {
                 const uint32_t e = (uint32_t)warp * (32u * LI) + (uint32_t)j * 32u + (uint32_t)lane;
-                if (e < m) { key[j] = sk[e]; val[j] = sv[e]; }
+                if (e < m) { sk[e] = key[j]; sv[e] = val[j]; }
             }
             __syncthreads();
         }
-    }
-    if (npass == 0)  // nothing below the top digit: the bucket as it is
-    {
-#pragma unroll
-        for (int j = 0; j < LI; j++)
-        {
-            const uint32_t e = (uint32_t)warp * (32u * LI) + (uint32_t)j * 32u + (uint32_t)lane;
-            if (e < m) { sk[e] = key[j]; sv[e] = val[j]; }
-        }
-        __syncthreads();
     }
     for (uint32_t i = threadIdx.x; i < m; i += LB)
     {
@@ -512,6 +665,8 @@ int radix_sort_pairs(K* keys, uint32_t* vals, bool vals_identity, uint32_t n, in
             K* kfin = (passes & 1) ? kalt : keys;
             uint32_t* vfin = (passes & 1) ? valt : vals;
             const int npass = sort_passes(key_bits - 8);
+            // more than 8 bits below the top digit: sub-buckets by the next 8 bits, sorted whole
+            const int sub_shift = key_bits - 8 > 8 ? key_bits - 16 : -1;
             // either this pass or the LSD passes use the look-back words (the flag picks one), so
             // one zeroing serves both
             if (!scratch_zeroed)
@@ -526,12 +681,12 @@ int radix_sort_pairs(K* keys, uint32_t* vals, bool vals_identity, uint32_t n, in
             if (small)
             {
                 k_local_sort<K, LS_SMALL_B, LS_SMALL_I, 2><<<256, LS_SMALL_B, sm_small, st>>>(kalt, valt, kfin, vfin, bstart,
-                                                                                           flag, npass);
+                                                                                           flag, npass, sub_shift);
             }
             else
             {
                 k_local_sort<K, LS_LARGE_B, LS_LARGE_I, 1><<<256, LS_LARGE_B, sm_large, st>>>(kalt, valt, kfin, vfin, bstart,
-                                                                                           flag, npass);
+                                                                                           flag, npass, sub_shift);
             }
             count_launch(3);
             RT_CUDA(cudaGetLastError());

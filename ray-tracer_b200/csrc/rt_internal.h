@@ -164,7 +164,8 @@ struct BuildScratch
     rtb::DevBuf knode;         // Karras inner nodes
     rtb::DevBuf parent;        // parent of every Karras node (2N-1)
     rtb::DevBuf kbox;          // boxes of kept Karras nodes (2N-1) x 6 floats
-    rtb::DevBuf visit;         // refit arrival counters
+    rtb::DevBuf lvbox;         // box hierarchy over the sorted keys (blocks of 16^k keys)
+    rtb::DevBuf kflag, ktab;   // per Karras node kept / Morton-split flags; bucket table of the sorted keys
     rtb::DevBuf rank;          // left-chain rank of kept Karras nodes
     rtb::DevBuf bnd;           // boundary node id per start key (or ~0)
     rtb::DevBuf wnode, wtri;   // per start key weights (nodes, triangles)
