@@ -28,6 +28,7 @@
 #include "cta_utils.cuh"
 #include "sah.cuh"
 #include "layout.cuh"
+#include "trace_core.cuh"
 
 #include <algorithm>
 #include <cstring>
@@ -506,7 +507,9 @@ __global__ void __launch_bounds__(BLK)
 k_karras(const K* __restrict__ keys, const uint32_t* __restrict__ perm, uint32_t n, const float4* __restrict__ lo,
          const float4* __restrict__ hi, uint4* __restrict__ knode, uint32_t* __restrict__ parent,
          uint8_t* __restrict__ kflag, const uint32_t* __restrict__ tab, int key_bits, int tb, uint32_t tm,
-         uint32_t sshift, BoxLevels V, uint32_t* __restrict__ status)
+         uint32_t sshift, BoxLevels V, const rt_triangle* __restrict__ tris, const rt_vertex* __restrict__ verts,
+         rt_triangle* __restrict__ out_tris, uint32_t* __restrict__ prim, float4* __restrict__ tp,
+         uint32_t* __restrict__ status)
 {
     static_assert(BLK == LV_FAN * LV_FAN, "one block of threads covers one level-2 element");
     __shared__ float4 s_mn[LV_FAN], s_mx[LV_FAN];
@@ -518,6 +521,21 @@ k_karras(const K* __restrict__ keys, const uint32_t* __restrict__ perm, uint32_t
         const uint32_t t = perm[i];
         mn = lo[t];
         mx = hi[t];
+        if (out_tris)
+        {
+            // the baked triangle at position i when the tree has no SAH subtrees (then every key is
+            // in a Morton leaf, in key order): the .bvh triangle, its input index and its
+            // traversal position record
+            const rt_triangle tr = tris[t];
+            out_tris[i] = tr;
+            prim[i] = t;
+            const rt_vertex& a = verts[tr.v[0]];
+            const rt_vertex& b = verts[tr.v[1]];
+            const rt_vertex& c = verts[tr.v[2]];
+            tp[3 * (size_t)i + 0] = make_float4(a.x, a.y, a.z, b.x);
+            tp[3 * (size_t)i + 1] = make_float4(b.y, b.z, c.x, c.y);
+            tp[3 * (size_t)i + 2] = make_float4(c.z, 0.f, 0.f, 0.f);
+        }
     }
     {
         float4 pmn, pmx, smn, smx;
@@ -762,7 +780,8 @@ __global__ void __launch_bounds__(BLK)
 k_emit(const K* __restrict__ keys, uint32_t n, const uint4* __restrict__ knode, const uint32_t* __restrict__ parent,
        uint32_t tm, uint32_t max_leaf, uint32_t sshift, const float4* __restrict__ kbox, const uint32_t* __restrict__ rank,
        const uint32_t* __restrict__ snode, const uint32_t* __restrict__ stri, rt_bvh_node* __restrict__ out,
-       uint32_t max_nodes, uint32_t* __restrict__ info, const uint8_t* __restrict__ kflag, uint32_t* __restrict__ status)
+       uint32_t max_nodes, uint32_t* __restrict__ info, const uint8_t* __restrict__ kflag, float* __restrict__ gn,
+       TraceRoot* __restrict__ root, uint32_t* __restrict__ status)
 {
     const uint32_t x = blockIdx.x * BLK + threadIdx.x;
     if (x >= 2 * n - 1) { return; }
@@ -795,6 +814,40 @@ k_emit(const K* __restrict__ keys, uint32_t n, const uint4* __restrict__ knode, 
     else
     {
         write_node(out, pre, b, 1, stri[f], l - f + 1u);
+    }
+    if (gn)
+    {
+        // the traversal layout (a tree without SAH subtrees): this node's box, reference and
+        // count in its parent's 64-byte record -- the left child's half is floats 0-5 and words
+        // 12 / 14, the right child's floats 6-11 and words 13 / 15 -- or the entry record (the root)
+        const uint32_t ref = is_m ? pre : stri[f];
+        const uint32_t cnt = is_m ? 0u : (LEAF_BIT | (l - f + 1u));
+        const uint32_t par = parent[x];
+        if (par == NONE)
+        {
+            TraceRoot r;
+            for (int k = 0; k < 3; k++) { r.box[k] = b.mn[k]; r.box[3 + k] = b.mx[k]; }
+            r.ref = is_m ? 0u : ref;
+            r.cnt = cnt;
+            *root = r;
+            return;
+        }
+        const uint4 pk = knode[par];
+        const bool left = pk.z == x;
+        // a left child follows its parent in pre-order; a right child's parent is found by its own slot
+        const uint32_t ppre = left ? pre - 1u : snode[pk.x] + rank[par];
+        float* g = gn + 16 * (size_t)ppre;
+        uint32_t* gu = reinterpret_cast<uint32_t*>(g);
+        if (left)
+        {
+            g[0] = b.mn[0]; g[1] = b.mn[1]; g[2] = b.mn[2]; g[3] = b.mx[0]; g[4] = b.mx[1]; g[5] = b.mx[2];
+            gu[12] = ref; gu[14] = cnt;
+        }
+        else
+        {
+            g[6] = b.mn[0]; g[7] = b.mn[1]; g[8] = b.mn[2]; g[9] = b.mx[0]; g[10] = b.mx[1]; g[11] = b.mx[2];
+            gu[13] = ref; gu[15] = cnt;
+        }
     }
 }
 
@@ -877,8 +930,7 @@ k_scan_apply(const uint32_t* __restrict__ in, uint32_t n, const uint32_t* __rest
     }
 }
 
-// The same scan over two arrays at once (the pre-order slot and triangle-offset weights):
-// three launches for both.
+// Exclusive scans of two arrays at once (the pre-order slot and triangle-offset weights).
 struct Scan2
 {
     const uint32_t* in[2];
@@ -886,65 +938,111 @@ struct Scan2
     uint32_t*       total[2];
 };
 
-__global__ void __launch_bounds__(256) k_scan2_reduce(Scan2 S, uint32_t n, uint32_t* __restrict__ part, uint32_t np)
-{
-    __shared__ uint32_t sh[9];
-    const uint32_t base = blockIdx.x * SCAN_TILE;
-    for (int a = 0; a < 2; a++)
-    {
-        uint32_t s = 0;
-        for (int j = 0; j < 8; j++)
-        {
-            const uint32_t i = base + j * 256 + threadIdx.x;
-            if (i < n) { s += S.in[a][i]; }
-        }
-        const uint32_t t = block_sum<256>(s, sh);
-        if (threadIdx.x == 0) { part[a * np + blockIdx.x] = t; }
-    }
-}
+// Both scans in one pass with decoupled look-back (Merrill and Garland, "Single-pass Parallel
+// Prefix Scan with Decoupled Look-back", 2016): blocks take tiles of SCAN_TILE elements in the
+// order they start (a ticket), publish each array's tile sum, then sum their predecessors'
+// published values back to the nearest inclusive prefix and publish their own. A descriptor is
+// one 64-bit word: flag in bits 62-63 (1 sum, 2 inclusive prefix), value in the low 32 bits.
+// desc (2 per tile) and the ticket after them start zeroed. Waits are bounded (ST_TIMEOUT).
+constexpr unsigned long long SC_AGG = 1ull << 62, SC_PRE = 2ull << 62, SC_FLAGS = 3ull << 62;
+constexpr uint32_t SC_SPIN_LIMIT = 1u << 22;
+// Large tiles: with every tile resident at once, a tile's look-back mostly finds sums, not
+// prefixes, so its walk is as long as the number of tiles before it (in windows of 32).
+constexpr int SC1_THREADS = 512, SC1_ITEMS = 16, SC1_TILE = SC1_THREADS * SC1_ITEMS;
 
-__global__ void __launch_bounds__(1024) k_scan2_partials(Scan2 S, uint32_t* __restrict__ part, uint32_t np)
+__global__ void __launch_bounds__(SC1_THREADS)
+k_scan2_onepass(Scan2 S, uint32_t n, unsigned long long* __restrict__ desc, uint32_t* __restrict__ ticket,
+                uint32_t* __restrict__ status)
 {
-    __shared__ uint32_t sh[33];
+    __shared__ uint32_t sh[SC1_THREADS / 32 + 1];
+    __shared__ uint32_t s_tile, s_prev[2];
+    if (threadIdx.x == 0) { s_tile = atomicAdd(ticket, 1u); }
+    __syncthreads();
+    const uint32_t tile = s_tile;
+    const uint32_t base = tile * SC1_TILE + threadIdx.x * SC1_ITEMS;
+    uint32_t v[2][SC1_ITEMS], excl[2], tot[2];
     for (int a = 0; a < 2; a++)
     {
-        uint32_t carry = 0;
-        for (uint32_t base = 0; base < np; base += 1024)
+        uint32_t sum = 0;
+        if (base + SC1_ITEMS <= n)
         {
-            const uint32_t i = base + threadIdx.x;
-            const uint32_t v = i < np ? part[a * np + i] : 0u;
-            uint32_t tot;
-            const uint32_t e = block_excl_scan<1024>(v, sh, &tot);
-            if (i < np) { part[a * np + i] = carry + e; }
-            carry += tot;
+            const uint4* q = reinterpret_cast<const uint4*>(S.in[a] + base);
+#pragma unroll
+            for (int j = 0; j < SC1_ITEMS / 4; j++)
+            {
+                const uint4 w = q[j];
+                v[a][4 * j] = w.x; v[a][4 * j + 1] = w.y; v[a][4 * j + 2] = w.z; v[a][4 * j + 3] = w.w;
+            }
         }
-        if (threadIdx.x == 0) { *S.total[a] = carry; }
+        else
+        {
+#pragma unroll
+            for (int j = 0; j < SC1_ITEMS; j++) { v[a][j] = base + j < n ? S.in[a][base + j] : 0u; }
+        }
+#pragma unroll
+        for (int j = 0; j < SC1_ITEMS; j++) { sum += v[a][j]; }
+        excl[a] = block_excl_scan<SC1_THREADS>(sum, sh, &tot[a]);
     }
-}
-
-__global__ void __launch_bounds__(256) k_scan2_apply(Scan2 S, uint32_t n, const uint32_t* __restrict__ part, uint32_t np)
-{
-    __shared__ uint32_t sh[9];
-    const uint32_t base = blockIdx.x * SCAN_TILE + threadIdx.x * 8;
+    // warp a (0, 1) publishes and looks back for array a, 32 predecessors at a time
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (warp < 2)
+    {
+        const int a = warp;
+        if (lane == 0)
+        {
+            cuda::atomic_ref<unsigned long long, cuda::thread_scope_device> mine(desc[2 * (size_t)tile + a]);
+            mine.store((tile == 0 ? SC_PRE : SC_AGG) | tot[a], cuda::memory_order_relaxed);
+        }
+        uint32_t prev = 0;
+        int64_t top = (int64_t)tile - 1;  // the window is tiles top - 31 .. top
+        while (top >= 0)
+        {
+            const int64_t p = top - lane;
+            unsigned long long w = SC_PRE;  // below tile 0: nothing to add
+            if (p >= 0)
+            {
+                cuda::atomic_ref<unsigned long long, cuda::thread_scope_device> d(desc[2 * (size_t)p + a]);
+                w = d.load(cuda::memory_order_relaxed);
+                for (uint32_t spin = 0; (w & SC_FLAGS) == 0; spin++)
+                {
+                    if (spin > SC_SPIN_LIMIT) { atomicOr(status, ST_TIMEOUT); w = SC_PRE; break; }
+                    w = d.load(cuda::memory_order_relaxed);
+                }
+            }
+            // the nearest inclusive prefix in the window ends the walk: lanes up to it add in
+            const unsigned pre = __ballot_sync(0xffffffffu, (w & SC_FLAGS) == SC_PRE);
+            const int stop = pre ? __ffs(pre) - 1 : 31;
+            uint32_t add = (lane <= stop && p >= 0) ? (uint32_t)w : 0u;
+            add = warp_sum(add);
+            prev += add;
+            if (pre) { break; }
+            top -= 32;
+        }
+        if (lane == 0)
+        {
+            if (tile > 0)
+            {
+                cuda::atomic_ref<unsigned long long, cuda::thread_scope_device> mine(desc[2 * (size_t)tile + a]);
+                mine.store(SC_PRE | (uint32_t)(prev + tot[a]), cuda::memory_order_relaxed);
+            }
+            s_prev[a] = prev;
+            if (tile == gridDim.x - 1) { *S.total[a] = prev + tot[a]; }
+        }
+    }
+    __syncthreads();
     for (int a = 0; a < 2; a++)
     {
-        uint32_t v[8];
-        uint32_t s = 0;
-        for (int j = 0; j < 8; j++)
-        {
-            const uint32_t i = base + j;
-            v[j] = i < n ? S.in[a][i] : 0u;
-            s += v[j];
-        }
-        uint32_t run = part[a * np + blockIdx.x] + block_excl_scan<256>(s, sh, nullptr);
-        for (int j = 0; j < 8; j++)
+        uint32_t run = s_prev[a] + excl[a];
+#pragma unroll
+        for (int j = 0; j < SC1_ITEMS; j++)
         {
             const uint32_t i = base + j;
             if (i < n) { S.out[a][i] = run; }
-            run += v[j];
+            run += v[a][j];
         }
     }
 }
+
 
 // All per-build initialisation in one launch: block 0 also does k_init's work.
 __global__ void __launch_bounds__(BLK)
@@ -956,7 +1054,7 @@ k_clear(uint32_t n, uint32_t* __restrict__ parent, uint8_t* __restrict__ kflag, 
     const uint32_t i = blockIdx.x * BLK + threadIdx.x;
     if (i < n_lookback) { lookback[i] = 0u; }  // the radix sort's look-back words (all its passes)
     if (i < 64) { tile_counters[i] = 0u; }
-    if (i < 2 * n - 1) { parent[i] = NONE; }
+    if (i == 0) { parent[0] = NONE; }  // the root (inner node 0, or the single leaf); k_karras sets the rest
     if (i == 0 && n == 1) { kflag[0] = KF_KEPT; }  // a single triangle: the root leaf (no k_karras)
     // every key starts in a Morton leaf (k_boundary clears the keys of SAH subtree roots)
     if (i < n) { kpos[i] = 1u; }
@@ -1018,6 +1116,11 @@ int build_typed(rt_bvh* B, const rt_vertex* d_verts, uint32_t V, const rt_triang
     // a captured bake leaves the sort's LSD fallback out and reports in counters[14] whether it
     // was needed (a top-digit bucket over one block); such a bake is then done again plainly
     bool msd_only = false;
+    // When the SAH threshold does not exceed the leaf size (the LBVH presets), subtrees for the
+    // binned SAH only come from runs of identical Morton codes; the layout is emitted at once
+    // and redone in the rare case such runs exist, which saves a host round trip.
+    const bool expect_sah = cfg.lbvh_threshold > cfg.max_leaf;
+    bool tris_fused = false;  // k_karras wrote the baked triangles (a build with no SAH subtree expected)
     // everything up to the boundary nodes, enqueued on st
     auto front = [&]() -> int {
         prof_mark(B, 0, st);
@@ -1064,9 +1167,15 @@ int build_typed(rt_bvh* B, const rt_vertex* d_verts, uint32_t V, const rt_triang
             const int tb = std::min(16, key_bits);
             k_bucket_table<K><<<blocks_for((uint64_t)N + 1), BLK, 0, st>>>(skeys, N, key_bits - tb, 1u << tb,
                                                                          S.ktab.as<uint32_t>());
+            // without expected SAH subtrees the baked triangles are written here (in key order); a
+            // bake that finds runs of equal codes after all writes them again in its second emit
+            const bool fuse = !expect_sah;
             k_karras<K><<<blocks_for(N), BLK, 0, st>>>(skeys, perm, N, S.tri_lo.as<float4>(), S.tri_hi.as<float4>(),
                                                        S.knode.as<uint4>(), S.parent.as<uint32_t>(), S.kflag.as<uint8_t>(),
-                                                       S.ktab.as<uint32_t>(), key_bits, tb, tm, sshift, bl, status);
+                                                       S.ktab.as<uint32_t>(), key_bits, tb, tm, sshift, bl, d_tris, d_verts,
+                                                       fuse ? B->tris.as<rt_triangle>() : nullptr, B->prim.as<uint32_t>(),
+                                                       B->tripos.as<float4>(), status);
+            tris_fused = fuse;
             count_launch();
             // counters[8]: the ticket that elects the last block to build the upper levels
             k_box_levels<<<blocks_for(lv_count(N, 2)), BLK, 0, st>>>(bl, counters + 8);
@@ -1120,28 +1229,34 @@ int build_typed(rt_bvh* B, const rt_vertex* d_verts, uint32_t V, const rt_triang
     // pre-order node slots and triangle offsets per start key, then the nodes and triangles
     auto emit_all = [&]() -> int {
         {
-            const uint32_t n1 = N + 1, np = (n1 + SCAN_TILE - 1) / SCAN_TILE;
-            if (S.scan.partials.ensure((size_t)2 * np * 4)) { return RT_E_CUDA; }
+            const uint32_t n1 = N + 1, np = (n1 + SC1_TILE - 1) / SC1_TILE;
+            // look-back descriptors (2 per tile) and the tile ticket, zeroed for every scan
+            if (S.scan.partials.ensure(((size_t)2 * np + 1) * 8)) { return RT_E_CUDA; }
+            unsigned long long* desc = S.scan.partials.as<unsigned long long>();
+            RT_CUDA(cudaMemsetAsync(desc, 0, ((size_t)2 * np + 1) * 8, st));
             Scan2 sc;
             sc.in[0] = S.wnode.as<uint32_t>(); sc.out[0] = S.snode.as<uint32_t>(); sc.total[0] = counters + 4;
             sc.in[1] = S.wtri.as<uint32_t>(); sc.out[1] = S.stri.as<uint32_t>(); sc.total[1] = counters + 5;
-            k_scan2_reduce<<<np, 256, 0, st>>>(sc, n1, S.scan.partials.as<uint32_t>(), np);
-            k_scan2_partials<<<1, 1024, 0, st>>>(sc, S.scan.partials.as<uint32_t>(), np);
-            k_scan2_apply<<<np, 256, 0, st>>>(sc, n1, S.scan.partials.as<uint32_t>(), np);
-            count_launch(3);
+            k_scan2_onepass<<<np, SC1_THREADS, 0, st>>>(sc, n1, desc, reinterpret_cast<uint32_t*>(desc + 2 * (size_t)np), status);
+            count_launch();
         }
         k_emit<K><<<blocks_for(nk), BLK, 0, st>>>(skeys, N, S.knode.as<uint4>(), S.parent.as<uint32_t>(), tm, cfg.max_leaf,
                                                   sshift, S.kbox.as<float4>(), S.rank.as<uint32_t>(), S.snode.as<uint32_t>(),
                                                   S.stri.as<uint32_t>(), B->nodes.as<rt_bvh_node>(), 2 * cap - 1,
                                                   batch ? B->scene_info.as<uint32_t>() : nullptr, S.kflag.as<uint8_t>(),
-                                                  status);
+                                                  n_roots == 0 ? B->gnodes.as<float>() : nullptr,
+                                                  B->rootbuf.as<TraceRoot>(), status);
         count_launch();
         // without SAH subtrees every triangle passes here: its traversal record is written too
-        // (input positions: the renormalisation changes only normals)
-        k_emit_tris<<<blocks_for(N), BLK, 0, st>>>(perm, S.bnd.as<uint8_t>(), S.stri.as<uint32_t>(), N, d_tris,
-                                                    B->tris.as<rt_triangle>(), B->prim.as<uint32_t>(), cap, d_verts,
-                                                    n_roots == 0 ? B->tripos.as<float4>() : nullptr, status);
-        count_launch();
+        // (input positions: the renormalisation changes only normals); k_karras wrote them already
+        // when no SAH subtree was expected and none came
+        if (!(tris_fused && n_roots == 0))
+        {
+            k_emit_tris<<<blocks_for(N), BLK, 0, st>>>(perm, S.bnd.as<uint8_t>(), S.stri.as<uint32_t>(), N, d_tris,
+                                                        B->tris.as<rt_triangle>(), B->prim.as<uint32_t>(), cap, d_verts,
+                                                        n_roots == 0 ? B->tripos.as<float4>() : nullptr, status);
+            count_launch();
+        }
         if (n_roots > 0)
         {
             if (int e = sah_emit(B, n_roots, S.snode.as<uint32_t>(), S.stri.as<uint32_t>(), d_tris, st, sah, 2 * cap - 1,
@@ -1153,17 +1268,18 @@ int build_typed(rt_bvh* B, const rt_vertex* d_verts, uint32_t V, const rt_triang
         return check_launch("emit");
     };
 
-    // When the SAH threshold does not exceed the leaf size (the LBVH presets), subtrees for the
-    // binned SAH only come from runs of identical Morton codes; the layout is emitted at once
-    // and redone in the rare case such runs exist, which saves a host round trip.
-    const bool expect_sah = cfg.lbvh_threshold > cfg.max_leaf;
     // emit and traversal layout, after the SAH subtrees if any
     auto tail = [&]() -> int {
         prof_mark(B, 4, st);
         if (int e = emit_all()) { return e; }
         prof_mark(B, 5, st);
         // traversal layout from the device-side counts: the build's only host round trip follows
-        if (int e = launch_traversal_layout(B, st, 2 * cap - 1, cap, counters + 4, status, n_roots == 0)) { return e; }
+        // without SAH subtrees k_emit wrote the traversal nodes and k_karras / k_emit_tris the
+        // triangle records
+        if (int e = launch_traversal_layout(B, st, 2 * cap - 1, cap, counters + 4, status, n_roots == 0, n_roots == 0))
+        {
+            return e;
+        }
         if (batch)
         {
             if (int e = launch_scene_roots(B, bt.S, counters + 4, status, st)) { return e; }
@@ -1347,6 +1463,7 @@ int build_bvh_batch(rt_bvh* B, const rt_vertex* d_verts, uint32_t V, const rt_tr
     if (cap < N) { cap = N; }
     const size_t max_nodes = (size_t)cap * 2 - 1;  // bvh_bfs.cpp:58
     if (B->tripos.ensure((size_t)cap * 48) ||  // written by k_emit_tris in builds without SAH subtrees
+        B->gnodes.ensure(max_nodes * sizeof(rt_gnode)) || B->rootbuf.ensure(sizeof(TraceRoot)) ||  // and by k_emit
         B->nodes.ensure(max_nodes * sizeof(rt_bvh_node)) || B->tris.ensure((size_t)cap * sizeof(rt_triangle)) ||
         B->prim.ensure((size_t)cap * 4) || B->verts.ensure((size_t)V * sizeof(rt_vertex)))
     {

@@ -262,9 +262,10 @@ int tree_depth(rt_bvh* b, cudaStream_t st, uint32_t* depth);
 int make_traversal_layout(rt_bvh* b, cudaStream_t st);
 // The same kernels without a host synchronisation: grids sized for max_nodes / max_tris,
 // d_counts (optional) = {nodes, triangles} on the device; structure violations set *vstatus;
-// tripos_ready: the triangle position records were written by the build already.
+// tripos_ready / gnodes_ready: the triangle position records / the traversal nodes and the
+// entry record were written by the build already.
 int launch_traversal_layout(rt_bvh* b, cudaStream_t st, uint32_t max_nodes, uint32_t max_tris, const uint32_t* d_counts,
-                            uint32_t* vstatus, bool tripos_ready = false);
+                            uint32_t* vstatus, bool tripos_ready = false, bool gnodes_ready = false);
 int trace(const rt_bvh* b, const rt_ray* d_rays, rt_hit* d_hits, uint64_t n, uint32_t flags, cudaStream_t st,
           uint32_t* d_status);
 // Launch options of the persistent trace kernel: block size (0: default), stack entries

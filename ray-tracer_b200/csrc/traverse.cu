@@ -239,16 +239,19 @@ TraceCtx make_trace_ctx(const rt_bvh* B)
 }
 
 int launch_traversal_layout(rt_bvh* B, cudaStream_t st, uint32_t max_nodes, uint32_t max_tris, const uint32_t* d_counts,
-                            uint32_t* vstatus, bool tripos_ready)
+                            uint32_t* vstatus, bool tripos_ready, bool gnodes_ready)
 {
     if (B->gnodes.ensure((size_t)max_nodes * sizeof(rt_gnode)) || B->tripos.ensure((size_t)(max_tris ? max_tris : 1) * 48) ||
         B->rootbuf.ensure(sizeof(TraceRoot)))
     {
         return RT_E_CUDA;
     }
-    k_make_gnodes<<<(max_nodes + 255) / 256, 256, 0, st>>>(B->nodes.as<rt_bvh_node>(), max_nodes, max_tris, d_counts,
-                                                           B->gnodes.as<rt_gnode>(), B->rootbuf.as<TraceRoot>(), vstatus);
-    count_launch();
+    if (!gnodes_ready)
+    {
+        k_make_gnodes<<<(max_nodes + 255) / 256, 256, 0, st>>>(B->nodes.as<rt_bvh_node>(), max_nodes, max_tris, d_counts,
+                                                               B->gnodes.as<rt_gnode>(), B->rootbuf.as<TraceRoot>(), vstatus);
+        count_launch();
+    }
     if (max_tris && !tripos_ready)
     {
         k_make_tripos<<<(max_tris + 255) / 256, 256, 0, st>>>(B->tris.as<rt_triangle>(), max_tris, d_counts,
