@@ -119,7 +119,7 @@ static void free_bvh(rt_bvh* b)
     DevBuf* bufs[] = { &b->nodes, &b->tris, &b->verts, &b->prim, &b->gnodes, &b->tripos, &b->trace_status, &b->trace_rays,
                        &b->trace_hits, &b->s.tri_lo, &b->s.tri_hi, &b->s.tri_cz, &b->s.keys, &b->s.vals, &b->s.hist,
                        &b->s.scene, &b->s.status, &b->s.sort.keys_alt, &b->s.sort.vals_alt, &b->s.sort.lookback,
-                       &b->s.sort.tile_counters, &b->s.scan.partials, &b->s.knode, &b->s.parent, &b->s.kbox, &b->s.lvbox, &b->s.kflag, &b->s.ktab,
+                       &b->s.sort.tile_counters, &b->s.scan.partials, &b->s.knode, &b->s.parent, &b->s.kbox, &b->s.lvbox, &b->s.kflag, &b->s.ktab, &b->s.tpin,
                        &b->s.rank, &b->s.bnd, &b->s.wnode, &b->s.wtri, &b->s.snode, &b->s.stri, &b->s.counters,
                        &b->s.sah_roots, &b->s.sah_refs_a, &b->s.sah_refs_b, &b->s.sah_tmp, &b->s.sah_pos,
                        &b->s.sah_lvl_a, &b->s.sah_lvl_b, &b->s.sah_dec, &b->s.sah_out, &b->s.sah_leaf_refs,

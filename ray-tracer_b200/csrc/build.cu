@@ -143,7 +143,7 @@ template <bool BATCH>
 __global__ void __launch_bounds__(BLK)
 k_tri_prep(const rt_triangle* __restrict__ tris, uint32_t N, const rt_vertex* __restrict__ verts, uint32_t V,
            float4* __restrict__ lo, float4* __restrict__ hi, float* __restrict__ cz, uint32_t* __restrict__ scene,
-           uint32_t* __restrict__ status, Batch bt, rt_triangle* __restrict__ gtris)
+           uint32_t* __restrict__ status, Batch bt, rt_triangle* __restrict__ gtris, float4* __restrict__ tpin)
 {
     const uint32_t i = blockIdx.x * BLK + threadIdx.x;
     __shared__ uint32_t soff[BATCH ? MAX_BATCH_SCENES + 1 : 1];
@@ -176,6 +176,14 @@ k_tri_prep(const rt_triangle* __restrict__ tris, uint32_t N, const rt_vertex* __
         lo[i] = make_float4(bx.mn[0], bx.mn[1], bx.mn[2], cx);
         hi[i] = make_float4(bx.mx[0], bx.mx[1], bx.mx[2], cy);
         cz[i] = czv;
+        if (tpin)
+        {
+            // the triangle's positions and vertex indices in one 48-byte record (input order), so
+            // that the sorted passes gather one record per triangle
+            tpin[3 * (size_t)i + 0] = make_float4(p0.x, p0.y, p0.z, p1.x);
+            tpin[3 * (size_t)i + 1] = make_float4(p1.y, p1.z, p2.x, p2.y);
+            tpin[3 * (size_t)i + 2] = make_float4(p2.z, __uint_as_float(a), __uint_as_float(b), __uint_as_float(c));
+        }
         for (int k = 0; k < 3; k++) { om[k] = f2ord(bx.mn[k]); oM[k] = f2ord(bx.mx[k]); }
     }
     if (BATCH)
@@ -507,7 +515,7 @@ __global__ void __launch_bounds__(BLK)
 k_karras(const K* __restrict__ keys, const uint32_t* __restrict__ perm, uint32_t n, const float4* __restrict__ lo,
          const float4* __restrict__ hi, uint4* __restrict__ knode, uint32_t* __restrict__ parent,
          uint8_t* __restrict__ kflag, const uint32_t* __restrict__ tab, int key_bits, int tb, uint32_t tm,
-         uint32_t sshift, BoxLevels V, const rt_triangle* __restrict__ tris, const rt_vertex* __restrict__ verts,
+         uint32_t sshift, BoxLevels V, const float4* __restrict__ tpin,
          rt_triangle* __restrict__ out_tris, uint32_t* __restrict__ prim, float4* __restrict__ tp,
          uint32_t* __restrict__ status)
 {
@@ -518,23 +526,26 @@ k_karras(const K* __restrict__ keys, const uint32_t* __restrict__ perm, uint32_t
     empty_box4(mn, mx);
     if (i < n)
     {
+        // key i's triangle: positions and vertex indices from its 48-byte record; its box as
+        // k_tri_prep forms it (the same min / max sequence over the three vertices)
         const uint32_t t = perm[i];
-        mn = lo[t];
-        mx = hi[t];
+        const float4 r0 = tpin[3 * (size_t)t], r1 = tpin[3 * (size_t)t + 1], r2 = tpin[3 * (size_t)t + 2];
+        box3 bx = box_empty();
+        box_pt(bx, mk3(r0.x, r0.y, r0.z));
+        box_pt(bx, mk3(r0.w, r1.x, r1.y));
+        box_pt(bx, mk3(r1.z, r1.w, r2.x));
+        mn = make_float4(bx.mn[0], bx.mn[1], bx.mn[2], 0.f);
+        mx = make_float4(bx.mx[0], bx.mx[1], bx.mx[2], 0.f);
         if (out_tris)
         {
             // the baked triangle at position i when the tree has no SAH subtrees (then every key is
             // in a Morton leaf, in key order): the .bvh triangle, its input index and its
             // traversal position record
-            const rt_triangle tr = tris[t];
-            out_tris[i] = tr;
+            out_tris[i] = rt_triangle{ { __float_as_uint(r2.y), __float_as_uint(r2.z), __float_as_uint(r2.w) } };
             prim[i] = t;
-            const rt_vertex& a = verts[tr.v[0]];
-            const rt_vertex& b = verts[tr.v[1]];
-            const rt_vertex& c = verts[tr.v[2]];
-            tp[3 * (size_t)i + 0] = make_float4(a.x, a.y, a.z, b.x);
-            tp[3 * (size_t)i + 1] = make_float4(b.y, b.z, c.x, c.y);
-            tp[3 * (size_t)i + 2] = make_float4(c.z, 0.f, 0.f, 0.f);
+            tp[3 * (size_t)i + 0] = r0;
+            tp[3 * (size_t)i + 1] = r1;
+            tp[3 * (size_t)i + 2] = make_float4(r2.x, 0.f, 0.f, 0.f);
         }
     }
     {
@@ -1085,6 +1096,7 @@ int build_typed(rt_bvh* B, const rt_vertex* d_verts, uint32_t V, const rt_triang
     const int lv_top_level = lv_top(N);
     const uint64_t n_ps = lv_off(N, lv_top_level, 0), n_blk = lv_off(N, lv_top_level + 1, 1);
     if (S.tri_lo.ensure((size_t)N * 16) || S.tri_hi.ensure((size_t)N * 16) || S.tri_cz.ensure((size_t)N * 4) ||
+        S.tpin.ensure((size_t)N * 48) ||
         S.keys.ensure((size_t)N * sizeof(K)) || S.vals.ensure((size_t)N * 4) || S.hist.ensure(9 * 256 * 4) ||
         S.scene.ensure((size_t)n_boxes * 24 + 64) || S.status.ensure(64) || S.counters.ensure(64) ||
         (batch && (S.gtris.ensure((size_t)N * sizeof(rt_triangle)) || B->scene_info.ensure((size_t)bt.S * 16) ||
@@ -1136,7 +1148,7 @@ int build_typed(rt_bvh* B, const rt_vertex* d_verts, uint32_t V, const rt_triang
         {
             k_tri_prep<true><<<blocks_for(N), BLK, 0, st>>>(d_tris, N, d_verts, V, S.tri_lo.as<float4>(), S.tri_hi.as<float4>(),
                                                              S.tri_cz.as<float>(), S.scene.as<uint32_t>(), status, bt,
-                                                             S.gtris.as<rt_triangle>());
+                                                             S.gtris.as<rt_triangle>(), S.tpin.as<float4>());
             d_tris = S.gtris.as<rt_triangle>();  // vertex indices of the concatenated array from here on
             k_morton<K, true><<<morton_blocks, BLK, 0, st>>>(S.tri_lo.as<float4>(), S.tri_hi.as<float4>(), S.tri_cz.as<float>(),
                                                              N, S.scene.as<uint32_t>(), cfg.morton_bits, passes,
@@ -1146,7 +1158,7 @@ int build_typed(rt_bvh* B, const rt_vertex* d_verts, uint32_t V, const rt_triang
         {
             k_tri_prep<false><<<blocks_for(N), BLK, 0, st>>>(d_tris, N, d_verts, V, S.tri_lo.as<float4>(), S.tri_hi.as<float4>(),
                                                               S.tri_cz.as<float>(), S.scene.as<uint32_t>(), status, bt,
-                                                              nullptr);
+                                                              nullptr, S.tpin.as<float4>());
             k_morton<K><<<morton_blocks, BLK, 0, st>>>(S.tri_lo.as<float4>(), S.tri_hi.as<float4>(), S.tri_cz.as<float>(), N,
                                                        S.scene.as<uint32_t>(), cfg.morton_bits, passes, S.keys.as<K>(),
                                                        S.hist.as<uint32_t>(), msd_shift);
@@ -1172,7 +1184,7 @@ int build_typed(rt_bvh* B, const rt_vertex* d_verts, uint32_t V, const rt_triang
             const bool fuse = !expect_sah;
             k_karras<K><<<blocks_for(N), BLK, 0, st>>>(skeys, perm, N, S.tri_lo.as<float4>(), S.tri_hi.as<float4>(),
                                                        S.knode.as<uint4>(), S.parent.as<uint32_t>(), S.kflag.as<uint8_t>(),
-                                                       S.ktab.as<uint32_t>(), key_bits, tb, tm, sshift, bl, d_tris, d_verts,
+                                                       S.ktab.as<uint32_t>(), key_bits, tb, tm, sshift, bl, S.tpin.as<float4>(),
                                                        fuse ? B->tris.as<rt_triangle>() : nullptr, B->prim.as<uint32_t>(),
                                                        B->tripos.as<float4>(), status);
             tris_fused = fuse;
@@ -1298,7 +1310,7 @@ int build_typed(rt_bvh* B, const rt_vertex* d_verts, uint32_t V, const rt_triang
     const bool graph_path = !batch && !B->prof && !expect_sah;
     auto bake_key = [&]() {
         const void* bufs[] = { S.tri_lo.p, S.tri_hi.p, S.tri_cz.p, S.keys.p, S.vals.p, S.hist.p, S.scene.p, S.counters.p,
-                               S.knode.p, S.parent.p, S.kbox.p, S.lvbox.p, S.kflag.p, S.ktab.p, S.rank.p, S.wnode.p, S.wtri.p, S.snode.p,
+                               S.knode.p, S.parent.p, S.kbox.p, S.lvbox.p, S.kflag.p, S.ktab.p, S.tpin.p, S.rank.p, S.wnode.p, S.wtri.p, S.snode.p,
                                S.stri.p, S.bnd.p, S.sah_roots.p, S.sort.keys_alt.p, S.sort.vals_alt.p, S.sort.lookback.p,
                                S.sort.tile_counters.p, S.scan.partials.p, B->nodes.p, B->tris.p, B->prim.p, B->verts.p,
                                B->gnodes.p, B->tripos.p, B->rootbuf.p, d_verts, d_tris };
@@ -1544,7 +1556,7 @@ int morton_order_noalloc_typed(unsigned char* base, const rt_vertex* verts, uint
     const int key_bits = 3 * (int)bits;
     k_init<<<1, 256, 0, st>>>(scene, hist, counters, status);
     k_tri_prep<false><<<blocks_for(N), BLK, 0, st>>>(tris, N, verts, V, lo, hi, cz, scene, status,
-                                                      Batch{ 0u, nullptr, nullptr, 63u, nullptr }, nullptr);
+                                                      Batch{ 0u, nullptr, nullptr, 63u, nullptr }, nullptr, nullptr);
     k_morton<K><<<blocks_for(N), BLK, 0, st>>>(lo, hi, cz, N, scene, bits, sort_passes(key_bits), keys, hist);
     count_launch(3);
     if (int e = check_launch("morton (no-alloc)")) { return e; }

@@ -166,6 +166,7 @@ struct BuildScratch
     rtb::DevBuf kbox;          // boxes of kept Karras nodes (2N-1) x 6 floats
     rtb::DevBuf lvbox;         // box hierarchy over the sorted keys (blocks of 16^k keys)
     rtb::DevBuf kflag, ktab;   // per Karras node kept / Morton-split flags; bucket table of the sorted keys
+    rtb::DevBuf tpin;          // per input triangle: positions and vertex indices (48-byte records)
     rtb::DevBuf rank;          // left-chain rank of kept Karras nodes
     rtb::DevBuf bnd;           // boundary node id per start key (or ~0)
     rtb::DevBuf wnode, wtri;   // per start key weights (nodes, triangles)
