@@ -761,8 +761,8 @@ k_boundary(const K* __restrict__ keys, const uint32_t* __restrict__ perm, uint32
     }
     else
     {
-        // an SAH subtree root: its keys' triangles are counted and placed by the SAH builder
-        for (uint32_t k = f; k <= l; k++) { wtri[k] = 0u; kpos[k] = 0u; }
+        // an SAH subtree root: the SAH builder clears its keys' wtri / kpos, then counts and places
+        // their triangles
         uint32_t depth = 0;
         for (uint32_t q = par; q != NONE; q = parent[q])
         {
@@ -1221,6 +1221,7 @@ int build_typed(rt_bvh* B, const rt_vertex* d_verts, uint32_t V, const rt_triang
         in.n_roots = n_roots;
         in.wnode = S.wnode.as<uint32_t>();
         in.wtri = S.wtri.as<uint32_t>();
+        in.kpos = S.bnd.as<uint8_t>();
         if (batch)
         {
             for (uint32_t k = 0; k < bt.S; k++)

@@ -107,8 +107,10 @@ RT_HD bool box_valid(const box3& b) { return b.mn[0] <= b.mx[0] && b.mn[1] <= b.
 
 // clipTriangleToAABB, src/bvh/AABB.cpp:86-171: Sutherland-Hodgman clip of the triangle
 // against the min then the max plane of x, y and z; returns the clipped polygon's box or
-// the empty box. At most 9 polygon vertices are live; 12 slots as in the reference.
-RT_HD box3 clip_triangle(f3 v0, f3 v1, f3 v2, const box3& region)
+// the empty box. At most 9 polygon vertices are live; 12 slots as in the reference. This is
+// the general form, with the polygon in indexed arrays; clip_triangle below computes the same
+// result in registers for the usual cases and falls back to it.
+RT_HD box3 clip_triangle_general(f3 v0, f3 v1, f3 v2, const box3& region)
 {
     // All three vertices inside the region: no plane removes or adds a vertex, so the clipped
     // polygon is the triangle and its box the vertices' box (the loop below would return the
@@ -160,6 +162,85 @@ RT_HD box3 clip_triangle(f3 v0, f3 v1, f3 v2, const box3& region)
     }
     box3 r = box_empty();
     for (int i = 0; i < n; i++) { box_pt(r, poly[i]); }
+    return r;
+}
+
+RT_HD float sel3(float x, float y, float z, int axis) { return axis == 0 ? x : (axis == 1 ? y : z); }
+
+// One Sutherland-Hodgman step (the loop body of clip_triangle_general for one plane) on a
+// polygon of at most 4 vertices held in registers; the result has at most 5.
+RT_HD void clip_step4(float (&px)[5], float (&py)[5], float (&pz)[5], int& n, int axis, int side, float plane)
+{
+    float qx[5] = { 0.f, 0.f, 0.f, 0.f, 0.f }, qy[5] = { 0.f, 0.f, 0.f, 0.f, 0.f }, qz[5] = { 0.f, 0.f, 0.f, 0.f, 0.f };
+    int m = 0;
+    auto push = [&](float x, float y, float z) {
+#pragma unroll
+        for (int k = 0; k < 5; k++)
+        {
+            if (k == m) { qx[k] = x; qy[k] = y; qz[k] = z; }
+        }
+        m++;
+    };
+#pragma unroll
+    for (int i = 0; i < 4; i++)
+    {
+        if (i < n)
+        {
+            const bool last = i + 1 == n;
+            const f3 a = mk3(px[i], py[i], pz[i]);
+            const f3 b = last ? mk3(px[0], py[0], pz[0]) : mk3(px[i + 1], py[i + 1], pz[i + 1]);
+            const float pi = sel3(a.x, a.y, a.z, axis), pn = sel3(b.x, b.y, b.z, axis);
+            const bool cin = side == 0 ? (pi >= plane) : (pi <= plane);
+            const bool nin = side == 0 ? (pn >= plane) : (pn <= plane);
+            if (cin) { push(a.x, a.y, a.z); }
+            if (cin != nin)
+            {
+                const float t = (plane - pi) / (pn - pi);
+                const f3 r = add3(a, muls(sub3(b, a), t));
+                push(r.x, r.y, r.z);
+            }
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < 5; k++) { px[k] = qx[k]; py[k] = qy[k]; pz[k] = qz[k]; }
+    n = m;
+}
+
+// clip_triangle_general's result with the polygon in registers: a plane every vertex lies
+// inside leaves the polygon as it is (no vertex dropped, no crossing), so it is skipped; the
+// planes that cut are applied while the polygon has at most 4 vertices (so at most 5 after),
+// and anything larger is handed to the general form.
+RT_HD box3 clip_triangle(f3 v0, f3 v1, f3 v2, const box3& region)
+{
+    float px[5] = { v0.x, v1.x, v2.x, 0.f, 0.f }, py[5] = { v0.y, v1.y, v2.y, 0.f, 0.f },
+          pz[5] = { v0.z, v1.z, v2.z, 0.f, 0.f };
+    int n = 3;
+    for (int pl = 0; pl < 6; pl++)
+    {
+        const int axis = pl >> 1, side = pl & 1;
+        const float plane = side == 0 ? sel3(region.mn[0], region.mn[1], region.mn[2], axis)
+                                      : sel3(region.mx[0], region.mx[1], region.mx[2], axis);
+        bool allin = true;
+#pragma unroll
+        for (int i = 0; i < 5; i++)
+        {
+            if (i < n)
+            {
+                const float c = sel3(px[i], py[i], pz[i], axis);
+                allin = allin && (side == 0 ? (c >= plane) : (c <= plane));
+            }
+        }
+        if (allin) { continue; }
+        if (n > 4) { return clip_triangle_general(v0, v1, v2, region); }
+        clip_step4(px, py, pz, n, axis, side, plane);
+        if (n == 0) { return box_empty(); }
+    }
+    box3 r = box_empty();
+#pragma unroll
+    for (int i = 0; i < 5; i++)
+    {
+        if (i < n) { box_pt(r, mk3(px[i], py[i], pz[i])); }
+    }
     return r;
 }
 

@@ -333,6 +333,62 @@ __device__ __forceinline__ void warp_eval_spatial_axis(const uint32_t* cin, cons
     }
 }
 
+// Spatial binning of references R[i0 + lane] (i0 + lane < n) along `axis` by one whole warp:
+// entry / exit counts, then every (triangle, bin) pair of the 32 references clipped and added to
+// its bin -- the pairs spread evenly over the lanes (a warp-wide scan of each reference's bin
+// count, each lane finding the owner of its pair by a binary search over the lanes), since the
+// references span different numbers of bins. The same clips as bvh_sah.cpp:175-193; the bin
+// boxes are exact unions, so their order does not matter.
+__device__ __forceinline__ void spatial_bin_warp(const Ctx& C, const uint32_t* R, uint32_t i0, uint32_t n, int axis,
+                                                 const box3& nbox, float node_min, float sscale, int nb, uint32_t* cin,
+                                                 uint32_t* cout, SBox* bins)
+{
+    const int lane = threadIdx.x & 31;
+    const uint32_t i = i0 + (uint32_t)lane;
+    uint32_t t = 0;
+    int bmin = 0, bmax = -1;
+    if (i < n)
+    {
+        t = R[i];
+        bmin = std_clampi(x86_f2i((tri_lo(C, t, axis) - node_min) * sscale), 0, nb - 1);
+        bmax = std_clampi(x86_f2i((tri_hi(C, t, axis) - node_min) * sscale), 0, nb - 1);
+        atomicAdd(&cin[bmin], 1u);
+        atomicAdd(&cout[bmax], 1u);
+    }
+    const uint32_t c = bmin <= bmax ? (uint32_t)(bmax - bmin + 1) : 0u;
+    const uint32_t incl = warp_incl_scan(c);
+    const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
+    for (uint32_t j0 = 0; j0 < total; j0 += 32)
+    {
+        const uint32_t j = j0 + (uint32_t)lane;
+        int o = 0;  // the lane whose pairs hold pair j: the number of lanes with incl <= j
+#pragma unroll
+        for (int step = 16; step >= 1; step >>= 1)
+        {
+            if (__shfl_sync(0xffffffffu, incl, o + step - 1) <= j) { o += step; }
+        }
+        const uint32_t to = __shfl_sync(0xffffffffu, t, o);
+        const int bo = __shfl_sync(0xffffffffu, bmin, o);
+        const uint32_t eo = __shfl_sync(0xffffffffu, incl - c, o);
+        if (j < total)
+        {
+            const int b = bo + (int)(j - eo);
+            f3 v0, v1, v2;
+            tri_verts(C, to, v0, v1, v2);
+            const float lo_b = node_min + (float)b / sscale, hi_b = node_min + (float)(b + 1) / sscale;
+            box3 region;
+#pragma unroll
+            for (int k = 0; k < 3; k++)
+            {
+                region.mn[k] = k == axis ? lo_b : nbox.mn[k];
+                region.mx[k] = k == axis ? hi_b : nbox.mx[k];
+            }
+            const box3 cl = clip_triangle(v0, v1, v2, region);
+            if (box_valid(cl)) { sbox_add(bins[b], cl); }
+        }
+    }
+}
+
 // Nodes with more references than this are evaluated and partitioned by many blocks (the
 // wide kernels below); nodes with at most WARP_MAX references are evaluated by one warp each
 // (k_sah_eval_warp); the rest by one block each.
@@ -413,26 +469,9 @@ k_sah_eval_warp(const LvlNode* __restrict__ lv, const uint32_t* __restrict__ ref
         const float sscale = (float)nb / (node_max - node_min);
         for (int b = lane; b < nb; b += 32) { S.cin[b] = 0u; S.cout[b] = 0u; sbox_clear(S.bins[b]); }
         __syncwarp();
-        for (uint32_t i = lane; i < n; i += 32)
+        for (uint32_t i0 = 0; i0 < n; i0 += 32)
         {
-            const uint32_t t = R[i];
-            const int bmin = std_clampi(x86_f2i((tri_lo(C, t, axis) - node_min) * sscale), 0, nb - 1);
-            const int bmax = std_clampi(x86_f2i((tri_hi(C, t, axis) - node_min) * sscale), 0, nb - 1);
-            atomicAdd(&S.cin[bmin], 1u);
-            atomicAdd(&S.cout[bmax], 1u);
-            if (bmin <= bmax)
-            {
-                f3 v0, v1, v2;
-                tri_verts(C, t, v0, v1, v2);
-                box3 region = nbox;
-                for (int b = bmin; b <= bmax; b++)
-                {
-                    region.mn[axis] = node_min + (float)b / sscale;
-                    region.mx[axis] = node_min + (float)(b + 1) / sscale;
-                    const box3 cl = clip_triangle(v0, v1, v2, region);
-                    if (box_valid(cl)) { sbox_add(S.bins[b], cl); }
-                }
-            }
+            spatial_bin_warp(C, R, i0, n, axis, nbox, node_min, sscale, nb, S.cin, S.cout, S.bins);
         }
         __syncwarp();
         warp_eval_spatial_axis(S.cin, S.cout, S.bins, nb, axis, node_min, sscale, parent_inv_area, C, Bw);
@@ -574,26 +613,9 @@ k_sah_eval(const LvlNode* __restrict__ lv, const uint32_t* __restrict__ refs, Ct
         const float sscale = (float)nb / (node_max - node_min);
         if (tid < nb) { cin[tid] = 0u; cout[tid] = 0u; sbox_clear(bins[tid]); }
         __syncthreads();
-        for (uint32_t i = tid; i < n; i += SBLK)
+        for (uint32_t i0 = (uint32_t)(tid & ~31); i0 < n; i0 += SBLK)
         {
-            const uint32_t t = R[i];
-            const int bmin = std_clampi(x86_f2i((tri_lo(C, t, axis) - node_min) * sscale), 0, nb - 1);
-            const int bmax = std_clampi(x86_f2i((tri_hi(C, t, axis) - node_min) * sscale), 0, nb - 1);
-            atomicAdd(&cin[bmin], 1u);
-            atomicAdd(&cout[bmax], 1u);
-            if (bmin <= bmax)
-            {
-                f3 v0, v1, v2;
-                tri_verts(C, t, v0, v1, v2);
-                box3 region = nbox;
-                for (int b = bmin; b <= bmax; b++)
-                {
-                    region.mn[axis] = node_min + (float)b / sscale;
-                    region.mx[axis] = node_min + (float)(b + 1) / sscale;
-                    const box3 cl = clip_triangle(v0, v1, v2, region);
-                    if (box_valid(cl)) { sbox_add(bins[b], cl); }
-                }
-            }
+            spatial_bin_warp(C, R, i0, n, axis, nbox, node_min, sscale, nb, cin, cout, bins);
         }
         __syncthreads();
         if (tid < 32)
@@ -1561,11 +1583,16 @@ __global__ void k_wp_final(WideSplit W)
 // Copies the Morton-sorted triangles of new subtree roots into the level's reference list.
 __global__ void __launch_bounds__(SBLK)
 k_sah_root_refs(const SahRoot* __restrict__ roots, const uint32_t* __restrict__ new_off, const uint32_t* __restrict__ perm,
-                uint32_t* __restrict__ refs)
+                uint32_t* __restrict__ refs, uint32_t* __restrict__ wtri, uint8_t* __restrict__ kpos)
 {
     const SahRoot r = roots[blockIdx.x];
     const uint32_t off = new_off[blockIdx.x];
-    for (uint32_t i = threadIdx.x; i < r.count; i += SBLK) { refs[off + i] = perm[r.first + i]; }
+    for (uint32_t i = threadIdx.x; i < r.count; i += SBLK)
+    {
+        refs[off + i] = perm[r.first + i];
+        wtri[r.first + i] = 0u;  // these keys' triangles are counted and placed by the subtree
+        kpos[r.first + i] = 0u;
+    }
 }
 
 // Merges new roots (sorted by key position) into the continuing nodes (sorted by their
@@ -1774,7 +1801,7 @@ int sah_build(rt_bvh* B, const rt_build_cfg& cfg, const SahInput& in, cudaStream
                 return fail(RT_E_CAPACITY, "SAH builder: level capacity exceeded");
             }
             RT_CUDA(cudaMemcpyAsync(new_off + ri, new_off_h.data() + ri, (size_t)m * 4, cudaMemcpyHostToDevice, st));
-            k_sah_root_refs<<<m, SBLK, 0, st>>>(d_roots + ri, new_off + ri, in.perm, refs_cur);
+            k_sah_root_refs<<<m, SBLK, 0, st>>>(d_roots + ri, new_off + ri, in.perm, refs_cur, in.wtri, in.kpos);
             k_sah_merge<<<nblk(n_cur + m), SBLK, 0, st>>>(lv_cur, n_cur, d_roots, ri, m, new_off + ri, out_total, lv_tmp,
                                                           out, root_out);
             count_launch(2);
