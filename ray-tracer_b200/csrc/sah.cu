@@ -19,6 +19,8 @@
 #include "cta_utils.cuh"
 #include "layout.cuh"
 
+#include <cuda/atomic>
+
 #include <algorithm>
 #include <vector>
 
@@ -1035,46 +1037,70 @@ __global__ void k_wide_final(const LvlNode* __restrict__ lv, Ctx C, const uint32
     dec[node] = d;
 }
 
-// One block: grants the spatial-split reference budget in queue order, then allocates child
-// slots (2 per split node), next-level references and leaf-store space by prefix sums.
+// The spatial-split reference budget and the next level's layout, in three launches.
 // Each scene of a batched build has its own budget (used[s] of cap[s]), as a bake of that
 // scene alone would; the scene of level node i is that of its subtree root.
-// io: [1] spatial taken, [2] spatial refused, [3] next-level nodes,
-//     [4] next-level references, [5] leaf-store entries of this level, [6] leaves
+//   k_sah_need    sums every scene's requests (right + straddle references of each spatial
+//                 candidate) over the level;
+//   k_sah_grant   grants them all when every scene's requests fit, else walks the candidates
+//                 in queue order (a refused request leaves the budget to later, smaller ones);
+//   k_sah_offsets allocates child slots (2 per split node), next-level references and
+//                 leaf-store space by a one-pass prefix scan.
+// io: [1] spatial taken, [2] spatial refused, [3] next-level nodes, [4] next-level references,
+//     [5] leaf-store entries of this level, [6] leaves, [10] largest next-level node bound,
+//     [11] spatial candidates of the level, [12] status (a bounded wait gave up)
 constexpr uint32_t MAX_BUDGET_SCENES = 1024;
+constexpr int NEED_THREADS = 256;
 
-__global__ void __launch_bounds__(1024)
-k_sah_resolve(Dec* __restrict__ dec, const LvlNode* __restrict__ lv, const SahRoot* __restrict__ roots, uint32_t n_lvl,
-              uint32_t n_scenes, uint32_t* __restrict__ used, const uint32_t* __restrict__ cap, uint32_t* __restrict__ io,
-              uint32_t* __restrict__ child_slot, uint32_t* __restrict__ ref_off, uint32_t* __restrict__ leaf_off)
+__global__ void __launch_bounds__(NEED_THREADS)
+k_sah_need(const Dec* __restrict__ dec, const LvlNode* __restrict__ lv, const SahRoot* __restrict__ roots, uint32_t n_lvl,
+           uint32_t n_scenes, unsigned long long* __restrict__ need, uint32_t* __restrict__ io)
 {
-    __shared__ uint32_t sh[33];
-    __shared__ unsigned long long s_need[MAX_BUDGET_SCENES];
-    __shared__ int s_all;
-    const int tid = threadIdx.x;
-    for (uint32_t k = tid; k < n_scenes; k += 1024) { s_need[k] = 0ull; }
-    if (tid == 0) { s_all = 1; }
-    __syncthreads();
-    uint32_t nsp = 0;
-    for (uint32_t i = tid; i < n_lvl; i += 1024)
+    __shared__ uint32_t sh[NEED_THREADS / 32 + 1];
+    const uint32_t i = blockIdx.x * NEED_THREADS + threadIdx.x;
+    uint32_t nd = 0, sp = 0;
+    if (i < n_lvl && dec[i].kind == K_SPATIAL)
     {
-        const Dec d = dec[i];
-        if (d.kind == K_SPATIAL)
+        nd = dec[i].right + dec[i].straddle;
+        sp = 1;
+        if (n_scenes > 1)
         {
-            atomicAdd(&s_need[min(roots[lv[i].root].scene, n_scenes - 1u)], (unsigned long long)d.right + d.straddle);
-            nsp++;
+            atomicAdd(&need[min(roots[lv[i].root].scene, n_scenes - 1u)], (unsigned long long)nd);
+            nd = 0;
         }
     }
-    nsp = block_sum<1024>(nsp, sh);  // (synchronises the block)
+    // one scene: one addition per block (a level's references fit 32 bits)
+    nd = block_sum<NEED_THREADS>(nd, sh);
+    sp = block_sum<NEED_THREADS>(sp, sh);
+    if (threadIdx.x == 0)
+    {
+        if (nd) { atomicAdd(&need[0], (unsigned long long)nd); }
+        if (sp) { atomicAdd(&io[11], sp); }
+    }
+}
+
+// One block. Afterwards need[], io[10], io[11] and the offset scan's descriptors and ticket
+// (3 * n_tiles + 1 words) are zero for the next launches.
+__global__ void __launch_bounds__(1024)
+k_sah_grant(Dec* __restrict__ dec, const LvlNode* __restrict__ lv, const SahRoot* __restrict__ roots, uint32_t n_lvl,
+            uint32_t n_scenes, uint32_t* __restrict__ used, const uint32_t* __restrict__ cap,
+            unsigned long long* __restrict__ need, uint32_t* __restrict__ io, uint32_t* __restrict__ leaf_off,
+            unsigned long long* __restrict__ desc, uint32_t n_tiles)
+{
+    __shared__ uint32_t sh[33];
+    __shared__ int s_all;
+    const int tid = threadIdx.x;
+    if (tid == 0) { s_all = 1; }
+    __syncthreads();
     for (uint32_t k = tid; k < n_scenes; k += 1024)
     {
-        if ((unsigned long long)used[k] + s_need[k] > (unsigned long long)cap[k]) { s_all = 0; }
+        if ((unsigned long long)used[k] + need[k] > (unsigned long long)cap[k]) { s_all = 0; }
     }
     __syncthreads();
     if (s_all)
     {
-        for (uint32_t k = tid; k < n_scenes; k += 1024) { used[k] = (uint32_t)(used[k] + s_need[k]); }
-        if (tid == 0) { io[1] += nsp; }
+        for (uint32_t k = tid; k < n_scenes; k += 1024) { used[k] = (uint32_t)(used[k] + need[k]); }
+        if (tid == 0) { io[1] += io[11]; }
     }
     else
     {
@@ -1145,31 +1171,112 @@ k_sah_resolve(Dec* __restrict__ dec, const LvlNode* __restrict__ lv, const SahRo
         if (tid == 0) { io[2] += refused; }
     }
     __syncthreads();
-    uint32_t c0 = 0, c1 = 0, c2 = 0, nleaf = 0, bmax = 0;
-    for (uint32_t base = 0; base < n_lvl; base += 1024)
+    for (uint32_t k = tid; k < n_scenes; k += 1024) { need[k] = 0ull; }
+    for (uint32_t k = tid; k <= 3 * n_tiles; k += 1024) { desc[k] = 0ull; }
+    if (tid == 0) { io[10] = 0u; io[11] = 0u; }
+}
+
+// Child slots, reference offsets and leaf offsets of a level: three exclusive scans in one pass
+// with decoupled look-back (the scheme of the bake's slot scan: blocks take tiles in the order
+// they start, warp a publishes array a's tile sum and walks its predecessors 32 at a time).
+// Descriptor: flag in bits 62-63 (1 sum, 2 inclusive prefix), value in the low 32 bits;
+// desc[3 * tile + a], the ticket in the word after the last tile's. Waits are bounded (io[12]).
+constexpr unsigned long long SO_AGG = 1ull << 62, SO_PRE = 2ull << 62, SO_FLAGS = 3ull << 62;
+constexpr uint32_t SO_SPIN_LIMIT = 1u << 22;
+constexpr int SO_THREADS = 512, SO_ITEMS = 8, SO_TILE = SO_THREADS * SO_ITEMS;
+
+__global__ void __launch_bounds__(SO_THREADS)
+k_sah_offsets(const Dec* __restrict__ dec, uint32_t n_lvl, unsigned long long* __restrict__ desc,
+              uint32_t* __restrict__ ticket, uint32_t* __restrict__ io, uint32_t* __restrict__ child_slot,
+              uint32_t* __restrict__ ref_off, uint32_t* __restrict__ leaf_off)
+{
+    __shared__ uint32_t sh[SO_THREADS / 32 + 1];
+    __shared__ uint32_t s_tile, s_prev[3];
+    if (threadIdx.x == 0) { s_tile = atomicAdd(ticket, 1u); }
+    __syncthreads();
+    const uint32_t tile = s_tile;
+    const uint32_t i0 = tile * SO_TILE + threadIdx.x * SO_ITEMS;
+    uint32_t v[3][SO_ITEMS], sum[3] = { 0, 0, 0 }, nleaf = 0, bmax = 0;
+#pragma unroll
+    for (int r = 0; r < SO_ITEMS; r++)
     {
-        const uint32_t i = base + tid;
-        uint32_t a = 0, b = 0, c = 0;
+        v[0][r] = v[1][r] = v[2][r] = 0;
+        const uint32_t i = i0 + r;
         if (i < n_lvl)
         {
-            const Dec d = dec[i];
-            if (d.kind == K_LEAF) { c = d.n; nleaf++; }
-            else { a = 2; b = d.kind == K_OBJECT ? d.n : d.n + d.straddle; bmax = max(bmax, b); }
+            const int kind = dec[i].kind;
+            const uint32_t n = dec[i].n;
+            if (kind == K_LEAF) { v[2][r] = n; nleaf++; }
+            else
+            {
+                v[0][r] = 2;
+                v[1][r] = kind == K_OBJECT ? n : n + dec[i].straddle;
+                bmax = max(bmax, v[1][r]);
+            }
         }
-        uint32_t ta, tb, tc;
-        const uint32_t ea = block_excl_scan<1024>(a, sh, &ta);
-        const uint32_t eb = block_excl_scan<1024>(b, sh, &tb);
-        const uint32_t ec = block_excl_scan<1024>(c, sh, &tc);
-        if (i < n_lvl) { child_slot[i] = c0 + ea; ref_off[i] = c1 + eb; leaf_off[i] = c2 + ec; }
-        c0 += ta; c1 += tb; c2 += tc;
+        sum[0] += v[0][r]; sum[1] += v[1][r]; sum[2] += v[2][r];
     }
-    nleaf = block_sum<1024>(nleaf, sh);
-    // an upper bound of the largest next-level node (its parent's references)
+    uint32_t excl[3], tot[3];
+#pragma unroll
+    for (int a = 0; a < 3; a++) { excl[a] = block_excl_scan<SO_THREADS>(sum[a], sh, &tot[a]); }
+    nleaf = block_sum<SO_THREADS>(nleaf, sh);
+    // (an upper bound of the largest next-level node: its parent's references)
     for (int o = 16; o > 0; o >>= 1) { bmax = max(bmax, __shfl_xor_sync(0xffffffffu, bmax, o)); }
-    if (tid == 0) { io[10] = 0u; }
+    if ((threadIdx.x & 31) == 0 && bmax) { atomicMax(&io[10], bmax); }
+    if (threadIdx.x == 0 && nleaf) { atomicAdd(&io[6], nleaf); }
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (warp < 3)
+    {
+        const int a = warp;
+        if (lane == 0)
+        {
+            cuda::atomic_ref<unsigned long long, cuda::thread_scope_device> mine(desc[3 * (size_t)tile + a]);
+            mine.store((tile == 0 ? SO_PRE : SO_AGG) | tot[a], cuda::memory_order_relaxed);
+        }
+        uint32_t prev = 0;
+        int64_t top = (int64_t)tile - 1;  // the window is tiles top - 31 .. top
+        while (top >= 0)
+        {
+            const int64_t p = top - lane;
+            unsigned long long w = SO_PRE;  // below tile 0: nothing to add
+            if (p >= 0)
+            {
+                cuda::atomic_ref<unsigned long long, cuda::thread_scope_device> d(desc[3 * (size_t)p + a]);
+                w = d.load(cuda::memory_order_relaxed);
+                for (uint32_t spin = 0; (w & SO_FLAGS) == 0; spin++)
+                {
+                    if (spin > SO_SPIN_LIMIT) { atomicOr(&io[12], 1u); w = SO_PRE; break; }
+                    w = d.load(cuda::memory_order_relaxed);
+                }
+            }
+            const unsigned pre = __ballot_sync(0xffffffffu, (w & SO_FLAGS) == SO_PRE);
+            const int stop = pre ? __ffs(pre) - 1 : 31;
+            uint32_t add = (lane <= stop && p >= 0) ? (uint32_t)w : 0u;
+            add = warp_sum(add);
+            prev += add;
+            if (pre) { break; }
+            top -= 32;
+        }
+        if (lane == 0)
+        {
+            if (tile > 0)
+            {
+                cuda::atomic_ref<unsigned long long, cuda::thread_scope_device> mine(desc[3 * (size_t)tile + a]);
+                mine.store(SO_PRE | (uint32_t)(prev + tot[a]), cuda::memory_order_relaxed);
+            }
+            s_prev[a] = prev;
+            if (tile == gridDim.x - 1) { io[3 + a] = prev + tot[a]; }
+        }
+    }
     __syncthreads();
-    if ((tid & 31) == 0) { atomicMax(&io[10], bmax); }
-    if (tid == 0) { io[3] = c0; io[4] = c1; io[5] = c2; io[6] += nleaf; }
+    uint32_t run[3] = { s_prev[0] + excl[0], s_prev[1] + excl[1], s_prev[2] + excl[2] };
+#pragma unroll
+    for (int r = 0; r < SO_ITEMS; r++)
+    {
+        const uint32_t i = i0 + r;
+        if (i < n_lvl) { child_slot[i] = run[0]; ref_off[i] = run[1]; leaf_off[i] = run[2]; }
+        run[0] += v[0][r]; run[1] += v[1][r]; run[2] += v[2][r];
+    }
 }
 
 __device__ __forceinline__ void set_node(LvlNode& L, uint32_t off, uint32_t cnt, uint32_t out, uint32_t root,
@@ -1718,9 +1825,29 @@ int sah_build(rt_bvh* B, const rt_build_cfg& cfg, const SahInput& in, cudaStream
     std::vector<SahRoot> roots(nr);
     RT_CUDA(cudaMemcpyAsync(roots.data(), in.roots, (size_t)nr * sizeof(SahRoot), cudaMemcpyDeviceToHost, st));
     RT_CUDA(cudaStreamSynchronize(st));
-    std::sort(roots.begin(), roots.end(), [](const SahRoot& a, const SahRoot& b) {
-        return a.depth != b.depth ? a.depth < b.depth : a.first < b.first;
-    });
+    {
+        // (depth, first) order by stable counting passes: four 8-bit passes over first, then one
+        // over the depth (a comparison sort of tens of thousands of records costs milliseconds)
+        std::vector<uint32_t> idx(nr), tmp(nr);
+        for (uint32_t i = 0; i < nr; i++) { idx[i] = i; }
+        uint32_t max_depth = 0;
+        for (uint32_t i = 0; i < nr; i++) { max_depth = std::max(max_depth, roots[i].depth); }
+        auto pass = [&](auto digit, uint32_t buckets) {
+            std::vector<uint32_t> cnt(buckets + 1, 0u);
+            for (uint32_t i = 0; i < nr; i++) { cnt[digit(roots[idx[i]]) + 1]++; }
+            for (uint32_t b = 0; b < buckets; b++) { cnt[b + 1] += cnt[b]; }
+            for (uint32_t i = 0; i < nr; i++) { tmp[cnt[digit(roots[idx[i]])]++] = idx[i]; }
+            idx.swap(tmp);
+        };
+        for (int sh = 0; sh < 32; sh += 8)
+        {
+            pass([sh](const SahRoot& r) { return (r.first >> sh) & 255u; }, 256u);
+        }
+        pass([](const SahRoot& r) { return r.depth; }, max_depth + 1u);
+        std::vector<SahRoot> sorted(nr);
+        for (uint32_t i = 0; i < nr; i++) { sorted[i] = roots[idx[i]]; }
+        roots.swap(sorted);
+    }
 
     if (S.sah_roots_lvl.ensure((size_t)nr * sizeof(SahRoot)) || S.sah_lvl_a.ensure((size_t)cap * sizeof(LvlNode)) ||
         S.sah_lvl_b.ensure((size_t)cap * sizeof(LvlNode)) || S.sah_node_ids.ensure((size_t)cap * sizeof(LvlNode)) ||
@@ -1759,10 +1886,17 @@ int sah_build(rt_bvh* B, const rt_build_cfg& cfg, const SahInput& in, cudaStream
     {
         return fail(RT_E_INVALID, "SAH builder: bad spatial-split budget");
     }
+    // budget scratch: need (n_budget words of 64 bits), the offset scan's descriptors and ticket
+    // (3 * max_tiles + 1), then used and cap (n_budget words of 32 bits each)
     std::vector<uint32_t> budget(in.budget_used);
     budget.insert(budget.end(), in.budget_cap.begin(), in.budget_cap.end());
-    if (S.sah_budget.ensure((size_t)budget.size() * 4)) { return RT_E_CUDA; }
-    uint32_t* d_used = S.sah_budget.as<uint32_t>();
+    const uint32_t max_tiles = (cap + SO_TILE - 1) / SO_TILE + 1;
+    const size_t n_zero64 = (size_t)n_budget + 3 * (size_t)max_tiles + 1;
+    if (S.sah_budget.ensure(n_zero64 * 8 + (size_t)budget.size() * 4)) { return RT_E_CUDA; }
+    unsigned long long* d_need = S.sah_budget.as<unsigned long long>();
+    unsigned long long* d_desc = d_need + n_budget;
+    uint32_t* d_used = reinterpret_cast<uint32_t*>(d_need + n_zero64);
+    RT_CUDA(cudaMemsetAsync(d_need, 0, n_zero64 * 8, st));
     RT_CUDA(cudaMemcpyAsync(d_used, budget.data(), budget.size() * 4, cudaMemcpyHostToDevice, st));
     // host copy of new-root offsets per level (uploaded as one array, sliced per level)
     std::vector<uint32_t> new_off_h(nr);
@@ -1818,6 +1952,7 @@ int sah_build(rt_bvh* B, const rt_build_cfg& cfg, const SahInput& in, cudaStream
             continue;
         }
         levels.emplace_back(lvl_begin, out_total);
+        const uint32_t level_bound = next_bound;  // no node of this level has more references
         uint32_t nw = 0, nch = 0;
         if (next_bound > WIDE_MIN)
         {
@@ -1847,21 +1982,40 @@ int sah_build(rt_bvh* B, const rt_build_cfg& cfg, const SahInput& in, cudaStream
             k_wide_final<<<(nw + 31) / 32, 32, 0, st>>>(lv_cur, C, wl, nw, wacc, S.sah_dec.as<Dec>());
             count_launch(6);
         }
-        k_sah_resolve<<<1, 1024, 0, st>>>(S.sah_dec.as<Dec>(), lv_cur, d_roots, n_cur, n_budget, d_used, d_used + n_budget,
-                                          io, child_slot, ref_offs, leaf_offs);
-        count_launch();
+        const uint32_t n_tiles = (n_cur + SO_TILE - 1) / SO_TILE;
+        k_sah_need<<<(n_cur + NEED_THREADS - 1) / NEED_THREADS, NEED_THREADS, 0, st>>>(S.sah_dec.as<Dec>(), lv_cur, d_roots,
+                                                                                        n_cur, n_budget, d_need, io);
+        k_sah_grant<<<1, 1024, 0, st>>>(S.sah_dec.as<Dec>(), lv_cur, d_roots, n_cur, n_budget, d_used, d_used + n_budget,
+                                        d_need, io, leaf_offs, d_desc, n_tiles);
+        k_sah_offsets<<<n_tiles, SO_THREADS, 0, st>>>(S.sah_dec.as<Dec>(), n_cur, d_desc,
+                                                      reinterpret_cast<uint32_t*>(d_desc + 3 * (size_t)n_tiles), io,
+                                                      child_slot, ref_offs, leaf_offs);
+        count_launch(3);
         if (int e = check_launch("sah eval")) { return e; }
         RT_CUDA(cudaMemcpyAsync(io_h, io, 64, cudaMemcpyDeviceToHost, st));
         RT_CUDA(cudaStreamSynchronize(st));
+        if (io_h[12]) { return fail(RT_E_TIMEOUT, "a bounded device wait gave up (SAH level offsets)"); }
         const uint32_t n_next = io_h[3], r_next = io_h[4], leaf_lvl = io_h[5];
         if (n_next > cap || r_next > cap || (uint64_t)out_total + n_next > 2ull * cap || (uint64_t)leaf_total + leaf_lvl > cap)
         {
             return fail(RT_E_CAPACITY, "SAH builder: capacity exceeded");
         }
-        k_sah_split<SBLK><<<n_cur, SBLK, 0, st>>>(lv_cur, refs_cur, S.sah_dec.as<Dec>(), child_slot, ref_offs, leaf_offs, C,
+        // levels of small nodes (the reference's default hybrid bake hands ranges of at most 64
+        // triangles to the SAH) split with 64-thread blocks
+        if (level_bound <= 64)
+        {
+            k_sah_split<64><<<n_cur, 64, 0, st>>>(lv_cur, refs_cur, S.sah_dec.as<Dec>(), child_slot, ref_offs, leaf_offs, C,
                                                   S.sah_tmp.as<uint32_t>(), S.sah_pos.as<uint32_t>(),
                                                   S.sah_scan_in.as<uint8_t>(), lv_next, refs_next, out, out_total, leaf_total,
                                                   S.sah_leaf_refs.as<uint32_t>(), nullptr);
+        }
+        else
+        {
+            k_sah_split<SBLK><<<n_cur, SBLK, 0, st>>>(lv_cur, refs_cur, S.sah_dec.as<Dec>(), child_slot, ref_offs, leaf_offs, C,
+                                                      S.sah_tmp.as<uint32_t>(), S.sah_pos.as<uint32_t>(),
+                                                      S.sah_scan_in.as<uint8_t>(), lv_next, refs_next, out, out_total, leaf_total,
+                                                      S.sah_leaf_refs.as<uint32_t>(), nullptr);
+        }
         count_launch();
         if (nw > 0)
         {
