@@ -62,6 +62,7 @@ struct Dec
     int      sp_axis;
     int      nb;
     uint32_t n, straddle, right;
+    uint32_t oleft;              // left side of the object split that kind K_OBJECT applies
     int      fb_kind, oaxis, obin;
     float    ocmin, oscale;
 };
@@ -113,6 +114,116 @@ __device__ __forceinline__ int obj_bin(float c, float cmin, float scale, int nb)
 {
     const int b = std_mini(x86_f2i((c - cmin) * scale), nb - 1);
     return b < 0 ? 0 : b;
+}
+
+// Where an evaluation reads its references' data: straight from the triangle arrays through
+// the node's reference list, or from a warp's copy of them in shared memory. Reference i is
+// the node's i-th; both give the same floats.
+struct GlobalRefs
+{
+    const float4*      lo;
+    const float4*      hi;
+    const float*       cz;
+    const rt_triangle* tris;
+    const rt_vertex*   verts;
+    const uint32_t*    R;
+    __device__ __forceinline__ GlobalRefs(const Ctx& C, const uint32_t* R_)
+        : lo(C.lo), hi(C.hi), cz(C.cz), tris(C.tris), verts(C.verts), R(R_) {}
+    __device__ __forceinline__ float cen(uint32_t i, int axis) const
+    {
+        const uint32_t t = R[i];
+        return axis == 0 ? lo[t].w : (axis == 1 ? hi[t].w : cz[t]);
+    }
+    __device__ __forceinline__ float lo_of(uint32_t i, int axis) const
+    {
+        const float4 a = lo[R[i]];
+        return axis == 0 ? a.x : (axis == 1 ? a.y : a.z);
+    }
+    __device__ __forceinline__ float hi_of(uint32_t i, int axis) const
+    {
+        const float4 a = hi[R[i]];
+        return axis == 0 ? a.x : (axis == 1 ? a.y : a.z);
+    }
+    __device__ __forceinline__ box3 box(uint32_t i) const
+    {
+        const uint32_t t = R[i];
+        const float4 a = lo[t], c = hi[t];
+        box3 b;
+        b.mn[0] = a.x; b.mn[1] = a.y; b.mn[2] = a.z; b.mx[0] = c.x; b.mx[1] = c.y; b.mx[2] = c.z;
+        return b;
+    }
+    __device__ __forceinline__ void tri_verts(uint32_t i, f3& a, f3& b, f3& c) const
+    {
+        const rt_triangle tr = tris[R[i]];
+        a = mk3(verts[tr.v[0]].x, verts[tr.v[0]].y, verts[tr.v[0]].z);
+        b = mk3(verts[tr.v[1]].x, verts[tr.v[1]].y, verts[tr.v[1]].z);
+        c = mk3(verts[tr.v[2]].x, verts[tr.v[2]].y, verts[tr.v[2]].z);
+    }
+};
+
+// A warp's shared copy of at most EVAL_STAGE references: bounds with the x / y centroids in
+// lane 3 (as in Ctx::lo / hi), z centroids, and the three vertices (9 floats: an odd stride,
+// so a warp reading consecutive references hits distinct banks).
+constexpr uint32_t EVAL_STAGE = 64;
+struct StageBuf
+{
+    float4 lo[EVAL_STAGE], hi[EVAL_STAGE];
+    float  cz[EVAL_STAGE];
+    float  v[EVAL_STAGE * 9];
+};
+struct StagedRefs
+{
+    const StageBuf* S;
+    const uint32_t* R;
+    __device__ __forceinline__ float cen(uint32_t i, int axis) const
+    {
+        return axis == 0 ? S->lo[i].w : (axis == 1 ? S->hi[i].w : S->cz[i]);
+    }
+    __device__ __forceinline__ float lo_of(uint32_t i, int axis) const
+    {
+        const float4 a = S->lo[i];
+        return axis == 0 ? a.x : (axis == 1 ? a.y : a.z);
+    }
+    __device__ __forceinline__ float hi_of(uint32_t i, int axis) const
+    {
+        const float4 a = S->hi[i];
+        return axis == 0 ? a.x : (axis == 1 ? a.y : a.z);
+    }
+    __device__ __forceinline__ box3 box(uint32_t i) const
+    {
+        const float4 a = S->lo[i], c = S->hi[i];
+        box3 b;
+        b.mn[0] = a.x; b.mn[1] = a.y; b.mn[2] = a.z; b.mx[0] = c.x; b.mx[1] = c.y; b.mx[2] = c.z;
+        return b;
+    }
+    __device__ __forceinline__ void tri_verts(uint32_t i, f3& a, f3& b, f3& c) const
+    {
+        const float* v = S->v + 9 * i;
+        a = mk3(v[0], v[1], v[2]);
+        b = mk3(v[3], v[4], v[5]);
+        c = mk3(v[6], v[7], v[8]);
+    }
+};
+
+// Copies references [0, n) of R (n <= EVAL_STAGE) into S, one warp.
+__device__ __forceinline__ void stage_refs(const Ctx& C, const uint32_t* R, uint32_t n, StageBuf& S)
+{
+    for (uint32_t i = threadIdx.x & 31; i < n; i += 32)
+    {
+        const uint32_t t = R[i];
+        S.lo[i] = C.lo[t];
+        S.hi[i] = C.hi[t];
+        S.cz[i] = C.cz[t];
+        const rt_triangle tr = C.tris[t];
+        float* v = S.v + 9 * i;
+#pragma unroll
+        for (int k = 0; k < 3; k++)
+        {
+            const rt_vertex& q = C.verts[tr.v[k]];
+            v[3 * k] = q.x; v[3 * k + 1] = q.y; v[3 * k + 2] = q.z;
+        }
+    }
+    __syncwarp();
 }
 
 // Shared box accumulator in the order-preserving uint encoding.
@@ -341,19 +452,18 @@ __device__ __forceinline__ void warp_eval_spatial_axis(const uint32_t* cin, cons
 // count, each lane finding the owner of its pair by a binary search over the lanes), since the
 // references span different numbers of bins. The same clips as bvh_sah.cpp:175-193; the bin
 // boxes are exact unions, so their order does not matter.
-__device__ __forceinline__ void spatial_bin_warp(const Ctx& C, const uint32_t* R, uint32_t i0, uint32_t n, int axis,
-                                                 const box3& nbox, float node_min, float sscale, int nb, uint32_t* cin,
-                                                 uint32_t* cout, SBox* bins)
+template <class Src>
+__device__ __forceinline__ void spatial_bin_warp(const Src& src, uint32_t i0, uint32_t n, int axis, const box3& nbox,
+                                                 float node_min, float sscale, int nb, uint32_t* cin, uint32_t* cout,
+                                                 SBox* bins)
 {
     const int lane = threadIdx.x & 31;
     const uint32_t i = i0 + (uint32_t)lane;
-    uint32_t t = 0;
     int bmin = 0, bmax = -1;
     if (i < n)
     {
-        t = R[i];
-        bmin = std_clampi(x86_f2i((tri_lo(C, t, axis) - node_min) * sscale), 0, nb - 1);
-        bmax = std_clampi(x86_f2i((tri_hi(C, t, axis) - node_min) * sscale), 0, nb - 1);
+        bmin = std_clampi(x86_f2i((src.lo_of(i, axis) - node_min) * sscale), 0, nb - 1);
+        bmax = std_clampi(x86_f2i((src.hi_of(i, axis) - node_min) * sscale), 0, nb - 1);
         atomicAdd(&cin[bmin], 1u);
         atomicAdd(&cout[bmax], 1u);
     }
@@ -369,14 +479,14 @@ __device__ __forceinline__ void spatial_bin_warp(const Ctx& C, const uint32_t* R
         {
             if (__shfl_sync(0xffffffffu, incl, o + step - 1) <= j) { o += step; }
         }
-        const uint32_t to = __shfl_sync(0xffffffffu, t, o);
+        const uint32_t to = i0 + (uint32_t)o;
         const int bo = __shfl_sync(0xffffffffu, bmin, o);
         const uint32_t eo = __shfl_sync(0xffffffffu, incl - c, o);
         if (j < total)
         {
             const int b = bo + (int)(j - eo);
             f3 v0, v1, v2;
-            tri_verts(C, to, v0, v1, v2);
+            src.tri_verts(to, v0, v1, v2);
             const float lo_b = node_min + (float)b / sscale, hi_b = node_min + (float)(b + 1) / sscale;
             box3 region;
 #pragma unroll
@@ -400,32 +510,17 @@ constexpr int      EVAL_WPB = 8;  // warps (nodes) per block of k_sah_eval_warp
 
 // The evaluation of k_sah_eval below for one small node per warp: the same candidates, bins
 // and serial sweeps (lane 0), with warp reductions in place of block ones.
-__global__ void __launch_bounds__(EVAL_WPB * 32)
-k_sah_eval_warp(const LvlNode* __restrict__ lv, const uint32_t* __restrict__ refs, Ctx C, Dec* __restrict__ dec,
-                uint32_t n_lvl)
+struct EvalWS
 {
-    struct WS
-    {
-        uint32_t cnt[SAH_MAX_BINS], cin[SAH_MAX_BINS], cout[SAH_MAX_BINS];
-        SBox     bins[SAH_MAX_BINS];
-    };
-    __shared__ WS ws[EVAL_WPB];
-    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const uint32_t node = blockIdx.x * EVAL_WPB + (uint32_t)w;
-    if (node >= n_lvl) { return; }
-    const LvlNode nd = lv[node];
-    const uint32_t n = nd.count;
-    if (n > WARP_MAX) { return; }  // a block or the wide kernels decide this node
-    WS& S = ws[w];
-    const uint32_t* R = refs + nd.ref_off;
-    Dec d;
-    memset(&d, 0, sizeof(d));
-    d.n = n;
-    if (n <= C.max_leaf)
-    {
-        if (lane == 0) { d.kind = K_LEAF; dec[node] = d; }
-        return;
-    }
+    uint32_t cnt[SAH_MAX_BINS], cin[SAH_MAX_BINS], cout[SAH_MAX_BINS];
+    SBox     bins[SAH_MAX_BINS];
+};
+
+template <class Src>
+__device__ __forceinline__ void eval_node_warp(const Src& src, const LvlNode& nd, uint32_t n, const Ctx& C, EvalWS& S,
+                                               Dec& d)
+{
+    const int lane = threadIdx.x & 31;
     const int nb = std_clampi((int)n / 4, (int)C.bins_min, (int)C.bins_max);
     box3 nbox;
     for (int k = 0; k < 3; k++) { nbox.mn[k] = nd.box[k]; nbox.mx[k] = nd.box[3 + k]; }
@@ -439,7 +534,7 @@ k_sah_eval_warp(const LvlNode* __restrict__ lv, const uint32_t* __restrict__ ref
         uint32_t m = 0xffffffffu, M = 0u;
         for (uint32_t i = lane; i < n; i += 32)
         {
-            const uint32_t o = f2ord(centroid(C, R[i], axis));
+            const uint32_t o = f2ord(src.cen(i, axis));
             m = min(m, o); M = max(M, o);
         }
         m = __reduce_min_sync(0xffffffffu, m);
@@ -452,10 +547,9 @@ k_sah_eval_warp(const LvlNode* __restrict__ lv, const uint32_t* __restrict__ ref
         __syncwarp();
         for (uint32_t i = lane; i < n; i += 32)
         {
-            const uint32_t t = R[i];
-            const int b = obj_bin(centroid(C, t, axis), cmin, scale, nb);
+            const int b = obj_bin(src.cen(i, axis), cmin, scale, nb);
             atomicAdd(&S.cnt[b], 1u);
-            sbox_add(S.bins[b], tri_box(C, t));
+            sbox_add(S.bins[b], src.box(i));
         }
         __syncwarp();
         warp_eval_object_axis(S.cnt, S.bins, nb, axis, cmin, scale, parent_inv_area, C, Bw);
@@ -473,7 +567,7 @@ k_sah_eval_warp(const LvlNode* __restrict__ lv, const uint32_t* __restrict__ ref
         __syncwarp();
         for (uint32_t i0 = 0; i0 < n; i0 += 32)
         {
-            spatial_bin_warp(C, R, i0, n, axis, nbox, node_min, sscale, nb, S.cin, S.cout, S.bins);
+            spatial_bin_warp(src, i0, n, axis, nbox, node_min, sscale, nb, S.cin, S.cout, S.bins);
         }
         __syncwarp();
         warp_eval_spatial_axis(S.cin, S.cout, S.bins, nb, axis, node_min, sscale, parent_inv_area, C, Bw);
@@ -492,10 +586,11 @@ k_sah_eval_warp(const LvlNode* __restrict__ lv, const uint32_t* __restrict__ ref
         uint32_t l = 0;
         for (uint32_t i = lane; i < n; i += 32)
         {
-            l += obj_bin(centroid(C, R[i], B.axis), B.cmin, B.scale, nb) < B.bin ? 1u : 0u;
+            l += obj_bin(src.cen(i, B.axis), B.cmin, B.scale, nb) < B.bin ? 1u : 0u;
         }
         l = __reduce_add_sync(0xffffffffu, l);
         d.kind = (l == 0 || l == n) ? K_LEAF : K_OBJECT;
+        d.oleft = l;
         d.axis = B.axis; d.bin = B.bin; d.cmin = B.cmin; d.scale = B.scale;
     }
     else
@@ -505,17 +600,16 @@ k_sah_eval_warp(const LvlNode* __restrict__ lv, const uint32_t* __restrict__ ref
         uint32_t lo_ = 0, st_ = 0, ol = 0;
         for (uint32_t i = lane; i < n; i += 32)
         {
-            const uint32_t t = R[i];
-            if (tri_hi(C, t, axis) <= plane) { lo_++; }
-            else if (tri_lo(C, t, axis) < plane) { st_++; }
-            if (oa != -1) { ol += obj_bin(centroid(C, t, oa), oc, os, nb) < ob ? 1u : 0u; }
+            if (src.hi_of(i, axis) <= plane) { lo_++; }
+            else if (src.lo_of(i, axis) < plane) { st_++; }
+            if (oa != -1) { ol += obj_bin(src.cen(i, oa), oc, os, nb) < ob ? 1u : 0u; }
         }
         lo_ = __reduce_add_sync(0xffffffffu, lo_);
         st_ = __reduce_add_sync(0xffffffffu, st_);
         ol = __reduce_add_sync(0xffffffffu, ol);
         const uint32_t ri = n - lo_ - st_;
         const int fb = (oa == -1 || ol == 0 || ol == n) ? K_LEAF : K_OBJECT;
-        d.sp_axis = axis; d.plane = plane; d.straddle = st_; d.right = ri; d.fb_kind = fb;
+        d.sp_axis = axis; d.plane = plane; d.straddle = st_; d.right = ri; d.fb_kind = fb; d.oleft = ol;
         if ((lo_ + st_ == 0) || (st_ + ri == 0))
         {
             // the saved object split, applied after the spatial partitions (bvh_sah.cpp:331-333)
@@ -527,6 +621,41 @@ k_sah_eval_warp(const LvlNode* __restrict__ lv, const uint32_t* __restrict__ ref
             d.kind = K_SPATIAL;
             d.axis = axis;
         }
+    }
+}
+
+// STAGED: the nodes of at most EVAL_STAGE references (leaves included), read from a shared
+// copy; else the nodes of EVAL_STAGE + 1 .. WARP_MAX references, read from global memory.
+template <bool STAGED>
+__global__ void __launch_bounds__(EVAL_WPB * 32)
+k_sah_eval_warp(const LvlNode* __restrict__ lv, const uint32_t* __restrict__ refs, Ctx C, Dec* __restrict__ dec,
+                uint32_t n_lvl)
+{
+    __shared__ EvalWS ws[EVAL_WPB];
+    __shared__ StageBuf stage[STAGED ? EVAL_WPB : 1];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t node = blockIdx.x * EVAL_WPB + (uint32_t)w;
+    if (node >= n_lvl) { return; }
+    const LvlNode nd = lv[node];
+    const uint32_t n = nd.count;
+    if (STAGED ? n > EVAL_STAGE : (n <= EVAL_STAGE || n > WARP_MAX)) { return; }  // another kernel decides this node
+    const uint32_t* R = refs + nd.ref_off;
+    Dec d;
+    memset(&d, 0, sizeof(d));
+    d.n = n;
+    if (n <= C.max_leaf)
+    {
+        if (lane == 0) { d.kind = K_LEAF; dec[node] = d; }
+        return;
+    }
+    if constexpr (STAGED)
+    {
+        stage_refs(C, R, n, stage[w]);
+        eval_node_warp(StagedRefs{ &stage[w], R }, nd, n, C, ws[w], d);
+    }
+    else
+    {
+        eval_node_warp(GlobalRefs(C, R), nd, n, C, ws[w], d);
     }
     if (lane == 0) { dec[node] = d; }
 }
@@ -617,7 +746,7 @@ k_sah_eval(const LvlNode* __restrict__ lv, const uint32_t* __restrict__ refs, Ct
         __syncthreads();
         for (uint32_t i0 = (uint32_t)(tid & ~31); i0 < n; i0 += SBLK)
         {
-            spatial_bin_warp(C, R, i0, n, axis, nbox, node_min, sscale, nb, cin, cout, bins);
+            spatial_bin_warp(GlobalRefs(C, R), i0, n, axis, nbox, node_min, sscale, nb, cin, cout, bins);
         }
         __syncthreads();
         if (tid < 32)
@@ -646,6 +775,7 @@ k_sah_eval(const LvlNode* __restrict__ lv, const uint32_t* __restrict__ refs, Ct
         }
         l = block_sum<SBLK>(l, s_red);
         d.kind = (l == 0 || l == n) ? K_LEAF : K_OBJECT;
+        d.oleft = l;
         d.axis = B.axis; d.bin = B.bin; d.cmin = B.cmin; d.scale = B.scale;
     }
     else
@@ -667,7 +797,7 @@ k_sah_eval(const LvlNode* __restrict__ lv, const uint32_t* __restrict__ refs, Ct
         ol = block_sum<SBLK>(ol, s_red);
         const uint32_t ri = n - lo_ - st_;
         const int fb = (oa == -1 || ol == 0 || ol == n) ? K_LEAF : K_OBJECT;
-        d.sp_axis = axis; d.plane = plane; d.straddle = st_; d.right = ri; d.fb_kind = fb;
+        d.sp_axis = axis; d.plane = plane; d.straddle = st_; d.right = ri; d.fb_kind = fb; d.oleft = ol;
         if ((lo_ + st_ == 0) || (st_ + ri == 0))
         {
             // the saved object split, applied after the spatial partitions (bvh_sah.cpp:331-333)
@@ -1014,6 +1144,7 @@ __global__ void k_wide_final(const LvlNode* __restrict__ lv, Ctx C, const uint32
     {
         const uint32_t l = A.cnt[0];
         d.kind = (l == 0 || l == n) ? K_LEAF : K_OBJECT;
+        d.oleft = l;
         d.axis = B.axis; d.bin = B.bin; d.cmin = B.cmin; d.scale = B.scale;
     }
     else
@@ -1021,7 +1152,7 @@ __global__ void k_wide_final(const LvlNode* __restrict__ lv, Ctx C, const uint32
         const uint32_t lo_ = A.cnt[0], st_ = A.cnt[1], ol = A.cnt[2];
         const uint32_t ri = n - lo_ - st_;
         const int fb = (A.o_axis == -1 || ol == 0 || ol == n) ? K_LEAF : K_OBJECT;
-        d.sp_axis = B.axis; d.plane = B.node_min + (float)B.bin / B.sscale; d.straddle = st_; d.right = ri; d.fb_kind = fb;
+        d.sp_axis = B.axis; d.plane = B.node_min + (float)B.bin / B.sscale; d.straddle = st_; d.right = ri; d.fb_kind = fb; d.oleft = ol;
         if ((lo_ + st_ == 0) || (st_ + ri == 0))
         {
             // the saved object split, applied after the spatial partitions (bvh_sah.cpp:331-333)
@@ -1047,7 +1178,7 @@ __global__ void k_wide_final(const LvlNode* __restrict__ lv, Ctx C, const uint32
 //   k_sah_offsets allocates child slots (2 per split node), next-level references and
 //                 leaf-store space by a one-pass prefix scan.
 // io: [1] spatial taken, [2] spatial refused, [3] next-level nodes, [4] next-level references,
-//     [5] leaf-store entries of this level, [6] leaves, [10] largest next-level node bound,
+//     [5] leaf-store entries of this level, [6] leaves, [10] largest next-level node,
 //     [11] spatial candidates of the level, [12] status (a bounded wait gave up)
 constexpr uint32_t MAX_BUDGET_SCENES = 1024;
 constexpr int NEED_THREADS = 256;
@@ -1207,11 +1338,19 @@ k_sah_offsets(const Dec* __restrict__ dec, uint32_t n_lvl, unsigned long long* _
             const int kind = dec[i].kind;
             const uint32_t n = dec[i].n;
             if (kind == K_LEAF) { v[2][r] = n; nleaf++; }
+            else if (kind == K_OBJECT)
+            {
+                const uint32_t l = dec[i].oleft;
+                v[0][r] = 2;
+                v[1][r] = n;
+                bmax = max(bmax, max(l, n - l));
+            }
             else
             {
+                const uint32_t st = dec[i].straddle, ri = dec[i].right;
                 v[0][r] = 2;
-                v[1][r] = kind == K_OBJECT ? n : n + dec[i].straddle;
-                bmax = max(bmax, v[1][r]);
+                v[1][r] = n + st;
+                bmax = max(bmax, max(n - ri, ri + st));
             }
         }
         sum[0] += v[0][r]; sum[1] += v[1][r]; sum[2] += v[2][r];
@@ -1220,7 +1359,7 @@ k_sah_offsets(const Dec* __restrict__ dec, uint32_t n_lvl, unsigned long long* _
 #pragma unroll
     for (int a = 0; a < 3; a++) { excl[a] = block_excl_scan<SO_THREADS>(sum[a], sh, &tot[a]); }
     nleaf = block_sum<SO_THREADS>(nleaf, sh);
-    // (an upper bound of the largest next-level node: its parent's references)
+    // the largest next-level node
     for (int o = 16; o > 0; o >>= 1) { bmax = max(bmax, __shfl_xor_sync(0xffffffffu, bmax, o)); }
     if ((threadIdx.x & 31) == 0 && bmax) { atomicMax(&io[10], bmax); }
     if (threadIdx.x == 0 && nleaf) { atomicAdd(&io[6], nleaf); }
@@ -1297,7 +1436,8 @@ __device__ __forceinline__ void set_out_child(OutNode& o, const box3& b, uint32_
 // children's reference lists and boxes (computeRangeAABB for object splits, the union of
 // the triangles clipped to each side for spatial splits, bvh_sah.cpp:426-444).
 // node_list: the level nodes this launch covers (the wide nodes, with BS = 1024), or nullptr
-// for one block per level node, which then leaves the wide nodes out.
+// for one block per level node, which then leaves out the wide nodes and those of fewer than
+// min_refs references.
 template <int BS>
 __global__ void __launch_bounds__(BS)
 k_sah_split(const LvlNode* __restrict__ lv, const uint32_t* __restrict__ refs, const Dec* __restrict__ dec,
@@ -1305,13 +1445,13 @@ k_sah_split(const LvlNode* __restrict__ lv, const uint32_t* __restrict__ refs, c
             const uint32_t* __restrict__ leaf_off, Ctx C, uint32_t* __restrict__ tmp, uint32_t* __restrict__ pos,
             uint8_t* __restrict__ flags, LvlNode* __restrict__ lv_next, uint32_t* __restrict__ refs_next,
             OutNode* __restrict__ out, uint32_t out_base, uint32_t leaf_base, uint32_t* __restrict__ leaf_refs,
-            const uint32_t* __restrict__ node_list)
+            const uint32_t* __restrict__ node_list, uint32_t min_refs)
 {
     __shared__ uint32_t sh[BS / 32 + 1];
     __shared__ SBox sb[2];
     const uint32_t ni = node_list ? node_list[blockIdx.x] : blockIdx.x;
     const LvlNode nd = lv[ni];
-    if (!node_list && nd.count > WIDE_MIN) { return; }
+    if (!node_list && (nd.count > WIDE_MIN || nd.count < min_refs)) { return; }
     const Dec d = dec[ni];
     const uint32_t n = nd.count;
     const uint32_t* R = refs + nd.ref_off;
@@ -1390,6 +1530,209 @@ k_sah_split(const LvlNode* __restrict__ lv, const uint32_t* __restrict__ refs, c
     if (tid == 0)
     {
         const box3 lb = sbox_result(sb[0]), rb = sbox_result(sb[1]);
+        LvlNode L, Rn;
+        set_node(L, roff, lsz, lid, nd.root, nd.root_first, lb);
+        set_node(Rn, roff + lsz, rsz, rid, nd.root, nd.root_first, rb);
+        lv_next[slot] = L;
+        lv_next[slot + 1] = Rn;
+        set_out_child(out[lid], lb, nd.root);
+        set_out_child(out[rid], rb, nd.root);
+        o->is_leaf = 0; o->a = lid; o->b = rid;
+    }
+}
+
+// ---- small nodes: one warp each, the references in registers ----
+// Position p of a node's (at most 64) references lives in lane p & 31 of w[p >> 5].
+__device__ __forceinline__ uint64_t low_bits(uint32_t k) { return k >= 64 ? ~0ull : (1ull << k) - 1ull; }
+
+// Position of the k-th (from 0) set bit of m (which has more than k).
+__device__ __forceinline__ uint32_t select_bit(uint64_t m, uint32_t k)
+{
+    uint32_t p = 0;
+#pragma unroll
+    for (int s = 32; s > 0; s >>= 1)
+    {
+        const uint32_t c = __popcll(m & low_bits((uint32_t)s));
+        if (k >= c) { k -= c; m >>= s; p += (uint32_t)s; }
+    }
+    return p;
+}
+
+// cta_partition's Hoare scheme over positions [lo, hi) by the flags f (per position, false
+// outside the range): the k-th failing element left of the split point trades places with the
+// k-th satisfying one from the right end. Returns the number satisfying.
+__device__ __forceinline__ uint32_t warp_partition64(uint32_t (&w)[2], const bool (&f)[2], uint32_t lo, uint32_t hi)
+{
+    const int lane = threadIdx.x & 31;
+    const uint64_t range = low_bits(hi) & ~low_bits(lo);
+    const uint64_t F = (((uint64_t)__ballot_sync(0xffffffffu, f[1]) << 32) | __ballot_sync(0xffffffffu, f[0])) & range;
+    const uint32_t m = __popcll(F);
+    const uint64_t below = low_bits(lo + m);
+    const uint64_t fail_l = ~F & range & below, sat_r = F & ~below;
+    const uint32_t tr = __popcll(sat_r);
+    uint32_t nw[2];
+#pragma unroll
+    for (int h = 0; h < 2; h++)
+    {
+        const uint32_t p = (uint32_t)lane + 32u * h;
+        const uint64_t bit = 1ull << p;
+        uint32_t q = p;
+        if (fail_l & bit) { q = select_bit(sat_r, tr - 1u - __popcll(fail_l & (bit - 1ull))); }
+        else if (sat_r & bit) { q = select_bit(fail_l, tr - 1u - __popcll(sat_r & (bit - 1ull))); }
+        const uint32_t a = __shfl_sync(0xffffffffu, w[0], q & 31), b = __shfl_sync(0xffffffffu, w[1], q & 31);
+        nw[h] = q < 32 ? a : b;
+    }
+    w[0] = nw[0];
+    w[1] = nw[1];
+    return m;
+}
+
+// The union of the lanes' boxes; the empty box when none.
+__device__ __forceinline__ box3 obox_warp_union(OBox o)
+{
+    for (int k = 0; k < 3; k++)
+    {
+        o.m[k] = __reduce_min_sync(0xffffffffu, o.m[k]);
+        o.M[k] = __reduce_max_sync(0xffffffffu, o.M[k]);
+    }
+    box3 b = box_empty();
+    if (o.m[0] != 0xffffffffu) { for (int k = 0; k < 3; k++) { b.mn[k] = ord2f(o.m[k]); b.mx[k] = ord2f(o.M[k]); } }
+    return b;
+}
+
+// k_sah_split for the nodes of at most EVAL_STAGE references, one warp each: the same
+// partitions, children and boxes.
+constexpr int SPLIT_WPB = 8;
+static_assert(EVAL_STAGE <= 64, "two register positions per lane");
+
+__global__ void __launch_bounds__(SPLIT_WPB * 32)
+k_sah_split_warp(const LvlNode* __restrict__ lv, const uint32_t* __restrict__ refs, const Dec* __restrict__ dec,
+                 const uint32_t* __restrict__ child_slot, const uint32_t* __restrict__ ref_off,
+                 const uint32_t* __restrict__ leaf_off, Ctx C, LvlNode* __restrict__ lv_next,
+                 uint32_t* __restrict__ refs_next, OutNode* __restrict__ out, uint32_t out_base, uint32_t leaf_base,
+                 uint32_t* __restrict__ leaf_refs, uint32_t n_lvl)
+{
+    const int lane = threadIdx.x & 31;
+    const uint32_t ni = blockIdx.x * SPLIT_WPB + (threadIdx.x >> 5);
+    if (ni >= n_lvl) { return; }
+    const LvlNode nd = lv[ni];
+    const uint32_t n = nd.count;
+    if (n > EVAL_STAGE) { return; }  // k_sah_split applies this one
+    const Dec d = dec[ni];
+    const uint32_t* R = refs + nd.ref_off;
+    uint32_t w[2];
+    bool f[2];
+#pragma unroll
+    for (int h = 0; h < 2; h++)
+    {
+        const uint32_t p = (uint32_t)lane + 32u * h;
+        w[h] = p < n ? R[p] : 0u;
+    }
+    uint32_t left_end = 0, straddle_end = 0;
+    if (d.pre_spatial || d.kind == K_SPATIAL)
+    {
+        const int ax = d.sp_axis;
+        const float plane = d.plane;
+#pragma unroll
+        for (int h = 0; h < 2; h++)
+        {
+            const uint32_t p = (uint32_t)lane + 32u * h;
+            f[h] = p < n && tri_hi(C, w[h], ax) <= plane;
+        }
+        left_end = warp_partition64(w, f, 0, n);
+#pragma unroll
+        for (int h = 0; h < 2; h++)
+        {
+            const uint32_t p = (uint32_t)lane + 32u * h;
+            f[h] = p >= left_end && p < n && tri_lo(C, w[h], ax) < plane;
+        }
+        straddle_end = left_end + warp_partition64(w, f, left_end, n);
+    }
+    OutNode* o = &out[nd.out];
+    if (d.kind == K_LEAF)
+    {
+        const uint32_t lo = leaf_base + leaf_off[ni];
+#pragma unroll
+        for (int h = 0; h < 2; h++)
+        {
+            const uint32_t p = (uint32_t)lane + 32u * h;
+            if (p < n) { leaf_refs[lo + p] = w[h]; }
+        }
+        if (lane == 0) { o->is_leaf = 1; o->a = lo; o->b = n; }
+        return;
+    }
+    const uint32_t slot = child_slot[ni];
+    const uint32_t roff = ref_off[ni];
+    const uint32_t lid = out_base + slot, rid = lid + 1;
+    uint32_t* Q = refs_next + roff;
+    uint32_t lsz, rsz;
+    OBox ob[2];
+    obox_clear(ob[0]);
+    obox_clear(ob[1]);
+    if (d.kind == K_OBJECT)
+    {
+        const int ax = d.axis, bin = d.bin, nb = d.nb;
+        const float cmin = d.cmin, scale = d.scale;
+#pragma unroll
+        for (int h = 0; h < 2; h++)
+        {
+            const uint32_t p = (uint32_t)lane + 32u * h;
+            f[h] = p < n && obj_bin(centroid(C, w[h], ax), cmin, scale, nb) < bin;
+        }
+        const uint32_t m = warp_partition64(w, f, 0, n);
+        lsz = m;
+        rsz = n - m;
+#pragma unroll
+        for (int h = 0; h < 2; h++)
+        {
+            const uint32_t p = (uint32_t)lane + 32u * h;
+            if (p < n)
+            {
+                Q[p] = w[h];
+                obox_add(ob[p < m ? 0 : 1], tri_box(C, w[h]));
+            }
+        }
+    }
+    else
+    {
+        // left child: positions [0, straddle_end); right child: [straddle_end, n), then the
+        // straddling [left_end, straddle_end) again -- position p keeps index p of the list
+        // and a straddling one is repeated at n + p - left_end
+        const uint32_t st = straddle_end - left_end, rc = n - straddle_end;
+        lsz = left_end + st;
+        rsz = rc + st;
+        const int ax = d.axis;
+        box3 lclip, rclip;
+        for (int k = 0; k < 3; k++) { lclip.mn[k] = rclip.mn[k] = nd.box[k]; lclip.mx[k] = rclip.mx[k] = nd.box[3 + k]; }
+        lclip.mx[ax] = d.plane;
+        rclip.mn[ax] = d.plane;
+#pragma unroll
+        for (int h = 0; h < 2; h++)
+        {
+            const uint32_t p = (uint32_t)lane + 32u * h;
+            if (p < n)
+            {
+                Q[p] = w[h];
+                const bool straddles = p >= left_end && p < straddle_end;
+                if (straddles) { Q[n + p - left_end] = w[h]; }
+                f3 v0, v1, v2;
+                tri_verts(C, w[h], v0, v1, v2);
+                if (p < straddle_end)
+                {
+                    const box3 cl = clip_triangle(v0, v1, v2, lclip);
+                    if (box_valid(cl)) { obox_add(ob[0], cl); }
+                }
+                if (p >= straddle_end || straddles)
+                {
+                    const box3 cl = clip_triangle(v0, v1, v2, rclip);
+                    if (box_valid(cl)) { obox_add(ob[1], cl); }
+                }
+            }
+        }
+    }
+    const box3 lb = obox_warp_union(ob[0]), rb = obox_warp_union(ob[1]);
+    if (lane == 0)
+    {
         LvlNode L, Rn;
         set_node(L, roff, lsz, lid, nd.root, nd.root_first, lb);
         set_node(Rn, roff + lsz, rsz, rid, nd.root, nd.root_first, rb);
@@ -1964,9 +2307,15 @@ int sah_build(rt_bvh* B, const rt_build_cfg& cfg, const SahInput& in, cudaStream
             nch = io_h[9];
             if (nw > max_wide) { return fail(RT_E_CAPACITY, "SAH builder: too many wide nodes"); }
         }
-        k_sah_eval_warp<<<(n_cur + EVAL_WPB - 1) / EVAL_WPB, EVAL_WPB * 32, 0, st>>>(lv_cur, refs_cur, C, S.sah_dec.as<Dec>(),
-                                                                                       n_cur);
+        k_sah_eval_warp<true><<<(n_cur + EVAL_WPB - 1) / EVAL_WPB, EVAL_WPB * 32, 0, st>>>(lv_cur, refs_cur, C,
+                                                                                             S.sah_dec.as<Dec>(), n_cur);
         count_launch();
+        if (next_bound > EVAL_STAGE)
+        {
+            k_sah_eval_warp<false><<<(n_cur + EVAL_WPB - 1) / EVAL_WPB, EVAL_WPB * 32, 0, st>>>(lv_cur, refs_cur, C,
+                                                                                                  S.sah_dec.as<Dec>(), n_cur);
+            count_launch();
+        }
         if (next_bound > WARP_MAX)
         {
             k_sah_eval<<<n_cur, SBLK, 0, st>>>(lv_cur, refs_cur, C, S.sah_dec.as<Dec>());
@@ -2000,23 +2349,20 @@ int sah_build(rt_bvh* B, const rt_build_cfg& cfg, const SahInput& in, cudaStream
         {
             return fail(RT_E_CAPACITY, "SAH builder: capacity exceeded");
         }
-        // levels of small nodes (the reference's default hybrid bake hands ranges of at most 64
-        // triangles to the SAH) split with 64-thread blocks
-        if (level_bound <= 64)
-        {
-            k_sah_split<64><<<n_cur, 64, 0, st>>>(lv_cur, refs_cur, S.sah_dec.as<Dec>(), child_slot, ref_offs, leaf_offs, C,
-                                                  S.sah_tmp.as<uint32_t>(), S.sah_pos.as<uint32_t>(),
-                                                  S.sah_scan_in.as<uint8_t>(), lv_next, refs_next, out, out_total, leaf_total,
-                                                  S.sah_leaf_refs.as<uint32_t>(), nullptr);
-        }
-        else
+        // nodes of at most EVAL_STAGE references (all of them in the reference's default hybrid
+        // bake, which hands ranges of at most 64 triangles to the SAH) split by one warp each
+        k_sah_split_warp<<<(n_cur + SPLIT_WPB - 1) / SPLIT_WPB, SPLIT_WPB * 32, 0, st>>>(
+            lv_cur, refs_cur, S.sah_dec.as<Dec>(), child_slot, ref_offs, leaf_offs, C, lv_next, refs_next, out, out_total,
+            leaf_total, S.sah_leaf_refs.as<uint32_t>(), n_cur);
+        count_launch();
+        if (level_bound > EVAL_STAGE)
         {
             k_sah_split<SBLK><<<n_cur, SBLK, 0, st>>>(lv_cur, refs_cur, S.sah_dec.as<Dec>(), child_slot, ref_offs, leaf_offs, C,
                                                       S.sah_tmp.as<uint32_t>(), S.sah_pos.as<uint32_t>(),
                                                       S.sah_scan_in.as<uint8_t>(), lv_next, refs_next, out, out_total, leaf_total,
-                                                      S.sah_leaf_refs.as<uint32_t>(), nullptr);
+                                                      S.sah_leaf_refs.as<uint32_t>(), nullptr, EVAL_STAGE + 1);
+            count_launch();
         }
-        count_launch();
         if (nw > 0)
         {
             WideSplit W;
