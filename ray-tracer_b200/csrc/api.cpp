@@ -123,7 +123,8 @@ static void free_bvh(rt_bvh* b)
                        &b->s.rank, &b->s.bnd, &b->s.wnode, &b->s.wtri, &b->s.snode, &b->s.stri, &b->s.counters,
                        &b->s.sah_roots, &b->s.sah_refs_a, &b->s.sah_refs_b, &b->s.sah_tmp, &b->s.sah_pos,
                        &b->s.sah_lvl_a, &b->s.sah_lvl_b, &b->s.sah_dec, &b->s.sah_out, &b->s.sah_leaf_refs,
-                       &b->s.sah_scan_in, &b->s.sah_scan_out, &b->s.sah_node_ids, &b->s.sah_roots_lvl,
+                       &b->s.sah_scan_in, &b->s.sah_scan_out, &b->s.sah_node_ids, &b->s.sah_roots_lvl, &b->s.sah_root_ord, &b->s.root_sort.keys_alt,
+                       &b->s.root_sort.vals_alt, &b->s.root_sort.lookback, &b->s.root_sort.tile_counters,
                        &b->s.in_verts, &b->s.in_tris, &b->s.gtris, &b->s.batch_off, &b->s.sah_budget, &b->s.sah_wide, &b->s.sah_tmp2, &b->s.sah_pos2, &b->s.wide_flag, &b->s.wide_par, &b->wnodes, &b->wid, &b->scene_info, &b->scene_roots,
                        &b->wf_cams };
     for (DevBuf* x : bufs) { x->release(); }

@@ -1222,6 +1222,7 @@ int build_typed(rt_bvh* B, const rt_vertex* d_verts, uint32_t V, const rt_triang
         in.wnode = S.wnode.as<uint32_t>();
         in.wtri = S.wtri.as<uint32_t>();
         in.kpos = S.bnd.as<uint8_t>();
+        in.status = status;
         if (batch)
         {
             for (uint32_t k = 0; k < bt.S; k++)

@@ -176,6 +176,8 @@ struct BuildScratch
     // SAH builder state
     rtb::DevBuf sah_refs_a, sah_refs_b, sah_tmp, sah_pos, sah_lvl_a, sah_lvl_b, sah_dec, sah_out, sah_leaf_refs,
         sah_scan_in, sah_scan_out, sah_node_ids, sah_roots_lvl;
+    rtb::DevBuf sah_root_ord;       // the roots' sort keys, order, counts and their scan, per-depth runs
+    rtb::SortScratch root_sort;     // (their sort's own scratch: the bake's sorted keys stay live)
     rtb::DevBuf in_verts, in_tris;  // staging for host geometry
     rtb::DevBuf gtris;              // batched build: triangles with concatenated-array vertex indices
     rtb::DevBuf batch_off;          // batched build: triangle and vertex offsets per scene

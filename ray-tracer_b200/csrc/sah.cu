@@ -2030,13 +2030,85 @@ __global__ void k_wp_final(WideSplit W)
     o->is_leaf = 0; o->a = lid; o->b = rid;
 }
 
-// Copies the Morton-sorted triangles of new subtree roots into the level's reference list.
+// ---- the subtree roots in the reference's queue order: by depth, then key position ----
+// Key of root i: depth << fb | first (first < 2^fb, depth < 256), and the counts of every 8-bit
+// digit of the sort's passes (hist, zeroed). grp[512] = the largest root, grp[513] = the
+// deepest root (both zeroed).
+constexpr uint32_t ROOT_MAX_DEPTH = 255;
+constexpr int      ROOT_HIST_PASSES = 8;
+
 __global__ void __launch_bounds__(SBLK)
-k_sah_root_refs(const SahRoot* __restrict__ roots, const uint32_t* __restrict__ new_off, const uint32_t* __restrict__ perm,
-                uint32_t* __restrict__ refs, uint32_t* __restrict__ wtri, uint8_t* __restrict__ kpos)
+k_root_keys(const SahRoot* __restrict__ roots, uint32_t nr, int fb, int passes, uint64_t* __restrict__ keys,
+            uint32_t* __restrict__ hist, uint32_t* __restrict__ grp)
+{
+    __shared__ uint32_t sh[ROOT_HIST_PASSES][256];
+    for (int k = threadIdx.x; k < ROOT_HIST_PASSES * 256; k += SBLK) { (&sh[0][0])[k] = 0u; }
+    __syncthreads();
+    const uint32_t i = blockIdx.x * SBLK + threadIdx.x;
+    uint32_t cnt = 0, dep = 0;
+    if (i < nr)
+    {
+        const SahRoot r = roots[i];
+        cnt = r.count;
+        dep = r.depth;
+        const uint64_t key = ((uint64_t)min(dep, ROOT_MAX_DEPTH) << fb) | r.first;
+        keys[i] = key;
+        for (int p = 0; p < passes; p++) { atomicAdd(&sh[p][(key >> (8 * p)) & 255u], 1u); }
+    }
+    cnt = __reduce_max_sync(0xffffffffu, cnt);
+    dep = __reduce_max_sync(0xffffffffu, dep);
+    if ((threadIdx.x & 31) == 0)
+    {
+        atomicMax(&grp[512], cnt);
+        atomicMax(&grp[513], dep);
+    }
+    __syncthreads();
+    for (int k = threadIdx.x; k < passes * 256; k += SBLK)
+    {
+        const uint32_t c = (&sh[0][0])[k];
+        if (c) { atomicAdd(&hist[k], c); }
+    }
+}
+
+// sorted[j] = roots[order[j]] (order: nullptr for the identity), and its triangle count.
+__global__ void __launch_bounds__(SBLK)
+k_root_gather(const SahRoot* __restrict__ roots, const uint32_t* __restrict__ order, uint32_t nr,
+              SahRoot* __restrict__ sorted, uint32_t* __restrict__ cnt)
+{
+    const uint32_t j = blockIdx.x * SBLK + threadIdx.x;
+    if (j >= nr) { return; }
+    const SahRoot r = roots[order ? order[j] : j];
+    sorted[j] = r;
+    cnt[j] = r.count;
+}
+
+// Where each depth's run of sorted roots starts: grp[d] = its first index, grp[256 + d] = the
+// triangles of all shallower roots (pre: the exclusive scan of the counts). grp[0..255] start
+// at ~0: depths without roots keep it.
+__global__ void __launch_bounds__(SBLK)
+k_root_groups(const SahRoot* __restrict__ sorted, const uint32_t* __restrict__ pre, uint32_t nr, uint32_t* __restrict__ grp)
+{
+    const uint32_t j = blockIdx.x * SBLK + threadIdx.x;
+    if (j >= nr) { return; }
+    const uint32_t d = min(sorted[j].depth, ROOT_MAX_DEPTH);
+    if (j == 0 || min(sorted[j - 1].depth, ROOT_MAX_DEPTH) != d)
+    {
+        grp[d] = j;
+        grp[256 + d] = pre[j];
+    }
+}
+
+// Copies the Morton-sorted triangles of new subtree roots into the level's reference list, at
+// offsets pre[b] + delta (pre: the sorted roots' exclusive count scan), which it also stores
+// in new_off for k_sah_merge.
+__global__ void __launch_bounds__(SBLK)
+k_sah_root_refs(const SahRoot* __restrict__ roots, const uint32_t* __restrict__ pre, uint32_t delta,
+                uint32_t* __restrict__ new_off, const uint32_t* __restrict__ perm, uint32_t* __restrict__ refs,
+                uint32_t* __restrict__ wtri, uint8_t* __restrict__ kpos)
 {
     const SahRoot r = roots[blockIdx.x];
-    const uint32_t off = new_off[blockIdx.x];
+    const uint32_t off = pre[blockIdx.x] + delta;  // (modulo 2^32: delta may be "negative")
+    if (threadIdx.x == 0) { new_off[blockIdx.x] = off; }
     for (uint32_t i = threadIdx.x; i < r.count; i += SBLK)
     {
         refs[off + i] = perm[r.first + i];
@@ -2164,34 +2236,6 @@ int sah_build(rt_bvh* B, const rt_build_cfg& cfg, const SahInput& in, cudaStream
     const uint32_t cap = in.cap;
     const uint32_t nr = in.n_roots;
 
-    // subtree roots in the reference's queue order: by depth, then key position
-    std::vector<SahRoot> roots(nr);
-    RT_CUDA(cudaMemcpyAsync(roots.data(), in.roots, (size_t)nr * sizeof(SahRoot), cudaMemcpyDeviceToHost, st));
-    RT_CUDA(cudaStreamSynchronize(st));
-    {
-        // (depth, first) order by stable counting passes: four 8-bit passes over first, then one
-        // over the depth (a comparison sort of tens of thousands of records costs milliseconds)
-        std::vector<uint32_t> idx(nr), tmp(nr);
-        for (uint32_t i = 0; i < nr; i++) { idx[i] = i; }
-        uint32_t max_depth = 0;
-        for (uint32_t i = 0; i < nr; i++) { max_depth = std::max(max_depth, roots[i].depth); }
-        auto pass = [&](auto digit, uint32_t buckets) {
-            std::vector<uint32_t> cnt(buckets + 1, 0u);
-            for (uint32_t i = 0; i < nr; i++) { cnt[digit(roots[idx[i]]) + 1]++; }
-            for (uint32_t b = 0; b < buckets; b++) { cnt[b + 1] += cnt[b]; }
-            for (uint32_t i = 0; i < nr; i++) { tmp[cnt[digit(roots[idx[i]])]++] = idx[i]; }
-            idx.swap(tmp);
-        };
-        for (int sh = 0; sh < 32; sh += 8)
-        {
-            pass([sh](const SahRoot& r) { return (r.first >> sh) & 255u; }, 256u);
-        }
-        pass([](const SahRoot& r) { return r.depth; }, max_depth + 1u);
-        std::vector<SahRoot> sorted(nr);
-        for (uint32_t i = 0; i < nr; i++) { sorted[i] = roots[idx[i]]; }
-        roots.swap(sorted);
-    }
-
     if (S.sah_roots_lvl.ensure((size_t)nr * sizeof(SahRoot)) || S.sah_lvl_a.ensure((size_t)cap * sizeof(LvlNode)) ||
         S.sah_lvl_b.ensure((size_t)cap * sizeof(LvlNode)) || S.sah_node_ids.ensure((size_t)cap * sizeof(LvlNode)) ||
         S.sah_refs_a.ensure((size_t)cap * 4) || S.sah_refs_b.ensure((size_t)cap * 4) || S.sah_tmp.ensure((size_t)cap * 4) ||
@@ -2202,7 +2246,62 @@ int sah_build(rt_bvh* B, const rt_build_cfg& cfg, const SahInput& in, cudaStream
         return RT_E_CUDA;
     }
     SahRoot* d_roots = S.sah_roots_lvl.as<SahRoot>();
-    RT_CUDA(cudaMemcpyAsync(d_roots, roots.data(), (size_t)nr * sizeof(SahRoot), cudaMemcpyHostToDevice, st));
+    // subtree roots in the reference's queue order -- by depth, then key position -- sorted on
+    // the device; the host reads back where each depth's run starts
+    int fb = 1;
+    while (fb < 32 && (1ull << fb) < (uint64_t)in.n) { fb++; }
+    const int key_bits = fb + 8, passes = sort_passes(key_bits);
+    const size_t o_vals = (size_t)nr * 8, o_cnt = o_vals + (size_t)nr * 4, o_pre = o_cnt + (size_t)nr * 4,
+                 o_hist = o_pre + (size_t)nr * 4, o_grp = o_hist + (size_t)ROOT_HIST_PASSES * 256 * 4;
+    if (S.sah_root_ord.ensure(o_grp + 520 * 4)) { return RT_E_CUDA; }
+    uint8_t* ob = S.sah_root_ord.as<uint8_t>();
+    uint64_t* rkeys = reinterpret_cast<uint64_t*>(ob);
+    uint32_t* rvals = reinterpret_cast<uint32_t*>(ob + o_vals);
+    uint32_t* rcnt = reinterpret_cast<uint32_t*>(ob + o_cnt);
+    uint32_t* rpre = reinterpret_cast<uint32_t*>(ob + o_pre);
+    uint32_t* rhist = reinterpret_cast<uint32_t*>(ob + o_hist);
+    uint32_t* rgrp = reinterpret_cast<uint32_t*>(ob + o_grp);
+    RT_CUDA(cudaMemsetAsync(rhist, 0, (size_t)ROOT_HIST_PASSES * 256 * 4, st));
+    RT_CUDA(cudaMemsetAsync(rgrp, 0xff, 256 * 4, st));
+    RT_CUDA(cudaMemsetAsync(rgrp + 256, 0, 264 * 4, st));
+    const uint32_t* order = nullptr;
+    if (nr > 1)
+    {
+        k_root_keys<<<nblk(nr), SBLK, 0, st>>>(in.roots, nr, fb, passes, rkeys, rhist, rgrp);
+        count_launch();
+        uint64_t* kout = nullptr;
+        uint32_t* vout = nullptr;
+        if (int e = radix_sort_pairs<uint64_t>(rkeys, rvals, true, nr, key_bits, rhist, nullptr, S.root_sort, in.status, st,
+                                               &kout, &vout))
+        {
+            return e;
+        }
+        order = vout;
+    }
+    else
+    {
+        k_root_keys<<<1, SBLK, 0, st>>>(in.roots, nr, fb, 0, rkeys, rhist, rgrp);
+        count_launch();
+    }
+    k_root_gather<<<nblk(nr), SBLK, 0, st>>>(in.roots, order, nr, d_roots, rcnt);
+    count_launch();
+    if (int e = exclusive_scan_u32(rcnt, rpre, nr, rgrp + 514, S.scan, st)) { return e; }
+    k_root_groups<<<nblk(nr), SBLK, 0, st>>>(d_roots, rpre, nr, rgrp);
+    count_launch();
+    if (int e = check_launch("sah roots")) { return e; }
+    uint32_t grp[520];
+    RT_CUDA(cudaMemcpyAsync(grp, rgrp, sizeof(grp), cudaMemcpyDeviceToHost, st));
+    RT_CUDA(cudaStreamSynchronize(st));
+    if (grp[513] > ROOT_MAX_DEPTH) { return fail(RT_E_CAPACITY, "SAH builder: subtree roots deeper than 255 levels"); }
+    // runs of roots per depth: {depth, first index, triangles of the shallower roots}
+    struct Run { uint32_t depth, start, pre; };
+    std::vector<Run> runs;
+    for (uint32_t d = 0; d <= ROOT_MAX_DEPTH; d++)
+    {
+        if (grp[d] != 0xffffffffu) { runs.push_back({ d, grp[d], grp[256 + d] }); }
+    }
+    if (runs.empty() || runs[0].start != 0) { return fail(RT_E_CAPACITY, "SAH builder: root runs out of order"); }
+    const uint32_t root_total = grp[514], root_max = grp[512];
     uint32_t* child_slot = S.sah_scan_out.as<uint32_t>();
     uint32_t* ref_offs = child_slot + cap;
     uint32_t* leaf_offs = ref_offs + cap;
@@ -2241,8 +2340,6 @@ int sah_build(rt_bvh* B, const rt_build_cfg& cfg, const SahInput& in, cudaStream
     uint32_t* d_used = reinterpret_cast<uint32_t*>(d_need + n_zero64);
     RT_CUDA(cudaMemsetAsync(d_need, 0, n_zero64 * 8, st));
     RT_CUDA(cudaMemcpyAsync(d_used, budget.data(), budget.size() * 4, cudaMemcpyHostToDevice, st));
-    // host copy of new-root offsets per level (uploaded as one array, sliced per level)
-    std::vector<uint32_t> new_off_h(nr);
 
     Ctx C;
     C.verts = in.verts; C.tris = in.tris; C.lo = in.lo; C.hi = in.hi; C.cz = in.cz;
@@ -2258,17 +2355,22 @@ int sah_build(rt_bvh* B, const rt_build_cfg& cfg, const SahInput& in, cudaStream
 
     std::vector<std::pair<uint32_t, uint32_t>> levels;
     uint32_t out_total = 0, n_cur = 0, r_cur = 0, leaf_total = 0, ri = 0;
-    uint32_t depth = nr ? roots[0].depth : 0;
+    size_t run = 0;
+    uint32_t depth = runs[0].depth;
     for (int guard = 0; guard < 100000; guard++)
     {
         // subtree roots entering at this depth
-        uint32_t m = 0, add = 0;
-        while (ri + m < nr && roots[ri + m].depth == depth)
+        uint32_t m = 0, add = 0, delta = 0;
+        if (run < runs.size() && runs[run].depth == depth)
         {
-            new_off_h[ri + m] = r_cur + add;
-            add += roots[ri + m].count;
-            next_bound = std::max(next_bound, roots[ri + m].count);
-            m++;
+            const uint32_t end = run + 1 < runs.size() ? runs[run + 1].start : nr;
+            const uint32_t pend = run + 1 < runs.size() ? runs[run + 1].pre : root_total;
+            if (runs[run].start != ri || end < ri) { return fail(RT_E_CAPACITY, "SAH builder: root runs out of order"); }
+            m = end - ri;
+            add = pend - runs[run].pre;
+            delta = r_cur - runs[run].pre;
+            next_bound = std::max(next_bound, root_max);
+            run++;
         }
         const uint32_t lvl_begin = out_total - n_cur;
         if (m > 0)
@@ -2277,8 +2379,8 @@ int sah_build(rt_bvh* B, const rt_build_cfg& cfg, const SahInput& in, cudaStream
             {
                 return fail(RT_E_CAPACITY, "SAH builder: level capacity exceeded");
             }
-            RT_CUDA(cudaMemcpyAsync(new_off + ri, new_off_h.data() + ri, (size_t)m * 4, cudaMemcpyHostToDevice, st));
-            k_sah_root_refs<<<m, SBLK, 0, st>>>(d_roots + ri, new_off + ri, in.perm, refs_cur, in.wtri, in.kpos);
+            k_sah_root_refs<<<m, SBLK, 0, st>>>(d_roots + ri, rpre + ri, delta, new_off + ri, in.perm, refs_cur, in.wtri,
+                                                in.kpos);
             k_sah_merge<<<nblk(n_cur + m), SBLK, 0, st>>>(lv_cur, n_cur, d_roots, ri, m, new_off + ri, out_total, lv_tmp,
                                                           out, root_out);
             count_launch(2);
@@ -2290,8 +2392,8 @@ int sah_build(rt_bvh* B, const rt_build_cfg& cfg, const SahInput& in, cudaStream
         }
         if (n_cur == 0)
         {
-            if (ri >= nr) { break; }
-            depth = roots[ri].depth;
+            if (run >= runs.size()) { break; }
+            depth = runs[run].depth;
             continue;
         }
         levels.emplace_back(lvl_begin, out_total);

@@ -37,6 +37,7 @@ struct SahInput
     uint32_t*          wnode;  // per start key weights to fill for the roots
     uint32_t*          wtri;   // (the roots' keys are cleared here and in kpos: not in Morton leaves)
     uint8_t*           kpos;
+    uint32_t*          status;  // the build's status word (ST_* flags)
     // spatial-split budget per scene (one scene unless batched): references in use at the
     // start (the scene's triangles) and the cap (bvh_morton.cpp:46-47)
     std::vector<uint32_t> budget_used, budget_cap;
