@@ -626,38 +626,47 @@ __device__ __forceinline__ void eval_node_warp(const Src& src, const LvlNode& nd
 
 // STAGED: the nodes of at most EVAL_STAGE references (leaves included), read from a shared
 // copy; else the nodes of EVAL_STAGE + 1 .. WARP_MAX references, read from global memory.
+// Each warp takes the level's nodes one at a time from a counter (*ctr, zero at launch), so a
+// warp that meets leaves or another kernel's nodes moves on at once and the grid need only
+// fill the GPU.
 template <bool STAGED>
 __global__ void __launch_bounds__(EVAL_WPB * 32)
 k_sah_eval_warp(const LvlNode* __restrict__ lv, const uint32_t* __restrict__ refs, Ctx C, Dec* __restrict__ dec,
-                uint32_t n_lvl)
+                uint32_t n_lvl, uint32_t* __restrict__ ctr)
 {
     __shared__ EvalWS ws[EVAL_WPB];
     __shared__ StageBuf stage[STAGED ? EVAL_WPB : 1];
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const uint32_t node = blockIdx.x * EVAL_WPB + (uint32_t)w;
-    if (node >= n_lvl) { return; }
-    const LvlNode nd = lv[node];
-    const uint32_t n = nd.count;
-    if (STAGED ? n > EVAL_STAGE : (n <= EVAL_STAGE || n > WARP_MAX)) { return; }  // another kernel decides this node
-    const uint32_t* R = refs + nd.ref_off;
-    Dec d;
-    memset(&d, 0, sizeof(d));
-    d.n = n;
-    if (n <= C.max_leaf)
+    for (;;)
     {
-        if (lane == 0) { d.kind = K_LEAF; dec[node] = d; }
-        return;
+        uint32_t node = 0;
+        if (lane == 0) { node = atomicAdd(ctr, 1u); }
+        node = __shfl_sync(0xffffffffu, node, 0);
+        if (node >= n_lvl) { return; }
+        const LvlNode nd = lv[node];
+        const uint32_t n = nd.count;
+        if (STAGED ? n > EVAL_STAGE : (n <= EVAL_STAGE || n > WARP_MAX)) { continue; }  // another kernel's node
+        const uint32_t* R = refs + nd.ref_off;
+        Dec d;
+        memset(&d, 0, sizeof(d));
+        d.n = n;
+        if (n <= C.max_leaf)
+        {
+            if (lane == 0) { d.kind = K_LEAF; dec[node] = d; }
+            continue;
+        }
+        if constexpr (STAGED)
+        {
+            stage_refs(C, R, n, stage[w]);
+            eval_node_warp(StagedRefs{ &stage[w], R }, nd, n, C, ws[w], d);
+        }
+        else
+        {
+            eval_node_warp(GlobalRefs(C, R), nd, n, C, ws[w], d);
+        }
+        if (lane == 0) { dec[node] = d; }
+        __syncwarp();  // every lane done with the shared copy and bins before the next node
     }
-    if constexpr (STAGED)
-    {
-        stage_refs(C, R, n, stage[w]);
-        eval_node_warp(StagedRefs{ &stage[w], R }, nd, n, C, ws[w], d);
-    }
-    else
-    {
-        eval_node_warp(GlobalRefs(C, R), nd, n, C, ws[w], d);
-    }
-    if (lane == 0) { dec[node] = d; }
 }
 
 // One block per node: evaluates every object and spatial candidate in the reference's order
@@ -1179,7 +1188,9 @@ __global__ void k_wide_final(const LvlNode* __restrict__ lv, Ctx C, const uint32
 //                 leaf-store space by a one-pass prefix scan.
 // io: [1] spatial taken, [2] spatial refused, [3] next-level nodes, [4] next-level references,
 //     [5] leaf-store entries of this level, [6] leaves, [10] largest next-level node,
-//     [11] spatial candidates of the level, [12] status (a bounded wait gave up)
+//     [7] every spatial candidate of the level refused, [11] spatial candidates of the level,
+//     [12] status (a bounded wait gave up), [13] / [14] the warp evaluations' node counters,
+//     [15] the smallest request of the level
 constexpr uint32_t MAX_BUDGET_SCENES = 1024;
 constexpr int NEED_THREADS = 256;
 
@@ -1189,10 +1200,11 @@ k_sah_need(const Dec* __restrict__ dec, const LvlNode* __restrict__ lv, const Sa
 {
     __shared__ uint32_t sh[NEED_THREADS / 32 + 1];
     const uint32_t i = blockIdx.x * NEED_THREADS + threadIdx.x;
-    uint32_t nd = 0, sp = 0;
+    uint32_t nd = 0, sp = 0, mn = 0xffffffffu;
     if (i < n_lvl && dec[i].kind == K_SPATIAL)
     {
         nd = dec[i].right + dec[i].straddle;
+        mn = nd;
         sp = 1;
         if (n_scenes > 1)
         {
@@ -1200,6 +1212,8 @@ k_sah_need(const Dec* __restrict__ dec, const LvlNode* __restrict__ lv, const Sa
             nd = 0;
         }
     }
+    mn = __reduce_min_sync(0xffffffffu, mn);
+    if ((threadIdx.x & 31) == 0 && mn != 0xffffffffu) { atomicMin(&io[15], mn); }
     // one scene: one addition per block (a level's references fit 32 bits)
     nd = block_sum<NEED_THREADS>(nd, sh);
     sp = block_sum<NEED_THREADS>(sp, sh);
@@ -1221,7 +1235,7 @@ k_sah_grant(Dec* __restrict__ dec, const LvlNode* __restrict__ lv, const SahRoot
     __shared__ uint32_t sh[33];
     __shared__ int s_all;
     const int tid = threadIdx.x;
-    if (tid == 0) { s_all = 1; }
+    if (tid == 0) { s_all = 1; io[7] = 0u; }
     __syncthreads();
     for (uint32_t k = tid; k < n_scenes; k += 1024)
     {
@@ -1232,6 +1246,11 @@ k_sah_grant(Dec* __restrict__ dec, const LvlNode* __restrict__ lv, const SahRoot
     {
         for (uint32_t k = tid; k < n_scenes; k += 1024) { used[k] = (uint32_t)(used[k] + need[k]); }
         if (tid == 0) { io[1] += io[11]; }
+    }
+    else if (n_scenes == 1 && (unsigned long long)used[0] + io[15] > (unsigned long long)cap[0])
+    {
+        // not even the smallest request fits: k_sah_offsets refuses every candidate
+        if (tid == 0) { io[7] = 1u; }
     }
     else
     {
@@ -1304,7 +1323,7 @@ k_sah_grant(Dec* __restrict__ dec, const LvlNode* __restrict__ lv, const SahRoot
     __syncthreads();
     for (uint32_t k = tid; k < n_scenes; k += 1024) { need[k] = 0ull; }
     for (uint32_t k = tid; k <= 3 * n_tiles; k += 1024) { desc[k] = 0ull; }
-    if (tid == 0) { io[10] = 0u; io[11] = 0u; }
+    if (tid == 0) { io[10] = 0u; io[11] = 0u; io[13] = 0u; io[14] = 0u; io[15] = 0xffffffffu; }
 }
 
 // Child slots, reference offsets and leaf offsets of a level: three exclusive scans in one pass
@@ -1317,7 +1336,7 @@ constexpr uint32_t SO_SPIN_LIMIT = 1u << 22;
 constexpr int SO_THREADS = 512, SO_ITEMS = 8, SO_TILE = SO_THREADS * SO_ITEMS;
 
 __global__ void __launch_bounds__(SO_THREADS)
-k_sah_offsets(const Dec* __restrict__ dec, uint32_t n_lvl, unsigned long long* __restrict__ desc,
+k_sah_offsets(Dec* __restrict__ dec, uint32_t n_lvl, unsigned long long* __restrict__ desc,
               uint32_t* __restrict__ ticket, uint32_t* __restrict__ io, uint32_t* __restrict__ child_slot,
               uint32_t* __restrict__ ref_off, uint32_t* __restrict__ leaf_off)
 {
@@ -1327,7 +1346,8 @@ k_sah_offsets(const Dec* __restrict__ dec, uint32_t n_lvl, unsigned long long* _
     __syncthreads();
     const uint32_t tile = s_tile;
     const uint32_t i0 = tile * SO_TILE + threadIdx.x * SO_ITEMS;
-    uint32_t v[3][SO_ITEMS], sum[3] = { 0, 0, 0 }, nleaf = 0, bmax = 0;
+    const bool refuse_all = io[7] != 0u;
+    uint32_t v[3][SO_ITEMS], sum[3] = { 0, 0, 0 }, nleaf = 0, bmax = 0, refused = 0;
 #pragma unroll
     for (int r = 0; r < SO_ITEMS; r++)
     {
@@ -1335,7 +1355,16 @@ k_sah_offsets(const Dec* __restrict__ dec, uint32_t n_lvl, unsigned long long* _
         const uint32_t i = i0 + r;
         if (i < n_lvl)
         {
-            const int kind = dec[i].kind;
+            int kind = dec[i].kind;
+            if (refuse_all && kind == K_SPATIAL)
+            {
+                // the saved object split (or a leaf) in place of the refused spatial split
+                Dec& d = dec[i];
+                kind = d.fb_kind;
+                d.kind = kind; d.pre_spatial = 1;
+                d.axis = d.oaxis; d.bin = d.obin; d.cmin = d.ocmin; d.scale = d.oscale;
+                refused++;
+            }
             const uint32_t n = dec[i].n;
             if (kind == K_LEAF) { v[2][r] = n; nleaf++; }
             else if (kind == K_OBJECT)
@@ -1359,6 +1388,11 @@ k_sah_offsets(const Dec* __restrict__ dec, uint32_t n_lvl, unsigned long long* _
 #pragma unroll
     for (int a = 0; a < 3; a++) { excl[a] = block_excl_scan<SO_THREADS>(sum[a], sh, &tot[a]); }
     nleaf = block_sum<SO_THREADS>(nleaf, sh);
+    if (refuse_all)
+    {
+        refused = block_sum<SO_THREADS>(refused, sh);
+        if (threadIdx.x == 0 && refused) { atomicAdd(&io[2], refused); }
+    }
     // the largest next-level node
     for (int o = 16; o > 0; o >>= 1) { bmax = max(bmax, __shfl_xor_sync(0xffffffffu, bmax, o)); }
     if ((threadIdx.x & 31) == 0 && bmax) { atomicMax(&io[10], bmax); }
@@ -2308,7 +2342,7 @@ int sah_build(rt_bvh* B, const rt_build_cfg& cfg, const SahInput& in, cudaStream
     uint32_t* root_out = leaf_offs + cap;
     uint32_t* new_off = root_out + nr;
     uint32_t* io = new_off + nr;
-    uint32_t io_h[16] = { in.n, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0 };
+    uint32_t io_h[16] = { in.n, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0xffffffffu };
     RT_CUDA(cudaMemcpyAsync(io, io_h, 64, cudaMemcpyHostToDevice, st));
     // wide-node scratch: at most cap / WIDE_MIN nodes of a level have more than WIDE_MIN references
     const uint32_t max_wide = cap / WIDE_MIN + 2;
@@ -2409,13 +2443,13 @@ int sah_build(rt_bvh* B, const rt_build_cfg& cfg, const SahInput& in, cudaStream
             nch = io_h[9];
             if (nw > max_wide) { return fail(RT_E_CAPACITY, "SAH builder: too many wide nodes"); }
         }
-        k_sah_eval_warp<true><<<(n_cur + EVAL_WPB - 1) / EVAL_WPB, EVAL_WPB * 32, 0, st>>>(lv_cur, refs_cur, C,
-                                                                                             S.sah_dec.as<Dec>(), n_cur);
+        const uint32_t eval_blocks = std::min<uint32_t>((n_cur + EVAL_WPB - 1) / EVAL_WPB, 8u * (uint32_t)device_sm_count());
+        k_sah_eval_warp<true><<<eval_blocks, EVAL_WPB * 32, 0, st>>>(lv_cur, refs_cur, C, S.sah_dec.as<Dec>(), n_cur, io + 13);
         count_launch();
         if (next_bound > EVAL_STAGE)
         {
-            k_sah_eval_warp<false><<<(n_cur + EVAL_WPB - 1) / EVAL_WPB, EVAL_WPB * 32, 0, st>>>(lv_cur, refs_cur, C,
-                                                                                                  S.sah_dec.as<Dec>(), n_cur);
+            k_sah_eval_warp<false><<<eval_blocks, EVAL_WPB * 32, 0, st>>>(lv_cur, refs_cur, C, S.sah_dec.as<Dec>(), n_cur,
+                                                                           io + 14);
             count_launch();
         }
         if (next_bound > WARP_MAX)
