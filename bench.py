@@ -74,6 +74,9 @@ def parse_args():
                    help="time the device bake alone: no end-to-end or CPU legs (for profiling runs)")
     p.add_argument("--only", choices=["trace", "sah5m", "c1", "c3", "c4", "c5"],
                    help="run one secondary workload alone and print its figures (for profiling runs)")
+    p.add_argument("--n-rays", type=int, default=N_RAYS, help="incoherent rays of the traversal measurements")
+    p.add_argument("--trace-preset", default="lbvh63,hybrid,sah4",
+                   help="trees of the traversal measurements (comma-separated presets)")
     return p.parse_args()
 
 
@@ -485,17 +488,19 @@ def secondary(a, bvh, dv, dt, verts, stream, dev, flush, builds=True):
         res[f"build_{preset}_mtri_s"] = round(n / (ms * 1e-3) / 1e6, 3)
         b.free()
     lo, hi = verts[:, :3].min(0), verts[:, :3].max(0)
-    rays = torch.from_numpy(scenes.incoherent_rays(N_RAYS, lo, hi, seed=scenes.BASE_SEED + 9)).to(dev)
+    n_rays = getattr(a, "n_rays", N_RAYS)
+    rays = torch.from_numpy(scenes.incoherent_rays(n_rays, lo, hi, seed=scenes.BASE_SEED + 9)).to(dev)
     prim = torch.from_numpy(scenes.pinhole_rays(1920, 1080, (0.5, 0.5, -1.5), (0.5, 0.5, 0.5), 60.0)).to(dev)
-    for preset in ("lbvh63", "hybrid", "sah4"):
+    inc = "incoherent16M" if n_rays == N_RAYS else f"incoherent{n_rays}"
+    for preset in getattr(a, "trace_preset", "lbvh63,hybrid,sah4").split(","):
         b = rtb200.Bvh.build(dv, dt, preset, stream=stream)
-        for name, r in (("incoherent16M", rays), ("primary1080p", prim)):
+        for name, r in ((inc, rays), ("primary1080p", prim)):
             for fl, fname in ((rtb200.TRACE_CLOSEST, "closest"), (rtb200.TRACE_ANY_HIT, "anyhit")):
                 ms = timed(lambda: b.trace(r, fl, stream=stream), 3)
                 res[f"trace_{preset}_{name}_{fname}_mray_s"] = round(r.shape[0] / (ms * 1e-3) / 1e6, 1)
         # the 8-wide layout (opt-in form: same closest distances, ties may name another triangle)
         b.trace_loop(2)
-        for name, r in (("incoherent16M", rays), ("primary1080p", prim)):
+        for name, r in ((inc, rays), ("primary1080p", prim)):
             ms = timed(lambda: b.trace(r, rtb200.TRACE_CLOSEST, stream=stream), 3)
             res[f"trace_{preset}_wide8_{name}_closest_mray_s"] = round(r.shape[0] / (ms * 1e-3) / 1e6, 1)
         b.free()

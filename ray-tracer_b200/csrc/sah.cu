@@ -108,12 +108,23 @@ __device__ __forceinline__ void tri_verts(const Ctx& C, uint32_t t, f3& a, f3& b
     c = mk3(v[tr.v[2]].x, v[tr.v[2]].y, v[tr.v[2]].z);
 }
 
+// std_clampi(x86_f2i(x), 0, nb - 1) with top = nb - 1 (at most 31) as a float, without a
+// float-to-int conversion (those issue on the narrow conversion pipe, which the binning loops
+// would saturate): NaN, x < 1 and x >= 2^31 (x86's out-of-range result, INT_MIN) give 0, any
+// other x min(floor(x), top). floor(y) of y in [0, 31] is read from the bits of y + 2^23 added
+// with rounding toward zero (the sum's unit in the last place is 1).
+__device__ __forceinline__ int bin_clamp(float x, float top)
+{
+    const float y = fminf(fmaxf(x, 0.0f), top);  // fmaxf(NaN, 0) = 0
+    const int b = __float_as_int(__fadd_rz(y, 8388608.0f)) - 0x4B000000;
+    return x < 2147483648.0f ? b : 0;
+}
+
 // Object-split bin of a centroid (bvh_sah.cpp:85, :260); in [0, nb) for centroids inside
 // [cmin, cmax], which is the only case the reference meets.
 __device__ __forceinline__ int obj_bin(float c, float cmin, float scale, int nb)
 {
-    const int b = std_mini(x86_f2i((c - cmin) * scale), nb - 1);
-    return b < 0 ? 0 : b;
+    return bin_clamp((c - cmin) * scale, (float)(nb - 1));
 }
 
 // Where an evaluation reads its references' data: straight from the triangle arrays through
@@ -446,24 +457,33 @@ __device__ __forceinline__ void warp_eval_spatial_axis(const uint32_t* cin, cons
     }
 }
 
+// bnd[b] = node_min + b / sscale for b = 0 .. nb, by threads t of `count` (the region bounds of
+// bvh_sah.cpp:180-181, computed once per axis instead of once per clipped triangle).
+__device__ __forceinline__ void bin_bounds(float* bnd, float node_min, float sscale, int nb, int t, int count)
+{
+    for (int b = t; b <= nb; b += count) { bnd[b] = node_min + (float)b / sscale; }
+}
+
 // Spatial binning of references R[i0 + lane] (i0 + lane < n) along `axis` by one whole warp:
 // entry / exit counts, then every (triangle, bin) pair of the 32 references clipped and added to
 // its bin -- the pairs spread evenly over the lanes (a warp-wide scan of each reference's bin
 // count, each lane finding the owner of its pair by a binary search over the lanes), since the
 // references span different numbers of bins. The same clips as bvh_sah.cpp:175-193; the bin
-// boxes are exact unions, so their order does not matter.
+// boxes are exact unions, so their order does not matter. bnd[b] = node_min + b / sscale, the
+// bins' bounds (b = 0 .. nb), computed once per axis by the caller (bin_bounds).
 template <class Src>
 __device__ __forceinline__ void spatial_bin_warp(const Src& src, uint32_t i0, uint32_t n, int axis, const box3& nbox,
-                                                 float node_min, float sscale, int nb, uint32_t* cin, uint32_t* cout,
-                                                 SBox* bins)
+                                                 float node_min, float sscale, int nb, const float* bnd, uint32_t* cin,
+                                                 uint32_t* cout, SBox* bins)
 {
     const int lane = threadIdx.x & 31;
     const uint32_t i = i0 + (uint32_t)lane;
+    const float top = (float)(nb - 1);
     int bmin = 0, bmax = -1;
     if (i < n)
     {
-        bmin = std_clampi(x86_f2i((src.lo_of(i, axis) - node_min) * sscale), 0, nb - 1);
-        bmax = std_clampi(x86_f2i((src.hi_of(i, axis) - node_min) * sscale), 0, nb - 1);
+        bmin = bin_clamp((src.lo_of(i, axis) - node_min) * sscale, top);
+        bmax = bin_clamp((src.hi_of(i, axis) - node_min) * sscale, top);
         atomicAdd(&cin[bmin], 1u);
         atomicAdd(&cout[bmax], 1u);
     }
@@ -487,7 +507,7 @@ __device__ __forceinline__ void spatial_bin_warp(const Src& src, uint32_t i0, ui
             const int b = bo + (int)(j - eo);
             f3 v0, v1, v2;
             src.tri_verts(to, v0, v1, v2);
-            const float lo_b = node_min + (float)b / sscale, hi_b = node_min + (float)(b + 1) / sscale;
+            const float lo_b = bnd[b], hi_b = bnd[b + 1];
             box3 region;
 #pragma unroll
             for (int k = 0; k < 3; k++)
@@ -514,6 +534,7 @@ struct EvalWS
 {
     uint32_t cnt[SAH_MAX_BINS], cin[SAH_MAX_BINS], cout[SAH_MAX_BINS];
     SBox     bins[SAH_MAX_BINS];
+    float    bnd[SAH_MAX_BINS + 1];
 };
 
 template <class Src>
@@ -564,10 +585,11 @@ __device__ __forceinline__ void eval_node_warp(const Src& src, const LvlNode& nd
         if (node_max - node_min < C.spatial_eps) { continue; }
         const float sscale = (float)nb / (node_max - node_min);
         for (int b = lane; b < nb; b += 32) { S.cin[b] = 0u; S.cout[b] = 0u; sbox_clear(S.bins[b]); }
+        bin_bounds(S.bnd, node_min, sscale, nb, lane, 32);
         __syncwarp();
         for (uint32_t i0 = 0; i0 < n; i0 += 32)
         {
-            spatial_bin_warp(src, i0, n, axis, nbox, node_min, sscale, nb, S.cin, S.cout, S.bins);
+            spatial_bin_warp(src, i0, n, axis, nbox, node_min, sscale, nb, S.bnd, S.cin, S.cout, S.bins);
         }
         __syncwarp();
         warp_eval_spatial_axis(S.cin, S.cout, S.bins, nb, axis, node_min, sscale, parent_inv_area, C, Bw);
@@ -676,6 +698,7 @@ k_sah_eval(const LvlNode* __restrict__ lv, const uint32_t* __restrict__ refs, Ct
 {
     __shared__ uint32_t cnt[SAH_MAX_BINS], cin[SAH_MAX_BINS], cout[SAH_MAX_BINS];
     __shared__ SBox bins[SAH_MAX_BINS];
+    __shared__ float bnd[SAH_MAX_BINS + 1];
     __shared__ uint32_t s_red[SBLK / 32 + 1];
     __shared__ uint32_t s_cm, s_cM;
     __shared__ Best sB;
@@ -752,10 +775,11 @@ k_sah_eval(const LvlNode* __restrict__ lv, const uint32_t* __restrict__ refs, Ct
         if (node_max - node_min < C.spatial_eps) { continue; }
         const float sscale = (float)nb / (node_max - node_min);
         if (tid < nb) { cin[tid] = 0u; cout[tid] = 0u; sbox_clear(bins[tid]); }
+        bin_bounds(bnd, node_min, sscale, nb, tid, SBLK);
         __syncthreads();
         for (uint32_t i0 = (uint32_t)(tid & ~31); i0 < n; i0 += SBLK)
         {
-            spatial_bin_warp(GlobalRefs(C, R), i0, n, axis, nbox, node_min, sscale, nb, cin, cout, bins);
+            spatial_bin_warp(GlobalRefs(C, R), i0, n, axis, nbox, node_min, sscale, nb, bnd, cin, cout, bins);
         }
         __syncthreads();
         if (tid < 32)
@@ -973,6 +997,7 @@ k_wide_bins(const LvlNode* __restrict__ lv, const uint32_t* __restrict__ refs, C
 {
     __shared__ uint32_t ocnt[3][SAH_MAX_BINS], cin[3][SAH_MAX_BINS], cout[3][SAH_MAX_BINS];
     __shared__ SBox obox[3][SAH_MAX_BINS], sbx[3][SAH_MAX_BINS];
+    __shared__ float bnd[3][SAH_MAX_BINS + 1];
     uint32_t c;
     const uint32_t k = wide_item(wco, nw, blockIdx.x, c);
     const LvlNode nd = lv[wl[k]];
@@ -998,6 +1023,10 @@ k_wide_bins(const LvlNode* __restrict__ lv, const uint32_t* __restrict__ refs, C
         ocnt[a][bb] = 0u; cin[a][bb] = 0u; cout[a][bb] = 0u;
         sbox_clear(obox[a][bb]); sbox_clear(sbx[a][bb]);
     }
+    for (int a = 0; a < 3; a++)
+    {
+        if (sscale[a] != 0.f) { bin_bounds(bnd[a], node_min[a], sscale[a], nb, threadIdx.x, SBLK); }
+    }
     __syncthreads();
     for (uint32_t i = b0 + threadIdx.x; i < e0; i += SBLK)
     {
@@ -1012,11 +1041,12 @@ k_wide_bins(const LvlNode* __restrict__ lv, const uint32_t* __restrict__ refs, C
         }
         f3 v0, v1, v2;
         bool have_v = false;
+        const float top = (float)(nb - 1);
         for (int a = 0; a < 3; a++)
         {
             if (sscale[a] == 0.f) { continue; }
-            const int bmin = std_clampi(x86_f2i((tri_lo(C, t, a) - node_min[a]) * sscale[a]), 0, nb - 1);
-            const int bmax = std_clampi(x86_f2i((tri_hi(C, t, a) - node_min[a]) * sscale[a]), 0, nb - 1);
+            const int bmin = bin_clamp((tri_lo(C, t, a) - node_min[a]) * sscale[a], top);
+            const int bmax = bin_clamp((tri_hi(C, t, a) - node_min[a]) * sscale[a], top);
             atomicAdd(&cin[a][bmin], 1u);
             atomicAdd(&cout[a][bmax], 1u);
             if (bmin <= bmax)
@@ -1025,8 +1055,8 @@ k_wide_bins(const LvlNode* __restrict__ lv, const uint32_t* __restrict__ refs, C
                 box3 region = nbox;
                 for (int b = bmin; b <= bmax; b++)
                 {
-                    region.mn[a] = node_min[a] + (float)b / sscale[a];
-                    region.mx[a] = node_min[a] + (float)(b + 1) / sscale[a];
+                    region.mn[a] = bnd[a][b];
+                    region.mx[a] = bnd[a][b + 1];
                     const box3 cl = clip_triangle(v0, v1, v2, region);
                     if (box_valid(cl)) { sbox_add(sbx[a][b], cl); }
                 }
