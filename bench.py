@@ -48,12 +48,14 @@ WORKLOAD = "BVH build microbenchmark: 1,048,576-triangle soup, LBVH 63-bit Morto
 # takes four passes over 16-byte pairs (68), with a 16-byte topology: 260.
 ROOFLINE_BYTES_PER_TRI = {21: 400, 10: 260}
 # What this library's bake moves per triangle by its own count (each array once per read and
-# once per write, per kernel; V = 3N vertices): clear 30, vertex renormalisation 144, triangle
-# prep 84, Morton codes 20, radix tree with boxes 100, boundary 40, scans 24, .bvh nodes and
-# triangles 93, traversal layout 158; plus the sort: 44 up to 2^21 keys (top-digit onesweep
-# pass 20 + per-bucket pass 24), else 188 (eight onesweep passes). It includes the outputs the
-# minimal count leaves out (renormalised normals, the .bvh layout, the traversal layout).
-BAKE_BYTES_PER_TRI_EXCL_SORT = 30 + 144 + 84 + 20 + 100 + 40 + 24 + 93 + 158
+# once per write, per kernel; V = 3N vertices): clear 12, vertex renormalisation 144, triangle
+# prep 132 (boxes, centroids and the 48-byte triangle records), Morton codes 20, bucket table 8,
+# Karras topology with leaf boxes, box-hierarchy level 0 and the baked triangles 198, box levels
+# 1, boundary 80, slot scans 16, .bvh and traversal nodes 45; plus the sort: 44 up to 2^21 keys
+# (top-digit onesweep pass 20 + per-bucket pass 24), else 188 (eight onesweep passes). It
+# includes the outputs the minimal count leaves out (renormalised normals, the .bvh layout, the
+# traversal layout).
+BAKE_BYTES_PER_TRI_EXCL_SORT = 12 + 144 + 132 + 20 + 8 + 198 + 1 + 80 + 16 + 45
 
 
 def bake_bytes_per_tri(n: int) -> int:
