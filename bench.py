@@ -549,9 +549,9 @@ def _trace_ceiling(b, verts, stream, dev, n=1 << 22):
 
 
 def profiled_render_counters(key):
-    """Issue-slot and cache figures of a path-loop kernel from the committed ncu summary
-    (profiles/render_kernels_c1.md: lines `key: name=value, ...`), if present."""
-    path = os.path.join(HERE, "profiles", "render_kernels_c1.md")
+    """Issue-slot and cache figures of a path-loop kernel from the committed ncu summaries
+    (profiles/render_kernels_<workload>.md: lines `key: name=value, ...`), if present."""
+    path = os.path.join(HERE, "profiles", f"render_kernels_{key.split('_')[0]}.md")
     try:
         for line in open(path):
             if line.startswith(key + ":"):
@@ -715,7 +715,7 @@ def render_c3(stream, dev):
         "autotuned": tuned.as_dict(), "autotune_s": round(tune_s, 2),
         "batched_vs_plain_max_rel_diff": max(diffs),
         "roofline": _render_roofline(counts, len(sub) * 8 * 512 * 4, nb, tbr, statistics.mean(ceil),
-                                     "batched wavefront (autotuned)"),
+                                     "batched wavefront (autotuned)", "c3_wavefront_trace"),
         "cpu_baseline": {"value": round(nb / cpu_total_s / 1e6, 4), "unit": "Mpx*spp/s (bake + render)", "cores": cores,
                          "kind": "reference bake + port (the oracle's restated path loop)",
                          "sample": f"scenes {sub}: the reference's bake of each (1 thread, {bake_s:.2f} s) and the "
@@ -802,7 +802,8 @@ def render_c5(stream, dev):
         "wavefront_tuned_mpx_spp_s": _mpx(nl, tlt), "autotuned": tuned.as_dict(),
         "plain_ms": round(tlp, 1), "wavefront_ms": round(tlw, 1), "wavefront_tuned_ms": round(tlt, 1),
         "roofline": _render_roofline(counts, 1920 * (rows[1] - rows[0]) * 64, nl, best, ceiling,
-                                     {tlp: "plain", tlw: "wavefront", tlt: "wavefront (autotuned)"}[best]),
+                                     {tlp: "plain", tlw: "wavefront", tlt: "wavefront (autotuned)"}[best],
+                                     "c5_wavefront_trace"),
         "cpu_baseline": {"value": round(1920 * (rows[1] - rows[0]) * 64 / cpu_s / 1e6, 4), "unit": "Mpx*spp/s",
                          "cores": cores, "kind": "port (the oracle's restated path loop over the reference traversal)",
                          "sample": f"rows {rows[0]}-{rows[1] - 1} of 1080 at 64 spp, scaled to the metric"}}

@@ -480,10 +480,11 @@ __device__ __forceinline__ int prefix_len(const K* __restrict__ keys, uint32_t n
 // predecessor's bucket and its own; thread n the entries past the last key.
 template <typename K>
 __global__ void __launch_bounds__(BLK)
-k_bucket_table(const K* __restrict__ keys, uint32_t n, int kshift, uint32_t tb_size, uint32_t* __restrict__ tab)
+k_bucket_table(const K* __restrict__ keys, uint32_t n, int kshift, uint32_t tb_size, uint32_t* __restrict__ tab,
+               const uint32_t* __restrict__ abort_flag)
 {
     const uint32_t i = blockIdx.x * BLK + threadIdx.x;
-    if (i > n) { return; }
+    if (i > n || *abort_flag) { return; }
     const uint64_t b = i < n ? (uint64_t)(keys[i] >> kshift) : (uint64_t)tb_size;
     const uint64_t b0 = i == 0 ? 0 : (uint64_t)(keys[i - 1] >> kshift) + 1u;
     for (uint64_t q = b0; q <= b; q++) { tab[q] = i; }
@@ -517,10 +518,11 @@ k_karras(const K* __restrict__ keys, const uint32_t* __restrict__ perm, uint32_t
          uint8_t* __restrict__ kflag, const uint32_t* __restrict__ tab, int key_bits, int tb, uint32_t tm,
          uint32_t sshift, BoxLevels V, const float4* __restrict__ tpin,
          rt_triangle* __restrict__ out_tris, uint32_t* __restrict__ prim, float4* __restrict__ tp,
-         uint32_t* __restrict__ status)
+         uint32_t* __restrict__ status, const uint32_t* __restrict__ abort_flag)
 {
     static_assert(BLK == LV_FAN * LV_FAN, "one block of threads covers one level-2 element");
     __shared__ float4 s_mn[LV_FAN], s_mx[LV_FAN];
+    if (*abort_flag) { return; }  // (uniform over the grid)
     const uint32_t i = blockIdx.x * BLK + threadIdx.x;
     float4 mn, mx;
     empty_box4(mn, mx);
@@ -664,9 +666,11 @@ k_karras(const K* __restrict__ keys, const uint32_t* __restrict__ perm, uint32_t
 
 // Level 2 from level 1 (one thread per level-1 group), then, in the last block to finish, the
 // levels above.
-__global__ void __launch_bounds__(BLK) k_box_levels(BoxLevels V, uint32_t* __restrict__ ticket)
+__global__ void __launch_bounds__(BLK) k_box_levels(BoxLevels V, uint32_t* __restrict__ ticket,
+                                                    const uint32_t* __restrict__ abort_flag)
 {
     __shared__ uint32_t s_last;
+    if (*abort_flag) { return; }  // (uniform over the grid)
     if (V.top >= 3)
     {
         const uint64_t e = (uint64_t)blockIdx.x * BLK + threadIdx.x;  // level-2 element
@@ -718,10 +722,10 @@ k_boundary(const K* __restrict__ keys, const uint32_t* __restrict__ perm, uint32
            uint32_t tm, uint32_t max_leaf, uint32_t sshift, float4* __restrict__ kbox, uint32_t* __restrict__ rank,
            uint32_t* __restrict__ wnode, uint32_t* __restrict__ wtri,
            uint8_t* __restrict__ kpos, SahRoot* __restrict__ roots, uint32_t* __restrict__ counters,
-           const uint8_t* __restrict__ kflag, uint32_t* __restrict__ status)
+           const uint8_t* __restrict__ kflag, uint32_t* __restrict__ status, const uint32_t* __restrict__ abort_flag)
 {
     const uint32_t x = blockIdx.x * BLK + threadIdx.x;
-    if (x >= 2 * n - 1) { return; }
+    if (x >= 2 * n - 1 || *abort_flag) { return; }
     const uint8_t fl = kflag[x];
     if (!(fl & KF_KEPT)) { return; }
     const bool is_m = (fl & KF_MSPLIT) != 0;
@@ -792,10 +796,11 @@ k_emit(const K* __restrict__ keys, uint32_t n, const uint4* __restrict__ knode, 
        uint32_t tm, uint32_t max_leaf, uint32_t sshift, const float4* __restrict__ kbox, const uint32_t* __restrict__ rank,
        const uint32_t* __restrict__ snode, const uint32_t* __restrict__ stri, rt_bvh_node* __restrict__ out,
        uint32_t max_nodes, uint32_t* __restrict__ info, const uint8_t* __restrict__ kflag, float* __restrict__ gn,
-       TraceRoot* __restrict__ root, uint32_t* __restrict__ status)
+       TraceRoot* __restrict__ root, uint32_t* __restrict__ status,
+       const uint32_t* __restrict__ abort_flag)
 {
     const uint32_t x = blockIdx.x * BLK + threadIdx.x;
-    if (x >= 2 * n - 1) { return; }
+    if (x >= 2 * n - 1 || *abort_flag) { return; }
     const uint8_t fl = kflag[x];
     if (!(fl & KF_KEPT)) { return; }
     const bool is_m = (fl & KF_MSPLIT) != 0;
@@ -963,10 +968,11 @@ constexpr int SC1_THREADS = 512, SC1_ITEMS = 16, SC1_TILE = SC1_THREADS * SC1_IT
 
 __global__ void __launch_bounds__(SC1_THREADS)
 k_scan2_onepass(Scan2 S, uint32_t n, unsigned long long* __restrict__ desc, uint32_t* __restrict__ ticket,
-                uint32_t* __restrict__ status)
+                uint32_t* __restrict__ status, const uint32_t* __restrict__ abort_flag)
 {
     __shared__ uint32_t sh[SC1_THREADS / 32 + 1];
     __shared__ uint32_t s_tile, s_prev[2];
+    if (*abort_flag) { return; }  // (uniform over the grid)
     if (threadIdx.x == 0) { s_tile = atomicAdd(ticket, 1u); }
     __syncthreads();
     const uint32_t tile = s_tile;
@@ -1178,7 +1184,7 @@ int build_typed(rt_bvh* B, const rt_vertex* d_verts, uint32_t V, const rt_triang
         {
             const int tb = std::min(16, key_bits);
             k_bucket_table<K><<<blocks_for((uint64_t)N + 1), BLK, 0, st>>>(skeys, N, key_bits - tb, 1u << tb,
-                                                                         S.ktab.as<uint32_t>());
+                                                                         S.ktab.as<uint32_t>(), counters + 14);
             // without expected SAH subtrees the baked triangles are written here (in key order); a
             // bake that finds runs of equal codes after all writes them again in its second emit
             const bool fuse = !expect_sah;
@@ -1186,11 +1192,11 @@ int build_typed(rt_bvh* B, const rt_vertex* d_verts, uint32_t V, const rt_triang
                                                        S.knode.as<uint4>(), S.parent.as<uint32_t>(), S.kflag.as<uint8_t>(),
                                                        S.ktab.as<uint32_t>(), key_bits, tb, tm, sshift, bl, S.tpin.as<float4>(),
                                                        fuse ? B->tris.as<rt_triangle>() : nullptr, B->prim.as<uint32_t>(),
-                                                       B->tripos.as<float4>(), status);
+                                                       B->tripos.as<float4>(), status, counters + 14);
             tris_fused = fuse;
             count_launch();
             // counters[8]: the ticket that elects the last block to build the upper levels
-            k_box_levels<<<blocks_for(lv_count(N, 2)), BLK, 0, st>>>(bl, counters + 8);
+            k_box_levels<<<blocks_for(lv_count(N, 2)), BLK, 0, st>>>(bl, counters + 8, counters + 14);
             count_launch(2);
         }
         k_boundary<K><<<blocks_for(nk), BLK, 0, st>>>(skeys, perm, N, S.knode.as<uint4>(), S.parent.as<uint32_t>(),
@@ -1198,7 +1204,8 @@ int build_typed(rt_bvh* B, const rt_vertex* d_verts, uint32_t V, const rt_triang
                                                       tm, cfg.max_leaf, sshift,
                                                       S.kbox.as<float4>(), S.rank.as<uint32_t>(),
                                                       S.wnode.as<uint32_t>(), S.wtri.as<uint32_t>(), S.bnd.as<uint8_t>(),
-                                                      S.sah_roots.as<SahRoot>(), counters, S.kflag.as<uint8_t>(), status);
+                                                      S.sah_roots.as<SahRoot>(), counters, S.kflag.as<uint8_t>(), status,
+                                                      counters + 14);
         count_launch();
         if (int e = check_launch("boundary")) { return e; }
         prof_mark(B, 3, st);
@@ -1251,7 +1258,8 @@ int build_typed(rt_bvh* B, const rt_vertex* d_verts, uint32_t V, const rt_triang
             Scan2 sc;
             sc.in[0] = S.wnode.as<uint32_t>(); sc.out[0] = S.snode.as<uint32_t>(); sc.total[0] = counters + 4;
             sc.in[1] = S.wtri.as<uint32_t>(); sc.out[1] = S.stri.as<uint32_t>(); sc.total[1] = counters + 5;
-            k_scan2_onepass<<<np, SC1_THREADS, 0, st>>>(sc, n1, desc, reinterpret_cast<uint32_t*>(desc + 2 * (size_t)np), status);
+            k_scan2_onepass<<<np, SC1_THREADS, 0, st>>>(sc, n1, desc, reinterpret_cast<uint32_t*>(desc + 2 * (size_t)np), status,
+                                                        counters + 14);
             count_launch();
         }
         k_emit<K><<<blocks_for(nk), BLK, 0, st>>>(skeys, N, S.knode.as<uint4>(), S.parent.as<uint32_t>(), tm, cfg.max_leaf,
@@ -1259,7 +1267,7 @@ int build_typed(rt_bvh* B, const rt_vertex* d_verts, uint32_t V, const rt_triang
                                                   S.stri.as<uint32_t>(), B->nodes.as<rt_bvh_node>(), 2 * cap - 1,
                                                   batch ? B->scene_info.as<uint32_t>() : nullptr, S.kflag.as<uint8_t>(),
                                                   n_roots == 0 ? B->gnodes.as<float>() : nullptr,
-                                                  B->rootbuf.as<TraceRoot>(), status);
+                                                  B->rootbuf.as<TraceRoot>(), status, counters + 14);
         count_launch();
         // without SAH subtrees every triangle passes here: its traversal record is written too
         // (input positions: the renormalisation changes only normals); k_karras wrote them already

@@ -2162,6 +2162,8 @@ k_root_groups(const SahRoot* __restrict__ sorted, const uint32_t* __restrict__ p
     }
 }
 
+constexpr uint32_t ROOT_CHUNK = 8192;  // references per block of k_sah_root_refs
+
 // Copies the Morton-sorted triangles of new subtree roots into the level's reference list, at
 // offsets pre[b] + delta (pre: the sorted roots' exclusive count scan), which it also stores
 // in new_off for k_sah_merge.
@@ -2172,8 +2174,10 @@ k_sah_root_refs(const SahRoot* __restrict__ roots, const uint32_t* __restrict__ 
 {
     const SahRoot r = roots[blockIdx.x];
     const uint32_t off = pre[blockIdx.x] + delta;  // (modulo 2^32: delta may be "negative")
-    if (threadIdx.x == 0) { new_off[blockIdx.x] = off; }
-    for (uint32_t i = threadIdx.x; i < r.count; i += SBLK)
+    if (threadIdx.x == 0 && blockIdx.y == 0) { new_off[blockIdx.x] = off; }
+    // blockIdx.y: this block's ROOT_CHUNK references of the root
+    const uint32_t e = min(r.count, (blockIdx.y + 1) * ROOT_CHUNK);
+    for (uint32_t i = blockIdx.y * ROOT_CHUNK + threadIdx.x; i < e; i += SBLK)
     {
         refs[off + i] = perm[r.first + i];
         wtri[r.first + i] = 0u;  // these keys' triangles are counted and placed by the subtree
@@ -2443,8 +2447,9 @@ int sah_build(rt_bvh* B, const rt_build_cfg& cfg, const SahInput& in, cudaStream
             {
                 return fail(RT_E_CAPACITY, "SAH builder: level capacity exceeded");
             }
-            k_sah_root_refs<<<m, SBLK, 0, st>>>(d_roots + ri, rpre + ri, delta, new_off + ri, in.perm, refs_cur, in.wtri,
-                                                in.kpos);
+            const dim3 rgrid(m, (root_max + ROOT_CHUNK - 1) / ROOT_CHUNK);
+            k_sah_root_refs<<<rgrid, SBLK, 0, st>>>(d_roots + ri, rpre + ri, delta, new_off + ri, in.perm, refs_cur, in.wtri,
+                                                    in.kpos);
             k_sah_merge<<<nblk(n_cur + m), SBLK, 0, st>>>(lv_cur, n_cur, d_roots, ri, m, new_off + ri, out_total, lv_tmp,
                                                           out, root_out);
             count_launch(2);
