@@ -814,7 +814,8 @@ k_emit(const K* __restrict__ keys, uint32_t n, const uint4* __restrict__ knode, 
             (l == n - 1 || ((uint64_t)keys[l + 1] >> sshift) != sl))
         {
             uint32_t* o = info + 4 * (size_t)sf;
-            o[0] = pre; o[1] = snode[l + 1] - pre; o[2] = stri[f]; o[3] = stri[l + 1] - stri[f];
+            const uint32_t tf = stri ? stri[f] : f, tl = stri ? stri[l + 1] : l + 1u;
+            o[0] = pre; o[1] = snode[l + 1] - pre; o[2] = tf; o[3] = tl - tf;
         }
     }
     if (!is_m && l - f + 1u > max_leaf) { return; }  // SAH subtree root: emitted by the SAH builder
@@ -829,14 +830,14 @@ k_emit(const K* __restrict__ keys, uint32_t n, const uint4* __restrict__ knode, 
     }
     else
     {
-        write_node(out, pre, b, 1, stri[f], l - f + 1u);
+        write_node(out, pre, b, 1, stri ? stri[f] : f, l - f + 1u);
     }
     if (gn)
     {
         // the traversal layout (a tree without SAH subtrees): this node's box, reference and
         // count in its parent's 64-byte record -- the left child's half is floats 0-5 and words
         // 12 / 14, the right child's floats 6-11 and words 13 / 15 -- or the entry record (the root)
-        const uint32_t ref = is_m ? pre : stri[f];
+        const uint32_t ref = is_m ? pre : (stri ? stri[f] : f);
         const uint32_t cnt = is_m ? 0u : (LEAF_BIT | (l - f + 1u));
         const uint32_t par = parent[x];
         if (par == NONE)
@@ -966,6 +967,9 @@ constexpr uint32_t SC_SPIN_LIMIT = 1u << 22;
 // prefixes, so its walk is as long as the number of tiles before it (in windows of 32).
 constexpr int SC1_THREADS = 512, SC1_ITEMS = 16, SC1_TILE = SC1_THREADS * SC1_ITEMS;
 
+// NA = 1: the first array only; the second is then the identity (every key places one
+// triangle: a tree without SAH subtrees), whose total n - 1 the last tile writes.
+template <int NA>
 __global__ void __launch_bounds__(SC1_THREADS)
 k_scan2_onepass(Scan2 S, uint32_t n, unsigned long long* __restrict__ desc, uint32_t* __restrict__ ticket,
                 uint32_t* __restrict__ status, const uint32_t* __restrict__ abort_flag)
@@ -978,7 +982,8 @@ k_scan2_onepass(Scan2 S, uint32_t n, unsigned long long* __restrict__ desc, uint
     const uint32_t tile = s_tile;
     const uint32_t base = tile * SC1_TILE + threadIdx.x * SC1_ITEMS;
     uint32_t v[2][SC1_ITEMS], excl[2], tot[2];
-    for (int a = 0; a < 2; a++)
+#pragma unroll
+    for (int a = 0; a < NA; a++)
     {
         uint32_t sum = 0;
         if (base + SC1_ITEMS <= n)
@@ -1002,7 +1007,7 @@ k_scan2_onepass(Scan2 S, uint32_t n, unsigned long long* __restrict__ desc, uint
     }
     // warp a (0, 1) publishes and looks back for array a, 32 predecessors at a time
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    if (warp < 2)
+    if (warp < NA)
     {
         const int a = warp;
         if (lane == 0)
@@ -1043,11 +1048,16 @@ k_scan2_onepass(Scan2 S, uint32_t n, unsigned long long* __restrict__ desc, uint
                 mine.store(SC_PRE | (uint32_t)(prev + tot[a]), cuda::memory_order_relaxed);
             }
             s_prev[a] = prev;
-            if (tile == gridDim.x - 1) { *S.total[a] = prev + tot[a]; }
+            if (tile == gridDim.x - 1)
+            {
+                *S.total[a] = prev + tot[a];
+                if (NA == 1) { *S.total[1] = n - 1u; }
+            }
         }
     }
     __syncthreads();
-    for (int a = 0; a < 2; a++)
+#pragma unroll
+    for (int a = 0; a < NA; a++)
     {
         uint32_t run = s_prev[a] + excl[a];
 #pragma unroll
@@ -1249,6 +1259,9 @@ int build_typed(rt_bvh* B, const rt_vertex* d_verts, uint32_t V, const rt_triang
     };
     // pre-order node slots and triangle offsets per start key, then the nodes and triangles
     auto emit_all = [&]() -> int {
+        // without SAH subtrees every key places its own triangle at its own position, so the
+        // triangle offsets are the identity and only the node slots are scanned
+        const bool tri_identity = !expect_sah && n_roots == 0 && tris_fused;
         {
             const uint32_t n1 = N + 1, np = (n1 + SC1_TILE - 1) / SC1_TILE;
             // look-back descriptors (2 per tile) and the tile ticket, zeroed for every scan
@@ -1258,13 +1271,21 @@ int build_typed(rt_bvh* B, const rt_vertex* d_verts, uint32_t V, const rt_triang
             Scan2 sc;
             sc.in[0] = S.wnode.as<uint32_t>(); sc.out[0] = S.snode.as<uint32_t>(); sc.total[0] = counters + 4;
             sc.in[1] = S.wtri.as<uint32_t>(); sc.out[1] = S.stri.as<uint32_t>(); sc.total[1] = counters + 5;
-            k_scan2_onepass<<<np, SC1_THREADS, 0, st>>>(sc, n1, desc, reinterpret_cast<uint32_t*>(desc + 2 * (size_t)np), status,
-                                                        counters + 14);
+            if (tri_identity)
+            {
+                k_scan2_onepass<1><<<np, SC1_THREADS, 0, st>>>(sc, n1, desc, reinterpret_cast<uint32_t*>(desc + 2 * (size_t)np),
+                                                               status, counters + 14);
+            }
+            else
+            {
+                k_scan2_onepass<2><<<np, SC1_THREADS, 0, st>>>(sc, n1, desc, reinterpret_cast<uint32_t*>(desc + 2 * (size_t)np),
+                                                               status, counters + 14);
+            }
             count_launch();
         }
         k_emit<K><<<blocks_for(nk), BLK, 0, st>>>(skeys, N, S.knode.as<uint4>(), S.parent.as<uint32_t>(), tm, cfg.max_leaf,
                                                   sshift, S.kbox.as<float4>(), S.rank.as<uint32_t>(), S.snode.as<uint32_t>(),
-                                                  S.stri.as<uint32_t>(), B->nodes.as<rt_bvh_node>(), 2 * cap - 1,
+                                                  tri_identity ? nullptr : S.stri.as<uint32_t>(), B->nodes.as<rt_bvh_node>(), 2 * cap - 1,
                                                   batch ? B->scene_info.as<uint32_t>() : nullptr, S.kflag.as<uint8_t>(),
                                                   n_roots == 0 ? B->gnodes.as<float>() : nullptr,
                                                   B->rootbuf.as<TraceRoot>(), status, counters + 14);
