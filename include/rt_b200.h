@@ -269,8 +269,9 @@ typedef struct rt_wavefront_params
 int rt_render_batch(rt_bvh* bvh, const rt_render_cfg* cfgs, uint32_t n_scenes, const rt_shading* shading,
                     const rt_wavefront_params* params, float* rgb, float* rgb2, void* stream);
 /* Times each candidate parameter set (trace block 64/128/256, chunk 1-8 Mi paths, stack
- * 32/64 where the tree allows) on a one-sample render of the batch and keeps the fastest in
- * the handle (and in *best). */
+ * 32/64 where the tree allows) on a short render of the batch -- enough samples per pixel for
+ * 8 Mi paths, at most the configuration's own -- and keeps the fastest in the handle (and in
+ * *best). */
 int rt_autotune_wavefront(rt_bvh* bvh, const rt_render_cfg* cfgs, uint32_t n_scenes, const rt_shading* shading,
                           rt_wavefront_params* best, void* stream);
 

@@ -667,10 +667,19 @@ int autotune_wavefront(rt_bvh* B, const rt_render_cfg* cfgs, uint32_t S, const r
 {
     uint32_t depth = 0;
     if (int e = tree_depth(B, st, &depth)) { return e; }
-    std::vector<rt_render_cfg> c1(cfgs, cfgs + S);
-    for (auto& c : c1) { c.spp = 1; c.sample_offset = 0; }
     const uint32_t blocks[] = { 64, 128, 256 };
     const uint32_t chunks[] = { 1u << 20, 1u << 21, 1u << 22, 1u << 23 };
+    // trial renders with enough samples per pixel that the largest chunk fills (a one-sample
+    // trial of a small image cannot tell the chunk sizes apart), at most the configs' own
+    uint64_t px = 0;
+    for (uint32_t k = 0; k < S; k++) { px += (uint64_t)cfgs[k].width * cfgs[k].height; }
+    const uint64_t want = px ? (((uint64_t)chunks[3] + px - 1) / px) : 1;
+    std::vector<rt_render_cfg> c1(cfgs, cfgs + S);
+    for (auto& c : c1)
+    {
+        c.spp = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(want, c.spp));
+        c.sample_offset = 0;
+    }
     const uint32_t stacks[] = { 32, 64 };
     cudaEvent_t a, b;
     RT_CUDA(cudaEventCreate(&a));
