@@ -652,7 +652,7 @@ __device__ __forceinline__ void eval_node_warp(const Src& src, const LvlNode& nd
 // warp that meets leaves or another kernel's nodes moves on at once and the grid need only
 // fill the GPU.
 template <bool STAGED>
-__global__ void __launch_bounds__(EVAL_WPB * 32)
+__global__ void __launch_bounds__(EVAL_WPB * 32, 4)  // (64 registers: occupancy over spills)
 k_sah_eval_warp(const LvlNode* __restrict__ lv, const uint32_t* __restrict__ refs, Ctx C, Dec* __restrict__ dec,
                 uint32_t n_lvl, uint32_t* __restrict__ ctr)
 {
