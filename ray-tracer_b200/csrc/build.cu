@@ -477,17 +477,23 @@ __device__ __forceinline__ int prefix_len(const K* __restrict__ keys, uint32_t n
 
 // Bucket table of the sorted keys: tab[b] = the first index whose top `tb` key bits are >= b,
 // for b = 0 .. 2^tb (tab[2^tb] = n). One thread per key writes the entries between its
-// predecessor's bucket and its own; thread n the entries past the last key.
+// predecessor's bucket and its own; thread n the entries past the last key. msd_flag (or
+// nullptr): the sort's MSD flag when its per-bucket pass writes the table; it is built here
+// only when that pass did not run (the flag is set).
 template <typename K>
 __global__ void __launch_bounds__(BLK)
 k_bucket_table(const K* __restrict__ keys, uint32_t n, int kshift, uint32_t tb_size, uint32_t* __restrict__ tab,
-               const uint32_t* __restrict__ abort_flag)
+               const uint32_t* __restrict__ abort_flag, const uint32_t* __restrict__ msd_flag)
 {
-    const uint32_t i = blockIdx.x * BLK + threadIdx.x;
-    if (i > n || *abort_flag) { return; }
-    const uint64_t b = i < n ? (uint64_t)(keys[i] >> kshift) : (uint64_t)tb_size;
-    const uint64_t b0 = i == 0 ? 0 : (uint64_t)(keys[i - 1] >> kshift) + 1u;
-    for (uint64_t q = b0; q <= b; q++) { tab[q] = i; }
+    if (*abort_flag) { return; }
+    if (msd_flag && *msd_flag == 0u) { return; }  // the sort's per-bucket pass wrote the table
+    // grid-stride (a small grid, so that the usual early return costs little)
+    for (uint32_t i = blockIdx.x * BLK + threadIdx.x; i <= n; i += gridDim.x * BLK)
+    {
+        const uint64_t b = i < n ? (uint64_t)(keys[i] >> kshift) : (uint64_t)tb_size;
+        const uint64_t b0 = i == 0 ? 0 : (uint64_t)(keys[i - 1] >> kshift) + 1u;
+        for (uint64_t q = b0; q <= b; q++) { tab[q] = i; }
+    }
 }
 
 // The reference splits a node by Morton code (it is "Morton-split") if it has more triangles
@@ -1152,7 +1158,7 @@ int build_typed(rt_bvh* B, const rt_vertex* d_verts, uint32_t V, const rt_triang
     // everything up to the boundary nodes, enqueued on st
     auto front = [&]() -> int {
         prof_mark(B, 0, st);
-        k_clear<<<blocks_for(std::max<uint32_t>(std::max<uint32_t>(nk + 1, 6 * n_boxes), (uint32_t)n_lookback)), BLK, 0, st>>>(
+        k_clear<<<blocks_for(std::max<uint32_t>(std::max<uint32_t>(N + 1, 6 * n_boxes), (uint32_t)n_lookback)), BLK, 0, st>>>(
             N, S.parent.as<uint32_t>(), S.kflag.as<uint8_t>(), S.wnode.as<uint32_t>(), S.wtri.as<uint32_t>(),
             S.bnd.as<uint8_t>(), S.scene.as<uint32_t>(), n_boxes, S.hist.as<uint32_t>(), counters, status,
             S.sort.lookback.as<uint32_t>(), (uint32_t)n_lookback, S.sort.tile_counters.as<uint32_t>());
@@ -1183,9 +1189,11 @@ int build_typed(rt_bvh* B, const rt_vertex* d_verts, uint32_t V, const rt_triang
         if (int e = check_launch("morton")) { return e; }
 
         prof_mark(B, 1, st);
+        const uint32_t* table_flag = nullptr;
         if (int e = radix_sort_pairs<K>(S.keys.as<K>(), S.vals.as<uint32_t>(), true, N, key_bits, S.hist.as<uint32_t>(),
                                         msd_shift >= 0 ? S.hist.as<uint32_t>() + 8 * 256 : nullptr, S.sort, status, st,
-                                        &skeys, &perm, true, msd_only ? counters + 14 : nullptr))
+                                        &skeys, &perm, true, msd_only ? counters + 14 : nullptr,
+                                        N >= 2 && key_bits > 16 ? S.ktab.as<uint32_t>() : nullptr, &table_flag))
         {
             return e;
         }
@@ -1193,8 +1201,9 @@ int build_typed(rt_bvh* B, const rt_vertex* d_verts, uint32_t V, const rt_triang
         if (N >= 2)
         {
             const int tb = std::min(16, key_bits);
-            k_bucket_table<K><<<blocks_for((uint64_t)N + 1), BLK, 0, st>>>(skeys, N, key_bits - tb, 1u << tb,
-                                                                         S.ktab.as<uint32_t>(), counters + 14);
+            const uint32_t table_blocks = std::min<uint32_t>(blocks_for((uint64_t)N + 1), 4u * (uint32_t)device_sm_count());
+            k_bucket_table<K><<<table_blocks, BLK, 0, st>>>(skeys, N, key_bits - tb, 1u << tb,
+                                                                         S.ktab.as<uint32_t>(), counters + 14, table_flag);
             // without expected SAH subtrees the baked triangles are written here (in key order); a
             // bake that finds runs of equal codes after all writes them again in its second emit
             const bool fuse = !expect_sah;

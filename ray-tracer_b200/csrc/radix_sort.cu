@@ -419,7 +419,7 @@ __device__ __forceinline__ void warp_sort_n(K* sk, uint32_t* sv, uint32_t start,
 template <typename K, int LB, int LI, int MINB>
 __global__ void __launch_bounds__(LB, MINB)
 k_local_sort(const K* kin, const uint32_t* vin, K* kout, uint32_t* vout, const uint32_t* __restrict__ bstart,
-             const uint32_t* __restrict__ flag, int npass, int sub_shift)
+             const uint32_t* __restrict__ flag, int npass, int sub_shift, uint32_t* __restrict__ tab)
 {
     constexpr uint32_t CAP = (uint32_t)LB * LI;
     if (*flag) { return; }
@@ -432,7 +432,15 @@ k_local_sort(const K* kin, const uint32_t* vin, K* kout, uint32_t* vout, const u
     __shared__ uint32_t s_tot[256];
     __shared__ uint32_t s_max;
     const uint32_t b0 = bstart[blockIdx.x], m = bstart[blockIdx.x + 1] - b0;
-    if (m == 0) { return; }
+    // tab (with sub-buckets): the bucket table of the top 16 key bits -- tab[v] = the first
+    // sorted index whose top 16 bits are >= v -- for this bucket's 256 values, from the
+    // sub-bucket starts; the last bucket also writes tab[65536] = n
+    if (tab && blockIdx.x == 255 && threadIdx.x == 0) { tab[65536] = bstart[256]; }
+    if (m == 0)
+    {
+        if (tab && threadIdx.x < 256) { tab[blockIdx.x * 256u + threadIdx.x] = b0; }
+        return;
+    }
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int nw = (int)((m + 32u * LI - 1) / (32u * LI));  // warps holding keys
     // element (warp, j, lane) = warp * 32 * LI + j * 32 + lane, so that order is input order
@@ -530,7 +538,11 @@ k_local_sort(const K* kin, const uint32_t* vin, K* kout, uint32_t* vout, const u
     {
         if (threadIdx.x == 0) { s_max = 0u; }
         pass(sub_shift);
-        if (threadIdx.x < 256) { atomicMax(&s_max, s_tot[threadIdx.x]); }
+        if (threadIdx.x < 256)
+        {
+            atomicMax(&s_max, s_tot[threadIdx.x]);
+            if (tab) { tab[blockIdx.x * 256u + threadIdx.x] = b0 + tstart[threadIdx.x]; }
+        }
         __syncthreads();
         if (s_max <= 64u)
         {
@@ -617,10 +629,12 @@ size_t sort_lookback_words(uint32_t n, int passes)
 template <typename K>
 int radix_sort_pairs(K* keys, uint32_t* vals, bool vals_identity, uint32_t n, int key_bits, const uint32_t* hist,
                      const uint32_t* msd_hist, SortScratch& s, uint32_t* status, cudaStream_t st, K** keys_out,
-                     uint32_t** vals_out, bool scratch_zeroed, uint32_t* msd_only_flag)
+                     uint32_t** vals_out, bool scratch_zeroed, uint32_t* msd_only_flag, uint32_t* msd_table,
+                     const uint32_t** table_flag)
 {
     *keys_out = keys;
     *vals_out = vals;
+    if (table_flag) { *table_flag = nullptr; }
     if (n == 0) { return RT_OK; }
     if (n > LB_VAL) { return fail(RT_E_CAPACITY, "radix sort: more than 2^30 keys"); }
     const int passes = sort_passes(key_bits);
@@ -667,6 +681,9 @@ int radix_sort_pairs(K* keys, uint32_t* vals, bool vals_identity, uint32_t n, in
             const int npass = sort_passes(key_bits - 8);
             // more than 8 bits below the top digit: sub-buckets by the next 8 bits, sorted whole
             const int sub_shift = key_bits - 8 > 8 ? key_bits - 16 : -1;
+            // the sub-buckets are the top 16 bits' values: the per-bucket sort writes their table
+            uint32_t* ltab = sub_shift >= 0 ? msd_table : nullptr;
+            if (table_flag) { *table_flag = ltab ? flag : nullptr; }
             // either this pass or the LSD passes use the look-back words (the flag picks one), so
             // one zeroing serves both
             if (!scratch_zeroed)
@@ -681,12 +698,12 @@ int radix_sort_pairs(K* keys, uint32_t* vals, bool vals_identity, uint32_t n, in
             if (small)
             {
                 k_local_sort<K, LS_SMALL_B, LS_SMALL_I, 2><<<256, LS_SMALL_B, sm_small, st>>>(kalt, valt, kfin, vfin, bstart,
-                                                                                           flag, npass, sub_shift);
+                                                                                           flag, npass, sub_shift, ltab);
             }
             else
             {
                 k_local_sort<K, LS_LARGE_B, LS_LARGE_I, 1><<<256, LS_LARGE_B, sm_large, st>>>(kalt, valt, kfin, vfin, bstart,
-                                                                                           flag, npass, sub_shift);
+                                                                                           flag, npass, sub_shift, ltab);
             }
             count_launch(3);
             RT_CUDA(cudaGetLastError());
@@ -707,9 +724,11 @@ int radix_sort_pairs(K* keys, uint32_t* vals, bool vals_identity, uint32_t n, in
 }
 
 template int radix_sort_pairs<uint64_t>(uint64_t*, uint32_t*, bool, uint32_t, int, const uint32_t*, const uint32_t*,
-                                        SortScratch&, uint32_t*, cudaStream_t, uint64_t**, uint32_t**, bool, uint32_t*);
+                                        SortScratch&, uint32_t*, cudaStream_t, uint64_t**, uint32_t**, bool, uint32_t*,
+                                        uint32_t*, const uint32_t**);
 template int radix_sort_pairs<uint32_t>(uint32_t*, uint32_t*, bool, uint32_t, int, const uint32_t*, const uint32_t*,
-                                        SortScratch&, uint32_t*, cudaStream_t, uint32_t**, uint32_t**, bool, uint32_t*);
+                                        SortScratch&, uint32_t*, cudaStream_t, uint32_t**, uint32_t**, bool, uint32_t*,
+                                        uint32_t*, const uint32_t**);
 
 } // namespace rtb
 

@@ -98,11 +98,17 @@ template <typename K>
 int radix_sort_pairs(K* keys, uint32_t* vals, bool vals_identity, uint32_t n, int key_bits,
                      const uint32_t* hist, const uint32_t* msd_hist, SortScratch& s, uint32_t* status,
                      cudaStream_t st, K** keys_out, uint32_t** vals_out, bool scratch_zeroed = false,
-                     uint32_t* msd_only_flag = nullptr);
+                     uint32_t* msd_only_flag = nullptr, uint32_t* msd_table = nullptr,
+                     const uint32_t** table_flag = nullptr);
 // (scratch_zeroed: the caller zeroed s.lookback's first sort_lookback_words(n, passes) words
 // and s.tile_counters' first 64 words, so the sort skips its memsets. msd_only_flag: when the
 // MSD path applies, launch no LSD fallback and write its flag there instead -- nonzero means a
-// bucket overflowed and the keys are NOT sorted: the caller must sort again without it.)
+// bucket overflowed and the keys are NOT sorted: the caller must sort again without it.
+// msd_table: where the MSD path writes the bucket table of the sorted keys' top 16 bits
+// (2^16 + 1 words: tab[v] = the first index whose top 16 bits are >= v) when its sub-buckets
+// are exactly those values (more than 16 key bits); *table_flag then points at the device word
+// that is nonzero when that path did not finish (a bucket overflowed: no table), and is
+// nullptr when no table is written.)
 // The same sort on caller-provided scratch; allocates nothing.
 template <typename K>
 int radix_sort_pairs_raw(K* keys, uint32_t* vals, uint32_t n, int key_bits, const uint32_t* hist, K* keys_alt,
