@@ -474,7 +474,7 @@ __device__ __forceinline__ void bin_bounds(float* bnd, float node_min, float ssc
 template <class Src>
 __device__ __forceinline__ void spatial_bin_warp(const Src& src, uint32_t i0, uint32_t n, int axis, const box3& nbox,
                                                  float node_min, float sscale, int nb, const float* bnd, uint32_t* cin,
-                                                 uint32_t* cout, SBox* bins)
+                                                 uint32_t* cout, SBox* bins, bool count = true)
 {
     const int lane = threadIdx.x & 31;
     const uint32_t i = i0 + (uint32_t)lane;
@@ -484,8 +484,11 @@ __device__ __forceinline__ void spatial_bin_warp(const Src& src, uint32_t i0, ui
     {
         bmin = bin_clamp((src.lo_of(i, axis) - node_min) * sscale, top);
         bmax = bin_clamp((src.hi_of(i, axis) - node_min) * sscale, top);
-        atomicAdd(&cin[bmin], 1u);
-        atomicAdd(&cout[bmax], 1u);
+        if (count)
+        {
+            atomicAdd(&cin[bmin], 1u);
+            atomicAdd(&cout[bmax], 1u);
+        }
     }
     const uint32_t c = bmin <= bmax ? (uint32_t)(bmax - bmin + 1) : 0u;
     const uint32_t incl = warp_incl_scan(c);
@@ -519,6 +522,79 @@ __device__ __forceinline__ void spatial_bin_warp(const Src& src, uint32_t i0, ui
             if (box_valid(cl)) { sbox_add(bins[b], cl); }
         }
     }
+}
+
+// Spatial candidates that cannot win, found before any clipping. The clipped box of a (triangle,
+// bin) pair contains every vertex of the triangle that lies in the bin's region (a clip keeps
+// such vertices unchanged), so the boxes of those vertices alone lie inside each bin's box, the
+// sweep's unions likewise, and -- the cost being monotone in the two areas when c_isect >= 0 --
+// every candidate's cost is bounded from below (an empty union counting as area 0; the float
+// operations are the cost's own, and rounding is monotone). When no candidate's bound is below
+// the best cost so far, none can win the strict comparison and the axis's clipping is skipped:
+// the decision is the one the full evaluation makes.
+//
+// The entry / exit counts (the exact ones) and the vertex boxes of references i0 + lane < n.
+template <class Src>
+__device__ __forceinline__ void spatial_bound_warp(const Src& src, uint32_t i0, uint32_t n, int axis, const box3& nbox,
+                                                   float node_min, float sscale, int nb, const float* bnd, uint32_t* cin,
+                                                   uint32_t* cout, SBox* bins)
+{
+    const uint32_t i = i0 + (threadIdx.x & 31u);
+    if (i >= n) { return; }
+    const float top = (float)(nb - 1);
+    const int bmin = bin_clamp((src.lo_of(i, axis) - node_min) * sscale, top);
+    const int bmax = bin_clamp((src.hi_of(i, axis) - node_min) * sscale, top);
+    atomicAdd(&cin[bmin], 1u);
+    atomicAdd(&cout[bmax], 1u);
+    if (bmin > bmax) { return; }
+    f3 v[3];
+    src.tri_verts(i, v[0], v[1], v[2]);
+#pragma unroll
+    for (int k = 0; k < 3; k++)
+    {
+        const float x = v[k].x, y = v[k].y, z = v[k].z;
+        const float c = axis == 0 ? x : (axis == 1 ? y : z);
+        bool in = true;
+        if (axis != 0) { in = in && x >= nbox.mn[0] && x <= nbox.mx[0]; }
+        if (axis != 1) { in = in && y >= nbox.mn[1] && y <= nbox.mx[1]; }
+        if (axis != 2) { in = in && z >= nbox.mn[2] && z <= nbox.mx[2]; }
+        const int vb = bin_clamp((c - node_min) * sscale, top);
+        if (!in || vb < bmin || vb > bmax || !(c >= bnd[vb] && c <= bnd[vb + 1])) { continue; }
+        SBox& sb = bins[vb];
+        atomicMin(&sb.m[0], f2ord(x)); atomicMin(&sb.m[1], f2ord(y)); atomicMin(&sb.m[2], f2ord(z));
+        atomicMax(&sb.M[0], f2ord(x)); atomicMax(&sb.M[1], f2ord(y)); atomicMax(&sb.M[2], f2ord(z));
+    }
+}
+
+// Whether any spatial candidate's lower bound (from spatial_bound_warp's bins) is below
+// best_cost, or is not a number; every lane of the calling warp returns the same.
+__device__ __forceinline__ bool warp_spatial_can_win(const uint32_t* cin, const uint32_t* cout, const SBox* bins, int nb,
+                                                     float parent_inv_area, const Ctx& C, float best_cost)
+{
+    const int lane = threadIdx.x & 31;
+    uint32_t lm[3], lM[3], rm[3], rM[3], lc = 0, rc = 0;
+    for (int k = 0; k < 3; k++) { lm[k] = rm[k] = 0xffffffffu; lM[k] = rM[k] = 0u; }
+    if (lane < nb)
+    {
+        const SBox& sb = bins[lane];
+        for (int k = 0; k < 3; k++) { lm[k] = rm[k] = sb.m[k]; lM[k] = rM[k] = sb.M[k]; }
+        lc = cin[lane];
+        rc = cout[lane];
+    }
+    warp_box_scan_up(lm, lM, lc, lane);
+    warp_box_scan_down(rm, rM, rc, lane);
+    uint32_t pm[3], pM[3];
+    for (int k = 0; k < 3; k++) { pm[k] = __shfl_up_sync(0xffffffffu, lm[k], 1); pM[k] = __shfl_up_sync(0xffffffffu, lM[k], 1); }
+    const uint32_t pc = __shfl_up_sync(0xffffffffu, lc, 1);
+    bool can = false;
+    if (lane >= 1 && lane < nb && pc != 0u && rc != 0u)
+    {
+        const float al = pm[0] == 0xffffffffu ? 0.f : box_half_area(ord_box(pm, pM));
+        const float ar = rm[0] == 0xffffffffu ? 0.f : box_half_area(ord_box(rm, rM));
+        const float cost = C.c_trav + C.c_isect * (al * (float)pc + ar * (float)rc) * parent_inv_area;
+        can = !(cost >= best_cost);
+    }
+    return __any_sync(0xffffffffu, can);
 }
 
 // Nodes with more references than this are evaluated and partitioned by many blocks (the
@@ -579,6 +655,7 @@ __device__ __forceinline__ void eval_node_warp(const Src& src, const LvlNode& nd
     const int oa = Bw.axis, ob = Bw.bin;
     const float oc = Bw.cmin, os = Bw.scale;
     // phase 2: spatial bins over the node box, triangles clipped per bin (bvh_sah.cpp:135-243)
+    const bool prune = C.c_isect >= 0.f;  // (the bound needs a cost monotone in the areas)
     for (int axis = 0; axis < 3; axis++)
     {
         const float node_min = nbox.mn[axis], node_max = nbox.mx[axis];
@@ -587,9 +664,22 @@ __device__ __forceinline__ void eval_node_warp(const Src& src, const LvlNode& nd
         for (int b = lane; b < nb; b += 32) { S.cin[b] = 0u; S.cout[b] = 0u; sbox_clear(S.bins[b]); }
         bin_bounds(S.bnd, node_min, sscale, nb, lane, 32);
         __syncwarp();
+        if (prune)
+        {
+            for (uint32_t i0 = 0; i0 < n; i0 += 32)
+            {
+                spatial_bound_warp(src, i0, n, axis, nbox, node_min, sscale, nb, S.bnd, S.cin, S.cout, S.bins);
+            }
+            __syncwarp();
+            const bool can = warp_spatial_can_win(S.cin, S.cout, S.bins, nb, parent_inv_area, C, Bw.cost);
+            __syncwarp();
+            if (!can) { continue; }
+            for (int b = lane; b < nb; b += 32) { sbox_clear(S.bins[b]); }  // the exact boxes; the counts stay
+            __syncwarp();
+        }
         for (uint32_t i0 = 0; i0 < n; i0 += 32)
         {
-            spatial_bin_warp(src, i0, n, axis, nbox, node_min, sscale, nb, S.bnd, S.cin, S.cout, S.bins);
+            spatial_bin_warp(src, i0, n, axis, nbox, node_min, sscale, nb, S.bnd, S.cin, S.cout, S.bins, !prune);
         }
         __syncwarp();
         warp_eval_spatial_axis(S.cin, S.cout, S.bins, nb, axis, node_min, sscale, parent_inv_area, C, Bw);
@@ -702,7 +792,7 @@ k_sah_eval(const LvlNode* __restrict__ lv, const uint32_t* __restrict__ refs, Ct
     __shared__ uint32_t s_red[SBLK / 32 + 1];
     __shared__ uint32_t s_cm, s_cM;
     __shared__ Best sB;
-    __shared__ int o_axis, o_bin;
+    __shared__ int o_axis, o_bin, s_can;
     __shared__ float o_cmin, o_scale;
 
     const LvlNode nd = lv[blockIdx.x];
@@ -769,6 +859,7 @@ k_sah_eval(const LvlNode* __restrict__ lv, const uint32_t* __restrict__ refs, Ct
     __syncthreads();
 
     // phase 2: spatial bins over the node box, triangles clipped per bin (bvh_sah.cpp:135-243)
+    const bool prune = C.c_isect >= 0.f;  // (the bound needs a cost monotone in the areas)
     for (int axis = 0; axis < 3; axis++)
     {
         const float node_min = nbox.mn[axis], node_max = nbox.mx[axis];
@@ -777,9 +868,27 @@ k_sah_eval(const LvlNode* __restrict__ lv, const uint32_t* __restrict__ refs, Ct
         if (tid < nb) { cin[tid] = 0u; cout[tid] = 0u; sbox_clear(bins[tid]); }
         bin_bounds(bnd, node_min, sscale, nb, tid, SBLK);
         __syncthreads();
+        if (prune)
+        {
+            // the lower bounds first (spatial_bound_warp): skip the clipping when none can win
+            for (uint32_t i0 = (uint32_t)(tid & ~31); i0 < n; i0 += SBLK)
+            {
+                spatial_bound_warp(GlobalRefs(C, R), i0, n, axis, nbox, node_min, sscale, nb, bnd, cin, cout, bins);
+            }
+            __syncthreads();
+            if (tid < 32)
+            {
+                const bool can = warp_spatial_can_win(cin, cout, bins, nb, parent_inv_area, C, sB.cost);
+                if (tid == 0) { s_can = can ? 1 : 0; }
+            }
+            __syncthreads();
+            if (!s_can) { continue; }
+            if (tid < nb) { sbox_clear(bins[tid]); }
+            __syncthreads();
+        }
         for (uint32_t i0 = (uint32_t)(tid & ~31); i0 < n; i0 += SBLK)
         {
-            spatial_bin_warp(GlobalRefs(C, R), i0, n, axis, nbox, node_min, sscale, nb, bnd, cin, cout, bins);
+            spatial_bin_warp(GlobalRefs(C, R), i0, n, axis, nbox, node_min, sscale, nb, bnd, cin, cout, bins, !prune);
         }
         __syncthreads();
         if (tid < 32)
