@@ -49,17 +49,18 @@ WORKLOAD = "BVH build microbenchmark: 1,048,576-triangle soup, LBVH 63-bit Morto
 ROOFLINE_BYTES_PER_TRI = {21: 400, 10: 260}
 # What this library's bake moves per triangle by its own count (each array once per read and
 # once per write, per kernel; V = 3N vertices): clear 12, vertex renormalisation 144, triangle
-# prep 132 (boxes, centroids and the 48-byte triangle records), Morton codes 20, bucket table 8,
-# Karras topology with leaf boxes, box-hierarchy level 0 and the baked triangles 198, box levels
-# 1, boundary 80, slot scans 16, .bvh and traversal nodes 45; plus the sort: 44 up to 2^21 keys
-# (top-digit onesweep pass 20 + per-bucket pass 24), else 188 (eight onesweep passes). It
-# includes the outputs the minimal count leaves out (renormalised normals, the .bvh layout, the
-# traversal layout).
-BAKE_BYTES_PER_TRI_EXCL_SORT = 12 + 144 + 132 + 20 + 8 + 198 + 1 + 80 + 16 + 45
+# prep 132 (boxes, centroids and the 48-byte triangle records), Morton codes 20, Karras
+# topology with leaf boxes, box-hierarchy level 0 and the baked triangles 198, box levels 1,
+# boundary 80, slot scan 8 (without SAH subtrees the triangle offsets are the identity), .bvh
+# and traversal nodes 45; plus the sort: 44 up to 2^21 keys (top-digit onesweep pass 20 +
+# per-bucket pass 24, which also writes the bucket table), else 188 (eight onesweep passes) and
+# the bucket-table kernel's 8. It includes the outputs the minimal count leaves out
+# (renormalised normals, the .bvh layout, the traversal layout).
+BAKE_BYTES_PER_TRI_EXCL_SORT = 12 + 144 + 132 + 20 + 198 + 1 + 80 + 8 + 45
 
 
 def bake_bytes_per_tri(n: int) -> int:
-    return BAKE_BYTES_PER_TRI_EXCL_SORT + (44 if n <= (1 << 21) else 188)
+    return BAKE_BYTES_PER_TRI_EXCL_SORT + (44 if n <= (1 << 21) else 188 + 8)
 
 
 def parse_args():
