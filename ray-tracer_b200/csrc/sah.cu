@@ -358,7 +358,7 @@ struct Best
 // these with the same B and return the same B.
 __device__ __forceinline__ void warp_box_scan_up(uint32_t (&m)[3], uint32_t (&M)[3], uint32_t& c, int lane)
 {
-#pragma unroll
+#pragma unroll 1  // (rolled: the sweeps are inlined at several places; code size over loop overhead)
     for (int o = 1; o < 32; o <<= 1)
     {
         uint32_t tm[3], tM[3];
@@ -373,7 +373,7 @@ __device__ __forceinline__ void warp_box_scan_up(uint32_t (&m)[3], uint32_t (&M)
 }
 __device__ __forceinline__ void warp_box_scan_down(uint32_t (&m)[3], uint32_t (&M)[3], uint32_t& c, int lane)
 {
-#pragma unroll
+#pragma unroll 1  // (rolled: the sweeps are inlined at several places; code size over loop overhead)
     for (int o = 1; o < 32; o <<= 1)
     {
         uint32_t tm[3], tM[3];
