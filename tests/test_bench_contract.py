@@ -22,3 +22,18 @@ def test_reference_arm_prints_one_contract_line():
     cb = d["cpu_baseline"]
     assert cb["kind"] in ("reference", "port") and cb["cores"] >= 1 and cb["value"] == d["value"] and cb["sample"]
     assert d["e2e"] == {"value": d["value"], "unit": "Mtri/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
+
+
+def test_committed_profile_figures_parse():
+    """The ncu figures bench.py attaches to its lines come from the committed summaries: the
+    bake's DRAM bytes per triangle and the trace kernel's counters of each render workload."""
+    sys.path.insert(0, ROOT)
+    import bench
+    traffic = bench.profiled_traffic()
+    assert traffic is not None and 100.0 < traffic < 2000.0
+    for key in ("c1_wavefront_trace", "c3_wavefront_trace", "c5_wavefront_trace"):
+        c = bench.profiled_render_counters(key)
+        assert c is not None, key
+        assert set(c) >= {"issue_active_pct", "threads_per_inst", "l1_hit_pct", "l2_hit_pct"}, key
+        assert 0.0 < c["issue_active_pct"] <= 100.0 and 0.0 < c["threads_per_inst"] <= 32.0, key
+    assert bench.bake_bytes_per_tri(1 << 20) < bench.bake_bytes_per_tri(1 << 24)
